@@ -1,0 +1,463 @@
+// Test-infrastructure harness around the reference (timo-eichhorn/Lettuce) CPU code.
+//
+// This file is NOT part of the product.  It is compiled by oracle/build_ref.py against a
+// copy of the reference headers whose compile-time lattice extents
+// (LettuceGauge/defines.hpp:34-37) are replaced by the macros LT_NT..LT_NZ, one shared
+// library per extent tuple, into oracle/_ref/.  Tests and the CPU-baseline leg of bench.py
+// load it through ctypes to
+//   * pin the C restatement in oracle/lt_oracle.c against the reference itself, and
+//   * generate the golden fixtures under tests/golden/.
+// Every entry point calls the reference's own functions/functors; nothing here restates
+// an algorithm.  Links cross this boundary in the reference AoS layout
+// double[V][4][3][3][2] (site index ((t*Nx+x)*Ny+y)*Nz+z, mu fastest, row-major 3x3,
+// re/im interleaved; LettuceGauge/lattice.hpp:366-382).
+//
+// Private members of the reference HMC functors (integrator hooks, Hamiltonian, the MetaD
+// force) are reached by compiling the two HMC headers with `private` mapped to `public`;
+// all standard, Eigen and other reference headers are included first so only those
+// classes are affected.
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <iterator>
+#include <limits>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+#include <omp.h>
+#include <Eigen/Dense>
+#include <unsupported/Eigen/MatrixFunctions>
+#include "PCG/pcg_random.hpp"
+
+#include "LettuceGauge/defines.hpp"
+#include "LettuceGauge/coords.hpp"
+#include "LettuceGauge/lattice.hpp"
+#include "LettuceGauge/actions/bias_potential/metadynamics.hpp"
+#include "LettuceGauge/actions/gauge/rectangular_action.hpp"
+#include "LettuceGauge/actions/gauge/wilson_action.hpp"
+#include "LettuceGauge/iterators/iterators.hpp"
+#include "LettuceGauge/math/su2.hpp"
+#include "LettuceGauge/math/su3.hpp"
+#include "LettuceGauge/math/su3_exp.hpp"
+#include "LettuceGauge/observables/clover.hpp"
+#include "LettuceGauge/observables/plaquette.hpp"
+#include "LettuceGauge/observables/field_strength_tensor.hpp"
+#include "LettuceGauge/observables/topological_charge.hpp"
+#include "LettuceGauge/smearing/stout_smearing.hpp"
+#include "LettuceGauge/smearing/gradient_flow.hpp"
+#include "LettuceGauge/updates/heatbath.hpp"
+#include "LettuceGauge/updates/overrelaxation.hpp"
+// Only the two HMC headers are compiled with `private` mapped to `public` (they hold no
+// OpenMP `private(...)` clauses, which the mapping would break).
+#define private public
+#include "LettuceGauge/updates/hmc_gauge.hpp"
+#include "LettuceGauge/updates/hmc_metadynamics.hpp"
+#undef private
+
+namespace
+{
+constexpr std::size_t kV = static_cast<std::size_t>(Nt) * Nx * Ny * Nz;
+constexpr std::size_t kL = 4 * kV;
+
+void load(GaugeField& U, const double* a)
+{
+    #pragma omp parallel for
+    for (std::size_t l = 0; l < kL; ++l)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+            {
+                const double* p = a + 18 * l + 2 * (3 * i + j);
+                U(l)(i, j) = std::complex<double>(p[0], p[1]);
+            }
+}
+
+void store(const GaugeField& U, double* a)
+{
+    #pragma omp parallel for
+    for (std::size_t l = 0; l < kL; ++l)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+            {
+                double* p = a + 18 * l + 2 * (3 * i + j);
+                p[0] = std::real(U(l)(i, j));
+                p[1] = std::imag(U(l)(i, j));
+            }
+}
+
+void set_beta(double b)
+{
+    beta = b;                                  // defines.hpp:52 (used by HMC momentum update)
+    GaugeAction::WilsonAction.SetBeta(b);      // rectangular_action.hpp:43
+}
+
+using PRNG = PRNG4D<Nt, Nx, Ny, Nz, pcg64, floatT, int>;
+std::unique_ptr<PRNG> g_prng;
+
+PRNG& prng()
+{
+    if (!g_prng)
+    {
+        auto gen = MakeRandomGenerator();
+        g_prng = std::make_unique<PRNG>(gen);
+    }
+    return *g_prng;
+}
+
+// A bias whose grid holds V(Q) = slope * Q, so that MetaBiasPotential::ReturnDerivative
+// returns `slope` (metadynamics.hpp:181-187) and the MetaD force is slope * dQ/dU.
+std::unique_ptr<MetaBiasPotential> linear_bias(double slope)
+{
+    auto bias = std::make_unique<MetaBiasPotential>(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0);
+    bias->GeneratePotentialFrom([slope](double cv) { return slope * cv; });
+    return bias;
+}
+} // namespace
+
+extern "C"
+{
+int ref_extent(int d)
+{
+    switch (d)
+    {
+        case 0: return Nt;
+        case 1: return Nx;
+        case 2: return Ny;
+        case 3: return Nz;
+        default: return 0;
+    }
+}
+
+int ref_threads()
+{
+    return omp_get_max_threads();
+}
+
+// plaquette.hpp:26-43
+double ref_plaquette_sum(const double* links)
+{
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    return PlaquetteSum(*U);
+}
+
+// rectangular_action.hpp:61-94 with (c_plaq, c_rect) = (1, 0)
+double ref_wilson_action(const double* links, double b)
+{
+    set_beta(b);
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    return GaugeAction::WilsonAction.Action(*U);
+}
+
+// rectangular_action.hpp:104-184 for every link
+void ref_staples(const double* links, double* out)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto S = std::make_unique<GaugeField>();
+    load(*U, links);
+    #pragma omp parallel for collapse(2)
+    for (int t = 0; t < Nt; ++t)
+    for (int x = 0; x < Nx; ++x)
+    for (int y = 0; y < Ny; ++y)
+    for (int z = 0; z < Nz; ++z)
+    for (int mu = 0; mu < 4; ++mu)
+    {
+        link_coord l {t, x, y, z, mu};
+        (*S)(l) = GaugeAction::WilsonAction.Staple(*U, l);
+    }
+    store(*S, out);
+}
+
+// overrelaxation.hpp:68-117 driven by iterators.hpp:65-87
+void ref_or_sweeps(double* links, int n)
+{
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    OverrelaxationSubgroupKernel OR(*U, GaugeAction::WilsonAction);
+    Iterator::Checkerboard(OR, n);
+    store(*U, links);
+}
+
+void ref_reset_prng()
+{
+    g_prng.reset();
+}
+
+// heatbath.hpp:30-130 driven by iterators.hpp:65-87; the per-link pcg64 streams persist
+// across calls until ref_reset_prng().
+void ref_hb_sweeps(double* links, double b, int n)
+{
+    set_beta(b);
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    HeatbathKernel HB(*U, GaugeAction::WilsonAction, prng());
+    Iterator::Checkerboard(HB, n);
+    store(*U, links);
+}
+
+// n_sweep rounds of (n_hb heatbath + n_or overrelaxation), plaquette sum recorded after each round
+void ref_hb_or_chain(double* links, double b, int n_sweep, int n_hb, int n_or, double* plaq)
+{
+    set_beta(b);
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    HeatbathKernel HB(*U, GaugeAction::WilsonAction, prng());
+    OverrelaxationSubgroupKernel OR(*U, GaugeAction::WilsonAction);
+    for (int s = 0; s < n_sweep; ++s)
+    {
+        Iterator::Checkerboard(HB, n_hb);
+        Iterator::Checkerboard(OR, n_or);
+        if (plaq) plaq[s] = PlaquetteSum(*U);
+    }
+    store(*U, links);
+}
+
+// gradient_flow.hpp:120-168 (RK3) and :252-367 (GradientFlowKernel)
+void ref_flow_rk3(const double* in, double* out, double eps, int n_step)
+{
+    auto U0 = std::make_unique<GaugeField>();
+    auto U1 = std::make_unique<GaugeField>();
+    auto Z  = std::make_unique<GaugeField>();
+    load(*U0, in);
+    Integrators::GradientFlow::RK3 rk3(*Z);
+    GradientFlowKernel Flow(*U0, *U1, rk3, GaugeAction::WilsonAction, eps);
+    Flow(n_step);
+    store(*U1, out);
+}
+
+// Flow with measurements every `every` steps: plaquette sum, clover Q (topological_charge.hpp:97-200)
+// and clover energy density (field_strength_tensor.hpp:28-66, :107-134, :154-175).
+void ref_flow_rk3_measure(const double* in, double eps, int n_meas, int every,
+                          double* plaq, double* q, double* e)
+{
+    auto U0 = std::make_unique<GaugeField>();
+    auto U1 = std::make_unique<GaugeField>();
+    auto Z  = std::make_unique<GaugeField>();
+    auto F  = std::make_unique<FullTensor>();
+    load(*U0, in);
+    Integrators::GradientFlow::RK3 rk3(*Z);
+    GradientFlowKernel Flow(*U0, *U1, rk3, GaugeAction::WilsonAction, eps);
+    for (int m = 0; m < n_meas; ++m)
+    {
+        if (m == 0) Flow(every); else Flow.Resume(every);
+        plaq[m] = PlaquetteSum(*U1);
+        q[m]    = TopChargeClover(*U1);
+        FieldStrengthTensor::Clover(*U1, *F);
+        FieldStrengthTensor::MakeComponentsTraceless(*F);
+        e[m]    = EnergyDensity::Clover(*F);
+    }
+}
+
+// stout_smearing.hpp:29-57 applied n times
+void ref_stout(const double* in, double* out, double rho, int n)
+{
+    auto A = std::make_unique<GaugeField>();
+    auto B = std::make_unique<GaugeField>();
+    load(*A, in);
+    for (int k = 0; k < n; ++k)
+    {
+        StoutSmearing4D(*A, *B, rho);
+        std::swap(A, B);
+    }
+    store(*A, out);
+}
+
+// topological_charge.hpp:97-200
+double ref_topcharge_clover(const double* links)
+{
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    return TopChargeClover(*U);
+}
+
+// E = sum_{mu<nu} ReTr(F_munu^2) / V with the traceless clover F, as measured by the driver
+// (SU3_main.cpp:128-141 through field_strength_tensor.hpp)
+double ref_energy_clover(const double* links)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto F = std::make_unique<FullTensor>();
+    load(*U, links);
+    FieldStrengthTensor::Clover(*U, *F);
+    FieldStrengthTensor::MakeComponentsTraceless(*F);
+    return EnergyDensity::Clover(*F);
+}
+
+// Gauge force beta/6 * Algebra(st U^dagger) per link: the HMC momentum kick
+// (hmc_gauge.hpp:450-464) applied with epsilon = 1 to zero momenta.
+void ref_gauge_force(const double* links, double b, double* out)
+{
+    set_beta(b);
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    P->SetToZero();
+    Integrators::HMC::OMF_2 omf2;
+    RunStatistics stats;
+    GaugeUpdates::HMCKernel hmc(*U, *Uc, *P, omf2, GaugeAction::WilsonAction, prng(), stats, std::cout, 1.0);
+    hmc.UpdateMomenta(1.0);
+    store(*P, out);
+}
+
+// dQ/dU_mu(x) of the clover charge on the given field (clover.hpp:94-152, :279-321)
+void ref_clover_derivative(const double* links, double* out)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto C = std::make_unique<FullTensor>();
+    auto D = std::make_unique<GaugeField>();
+    load(*U, links);
+    CalculateClover<1>(*U, *C);
+    #pragma omp parallel for collapse(2)
+    for (int t = 0; t < Nt; ++t)
+    for (int x = 0; x < Nx; ++x)
+    for (int y = 0; y < Ny; ++y)
+    for (int z = 0; z < Nz; ++z)
+    for (int mu = 0; mu < 4; ++mu)
+    {
+        site_coord s {t, x, y, z};
+        (*D)(s, mu) = CloverDerivative(*U, *C, s, mu);
+    }
+    store(*D, out);
+}
+
+// The MetaD force chain of HMCMetaDKernel::CalculateTopologicalForce (hmc_metadynamics.hpp:374-436)
+// with n_smear_meta (= 4, defines.hpp:74) stout levels of parameter rho, under a bias with
+// dV/dQ = slope.  Writes ForceFatLink (the force on the thin links) and returns the CV.
+double ref_metad_force(const double* links, double rho, double slope, double* out)
+{
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    auto bias = linear_bias(slope);
+    auto data = std::make_unique<GaugeUpdates::HMCMetaDData>(n_smear_meta);
+    Integrators::HMC::OMF_2 omf2;
+    RunStatistics stats;
+    std::string log_path {"/dev/null"};
+    GaugeUpdates::HMCMetaDKernel kern(*U, *Uc, *P, *bias, *data, omf2, GaugeAction::WilsonAction, prng(), stats,
+                                      std::cout, log_path, 1.0, rho);
+    kern.CalculateTopologicalForce(false);
+    store(data->ForceFatLink, out);
+    CalculateClover<1>(data->SmearedFields[n_smear_meta], data->Clover);
+    return TopChargeClover(data->Clover);
+}
+
+int ref_n_smear_meta()
+{
+    return n_smear_meta;
+}
+
+// Q after n_smear_meta stout steps (HMCMetaDKernel::MetaCharge, hmc_metadynamics.hpp:302-310)
+double ref_metad_charge(const double* links, double rho)
+{
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    auto bias = linear_bias(1.0);
+    auto data = std::make_unique<GaugeUpdates::HMCMetaDData>(n_smear_meta);
+    Integrators::HMC::OMF_2 omf2;
+    RunStatistics stats;
+    std::string log_path {"/dev/null"};
+    GaugeUpdates::HMCMetaDKernel kern(*U, *Uc, *P, *bias, *data, omf2, GaugeAction::WilsonAction, prng(), stats,
+                                      std::cout, log_path, 1.0, rho);
+    return kern.MetaCharge();
+}
+
+// Deterministic OMF2 molecular dynamics from given links and momenta (hmc_gauge.hpp:155-190,
+// :450-541).  Returns H before and after; links and momenta are updated in place.
+void ref_omf2(double* links, double* momenta, double b, double tau, int n_step, double* h_old, double* h_new)
+{
+    set_beta(b);
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    load(*P, momenta);
+    Integrators::HMC::OMF_2 omf2;
+    RunStatistics stats;
+    GaugeUpdates::HMCKernel hmc(*U, *Uc, *P, omf2, GaugeAction::WilsonAction, prng(), stats, std::cout, tau);
+    *h_old = hmc.Hamiltonian();
+    omf2(hmc, tau, n_step);
+    *h_new = hmc.Hamiltonian();
+    store(*U, links);
+    store(*P, momenta);
+}
+
+// Deterministic OMF2 MetaD molecular dynamics (hmc_metadynamics.hpp:441-535) under a linear
+// bias V(Q) = slope * Q.  Returns H + V before and after.
+void ref_metad_omf2(double* links, double* momenta, double b, double tau, int n_step, double rho, double slope,
+                    double* h_old, double* h_new)
+{
+    set_beta(b);
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    load(*P, momenta);
+    auto bias = linear_bias(slope);
+    auto data = std::make_unique<GaugeUpdates::HMCMetaDData>(n_smear_meta);
+    Integrators::HMC::OMF_2 omf2;
+    RunStatistics stats;
+    std::string log_path {"/dev/null"};
+    GaugeUpdates::HMCMetaDKernel kern(*U, *Uc, *P, *bias, *data, omf2, GaugeAction::WilsonAction, prng(), stats,
+                                      std::cout, log_path, tau, rho);
+    kern.cv_path_samples.clear();
+    *h_old = kern.Hamiltonian() + bias->ReturnPotential(kern.MetaCharge());
+    omf2(kern, tau, n_step);
+    *h_new = kern.Hamiltonian() + bias->ReturnPotential(kern.MetaCharge());
+    store(*U, links);
+    store(*P, momenta);
+}
+
+// MetaBiasPotential (metadynamics.hpp:29-187): deposits then samples potential and derivative.
+void ref_bias_probe(double cv_min, double cv_max, int bins, double weight, double width, double wt, double thr,
+                    const double* deposits, int n_dep, int symmetric,
+                    const double* probes, int n_probe, double* pot, double* der)
+{
+    MetaBiasPotential bias(cv_min, cv_max, bins, weight, width, wt, thr);
+    std::vector<double> cvs(deposits, deposits + n_dep);
+    if (symmetric) bias.UpdatePotentialSymmetric(cvs); else bias.UpdatePotential(cvs);
+    for (int i = 0; i < n_probe; ++i)
+    {
+        pot[i] = bias.ReturnPotential(probes[i]);
+        der[i] = bias.ReturnDerivative(probes[i]);
+    }
+}
+
+// SU3::exp (su3_exp.hpp:419-425) of n traceless Hermitian matrices (18 doubles each)
+void ref_su3_exp(const double* in, double* out, int n)
+{
+    for (int k = 0; k < n; ++k)
+    {
+        Matrix_3x3 M;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                M(i, j) = std::complex<double>(in[18 * k + 6 * i + 2 * j], in[18 * k + 6 * i + 2 * j + 1]);
+        Matrix_SU3 E = SU3::exp(M);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+            {
+                out[18 * k + 6 * i + 2 * j]     = std::real(E(i, j));
+                out[18 * k + 6 * i + 2 * j + 1] = std::imag(E(i, j));
+            }
+    }
+}
+} // extern "C"
