@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pure-gauge SU(3) hot path (one JSON line on rank 0).
+
+Workload (the large plain-vs-FP32 configuration): 32^4 SU(3) Wilson gauge theory at
+beta = 6.0 from a seeded Haar-random start.  One step = one round of 1 Cabibbo-Marinari
+heatbath sweep + 4 overrelaxation sweeps (5 * 4V = 20,971,520 link updates) on FP32-bulk
+links.  The headline `value` is link updates/s; flow steps/s (RK3, eps = 0.01), the plain
+FP64 path, the FP32/FP64 ratios and |dP| between FP32 and FP64 flows from identical
+configurations are measured in the same run.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1: launched by torchrun, one rank per GPU; each rank evolves its own lattice (replicas,
+weak scaling; the path has no data exchange), timed on the device, max over ranks.
+--impl reference: the reference's own multi-threaded CPU code (oracle/_ref, else the C
+oracle) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "link updates/s & flow steps/s at 32^4: FP32-bulk vs plain FP64 GPU, dP<=1e-6"
+UNIT = "link updates/s"
+BETA = 6.0
+SEED = 20251203
+N_HB, N_OR = 1, 4
+FLOW_EPS = 0.01
+BYTES_PER_LINK = {"fp64": 144, "fp32": 72, "fp32_12": 48}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=32)
+    ap.add_argument("--prec", choices=["fp32_12", "fp32", "fp64"], default="fp32_12")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP64 / flow / e2e / CPU side measurements")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` recorded from an ncu capture in profiles/ (a line
+    `traffic_bytes_per_launch <kernel> <bytes>`), else None."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if not f.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(d, f)):
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                return float(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) > 8 for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------- reference arm
+def cpu_reference_rate(size: int, steps: int, warmup: int, links):
+    """Link updates/s of the reference's own OpenMP CPU code (oracle/_ref) on this host, or of
+    the single-threaded C oracle when the reference harness was not built.  One sample =
+    1 heatbath + 1 overrelaxation sweep."""
+    import ctypes as C
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ltref import Oracle, ref_available, Reference
+    ext = (size,) * 4
+    V = size ** 4
+    if ref_available(ext):
+        ref = Reference(ext)
+        L = ref.lib
+        L.ref_field_load.argtypes = [np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")]
+        L.ref_field_sweeps.restype = C.c_double
+        L.ref_field_sweeps.argtypes = [C.c_double, C.c_int, C.c_int]
+        L.ref_field_flow.restype = C.c_double
+        L.ref_field_flow.argtypes = [C.c_double, C.c_int]
+        L.ref_field_load(np.ascontiguousarray(links))
+        for _ in range(warmup):
+            L.ref_field_sweeps(BETA, 1, 1)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            L.ref_field_sweeps(BETA, 1, 1)
+        dt = time.perf_counter() - t0
+        rate = steps * 2 * 4 * V / dt
+        t0 = time.perf_counter()
+        L.ref_field_flow(FLOW_EPS, 1)
+        flow_rate = 1.0 / (time.perf_counter() - t0)
+        return {"value": rate, "unit": UNIT, "cores": int(L.ref_threads()), "kind": "reference",
+                "sample": f"{steps} x (1 heatbath + 1 overrelaxation sweep) at {size}^4, FP64, "
+                          f"reference OpenMP code (oracle/_ref), plaquette after each sample",
+                "flow_steps_per_s": flow_rate}
+    o = Oracle()
+    e = np.array(ext, dtype=np.int32)
+    U = np.ascontiguousarray(links)
+    t0 = time.perf_counter()
+    o.lib.or_heatbath_sweeps(e, U, BETA, 1, 1, 0)
+    dt = time.perf_counter() - t0
+    return {"value": 4 * V / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 heatbath sweep at {size}^4, FP64, single-threaded C oracle"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+    import lettuce_b200 as lt
+    ext = (a.size,) * 4
+    links = lt.haar_links(ext, SEED)
+    steps = max(1, min(a.steps, 10))
+    cb = cpu_reference_rate(a.size, steps, max(1, min(a.warmup, 3)), links)
+    ms = 1000.0 * 2 * 4 * a.size ** 4 / cb["value"]
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus, "steps": steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded Haar-random SU(3) start",
+            "impl": "reference",
+            "config": {"workload": f"{a.size}^4 SU(3) Wilson beta={BETA}: heatbath + overrelaxation sweeps",
+                       "lattice": list(ext), "beta": BETA},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if "flow_steps_per_s" in cb:
+        line["flow_steps_per_s"] = cb["flow_steps_per_s"]
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------- our arm
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+
+    import numpy as np
+    import torch
+    import lettuce_b200 as lt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    ext = (a.size,) * 4
+    V = a.size ** 4
+    links = lt.haar_links(ext, SEED + rank)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(G, fn, n):
+        """Device time (ms) of n calls of fn, CUDA events on the handle's stream."""
+        s = torch.cuda.ExternalStream(G.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        G.synchronize()
+        e0.record(s)
+        for _ in range(n):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    counter = {"c": 0}
+
+    def sweep_round(G):
+        counter["c"] = lt.UpdateSweeps(G, BETA, 1, N_HB, N_OR, SEED + rank, counter["c"])
+
+    # ---- headline: FP32-bulk sweeps
+    G = lt.GaugeField(ext, a.prec)
+    G.upload(links)
+    for _ in range(max(a.warmup, 3)):
+        sweep_round(G)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ms = timed(G, lambda: sweep_round(G), a.steps)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(ms)
+    upd_per_step = (N_HB + N_OR) * 4 * V
+    value = world * a.steps * upd_per_step / (ms / 1000.0)
+    launches = a.steps * (N_HB + N_OR) * 8
+
+    # ---- dominant kernel: one overrelaxation sub-sweep, per-launch duration
+    n_or = 20
+    or_ms = timed(G, lambda: lt.Iterator.Checkerboard(lt.OverrelaxationSubgroupKernel(G), n_or), 1) / (8 * n_or)
+    hb_ms = timed(G, lambda: lt.Iterator.Checkerboard(lt.HeatbathKernel(G, lt.WilsonAction(BETA), 5), 5), 1) / 40
+    peak, peak_kind = peaks()
+    b = BYTES_PER_LINK[a.prec]
+    alg_bytes = 9 * b * (V // 2)                  # 9 link reads/writes per update, V/2 updates
+    achieved = alg_bytes / (or_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": ncu_traffic(f"k_overrelax<{a.prec}>"), "kernel": f"k_overrelax ({a.prec})",
+                "ms_per_launch": or_ms, "algorithmic_bytes_per_launch": alg_bytes,
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "heatbath_ms_per_launch": hb_ms,
+                "heatbath_achieved_gbs": alg_bytes / (hb_ms / 1000.0) / 1e9}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if a.prec != "fp64" else "f64",
+            "data": "synthetic: seeded Haar-random SU(3) start (per rank)",
+            "config": {"workload": f"{a.size}^4 SU(3) Wilson beta={BETA}: {N_HB} heatbath + {N_OR} overrelaxation "
+                                   f"sweeps per step, {a.prec} links",
+                       "lattice": list(ext), "beta": BETA, "storage": a.prec,
+                       "l2": f"inputs larger than L2 ({G.Volume() * 4 * b / 1e6:.0f} MB of links per sweep)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "clocks": clocks.summary(), "gpu_launches": launches}
+
+    if not a.no_extras:
+        # ---- flow steps/s (FP32-bulk and FP64) and |dP| from identical configurations
+        therm = G.download()
+        res = {}
+        for prec in (a.prec, "fp64"):
+            A, B = lt.GaugeField(ext, prec), lt.GaugeField(ext, prec)
+            A.upload(therm)
+            flow = lt.GradientFlowKernel(A, B, lt.RK3, None, FLOW_EPS)
+            flow(2)
+            n_flow = 10
+            t = timed(B, lambda: flow.Resume(n_flow), 1)
+            flow(100)                                   # t = 1.0 from the identical start
+            q, e = lt.CloverObservables(B)
+            res[prec] = {"flow_steps_per_s": n_flow / (t / 1000.0), "plaq_t1": lt.PlaquetteSum(B) / V / 18,
+                         "Q_t1": q, "E_t1": e}
+            # sweeps in this precision
+            C = lt.GaugeField(ext, prec)
+            C.upload(therm)
+            for _ in range(2):
+                sweep_round(C)
+            t = timed(C, lambda: sweep_round(C), 5)
+            res[prec]["link_updates_per_s"] = 5 * upd_per_step / (t / 1000.0)
+            del A, B, C
+        line["flow_steps_per_s"] = res[a.prec]["flow_steps_per_s"]
+        line["fp64"] = {k: res["fp64"][k] for k in ("link_updates_per_s", "flow_steps_per_s")}
+        line["fp32_over_fp64"] = {
+            "link_updates": res[a.prec]["link_updates_per_s"] / res["fp64"]["link_updates_per_s"],
+            "flow_steps": res[a.prec]["flow_steps_per_s"] / res["fp64"]["flow_steps_per_s"]}
+        line["dP_flow_t1"] = abs(res[a.prec]["plaq_t1"] - res["fp64"]["plaq_t1"])
+        line["dQ_flow_t1"] = abs(res[a.prec]["Q_t1"] - res["fp64"]["Q_t1"])
+
+        # ---- e2e through the public API with host buffers: H2D of the step's links from pinned
+        # memory, the sweep round, D2H of the plaquette
+        pinned = torch.empty(therm.size, dtype=torch.float64, pin_memory=True)
+        host = pinned.numpy().reshape(therm.shape)
+        host[...] = therm
+        E = lt.GaugeField(ext, a.prec)
+        E.upload(host)
+        sweep_round(E)
+        lt.PlaquetteSum(E)
+        n_e2e = max(3, min(a.steps, 10))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            E.upload(host)
+            sweep_round(E)
+            lt.PlaquetteSum(E)
+        dt = max_over_ranks(time.perf_counter() - t0)
+        line["e2e"] = {"value": world * n_e2e * upd_per_step / dt, "unit": UNIT,
+                       "h2d_bytes_per_step": int(therm.nbytes), "d2h_bytes_per_step": 8,
+                       "path": "lt_upload_links + lt_update_sweeps + lt_plaquette_sum"}
+
+        # ---- CPU baseline on this host, rank 0, bounded sample
+        if rank == 0:
+            cb = cpu_reference_rate(a.size, 2, 1, therm)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            if "flow_steps_per_s" in cb:
+                line["cpu_baseline"]["flow_steps_per_s"] = cb["flow_steps_per_s"]
+
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,178 @@
+/*
+ * lettuce_b200 -- C ABI of the B200-native pure-gauge SU(3) hot path.
+ *
+ * Drop-in boundary for the CPU reference timo-eichhorn/Lettuce (header-only C++20).  The
+ * reference has no FFI of its own; each entry point below replaces the reference
+ * function, functor or container member named beside it (paths relative to the
+ * reference project root).  Plain C types only: opaque handles, plain pointers and sizes,
+ * int status codes, no exceptions across the boundary.
+ *
+ * Link and algebra fields cross the boundary in the reference layout
+ * double[V][4][3][3][2]: site index ((t*Nx + x)*Ny + y)*Nz + z, direction mu fastest,
+ * row-major 3x3, real/imaginary interleaved (LettuceGauge/lattice.hpp:366-382).
+ *
+ * Threading: every lattice handle owns one CUDA stream; calls on one handle are
+ * serialised by the caller; distinct handles may be driven from distinct host threads.
+ * Calls that return a host value synchronise the handle's stream.  No device wait in this
+ * library spins without a bound.
+ */
+#ifndef LETTUCE_B200_H
+#define LETTUCE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define LT_OK          0
+#define LT_ERR_ARG     1   /* invalid argument: null pointer, odd extent, mismatched handles */
+#define LT_ERR_CUDA    2   /* CUDA runtime error (no device, launch failure, ...)            */
+#define LT_ERR_NOMEM   3   /* device or host allocation failed                                */
+#define LT_ERR_STATE   4   /* operation not valid in the handle's current state              */
+#define LT_ERR_NUMERIC 5   /* non-finite value detected in a result                          */
+
+/* Storage format of the link field. */
+#define LT_PREC_FP64    0  /* 18 doubles per link (the reference's Matrix_SU3, defines.hpp:122)   */
+#define LT_PREC_FP32    1  /* 18 floats per link                                                  */
+#define LT_PREC_FP32_12 2  /* 12 floats per link; third row rebuilt by RestoreLastRow
+                              (math/su3.hpp:362-367)                                              */
+
+typedef struct lt_lattice lt_lattice;
+typedef struct lt_bias lt_bias;
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* lt_last_error(void);
+/* Library version, major*10000 + minor*100 + patch. */
+int lt_version(void);
+
+/* ---- gauge field container: GaugeField4D (lattice.hpp:87-394) ---------------------- */
+/* Constructor; ext = {Nt, Nx, Ny, Nz}, all even and >= 2 (iterators/iterators.hpp:68).
+ * Links start as the unit matrix. */
+int lt_create(const int ext[4], int prec, lt_lattice** out);
+/* Destructor. */
+int lt_destroy(lt_lattice* h);
+int lt_get_extents(const lt_lattice* h, int ext[4], int* prec);
+/* Copy links from / to host memory in the reference layout (GaugeField4D element access,
+ * lattice.hpp:113-136). */
+int lt_upload_links(lt_lattice* h, const double* links);
+int lt_download_links(lt_lattice* h, double* links);
+/* One link: GaugeField4D::operator()(link_coord) (lattice.hpp:113-136); site index as in
+ * the reference layout, m = 18 doubles (row-major 3x3, re/im interleaved). */
+int lt_set_link(lt_lattice* h, int64_t site, int mu, const double* m);
+int lt_get_link(lt_lattice* h, int64_t site, int mu, double* m_out);
+/* Device-side copy dst = src (GaugeField4D::operator=, lattice.hpp:106-112); same extents,
+ * any storage formats. */
+int lt_copy(lt_lattice* dst, const lt_lattice* src);
+/* Exchange the link storage of two handles with identical extents and format
+ * (Swap, lattice.hpp:238-246). */
+int lt_swap(lt_lattice* a, lt_lattice* b);
+/* SetToIdentity (lattice.hpp:138-150). */
+int lt_set_identity(lt_lattice* h);
+/* Seeded Haar-random SU(3) start (the reference has none: SU3_main.cpp:296 starts cold).
+ * Host-only generator; no device needed. */
+int lt_haar_links(const int ext[4], uint64_t seed, double* links_out);
+/* lt_haar_links + lt_upload_links. */
+int lt_set_haar_random(lt_lattice* h, uint64_t seed);
+/* Block the calling thread until the handle's stream is idle. */
+int lt_synchronize(lt_lattice* h);
+/* The handle's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
+int lt_get_stream(const lt_lattice* h, void** stream_out);
+
+/* ---- observables --------------------------------------------------------------------- */
+/* PlaquetteSum (observables/plaquette.hpp:26-43): sum over sites, mu<nu of ReTr P. */
+int lt_plaquette_sum(lt_lattice* h, double* out);
+/* WilsonAction::Action / Rectangular<1>::Action (actions/gauge/wilson_action.hpp:24-41,
+ * rectangular_action.hpp:61-94): beta (6V - sum ReTr P / 3). */
+int lt_wilson_action(lt_lattice* h, double beta, double* out);
+/* TopChargeClover (observables/topological_charge.hpp:97-200). */
+int lt_topcharge_clover(lt_lattice* h, double* out);
+/* EnergyDensity::Clover on the traceless clover field strength
+ * (observables/field_strength_tensor.hpp:28-66, :107-134, :154-175). */
+int lt_energy_clover(lt_lattice* h, double* out);
+/* Both of the above from one pass over the clover leaves. */
+int lt_clover_observables(lt_lattice* h, double* q_out, double* e_out);
+/* WilsonAction::Staple for every link (rectangular_action.hpp:104-184), reference layout. */
+int lt_staples(lt_lattice* h, double* staples_out);
+
+/* ---- local updates: Iterator::Checkerboard (iterators/iterators.hpp:65-87) ------------- */
+/* n_sweep sweeps of OverrelaxationSubgroupKernel (updates/overrelaxation.hpp:68-117). */
+int lt_overrelax_sweeps(lt_lattice* h, int n_sweep);
+/* n_sweep sweeps of HeatbathKernel (updates/heatbath.hpp:30-130) at coupling beta.
+ * Random numbers: Philox4x32-10 keyed by seed, one counter value per sweep starting at
+ * *counter; *counter is advanced by n_sweep. */
+int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, uint64_t* counter);
+/* n_sweep rounds of (n_hb heatbath + n_or overrelaxation) sweeps, as the driver's update
+ * loop (SU3_main.cpp:381-402); launched as one CUDA graph. */
+int lt_update_sweeps(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed,
+                     uint64_t* counter);
+
+/* ---- smearing ------------------------------------------------------------------------ */
+/* GradientFlowKernel<RK3>::operator() (smearing/gradient_flow.hpp:120-168, :339-345):
+ * out = in flowed by n_step RK3 steps of size eps.  in == out continues in place
+ * (GradientFlowKernel::Resume, :347-351). */
+int lt_flow_rk3(lt_lattice* in, lt_lattice* out, double eps, int n_step);
+/* Flow with a measurement every `every` steps: plaquette sum, clover Q and clover energy
+ * density after steps every, 2*every, ..., n_meas*every (SU3_main.cpp:150-163). */
+int lt_flow_rk3_measure(lt_lattice* in, lt_lattice* out, double eps, int n_meas, int every,
+                        double* plaq_out, double* q_out, double* e_out);
+/* n steps of StoutSmearing4D (smearing/stout_smearing.hpp:29-57); in == out allowed. */
+int lt_stout(lt_lattice* in, lt_lattice* out, double rho, int n);
+
+/* ---- HMC: GaugeUpdates::HMCKernel (updates/hmc_gauge.hpp:381-600) ---------------------- */
+/* beta/6 Algebra(st U^dag) for every link: the momentum kick of UpdateMomenta (:450-464). */
+int lt_gauge_force(lt_lattice* h, double beta, double* force_out);
+/* The handle's momentum field (full anti-Hermitian 3x3 per link, reference layout). */
+int lt_set_momenta(lt_lattice* h, const double* p);
+int lt_get_momenta(lt_lattice* h, double* p_out);
+/* RandomMomentum (:400-428) from Philox Gaussians keyed by seed at `counter`. */
+int lt_random_momenta(lt_lattice* h, uint64_t seed, uint64_t counter);
+/* Hamiltonian (:525-541): Wilson action + (-sum ReTr P^2). */
+int lt_hamiltonian(lt_lattice* h, double beta, double* out);
+/* Integrators::HMC::OMF_2 (:155-190) molecular dynamics from the current links and momenta;
+ * H before and after in h_old / h_new (either may be NULL). */
+int lt_omf2(lt_lattice* h, double beta, double tau, int n_step, double* h_old, double* h_new);
+/* HMCKernel::operator() (:549-583) with OMF_2: momenta, MD, Metropolis (if metropolis != 0)
+ * from Philox streams at *counter (advanced by 1); dH and the decision are returned. */
+int lt_hmc_trajectory(lt_lattice* h, double beta, double tau, int n_step, uint64_t seed, uint64_t* counter,
+                      int metropolis, double* dH, int* accepted);
+
+/* ---- metadynamics: HMCMetaDKernel (updates/hmc_metadynamics.hpp:264-675) ---------------- */
+/* CloverDerivative for every link (observables/clover.hpp:279-321) on the handle's links. */
+int lt_clover_derivative(lt_lattice* h, double* out);
+/* MetaCharge (:302-310): clover Q after n_stout stout steps of parameter rho. */
+int lt_metad_charge(lt_lattice* h, double rho, int n_stout, double* q_out);
+/* CalculateTopologicalForce (:374-436): dvdq * dQ_stout/dU on the thin links through the
+ * hand-written stout-chain adjoint (smearing/stout_smearing.hpp:122-234); the smeared levels
+ * are kept, the exponential constants are recomputed.  force_out (may be NULL) in the
+ * reference layout; q_out (may be NULL) receives the smeared charge. */
+int lt_metad_force(lt_lattice* h, double rho, int n_stout, double dvdq, double* force_out, double* q_out);
+/* OMF_2 molecular dynamics with the bias force (UpdateMomenta :441-459); H + V(Q) before/after. */
+int lt_metad_omf2(lt_lattice* h, lt_bias* bias, double beta, double tau, int n_step, double rho, int n_stout,
+                  double* h_old, double* h_new);
+/* HMCMetaDKernel::operator() (:552-655): one MetaD-HMC trajectory, Metropolis, and the
+ * symmetric well-tempered bias update from the path samples (:615-643). */
+int lt_metad_hmc_trajectory(lt_lattice* h, lt_bias* bias, double beta, double tau, int n_step, double rho,
+                            int n_stout, uint64_t seed, uint64_t* counter, int metropolis, double* dH,
+                            int* accepted, double* cv_out);
+
+/* ---- bias potential: MetaBiasPotential (actions/bias_potential/metadynamics.hpp:29-507) -- */
+/* Constructor (:60-91); fails with LT_ERR_ARG where the reference throws (:70-77). */
+int lt_bias_create(double cv_min, double cv_max, int bin_number, double weight, double width,
+                   double well_tempered_parameter, double threshold_weight, lt_bias** out);
+int lt_bias_destroy(lt_bias* b);
+/* UpdatePotential (:103-131) or UpdatePotentialSymmetric (:134-147) for n CV samples. */
+int lt_bias_update(lt_bias* b, const double* cv, int n, int symmetric);
+/* ReturnPotential (:151-179). */
+int lt_bias_potential(const lt_bias* b, double cv, double* out);
+/* ReturnDerivative (:181-187). */
+int lt_bias_derivative(const lt_bias* b, double cv, double* out);
+/* The bin_number+1 grid values (read / overwrite). */
+int lt_bias_get_grid(const lt_bias* b, double* grid_out, int n);
+int lt_bias_set_grid(lt_bias* b, const double* grid, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LETTUCE_B200_H */

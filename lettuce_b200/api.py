@@ -1,0 +1,399 @@
+"""Python mirror of the reference's call surface over the C ABI.
+
+Names, argument meaning and error behaviour follow timo-eichhorn/Lettuce (paths relative to
+the reference project root); every call goes to liblettuce_b200.so.  Fields cross in the
+reference layout, numpy float64 arrays of shape [V, 4, 3, 3, 2].
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import PREC, LettuceError, check, lib
+
+
+def _ext(ext) -> np.ndarray:
+    e = np.ascontiguousarray([int(v) for v in ext], dtype=np.int32)
+    if e.shape != (4,):
+        raise ValueError("extents must be (Nt, Nx, Ny, Nz)")
+    return e
+
+
+def haar_links(ext, seed: int) -> np.ndarray:
+    """Seeded Haar-random SU(3) links in the reference layout (host generator)."""
+    e = _ext(ext)
+    out = np.empty((int(np.prod(e)), 4, 3, 3, 2))
+    check(lib().lt_haar_links(e, C.c_uint64(seed), out))
+    return out
+
+
+class GaugeField:
+    """GaugeField4D (LettuceGauge/lattice.hpp:87-394) resident on the GPU."""
+
+    def __init__(self, ext, prec: str = "fp64"):
+        self.ext = tuple(int(v) for v in ext)
+        self.prec = prec
+        h = C.c_void_p()
+        check(lib().lt_create(_ext(ext), PREC[prec], C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().lt_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Volume(self) -> int:
+        return int(np.prod(self.ext))
+
+    def Length(self, d: int) -> int:
+        return self.ext[d]
+
+    def upload(self, links: np.ndarray) -> None:
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        if a.size != self.Volume() * 72:
+            raise ValueError("link array has the wrong size")
+        check(lib().lt_upload_links(self._h, a.reshape(-1)))
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.Volume(), 4, 3, 3, 2))
+        check(lib().lt_download_links(self._h, out.reshape(-1)))
+        return out
+
+    def get_link(self, site: int, mu: int) -> np.ndarray:
+        """operator()(link_coord) read (lattice.hpp:113-136): 3x3 complex."""
+        m = np.empty(18)
+        check(lib().lt_get_link(self._h, int(site), int(mu), m))
+        return (m[0::2] + 1j * m[1::2]).reshape(3, 3)
+
+    def set_link(self, site: int, mu: int, M) -> None:
+        M = np.asarray(M, dtype=np.complex128).reshape(9)
+        m = np.empty(18)
+        m[0::2], m[1::2] = M.real, M.imag
+        check(lib().lt_set_link(self._h, int(site), int(mu), m))
+
+    def assign(self, other: "GaugeField") -> None:
+        """operator= (lattice.hpp:106-112)."""
+        check(lib().lt_copy(self._h, other._h))
+
+    def SetToIdentity(self) -> None:
+        check(lib().lt_set_identity(self._h))
+
+    def SetToHaarRandom(self, seed: int) -> None:
+        check(lib().lt_set_haar_random(self._h, C.c_uint64(seed)))
+
+    def synchronize(self) -> None:
+        check(lib().lt_synchronize(self._h))
+
+    @property
+    def stream(self) -> int:
+        """The handle's cudaStream_t as an integer (for event timing on that stream)."""
+        s = C.c_void_p()
+        check(lib().lt_get_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
+
+
+def Swap(U1: GaugeField, U2: GaugeField) -> None:
+    """Swap (lattice.hpp:238-246): exchanges the link storage."""
+    check(lib().lt_swap(U1.handle, U2.handle))
+
+
+def _out1(fn, *args) -> float:
+    v = C.c_double()
+    check(fn(*args, C.byref(v)))
+    return v.value
+
+
+def PlaquetteSum(U: GaugeField) -> float:
+    """observables/plaquette.hpp:26-43."""
+    return _out1(lib().lt_plaquette_sum, U.handle)
+
+
+def TopChargeClover(U: GaugeField) -> float:
+    """observables/topological_charge.hpp:97-200."""
+    return _out1(lib().lt_topcharge_clover, U.handle)
+
+
+def EnergyDensityClover(U: GaugeField) -> float:
+    """EnergyDensity::Clover of the traceless clover field strength
+    (observables/field_strength_tensor.hpp:154-175)."""
+    return _out1(lib().lt_energy_clover, U.handle)
+
+
+def CloverObservables(U: GaugeField) -> tuple[float, float]:
+    q, e = C.c_double(), C.c_double()
+    check(lib().lt_clover_observables(U.handle, C.byref(q), C.byref(e)))
+    return q.value, e.value
+
+
+def Staples(U: GaugeField) -> np.ndarray:
+    """WilsonAction::Staple for every link (actions/gauge/rectangular_action.hpp:104-184)."""
+    out = np.empty((U.Volume(), 4, 3, 3, 2))
+    check(lib().lt_staples(U.handle, out.reshape(-1)))
+    return out
+
+
+class WilsonAction:
+    """GaugeAction::Rectangular<1> with (c_plaq, c_rect) = (1, 0)
+    (actions/gauge/rectangular_action.hpp:23-294)."""
+
+    def __init__(self, beta: float = 6.0):
+        self.beta = float(beta)
+
+    def SetBeta(self, beta: float) -> None:
+        self.beta = float(beta)
+
+    def GetBeta(self) -> float:
+        return self.beta
+
+    def Action(self, U: GaugeField) -> float:
+        return _out1(lib().lt_wilson_action, U.handle, self.beta)
+
+    def ActionNormalized(self, U: GaugeField) -> float:
+        return self.Action(U) / (6.0 * self.beta * U.Volume())
+
+    def Force(self, U: GaugeField) -> np.ndarray:
+        """beta/6 Algebra(st U^dag) per link (updates/hmc_gauge.hpp:450-464)."""
+        out = np.empty((U.Volume(), 4, 3, 3, 2))
+        check(lib().lt_gauge_force(U.handle, self.beta, out.reshape(-1)))
+        return out
+
+
+class HeatbathKernel:
+    """HeatbathKernel (updates/heatbath.hpp:30-130).  beta is taken at construction, like the
+    reference's cached prefactor 3/beta (:40); random numbers come from Philox streams keyed
+    by `seed`, one counter value per sweep."""
+
+    def __init__(self, U: GaugeField, action: WilsonAction, seed: int = 1, counter: int = 0):
+        self.U, self.beta, self.seed = U, action.GetBeta(), int(seed)
+        self.counter = C.c_uint64(counter)
+
+    def sweeps(self, n: int) -> None:
+        check(lib().lt_heatbath_sweeps(self.U.handle, self.beta, int(n), C.c_uint64(self.seed), C.byref(self.counter)))
+
+
+class OverrelaxationSubgroupKernel:
+    """OverrelaxationSubgroupKernel (updates/overrelaxation.hpp:68-117)."""
+
+    def __init__(self, U: GaugeField, action: WilsonAction | None = None):
+        self.U = U
+
+    def sweeps(self, n: int) -> None:
+        check(lib().lt_overrelax_sweeps(self.U.handle, int(n)))
+
+
+class Iterator:
+    """Iterator::Checkerboard (iterators/iterators.hpp:65-87): a whole sweep (all mu and both
+    parities) is one call; a per-link functor cannot cross to the device."""
+
+    @staticmethod
+    def Checkerboard(kernel, n_sweep: int = 1) -> None:
+        kernel.sweeps(n_sweep)
+
+    Checkerboard4 = Checkerboard
+
+
+def UpdateSweeps(U: GaugeField, beta: float, n_sweep: int, n_hb: int, n_or: int, seed: int, counter: int = 0) -> int:
+    """n_sweep rounds of (n_hb heatbath + n_or overrelaxation); returns the next counter."""
+    c = C.c_uint64(counter)
+    check(lib().lt_update_sweeps(U.handle, float(beta), int(n_sweep), int(n_hb), int(n_or), C.c_uint64(seed), C.byref(c)))
+    return c.value
+
+
+class RK3:
+    """Integrators::GradientFlow::RK3 (smearing/gradient_flow.hpp:120-168)."""
+
+    @staticmethod
+    def ReturnName() -> str:
+        return "RK3"
+
+
+class GradientFlowKernel:
+    """GradientFlowKernel (smearing/gradient_flow.hpp:252-367) with the RK3 integrator."""
+
+    def __init__(self, U_unflowed: GaugeField, U_flowed: GaugeField, integrator=RK3, action=None, epsilon: float = 0.01):
+        if integrator is not RK3:
+            raise ValueError("only the RK3 integrator is provided")
+        self.U_unflowed, self.U_flowed, self.epsilon = U_unflowed, U_flowed, float(epsilon)
+
+    def __call__(self, n_step: int) -> None:
+        check(lib().lt_flow_rk3(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, int(n_step)))
+
+    def Resume(self, n_step: int) -> None:
+        check(lib().lt_flow_rk3(self.U_flowed.handle, self.U_flowed.handle, self.epsilon, int(n_step)))
+
+    def Measure(self, n_meas: int, every: int):
+        """Flow from U_unflowed with (plaquette sum, Q, E) after every `every` steps."""
+        p, q, e = np.empty(n_meas), np.empty(n_meas), np.empty(n_meas)
+        check(lib().lt_flow_rk3_measure(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, int(n_meas),
+                                        int(every), p.ctypes.data, q.ctypes.data, e.ctypes.data))
+        return p, q, e
+
+    def SetEpsilon(self, eps: float) -> None:
+        self.epsilon = float(eps)
+
+    def GetEpsilon(self) -> float:
+        return self.epsilon
+
+
+def StoutSmearing4D(U_unsmeared: GaugeField, U_smeared: GaugeField, smear_param: float = 0.12) -> None:
+    """smearing/stout_smearing.hpp:29-57."""
+    check(lib().lt_stout(U_unsmeared.handle, U_smeared.handle, float(smear_param), 1))
+
+
+def StoutSmearingN(U_in: GaugeField, U_out: GaugeField, N: int, smear_param: float = 0.12) -> None:
+    """N stout steps from U_in into U_out (smearing/stout_smearing.hpp:61-76)."""
+    check(lib().lt_stout(U_in.handle, U_out.handle, float(smear_param), int(N)))
+
+
+class MetaBiasPotential:
+    """MetaBiasPotential (actions/bias_potential/metadynamics.hpp:29-507)."""
+
+    def __init__(self, CV_min, CV_max, bin_number, weight, width, well_tempered_parameter, threshold_weight):
+        h = C.c_void_p()
+        code = lib().lt_bias_create(float(CV_min), float(CV_max), int(bin_number), float(weight), float(width),
+                                    float(well_tempered_parameter), float(threshold_weight), C.byref(h))
+        if code != 0:
+            raise ValueError(lib().lt_last_error().decode())   # the reference throws std::invalid_argument
+        self._h = h
+        self.bin_number = int(bin_number)
+        self._cv_min = float(CV_min)
+        self._bin_width = (float(CV_max) - float(CV_min)) / int(bin_number)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        try:
+            if self._h.value:
+                lib().lt_bias_destroy(self._h)
+        except Exception:
+            pass
+
+    def UpdatePotential(self, cv) -> None:
+        a = np.atleast_1d(np.asarray(cv, dtype=np.float64))
+        check(lib().lt_bias_update(self._h, a.ctypes.data, a.size, 0))
+
+    def UpdatePotentialSymmetric(self, cv) -> None:
+        a = np.atleast_1d(np.asarray(cv, dtype=np.float64))
+        check(lib().lt_bias_update(self._h, a.ctypes.data, a.size, 1))
+
+    def ReturnPotential(self, cv: float) -> float:
+        return _out1(lib().lt_bias_potential, self._h, float(cv))
+
+    def ReturnDerivative(self, cv: float) -> float:
+        return _out1(lib().lt_bias_derivative, self._h, float(cv))
+
+    def grid(self) -> np.ndarray:
+        g = np.empty(self.bin_number + 1)
+        check(lib().lt_bias_get_grid(self._h, g, g.size))
+        return g
+
+    def set_grid(self, g) -> None:
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        check(lib().lt_bias_set_grid(self._h, g, g.size))
+
+    def GeneratePotentialFrom(self, fn) -> None:
+        """GeneratePotentialFrom (metadynamics.hpp:93-100)."""
+        n = self.bin_number + 1
+        self.set_grid(np.array([fn(self._cv_min + i * self._bin_width) for i in range(n)], dtype=np.float64))
+
+
+class HMCKernel:
+    """GaugeUpdates::HMCKernel with Integrators::HMC::OMF_2 (updates/hmc_gauge.hpp:155-190,
+    :381-600)."""
+
+    def __init__(self, U: GaugeField, action: WilsonAction, trajectory_length: float = 1.0, seed: int = 1,
+                 counter: int = 0):
+        self.U, self.beta, self.tau, self.seed = U, action.GetBeta(), float(trajectory_length), int(seed)
+        self.counter = C.c_uint64(counter)
+        self.delta_H = 0.0
+
+    def __call__(self, n_step: int, metropolis_step: bool = True) -> bool:
+        dH, acc = C.c_double(), C.c_int()
+        check(lib().lt_hmc_trajectory(self.U.handle, self.beta, self.tau, int(n_step), C.c_uint64(self.seed),
+                                      C.byref(self.counter), int(bool(metropolis_step)), C.byref(dH), C.byref(acc)))
+        self.delta_H = dH.value
+        return bool(acc.value)
+
+    def SetMomenta(self, P: np.ndarray) -> None:
+        check(lib().lt_set_momenta(self.U.handle, np.ascontiguousarray(P, dtype=np.float64).reshape(-1)))
+
+    def GetMomenta(self) -> np.ndarray:
+        out = np.empty((self.U.Volume(), 4, 3, 3, 2))
+        check(lib().lt_get_momenta(self.U.handle, out.reshape(-1)))
+        return out
+
+    def RandomMomentum(self, counter: int) -> None:
+        check(lib().lt_random_momenta(self.U.handle, C.c_uint64(self.seed), C.c_uint64(counter)))
+
+    def Hamiltonian(self) -> float:
+        return _out1(lib().lt_hamiltonian, self.U.handle, self.beta)
+
+    def Integrate(self, n_step: int) -> tuple[float, float]:
+        """OMF_2 molecular dynamics only; returns (H_old, H_new)."""
+        ho, hn = C.c_double(), C.c_double()
+        check(lib().lt_omf2(self.U.handle, self.beta, self.tau, int(n_step), C.byref(ho), C.byref(hn)))
+        return ho.value, hn.value
+
+
+class HMCMetaDKernel(HMCKernel):
+    """GaugeUpdates::HMCMetaDKernel (updates/hmc_metadynamics.hpp:264-675) with OMF_2, CV =
+    clover Q after n_smear_meta stout steps of parameter rho_stout_cv."""
+
+    def __init__(self, U: GaugeField, bias: MetaBiasPotential, action: WilsonAction, trajectory_length: float = 1.0,
+                 rho_stout_cv: float = 0.12, n_smear_meta: int = 4, seed: int = 1, counter: int = 0):
+        super().__init__(U, action, trajectory_length, seed, counter)
+        self.bias, self.rho, self.n_smear = bias, float(rho_stout_cv), int(n_smear_meta)
+        self.cv = 0.0
+
+    def __call__(self, n_step: int, metropolis_step: bool = True) -> bool:
+        dH, acc, cv = C.c_double(), C.c_int(), C.c_double()
+        check(lib().lt_metad_hmc_trajectory(self.U.handle, self.bias.handle, self.beta, self.tau, int(n_step), self.rho,
+                                            self.n_smear, C.c_uint64(self.seed), C.byref(self.counter),
+                                            int(bool(metropolis_step)), C.byref(dH), C.byref(acc), C.byref(cv)))
+        self.delta_H, self.cv = dH.value, cv.value
+        return bool(acc.value)
+
+    def MetaCharge(self) -> float:
+        return _out1(lib().lt_metad_charge, self.U.handle, self.rho, self.n_smear)
+
+    def CalculateTopologicalForce(self, dvdq: float | None = None) -> tuple[np.ndarray, float]:
+        """dV/dQ * dQ_smeared/dU on the thin links; dV/dQ from the bias unless given."""
+        q = C.c_double()
+        if dvdq is None:
+            check(lib().lt_metad_force(self.U.handle, self.rho, self.n_smear, 0.0, None, C.byref(q)))
+            dvdq = self.bias.ReturnDerivative(q.value)
+        out = np.empty((self.U.Volume(), 4, 3, 3, 2))
+        check(lib().lt_metad_force(self.U.handle, self.rho, self.n_smear, float(dvdq), out.ctypes.data, C.byref(q)))
+        return out, q.value
+
+    def Integrate(self, n_step: int) -> tuple[float, float]:
+        ho, hn = C.c_double(), C.c_double()
+        check(lib().lt_metad_omf2(self.U.handle, self.bias.handle, self.beta, self.tau, int(n_step), self.rho,
+                                  self.n_smear, C.byref(ho), C.byref(hn)))
+        return ho.value, hn.value
+
+
+def CloverDerivative(U: GaugeField) -> np.ndarray:
+    """CloverDerivative for every link (observables/clover.hpp:279-321)."""
+    out = np.empty((U.Volume(), 4, 3, 3, 2))
+    check(lib().lt_clover_derivative(U.handle, out.reshape(-1)))
+    return out
+
+
+__all__ = ["GaugeField", "Swap", "haar_links", "PlaquetteSum", "TopChargeClover", "EnergyDensityClover",
+           "CloverObservables", "Staples", "WilsonAction", "HeatbathKernel", "OverrelaxationSubgroupKernel",
+           "Iterator", "UpdateSweeps", "RK3", "GradientFlowKernel", "StoutSmearing4D", "StoutSmearingN",
+           "MetaBiasPotential", "HMCKernel", "HMCMetaDKernel", "CloverDerivative", "LettuceError"]

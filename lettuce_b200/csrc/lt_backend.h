@@ -1,0 +1,71 @@
+// Precision-independent interface between the C ABI (lt_capi.cu) and the kernels.  One
+// implementation per storage format (FP64 18 reals, FP32 18 reals, FP32 12 reals) lives in
+// its own translation unit so the three are compiled in parallel.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lt_field.cuh"
+
+namespace lt {
+
+// Launch context: geometry, stream and the reduction scratch of one lattice handle.
+struct Ctx
+{
+    Geom g;
+    cudaStream_t stream;
+    double* partials;   // kNumSlots * kRedBlocks doubles
+    double* results;    // kNumSlots doubles
+};
+
+constexpr int kNumSlots = 8;
+
+class Backend
+{
+public:
+    virtual ~Backend() = default;
+    virtual int real_bytes() const = 0;                     // 8 (FP64) or 4 (FP32)
+    virtual size_t gauge_bytes(const Geom& g) const = 0;     // one link field
+    virtual size_t alg_bytes(const Geom& g) const = 0;       // one algebra field (8 reals/link)
+    virtual size_t full_bytes(const Geom& g) const = 0;      // one 3x3 complex per link
+    virtual size_t clov_bytes(const Geom& g) const = 0;      // six anti-Hermitian planes per site
+
+    virtual void from_aos(const Ctx& c, void* U, const double* aos) const = 0;
+    virtual void to_aos(const Ctx& c, const void* U, double* aos) const = 0;
+    virtual void alg_from_aos(const Ctx& c, void* P, const double* aos) const = 0;
+    virtual void alg_to_aos(const Ctx& c, const void* P, double* aos) const = 0;
+    virtual void set_unit(const Ctx& c, void* U) const = 0;
+    // single link (site = reference site index) from / to 18 doubles in device memory
+    virtual void link_io(const Ctx& c, void* U, int site, int mu, double* m, int write) const = 0;
+    virtual void staples_aos(const Ctx& c, const void* U, double* aos) const = 0;
+
+    // reductions write ctx.results[slot] (and slot+1 for clover_obs: q then e)
+    virtual void plaquette(const Ctx& c, const void* U, int slot) const = 0;
+    virtual void clover_obs(const Ctx& c, const void* U, int slot) const = 0;
+    virtual void kinetic(const Ctx& c, const void* P, int slot) const = 0;
+
+    virtual void overrelax(const Ctx& c, void* U, int mu, int par) const = 0;
+    virtual void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter,
+                          uint64_t seed, int max_iter) const = 0;
+    virtual void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new,
+                            double c_exp, int read_z, int write_z) const = 0;
+    virtual void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const = 0;
+
+    virtual void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const = 0;
+    virtual void fields(const Ctx& c, void* U, const void* P, double eps) const = 0;
+    virtual void random_momenta(const Ctx& c, void* P, uint64_t counter, uint64_t seed) const = 0;
+
+    virtual void clover_R(const Ctx& c, const void* U, void* R) const = 0;
+    virtual void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const = 0;
+    virtual void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam,
+                              void* Tloc, double rho) const = 0;
+    virtual void stout_recursion(const Ctx& c, const void* U, const void* Lam, const void* Tloc, void* Sigma,
+                                 double rho) const = 0;
+};
+
+const Backend* backend_fp64();
+const Backend* backend_fp32();
+const Backend* backend_fp32_12();
+
+} // namespace lt

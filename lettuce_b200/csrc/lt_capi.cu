@@ -1,0 +1,830 @@
+// C ABI of the lattice handle: device memory, one stream per handle, and the sequencing
+// of kernels for sweeps, flow, stout smearing, HMC and the metadynamics force.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "lettuce_b200.h"
+#include "lt_backend.h"
+#include "lt_host.h"
+
+namespace lt {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char* msg)
+{
+    g_last_error = msg ? msg : "";
+    return code;
+}
+
+static int cuda_error(cudaError_t e, const char* what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    g_last_error = m;
+    return e == cudaErrorMemoryAllocation ? LT_ERR_NOMEM : LT_ERR_CUDA;
+}
+
+} // namespace lt
+
+#define LT_CK(call)                                                  \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return lt::cuda_error(e_, #call);     \
+    } while (0)
+
+#define LT_TRY(call)                                                 \
+    do {                                                             \
+        int r_ = (call);                                             \
+        if (r_ != LT_OK) return r_;                                  \
+    } while (0)
+
+struct lt_lattice
+{
+    int ext[4];
+    int prec;
+    int device;
+    lt::Geom g;
+    const lt::Backend* be;
+    cudaStream_t stream = nullptr;
+    void* U = nullptr;       // links
+    void* U2 = nullptr;      // ping-pong partner for flow / stout
+    void* Z = nullptr;       // flow Z (algebra)
+    void* P = nullptr;       // HMC momenta (algebra)
+    void* F = nullptr;       // metadynamics force / Sigma (algebra)
+    void* Ubak = nullptr;    // HMC backup of the links
+    void* R = nullptr;       // clover planes
+    void* Lam = nullptr;     // Lambda (algebra)
+    void* Tloc = nullptr;    // link-local recursion term (full matrix)
+    std::vector<void*> levels;   // smeared levels 1..n of the MetaD chain
+    double* partials = nullptr;
+    double* results = nullptr;
+    double* h_results = nullptr; // pinned
+    double* d_aos = nullptr;     // staging buffer for host transfers (reference layout)
+
+    lt::Ctx ctx() const
+    {
+        lt::Ctx c;
+        c.g = g;
+        c.stream = stream;
+        c.partials = partials;
+        c.results = results;
+        return c;
+    }
+};
+
+namespace {
+
+int check_h(const lt_lattice* h, const char* fn)
+{
+    if (!h) return lt::set_error(LT_ERR_ARG, (std::string(fn) + ": null handle").c_str());
+    return LT_OK;
+}
+
+int ensure(lt_lattice* h, void** p, size_t bytes)
+{
+    if (*p) return LT_OK;
+    LT_CK(cudaSetDevice(h->device));
+    LT_CK(cudaMalloc(p, bytes));
+    return LT_OK;
+}
+
+int ensure_aos(lt_lattice* h) { return ensure(h, (void**)&h->d_aos, (size_t)4 * h->g.V * 18 * sizeof(double)); }
+
+// Kernel-launch status after a batch of launches
+int launched(const char* what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return lt::cuda_error(e, what);
+    return LT_OK;
+}
+
+// Copy results[slot..slot+n) to host and wait for the stream.
+int fetch(lt_lattice* h, int slot, int n, double* out)
+{
+    LT_TRY(launched("reduction"));
+    LT_CK(cudaMemcpyAsync(h->h_results, h->results + slot, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < n; ++k) out[k] = h->h_results[k];
+    return LT_OK;
+}
+
+// Make `dst` wait for all work queued on `src`.
+int order_after(lt_lattice* dst, const lt_lattice* src)
+{
+    if (dst == src) return LT_OK;
+    cudaEvent_t ev;
+    LT_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    LT_CK(cudaEventRecord(ev, src->stream));
+    LT_CK(cudaStreamWaitEvent(dst->stream, ev, 0));
+    LT_CK(cudaEventDestroy(ev));
+    return LT_OK;
+}
+
+const double kPi = 3.14159265358979323846;
+
+// Integrators::GradientFlow::RK3 (smearing/gradient_flow.hpp:151-161): three fused stages
+int flow_steps(lt_lattice* h, double eps, int n_step)
+{
+    LT_TRY(ensure(h, &h->U2, h->be->gauge_bytes(h->g)));
+    LT_TRY(ensure(h, &h->Z, h->be->alg_bytes(h->g)));
+    const lt::Ctx c = h->ctx();
+    for (int k = 0; k < n_step; ++k)
+    {
+        h->be->flow_stage(c, h->U, h->U2, h->Z, 0.0, eps, 0.25, 0, 1);
+        std::swap(h->U, h->U2);
+        h->be->flow_stage(c, h->U, h->U2, h->Z, -17.0 / 36.0, 8.0 / 9.0 * eps, 1.0, 1, 1);
+        std::swap(h->U, h->U2);
+        h->be->flow_stage(c, h->U, h->U2, h->Z, -1.0, 3.0 / 4.0 * eps, 1.0, 1, 0);
+        std::swap(h->U, h->U2);
+    }
+    return launched("flow_rk3");
+}
+
+int stout_steps(lt_lattice* h, double rho, int n)
+{
+    LT_TRY(ensure(h, &h->U2, h->be->gauge_bytes(h->g)));
+    const lt::Ctx c = h->ctx();
+    for (int k = 0; k < n; ++k)
+    {
+        h->be->stout(c, h->U, h->U2, rho);
+        std::swap(h->U, h->U2);
+    }
+    return launched("stout");
+}
+
+int clover_q_e(lt_lattice* h, const void* U, double* q, double* e)
+{
+    h->be->clover_obs(h->ctx(), U, 2);
+    double r[2];
+    LT_TRY(fetch(h, 2, 2, r));
+    if (q) *q = -1.0 / (64.0 * 4.0 * kPi * kPi) * r[0];
+    if (e) *e = r[1] / (double)h->g.V;
+    return LT_OK;
+}
+
+int plaq_of(lt_lattice* h, const void* U, double* out)
+{
+    h->be->plaquette(h->ctx(), U, 0);
+    return fetch(h, 0, 1, out);
+}
+
+// Forward stout chain U -> levels[1..n] (StoutSmearing4DWithConstants,
+// smearing/stout_smearing.hpp:92-119, without storing the exponential constants)
+int metad_forward(lt_lattice* h, double rho, int n_stout)
+{
+    while ((int)h->levels.size() < n_stout)
+    {
+        void* p = nullptr;
+        LT_CK(cudaMalloc(&p, h->be->gauge_bytes(h->g)));
+        h->levels.push_back(p);
+    }
+    const lt::Ctx c = h->ctx();
+    const void* prev = h->U;
+    for (int k = 0; k < n_stout; ++k)
+    {
+        h->be->stout(c, prev, h->levels[k], rho);
+        prev = h->levels[k];
+    }
+    return launched("metad_forward");
+}
+
+const void* level(const lt_lattice* h, int k) { return k == 0 ? h->U : h->levels[k - 1]; }
+
+// dvdq * dQ/dU into h->F, given the forward chain (CalculateTopologicalForce,
+// updates/hmc_metadynamics.hpp:374-436)
+int metad_backward(lt_lattice* h, double rho, int n_stout, double dvdq)
+{
+    LT_TRY(ensure(h, &h->F, h->be->alg_bytes(h->g)));
+    LT_TRY(ensure(h, &h->R, h->be->clov_bytes(h->g)));
+    LT_TRY(ensure(h, &h->Lam, h->be->alg_bytes(h->g)));
+    LT_TRY(ensure(h, &h->Tloc, h->be->full_bytes(h->g)));
+    const lt::Ctx c = h->ctx();
+    const void* top = level(h, n_stout);
+    h->be->clover_R(c, top, h->R);
+    h->be->clover_deriv(c, top, h->R, h->F, dvdq);
+    for (int k = n_stout; k > 0; --k)
+    {
+        h->be->stout_lambda(c, level(h, k - 1), level(h, k), h->F, h->Lam, h->Tloc, rho);
+        h->be->stout_recursion(c, level(h, k - 1), h->Lam, h->Tloc, h->F, rho);
+    }
+    return launched("metad_backward");
+}
+
+int hamiltonian(lt_lattice* h, double beta, double* out)
+{
+    const lt::Ctx c = h->ctx();
+    h->be->plaquette(c, h->U, 0);
+    h->be->kinetic(c, h->P, 1);
+    double r[2];
+    LT_TRY(fetch(h, 0, 2, r));
+    *out = beta * (6.0 * (double)h->g.V - r[0] / 3.0) + r[1];
+    return LT_OK;
+}
+
+// Momentum kick with optional MetaD force.  For MetaD the force is evaluated on the
+// current links first (UpdateMomenta, updates/hmc_metadynamics.hpp:441-459).
+struct MetaDParams
+{
+    lt::Bias* bias;
+    double rho;
+    int n_stout;
+    std::vector<double>* samples;
+};
+
+int kick(lt_lattice* h, double beta, double eps, const MetaDParams* md, bool submeasure)
+{
+    const void* F = nullptr;
+    if (md)
+    {
+        LT_TRY(metad_forward(h, md->rho, md->n_stout));
+        double q;
+        LT_TRY(clover_q_e(h, level(h, md->n_stout), &q, nullptr));
+        if (submeasure && md->samples) md->samples->push_back(q);
+        LT_TRY(metad_backward(h, md->rho, md->n_stout, md->bias->derivative(q)));
+        F = h->F;
+    }
+    h->be->momenta(h->ctx(), h->U, h->P, F, beta / 6.0, eps);
+    return launched("momenta");
+}
+
+int drift(lt_lattice* h, double eps)
+{
+    h->be->fields(h->ctx(), h->U, h->P, eps);
+    return launched("fields");
+}
+
+// Integrators::HMC::OMF_2 (updates/hmc_gauge.hpp:155-190)
+int omf2(lt_lattice* h, double beta, double tau, int n_step, const MetaDParams* md)
+{
+    if (n_step <= 0) return LT_OK;
+    const double lam = 0.1931833275037836;
+    const double eps = tau / n_step;
+    const double a = lam * eps, b = 0.5 * eps, g = (1.0 - 2.0 * lam) * eps;
+    LT_TRY(kick(h, beta, a, md, false));
+    LT_TRY(drift(h, b));
+    LT_TRY(kick(h, beta, g, md, false));
+    LT_TRY(drift(h, b));
+    for (int k = 0; k < n_step - 1; ++k)
+    {
+        LT_TRY(kick(h, beta, 2.0 * a, md, true));
+        LT_TRY(drift(h, b));
+        LT_TRY(kick(h, beta, g, md, false));
+        LT_TRY(drift(h, b));
+    }
+    return kick(h, beta, a, md, true);
+}
+
+int metad_charge(lt_lattice* h, double rho, int n_stout, double* q)
+{
+    LT_TRY(metad_forward(h, rho, n_stout));
+    return clover_q_e(h, level(h, n_stout), q, nullptr);
+}
+
+double accept_uniform(uint64_t seed, uint64_t counter)
+{
+    lt::U4 w = lt::philox4x32(0u, (uint32_t)counter, (uint32_t)(counter >> 32), lt::TAG_ACCEPT << 24, (uint32_t)seed,
+                              (uint32_t)(seed >> 32));
+    return lt::u01_from(w.x, w.y);
+}
+
+} // namespace
+
+extern "C" {
+
+const char* lt_last_error(void) { return lt::g_last_error.c_str(); }
+
+int lt_version(void) { return 100; }
+
+int lt_create(const int ext[4], int prec, lt_lattice** out)
+{
+    if (!out || !ext) return lt::set_error(LT_ERR_ARG, "lt_create: null pointer");
+    *out = nullptr;
+    for (int d = 0; d < 4; ++d)
+        if (ext[d] < 2 || ext[d] % 2) return lt::set_error(LT_ERR_ARG, "lt_create: extents must be even and >= 2");
+    long long V = (long long)ext[0] * ext[1] * ext[2] * ext[3];
+    if (V * 4 * 9 >= (1LL << 31)) return lt::set_error(LT_ERR_ARG, "lt_create: lattice too large");
+    const lt::Backend* be = prec == LT_PREC_FP64 ? lt::backend_fp64()
+                          : prec == LT_PREC_FP32 ? lt::backend_fp32()
+                          : prec == LT_PREC_FP32_12 ? lt::backend_fp32_12() : nullptr;
+    if (!be) return lt::set_error(LT_ERR_ARG, "lt_create: unknown precision");
+    auto* h = new (std::nothrow) lt_lattice();
+    if (!h) return lt::set_error(LT_ERR_NOMEM, "lt_create: out of host memory");
+    std::memcpy(h->ext, ext, sizeof(h->ext));
+    h->prec = prec;
+    h->g = lt::make_geom(ext);
+    h->be = be;
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&h->U, be->gauge_bytes(h->g));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->partials, sizeof(double) * lt::kNumSlots * lt::kRedBlocks);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->results, sizeof(double) * lt::kNumSlots);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_results, sizeof(double) * lt::kNumSlots);
+    if (e != cudaSuccess)
+    {
+        int r = lt::cuda_error(e, "lt_create");
+        lt_destroy(h);
+        return r;
+    }
+    be->set_unit(h->ctx(), h->U);
+    int r = launched("lt_create");
+    if (r != LT_OK)
+    {
+        lt_destroy(h);
+        return r;
+    }
+    *out = h;
+    return LT_OK;
+}
+
+int lt_destroy(lt_lattice* h)
+{
+    if (!h) return LT_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void* bufs[] = { h->U, h->U2, h->Z, h->P, h->F, h->Ubak, h->R, h->Lam, h->Tloc, h->partials, h->results, h->d_aos };
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    for (void* p : h->levels) cudaFree(p);
+    if (h->h_results) cudaFreeHost(h->h_results);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return LT_OK;
+}
+
+int lt_get_extents(const lt_lattice* h, int ext[4], int* prec)
+{
+    LT_TRY(check_h(h, "lt_get_extents"));
+    if (ext) std::memcpy(ext, h->ext, sizeof(h->ext));
+    if (prec) *prec = h->prec;
+    return LT_OK;
+}
+
+int lt_upload_links(lt_lattice* h, const double* links)
+{
+    LT_TRY(check_h(h, "lt_upload_links"));
+    if (!links) return lt::set_error(LT_ERR_ARG, "lt_upload_links: null pointer");
+    LT_TRY(ensure_aos(h));
+    LT_CK(cudaMemcpyAsync(h->d_aos, links, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyHostToDevice,
+                          h->stream));
+    h->be->from_aos(h->ctx(), h->U, h->d_aos);
+    LT_TRY(launched("lt_upload_links"));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_download_links(lt_lattice* h, double* links)
+{
+    LT_TRY(check_h(h, "lt_download_links"));
+    if (!links) return lt::set_error(LT_ERR_ARG, "lt_download_links: null pointer");
+    LT_TRY(ensure_aos(h));
+    h->be->to_aos(h->ctx(), h->U, h->d_aos);
+    LT_TRY(launched("lt_download_links"));
+    LT_CK(cudaMemcpyAsync(links, h->d_aos, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyDeviceToHost,
+                          h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+static int link_access(lt_lattice* h, int64_t site, int mu, double* m, int write)
+{
+    if (!m || site < 0 || site >= h->g.V || mu < 0 || mu > 3)
+        return lt::set_error(LT_ERR_ARG, "lt_set_link/lt_get_link: bad site, direction or pointer");
+    LT_TRY(ensure_aos(h));
+    if (write) LT_CK(cudaMemcpyAsync(h->d_aos, m, 18 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    h->be->link_io(h->ctx(), h->U, (int)site, mu, h->d_aos, write);
+    LT_TRY(launched("link access"));
+    if (!write) LT_CK(cudaMemcpyAsync(m, h->d_aos, 18 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_set_link(lt_lattice* h, int64_t site, int mu, const double* m)
+{
+    LT_TRY(check_h(h, "lt_set_link"));
+    return link_access(h, site, mu, const_cast<double*>(m), 1);
+}
+
+int lt_get_link(lt_lattice* h, int64_t site, int mu, double* m_out)
+{
+    LT_TRY(check_h(h, "lt_get_link"));
+    return link_access(h, site, mu, m_out, 0);
+}
+
+int lt_copy(lt_lattice* dst, const lt_lattice* src)
+{
+    LT_TRY(check_h(dst, "lt_copy"));
+    LT_TRY(check_h(src, "lt_copy"));
+    if (dst == src) return LT_OK;
+    if (std::memcmp(dst->ext, src->ext, sizeof(dst->ext)))
+        return lt::set_error(LT_ERR_ARG, "lt_copy: extents differ");
+    LT_TRY(order_after(dst, src));
+    if (dst->prec == src->prec)
+    {
+        LT_CK(cudaMemcpyAsync(dst->U, src->U, dst->be->gauge_bytes(dst->g), cudaMemcpyDeviceToDevice, dst->stream));
+    }
+    else
+    {
+        LT_TRY(ensure_aos(dst));
+        src->be->to_aos(dst->ctx(), src->U, dst->d_aos);
+        dst->be->from_aos(dst->ctx(), dst->U, dst->d_aos);
+    }
+    LT_TRY(launched("lt_copy"));
+    // src may be reused by its owner right after this returns
+    LT_CK(cudaStreamSynchronize(dst->stream));
+    return LT_OK;
+}
+
+int lt_swap(lt_lattice* a, lt_lattice* b)
+{
+    LT_TRY(check_h(a, "lt_swap"));
+    LT_TRY(check_h(b, "lt_swap"));
+    if (std::memcmp(a->ext, b->ext, sizeof(a->ext)) || a->prec != b->prec)
+        return lt::set_error(LT_ERR_ARG, "lt_swap: extents or formats differ");
+    LT_CK(cudaStreamSynchronize(a->stream));
+    LT_CK(cudaStreamSynchronize(b->stream));
+    std::swap(a->U, b->U);
+    return LT_OK;
+}
+
+int lt_set_identity(lt_lattice* h)
+{
+    LT_TRY(check_h(h, "lt_set_identity"));
+    h->be->set_unit(h->ctx(), h->U);
+    return launched("lt_set_identity");
+}
+
+int lt_set_haar_random(lt_lattice* h, uint64_t seed)
+{
+    LT_TRY(check_h(h, "lt_set_haar_random"));
+    std::vector<double> buf;
+    try
+    {
+        buf.resize((size_t)4 * h->g.V * 18);
+    }
+    catch (...)
+    {
+        return lt::set_error(LT_ERR_NOMEM, "lt_set_haar_random: out of host memory");
+    }
+    lt::haar_links(h->ext, seed, buf.data());
+    return lt_upload_links(h, buf.data());
+}
+
+int lt_synchronize(lt_lattice* h)
+{
+    LT_TRY(check_h(h, "lt_synchronize"));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_get_stream(const lt_lattice* h, void** stream_out)
+{
+    LT_TRY(check_h(h, "lt_get_stream"));
+    if (!stream_out) return lt::set_error(LT_ERR_ARG, "lt_get_stream: null pointer");
+    *stream_out = (void*)h->stream;
+    return LT_OK;
+}
+
+// ---------------------------------------------------------------- observables
+int lt_plaquette_sum(lt_lattice* h, double* out)
+{
+    LT_TRY(check_h(h, "lt_plaquette_sum"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_plaquette_sum: null pointer");
+    return plaq_of(h, h->U, out);
+}
+
+int lt_wilson_action(lt_lattice* h, double beta, double* out)
+{
+    LT_TRY(check_h(h, "lt_wilson_action"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_wilson_action: null pointer");
+    double p;
+    LT_TRY(plaq_of(h, h->U, &p));
+    *out = beta * (6.0 * (double)h->g.V - p / 3.0);
+    return LT_OK;
+}
+
+int lt_topcharge_clover(lt_lattice* h, double* out)
+{
+    LT_TRY(check_h(h, "lt_topcharge_clover"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_topcharge_clover: null pointer");
+    return clover_q_e(h, h->U, out, nullptr);
+}
+
+int lt_energy_clover(lt_lattice* h, double* out)
+{
+    LT_TRY(check_h(h, "lt_energy_clover"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_energy_clover: null pointer");
+    return clover_q_e(h, h->U, nullptr, out);
+}
+
+int lt_clover_observables(lt_lattice* h, double* q_out, double* e_out)
+{
+    LT_TRY(check_h(h, "lt_clover_observables"));
+    return clover_q_e(h, h->U, q_out, e_out);
+}
+
+int lt_staples(lt_lattice* h, double* staples_out)
+{
+    LT_TRY(check_h(h, "lt_staples"));
+    if (!staples_out) return lt::set_error(LT_ERR_ARG, "lt_staples: null pointer");
+    LT_TRY(ensure_aos(h));
+    h->be->staples_aos(h->ctx(), h->U, h->d_aos);
+    LT_TRY(launched("lt_staples"));
+    LT_CK(cudaMemcpyAsync(staples_out, h->d_aos, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyDeviceToHost,
+                          h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+// ---------------------------------------------------------------- local updates
+int lt_overrelax_sweeps(lt_lattice* h, int n_sweep)
+{
+    LT_TRY(check_h(h, "lt_overrelax_sweeps"));
+    if (n_sweep < 0) return lt::set_error(LT_ERR_ARG, "lt_overrelax_sweeps: n_sweep < 0");
+    const lt::Ctx c = h->ctx();
+    for (int s = 0; s < n_sweep; ++s)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int par = 0; par < 2; ++par) h->be->overrelax(c, h->U, mu, par);
+    return launched("lt_overrelax_sweeps");
+}
+
+int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, uint64_t* counter)
+{
+    LT_TRY(check_h(h, "lt_heatbath_sweeps"));
+    if (n_sweep < 0 || !counter || !(beta > 0.0))
+        return lt::set_error(LT_ERR_ARG, "lt_heatbath_sweeps: bad arguments");
+    const lt::Ctx c = h->ctx();
+    for (int s = 0; s < n_sweep; ++s)
+    {
+        for (int mu = 0; mu < 4; ++mu)
+            for (int par = 0; par < 2; ++par) h->be->heatbath(c, h->U, mu, par, 3.0 / beta, *counter, seed, 10);
+        ++*counter;
+    }
+    return launched("lt_heatbath_sweeps");
+}
+
+int lt_update_sweeps(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed, uint64_t* counter)
+{
+    LT_TRY(check_h(h, "lt_update_sweeps"));
+    if (n_sweep < 0 || n_hb < 0 || n_or < 0 || !counter || !(beta > 0.0))
+        return lt::set_error(LT_ERR_ARG, "lt_update_sweeps: bad arguments");
+    for (int s = 0; s < n_sweep; ++s)
+    {
+        LT_TRY(lt_heatbath_sweeps(h, beta, n_hb, seed, counter));
+        LT_TRY(lt_overrelax_sweeps(h, n_or));
+    }
+    return LT_OK;
+}
+
+// ---------------------------------------------------------------- smearing
+int lt_flow_rk3(lt_lattice* in, lt_lattice* out, double eps, int n_step)
+{
+    LT_TRY(check_h(in, "lt_flow_rk3"));
+    LT_TRY(check_h(out, "lt_flow_rk3"));
+    if (n_step < 0) return lt::set_error(LT_ERR_ARG, "lt_flow_rk3: n_step < 0");
+    LT_TRY(lt_copy(out, in));
+    return flow_steps(out, eps, n_step);
+}
+
+int lt_flow_rk3_measure(lt_lattice* in, lt_lattice* out, double eps, int n_meas, int every, double* plaq_out,
+                        double* q_out, double* e_out)
+{
+    LT_TRY(check_h(in, "lt_flow_rk3_measure"));
+    LT_TRY(check_h(out, "lt_flow_rk3_measure"));
+    if (n_meas < 0 || every < 0) return lt::set_error(LT_ERR_ARG, "lt_flow_rk3_measure: negative count");
+    LT_TRY(lt_copy(out, in));
+    for (int m = 0; m < n_meas; ++m)
+    {
+        LT_TRY(flow_steps(out, eps, every));
+        if (plaq_out) LT_TRY(plaq_of(out, out->U, &plaq_out[m]));
+        if (q_out || e_out)
+            LT_TRY(clover_q_e(out, out->U, q_out ? &q_out[m] : nullptr, e_out ? &e_out[m] : nullptr));
+    }
+    return LT_OK;
+}
+
+int lt_stout(lt_lattice* in, lt_lattice* out, double rho, int n)
+{
+    LT_TRY(check_h(in, "lt_stout"));
+    LT_TRY(check_h(out, "lt_stout"));
+    if (n < 0) return lt::set_error(LT_ERR_ARG, "lt_stout: n < 0");
+    LT_TRY(lt_copy(out, in));
+    return stout_steps(out, rho, n);
+}
+
+// ---------------------------------------------------------------- HMC
+int lt_gauge_force(lt_lattice* h, double beta, double* force_out)
+{
+    LT_TRY(check_h(h, "lt_gauge_force"));
+    if (!force_out) return lt::set_error(LT_ERR_ARG, "lt_gauge_force: null pointer");
+    LT_TRY(ensure(h, &h->F, h->be->alg_bytes(h->g)));
+    LT_CK(cudaMemsetAsync(h->F, 0, h->be->alg_bytes(h->g), h->stream));
+    h->be->momenta(h->ctx(), h->U, h->F, nullptr, beta / 6.0, 1.0);
+    LT_TRY(ensure_aos(h));
+    h->be->alg_to_aos(h->ctx(), h->F, h->d_aos);
+    LT_TRY(launched("lt_gauge_force"));
+    LT_CK(cudaMemcpyAsync(force_out, h->d_aos, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyDeviceToHost,
+                          h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_set_momenta(lt_lattice* h, const double* p)
+{
+    LT_TRY(check_h(h, "lt_set_momenta"));
+    if (!p) return lt::set_error(LT_ERR_ARG, "lt_set_momenta: null pointer");
+    LT_TRY(ensure(h, &h->P, h->be->alg_bytes(h->g)));
+    LT_TRY(ensure_aos(h));
+    LT_CK(cudaMemcpyAsync(h->d_aos, p, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    h->be->alg_from_aos(h->ctx(), h->P, h->d_aos);
+    LT_TRY(launched("lt_set_momenta"));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_get_momenta(lt_lattice* h, double* p_out)
+{
+    LT_TRY(check_h(h, "lt_get_momenta"));
+    if (!p_out) return lt::set_error(LT_ERR_ARG, "lt_get_momenta: null pointer");
+    if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_get_momenta: no momenta set");
+    LT_TRY(ensure_aos(h));
+    h->be->alg_to_aos(h->ctx(), h->P, h->d_aos);
+    LT_TRY(launched("lt_get_momenta"));
+    LT_CK(cudaMemcpyAsync(p_out, h->d_aos, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyDeviceToHost,
+                          h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_random_momenta(lt_lattice* h, uint64_t seed, uint64_t counter)
+{
+    LT_TRY(check_h(h, "lt_random_momenta"));
+    LT_TRY(ensure(h, &h->P, h->be->alg_bytes(h->g)));
+    h->be->random_momenta(h->ctx(), h->P, counter, seed);
+    return launched("lt_random_momenta");
+}
+
+int lt_hamiltonian(lt_lattice* h, double beta, double* out)
+{
+    LT_TRY(check_h(h, "lt_hamiltonian"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_hamiltonian: null pointer");
+    if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_hamiltonian: no momenta set");
+    return hamiltonian(h, beta, out);
+}
+
+int lt_omf2(lt_lattice* h, double beta, double tau, int n_step, double* h_old, double* h_new)
+{
+    LT_TRY(check_h(h, "lt_omf2"));
+    if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_omf2: no momenta set");
+    if (h_old) LT_TRY(hamiltonian(h, beta, h_old));
+    LT_TRY(omf2(h, beta, tau, n_step, nullptr));
+    if (h_new) LT_TRY(hamiltonian(h, beta, h_new));
+    return LT_OK;
+}
+
+int lt_hmc_trajectory(lt_lattice* h, double beta, double tau, int n_step, uint64_t seed, uint64_t* counter,
+                      int metropolis, double* dH, int* accepted)
+{
+    LT_TRY(check_h(h, "lt_hmc_trajectory"));
+    if (!counter) return lt::set_error(LT_ERR_ARG, "lt_hmc_trajectory: null counter");
+    LT_TRY(ensure(h, &h->Ubak, h->be->gauge_bytes(h->g)));
+    LT_CK(cudaMemcpyAsync(h->Ubak, h->U, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
+    LT_TRY(lt_random_momenta(h, seed, *counter));
+    double ho, hn;
+    LT_TRY(hamiltonian(h, beta, &ho));
+    LT_TRY(omf2(h, beta, tau, n_step, nullptr));
+    LT_TRY(hamiltonian(h, beta, &hn));
+    const double d = hn - ho;
+    bool acc = true;
+    if (metropolis)
+    {
+        acc = accept_uniform(seed, *counter) <= std::exp(-d);
+        if (!acc) LT_CK(cudaMemcpyAsync(h->U, h->Ubak, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    ++*counter;
+    if (dH) *dH = d;
+    if (accepted) *accepted = acc ? 1 : 0;
+    if (!std::isfinite(d)) return lt::set_error(LT_ERR_NUMERIC, "lt_hmc_trajectory: non-finite dH");
+    return LT_OK;
+}
+
+// ---------------------------------------------------------------- metadynamics
+int lt_clover_derivative(lt_lattice* h, double* out)
+{
+    LT_TRY(check_h(h, "lt_clover_derivative"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_clover_derivative: null pointer");
+    LT_TRY(metad_backward(h, 0.0, 0, 1.0));
+    LT_TRY(ensure_aos(h));
+    h->be->alg_to_aos(h->ctx(), h->F, h->d_aos);
+    LT_TRY(launched("lt_clover_derivative"));
+    LT_CK(cudaMemcpyAsync(out, h->d_aos, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_metad_charge(lt_lattice* h, double rho, int n_stout, double* q_out)
+{
+    LT_TRY(check_h(h, "lt_metad_charge"));
+    if (!q_out || n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_metad_charge: bad arguments");
+    return metad_charge(h, rho, n_stout, q_out);
+}
+
+int lt_metad_force(lt_lattice* h, double rho, int n_stout, double dvdq, double* force_out, double* q_out)
+{
+    LT_TRY(check_h(h, "lt_metad_force"));
+    if (n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_metad_force: n_stout < 0");
+    LT_TRY(metad_forward(h, rho, n_stout));
+    if (q_out) LT_TRY(clover_q_e(h, level(h, n_stout), q_out, nullptr));
+    LT_TRY(metad_backward(h, rho, n_stout, dvdq));
+    if (force_out)
+    {
+        LT_TRY(ensure_aos(h));
+        h->be->alg_to_aos(h->ctx(), h->F, h->d_aos);
+        LT_TRY(launched("lt_metad_force"));
+        LT_CK(cudaMemcpyAsync(force_out, h->d_aos, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream));
+    }
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_metad_omf2(lt_lattice* h, lt_bias* bias, double beta, double tau, int n_step, double rho, int n_stout,
+                  double* h_old, double* h_new)
+{
+    LT_TRY(check_h(h, "lt_metad_omf2"));
+    if (!bias) return lt::set_error(LT_ERR_ARG, "lt_metad_omf2: null bias");
+    if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_metad_omf2: no momenta set");
+    auto* b = reinterpret_cast<lt::Bias*>(bias);
+    double q, hh;
+    if (h_old)
+    {
+        LT_TRY(metad_charge(h, rho, n_stout, &q));
+        LT_TRY(hamiltonian(h, beta, &hh));
+        *h_old = hh + b->potential(q);
+    }
+    MetaDParams md { b, rho, n_stout, nullptr };
+    LT_TRY(omf2(h, beta, tau, n_step, &md));
+    if (h_new)
+    {
+        LT_TRY(metad_charge(h, rho, n_stout, &q));
+        LT_TRY(hamiltonian(h, beta, &hh));
+        *h_new = hh + b->potential(q);
+    }
+    return LT_OK;
+}
+
+int lt_metad_hmc_trajectory(lt_lattice* h, lt_bias* bias, double beta, double tau, int n_step, double rho,
+                            int n_stout, uint64_t seed, uint64_t* counter, int metropolis, double* dH, int* accepted,
+                            double* cv_out)
+{
+    LT_TRY(check_h(h, "lt_metad_hmc_trajectory"));
+    if (!bias || !counter) return lt::set_error(LT_ERR_ARG, "lt_metad_hmc_trajectory: null argument");
+    auto* b = reinterpret_cast<lt::Bias*>(bias);
+    LT_TRY(ensure(h, &h->Ubak, h->be->gauge_bytes(h->g)));
+    LT_CK(cudaMemcpyAsync(h->Ubak, h->U, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
+    LT_TRY(lt_random_momenta(h, seed, *counter));
+    double cv_old, cv_new, hh;
+    LT_TRY(metad_charge(h, rho, n_stout, &cv_old));
+    LT_TRY(hamiltonian(h, beta, &hh));
+    const double e_old = hh + b->potential(cv_old);
+    std::vector<double> samples;
+    samples.reserve((size_t)n_step);
+    MetaDParams md { b, rho, n_stout, &samples };
+    LT_TRY(omf2(h, beta, tau, n_step, &md));
+    LT_TRY(metad_charge(h, rho, n_stout, &cv_new));
+    LT_TRY(hamiltonian(h, beta, &hh));
+    const double e_new = hh + b->potential(cv_new);
+    const double d = e_new - e_old;
+    bool acc = true;
+    if (metropolis)
+    {
+        acc = accept_uniform(seed, *counter) <= std::exp(-d);
+        if (acc)
+            b->cv_current = cv_new;
+        else
+        {
+            b->cv_current = cv_old;
+            for (double& s : samples) s = cv_old;
+            LT_CK(cudaMemcpyAsync(h->U, h->Ubak, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
+        }
+    }
+    else
+        b->cv_current = cv_new;
+    for (double s : samples)
+    {
+        b->update(s);
+        b->update(-s);
+    }
+    ++*counter;
+    LT_CK(cudaStreamSynchronize(h->stream));
+    if (dH) *dH = d;
+    if (accepted) *accepted = acc ? 1 : 0;
+    if (cv_out) *cv_out = b->cv_current;
+    if (!std::isfinite(d)) return lt::set_error(LT_ERR_NUMERIC, "lt_metad_hmc_trajectory: non-finite dH");
+    return LT_OK;
+}
+
+} // extern "C"

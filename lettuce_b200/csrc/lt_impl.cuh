@@ -1,0 +1,141 @@
+// Backend implementation for one storage format: launches the kernels of lt_kernels.cuh.
+#pragma once
+#include "lt_backend.h"
+#include "lt_kernels.cuh"
+
+namespace lt {
+
+inline int nblocks(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+template <typename T, int NR> class BackendImpl final : public Backend
+{
+    using G = Gauge<T, NR>;
+
+    static G gauge(const void* p, const Geom& g) { G u; u.p = (cx<T>*)p; u.vh = g.vh; return u; }
+    static Alg<T> alg(const void* p, const Geom& g) { Alg<T> a; a.p = (T*)p; a.vh = g.vh; return a; }
+    static Full<T> full(const void* p, const Geom& g) { Full<T> a; a.p = (cx<T>*)p; a.vh = g.vh; return a; }
+    static Clov<T> clov(const void* p, const Geom& g) { Clov<T> a; a.p = (T*)p; a.vh = g.vh; return a; }
+
+    static void finish(const Ctx& c, int slot, int nslot)
+    {
+        k_reduce_final<<<nslot, kRedThreads, 0, c.stream>>>(c.partials + (size_t)slot * kRedBlocks, kRedBlocks,
+                                                              c.results + slot);
+    }
+
+public:
+    int real_bytes() const override { return (int)sizeof(T); }
+    size_t gauge_bytes(const Geom& g) const override { return (size_t)4 * g.V * 3 * NR * sizeof(cx<T>); }
+    size_t alg_bytes(const Geom& g) const override { return (size_t)4 * g.V * 8 * sizeof(T); }
+    size_t full_bytes(const Geom& g) const override { return (size_t)4 * g.V * 9 * sizeof(cx<T>); }
+    size_t clov_bytes(const Geom& g) const override { return (size_t)6 * g.V * 9 * sizeof(T); }
+
+    void from_aos(const Ctx& c, void* U, const double* aos) const override
+    {
+        k_from_aos<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(gauge(U, c.g), c.g, aos);
+    }
+    void to_aos(const Ctx& c, const void* U, double* aos) const override
+    {
+        k_to_aos<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(gauge(U, c.g), c.g, aos);
+    }
+    void alg_from_aos(const Ctx& c, void* P, const double* aos) const override
+    {
+        k_alg_from_aos<T><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(alg(P, c.g), c.g, aos);
+    }
+    void alg_to_aos(const Ctx& c, const void* P, double* aos) const override
+    {
+        k_alg_to_aos<T><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(alg(P, c.g), c.g, aos);
+    }
+    void set_unit(const Ctx& c, void* U) const override
+    {
+        k_set_unit<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(gauge(U, c.g), 4 * c.g.V);
+    }
+    void link_io(const Ctx& c, void* U, int site, int mu, double* m, int write) const override
+    {
+        k_link_io<T, NR><<<1, 32, 0, c.stream>>>(gauge(U, c.g), c.g, site, mu, m, write);
+    }
+    void staples_aos(const Ctx& c, const void* U, double* aos) const override
+    {
+        k_staple_aos<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), c.g, aos);
+    }
+
+    void plaquette(const Ctx& c, const void* U, int slot) const override
+    {
+        k_plaquette<T, NR><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g,
+                                                                      c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 1);
+    }
+    void clover_obs(const Ctx& c, const void* U, int slot) const override
+    {
+        k_clover_obs<T, NR><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g,
+                                                                       c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 2);
+    }
+    void kinetic(const Ctx& c, const void* P, int slot) const override
+    {
+        k_kinetic<T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(alg(P, c.g), 4 * c.g.V,
+                                                                c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 1);
+    }
+
+    void overrelax(const Ctx& c, void* U, int mu, int par) const override
+    {
+        k_overrelax<T, NR><<<nblocks(c.g.vh, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), c.g, mu, par);
+    }
+    void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter, uint64_t seed,
+                  int max_iter) const override
+    {
+        k_heatbath<T, NR><<<nblocks(c.g.vh, kThreads), kThreads, 0, c.stream>>>(
+            gauge(U, c.g), c.g, mu, par, (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter);
+    }
+    void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new, double c_exp,
+                    int read_z, int write_z) const override
+    {
+        k_flow_stage<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+            gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z, write_z);
+    }
+    void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
+    {
+        k_stout<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(Uin, c.g), gauge(Uout, c.g),
+                                                                                  c.g, (T)rho);
+    }
+
+    void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const override
+    {
+        k_momenta<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+            gauge(U, c.g), alg(P, c.g), alg(F, c.g), c.g, (T)coef, (T)eps, F != nullptr);
+    }
+    void fields(const Ctx& c, void* U, const void* P, double eps) const override
+    {
+        k_fields<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), alg(P, c.g),
+                                                                                   4 * c.g.V, (T)eps);
+    }
+    void random_momenta(const Ctx& c, void* P, uint64_t counter, uint64_t seed) const override
+    {
+        k_random_momenta<T><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(alg(P, c.g), c.g, counter,
+                                                                               (uint32_t)seed, (uint32_t)(seed >> 32));
+    }
+
+    void clover_R(const Ctx& c, const void* U, void* R) const override
+    {
+        k_clover_R<T, NR><<<nblocks(6LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), clov(R, c.g), c.g);
+    }
+    void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const override
+    {
+        k_clover_deriv<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+            gauge(U, c.g), clov(R, c.g), alg(out, c.g), c.g, (T)scale);
+    }
+    void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam, void* Tloc,
+                      double rho) const override
+    {
+        k_stout_lambda<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+            gauge(U, c.g), gauge(Up, c.g), alg(Sigma, c.g), alg(Lam, c.g), full(Tloc, c.g), c.g, (T)rho);
+    }
+    void stout_recursion(const Ctx& c, const void* U, const void* Lam, const void* Tloc, void* Sigma,
+                         double rho) const override
+    {
+        k_stout_recursion<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+            gauge(U, c.g), alg(Lam, c.g), full(Tloc, c.g), alg(Sigma, c.g), c.g, (T)rho);
+    }
+};
+
+} // namespace lt

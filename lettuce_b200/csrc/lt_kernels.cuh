@@ -1,0 +1,817 @@
+// CUDA kernels of the pure-gauge SU(3) hot path (sm_100a, CUDA cores; 3x3 complex products
+// are too small for a dense tensor-core contraction).  One thread owns one link (or one
+// site for site-local observables); neighbour links are gathered from the even/odd SoA
+// planes described in lt_field.cuh.
+#pragma once
+#include "lt_field.cuh"
+
+namespace lt {
+
+constexpr int kThreads = 128;
+constexpr int kRedThreads = 256;
+constexpr double kPi = 3.14159265358979323846;
+
+// ---------------------------------------------------------------- reductions
+// Kahan-compensated FP64 accumulation per thread, then a warp/block tree into one partial
+// per block; k_reduce_final sums the partials of a slot in a fixed order.
+struct Kahan
+{
+    double s = 0.0, c = 0.0;
+    LT_D void add(double v)
+    {
+        double y = v - c;
+        double t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+LT_D double block_sum(double v, double* sh)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sh[w];
+    __syncthreads();
+    return r;
+}
+
+// out[j] = sum of partials[j * nblk .. + nblk) (Kahan, fixed order), one block per slot j
+template <int Unused = 0>
+__global__ void k_reduce_final(const double* __restrict__ partials, int nblk, double* __restrict__ out)
+{
+    __shared__ double sh[32];
+    const double* p = partials + (size_t)blockIdx.x * nblk;
+    Kahan k;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) k.add(p[b]);
+    double r = block_sum(k.s - k.c, sh);
+    if (threadIdx.x == 0) out[blockIdx.x] = r;
+}
+
+// ---------------------------------------------------------------- staple
+// Rectangular<1>::StaplePlaq (actions/gauge/rectangular_action.hpp:104-184):
+//   sum_{nu != mu} U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag + U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu)
+// summed in ascending nu, each direction as (up + down).
+template <typename T, int NR>
+LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const int c[4], int mu)
+{
+    const int op = par ^ 1;
+    const int dmu = step_up(g, mu, c[mu]);
+    const int imu = i + dmu;
+    M3<T> acc = zero3<T>();
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu)
+    {
+        if (nu == mu) continue;
+        const int inu = i + step_up(g, nu, c[nu]);
+        const int ind = i + step_dn(g, nu, c[nu]);
+        M3<T> up = mul_nd(mul(U.ld(nu, par, i >> 1), U.ld(mu, op, inu >> 1)), U.ld(nu, op, imu >> 1));
+        M3<T> dn = mul(mul_dn(U.ld(nu, op, ind >> 1), U.ld(mu, op, ind >> 1)), U.ld(nu, par, (ind + dmu) >> 1));
+        acc = acc + (up + dn);
+    }
+    return acc;
+}
+
+// ---------------------------------------------------------------- layout conversion
+template <typename T, int NR>
+__global__ void k_from_aos(Gauge<T, NR> U, Geom g, const double* __restrict__ aos)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;   // reference link index site*4+mu
+    if (l >= 4 * g.V) return;
+    int i = l >> 2, mu = l & 3;
+    int c[4];
+    int r = i;
+    c[3] = r % g.n[3]; r /= g.n[3];
+    c[2] = r % g.n[2]; r /= g.n[2];
+    c[1] = r % g.n[1]; c[0] = r / g.n[1];
+    int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    const double* a = aos + (size_t)18 * l;
+    M3<T> m;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m.e[k / 3][k % 3] = mkc<T>((T)a[2 * k], (T)a[2 * k + 1]);
+    U.st(mu, par, i >> 1, m);
+}
+
+template <typename T, int NR>
+__global__ void k_to_aos(Gauge<T, NR> U, Geom g, double* __restrict__ aos)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    int i = l >> 2, mu = l & 3;
+    int c[4];
+    int r = i;
+    c[3] = r % g.n[3]; r /= g.n[3];
+    c[2] = r % g.n[2]; r /= g.n[2];
+    c[1] = r % g.n[1]; c[0] = r / g.n[1];
+    int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    M3<T> m = U.ld(mu, par, i >> 1);
+    double* a = aos + (size_t)18 * l;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+    {
+        a[2 * k] = (double)m.e[k / 3][k % 3].r;
+        a[2 * k + 1] = (double)m.e[k / 3][k % 3].i;
+    }
+}
+
+// Algebra field <-> reference AoS (full 3x3 anti-Hermitian per link)
+template <typename T>
+__global__ void k_alg_from_aos(Alg<T> P, Geom g, const double* __restrict__ aos)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    int i = l >> 2, mu = l & 3;
+    int c[4];
+    int r = i;
+    c[3] = r % g.n[3]; r /= g.n[3];
+    c[2] = r % g.n[2]; r /= g.n[2];
+    c[1] = r % g.n[1]; c[0] = r / g.n[1];
+    int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    const double* a = aos + (size_t)18 * l;
+    M3<T> m;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m.e[k / 3][k % 3] = mkc<T>((T)a[2 * k], (T)a[2 * k + 1]);
+    P.st(mu, par, i >> 1, algebra8(m));
+}
+
+template <typename T>
+__global__ void k_alg_to_aos(Alg<T> P, Geom g, double* __restrict__ aos)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    int i = l >> 2, mu = l & 3;
+    int c[4];
+    int r = i;
+    c[3] = r % g.n[3]; r /= g.n[3];
+    c[2] = r % g.n[2]; r /= g.n[2];
+    c[1] = r % g.n[1]; c[0] = r / g.n[1];
+    int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    M3<T> m = unpack_ah(P.ld(mu, par, i >> 1));
+    double* a = aos + (size_t)18 * l;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+    {
+        a[2 * k] = (double)m.e[k / 3][k % 3].r;
+        a[2 * k + 1] = (double)m.e[k / 3][k % 3].i;
+    }
+}
+
+template <typename T, int NR>
+__global__ void k_set_unit(Gauge<T, NR> U, int nlink)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlink) return;
+    int vh = U.vh;
+    int plane = l / vh, s = l - plane * vh;
+    U.st(plane >> 1, plane & 1, s, unit3<T>());
+}
+
+// One link <-> 18 doubles (element access of GaugeField4D, lattice.hpp:113-136)
+template <typename T, int NR>
+__global__ void k_link_io(Gauge<T, NR> U, Geom g, int site, int mu, double* __restrict__ m, int write)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int c[4];
+    int r = site;
+    c[3] = r % g.n[3]; r /= g.n[3];
+    c[2] = r % g.n[2]; r /= g.n[2];
+    c[1] = r % g.n[1]; c[0] = r / g.n[1];
+    int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    if (write)
+    {
+        M3<T> a;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a.e[k / 3][k % 3] = mkc<T>((T)m[2 * k], (T)m[2 * k + 1]);
+        U.st(mu, par, site >> 1, a);
+    }
+    else
+    {
+        M3<T> a = U.ld(mu, par, site >> 1);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+        {
+            m[2 * k] = (double)a.e[k / 3][k % 3].r;
+            m[2 * k + 1] = (double)a.e[k / 3][k % 3].i;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- plaquette
+// PlaquetteSum (observables/plaquette.hpp:26-43): sum over sites and mu<nu of ReTr P_{mu nu}
+template <typename T, int NR>
+__global__ void __launch_bounds__(kRedThreads) k_plaquette(Gauge<T, NR> U, Geom g, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    Kahan k;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.V; x += gridDim.x * blockDim.x)
+    {
+        int par = x >= g.vh, s = x - par * g.vh;
+        int c[4];
+        int i = site_coords(g, par, s, c);
+        const int op = par ^ 1;
+        double acc = 0.0;
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+        {
+            const int imu = i + step_up(g, mu, c[mu]);
+            M3<T> umu = U.ld(mu, par, s);
+#pragma unroll
+            for (int nu = mu + 1; nu < 4; ++nu)
+            {
+                const int inu = i + step_up(g, nu, c[nu]);
+                // ReTr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag) = ReTr[(U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag]
+                M3<T> a = mul(umu, U.ld(nu, op, imu >> 1));
+                M3<T> b = mul(U.ld(nu, par, s), U.ld(mu, op, inu >> 1));
+                acc += (double)retr_nd(a, b);
+            }
+        }
+        k.add(acc);
+    }
+    double r = block_sum(k.s - k.c, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
+// ---------------------------------------------------------------- staple output (tests)
+template <typename T, int NR>
+__global__ void k_staple_aos(Gauge<T, NR> U, Geom g, double* __restrict__ aos)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int mu = t / g.V, x = t - mu * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> st = staple(U, g, par, i, c, mu);
+    double* a = aos + (size_t)18 * (4 * i + mu);
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+    {
+        a[2 * k] = (double)st.e[k / 3][k % 3].r;
+        a[2 * k + 1] = (double)st.e[k / 3][k % 3].i;
+    }
+}
+
+// ---------------------------------------------------------------- overrelaxation
+// OverrelaxationSubgroupKernel (updates/overrelaxation.hpp:68-117) on the links of one
+// (mu, parity) sub-sweep of Iterator::Checkerboard (iterators/iterators.hpp:65-87).
+template <typename T> LT_D S2<T> or_su2(const S2<T>& A)
+{
+    T an = rsqrt_t<T>(s2_det(A));
+    S2<T> V;
+    V.e11 = an * A.e11;
+    V.e12 = an * A.e12;
+    return s2_adj(s2_mul(V, V));
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.vh) return;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> st = staple(U, g, par, i, c, mu);
+    M3<T> u = U.ld(mu, par, s);
+    M3<T> w = mul_nd(u, st);   // U st^dag
+#pragma unroll
+    for (int sg = 0; sg < 3; ++sg)
+    {
+        S2<T> h = or_su2(extract(w, sg));
+        embed_lmul(h, sg, u);
+        if (sg < 2) embed_lmul(h, sg, w);
+    }
+    gram_schmidt(u);
+    U.st(mu, par, s, u);
+}
+
+// ---------------------------------------------------------------- heatbath
+// HeatbathKernel::HeatbathSU2 (updates/heatbath.hpp:47-104): Kennedy-Pendleton /
+// Fabricius-Haan sampling of x0 with lambda^2 = -(prefactor/4)/sqrt(det A) (ln r1 + cos^2(2 pi r2) ln r3),
+// accept while r0^2 + lambda^2 < 1, at most max_iter+1 proposals, else the unit matrix.
+// Random numbers: Philox4x32-10, counter {link, counter lo, counter hi, tag|subgroup|call}.
+template <typename T> struct HB;
+
+template <> struct HB<double>
+{
+    LT_D static S2<double> su2(const S2<double>& A, double prefactor, uint32_t link, uint64_t counter,
+                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter)
+    {
+        double an = 1.0 / sqrt(s2_det(A));
+        const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
+        const uint32_t tw = (TAG_HEATBATH << 24) | (sg << 16);
+        double lsq = 0.0;
+        for (int k = 0;; ++k)
+        {
+            U4 a = philox4x32(link, c1, c2, tw | (uint32_t)(2 * k), k0, k1);
+            U4 b = philox4x32(link, c1, c2, tw | (uint32_t)(2 * k + 1), k0, k1);
+            double r1 = 1.0 - u01_from(a.x, a.y), r2 = 1.0 - u01_from(a.z, a.w);
+            double r3 = 1.0 - u01_from(b.x, b.y), r0 = u01_from(b.z, b.w);
+            double x2 = cospi(2.0 * r2);
+            lsq = -0.25 * prefactor * an * (log(r1) + x2 * x2 * log(r3));
+            if (k > max_iter)
+            {
+                S2<double> one;
+                one.e11 = mkc(1.0, 0.0);
+                one.e12 = mkc(0.0, 0.0);
+                return one;
+            }
+            if (r0 * r0 + lsq < 1.0) break;
+        }
+        double x0 = 1.0 - 2.0 * lsq;
+        double ax = sqrt(1.0 - x0 * x0);
+        U4 d = philox4x32(link, c1, c2, tw | 0xFFFFu, k0, k1);
+        double phi = u01_from(d.x, d.y);
+        double ct = 1.0 - 2.0 * u01_from(d.z, d.w);
+        double vn = ax * sqrt(1.0 - ct * ct);
+        double sp, cp;
+        sincospi(2.0 * phi, &sp, &cp);
+        S2<double> x, V;
+        x.e11 = mkc(x0, vn * cp);
+        x.e12 = mkc(vn * sp, ax * ct);
+        V.e11 = an * A.e11;
+        V.e12 = an * A.e12;
+        return s2_mul(x, s2_adj(V));
+    }
+};
+
+template <> struct HB<float>
+{
+    LT_D static S2<float> su2(const S2<float>& A, float prefactor, uint32_t link, uint64_t counter,
+                               uint32_t sg, uint32_t k0, uint32_t k1, int max_iter)
+    {
+        float an = 1.0f / sqrtf(s2_det(A));
+        const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
+        const uint32_t tw = (TAG_HEATBATH << 24) | (sg << 16);
+        float lsq = 0.0f;
+        for (int k = 0;; ++k)
+        {
+            U4 a = philox4x32(link, c1, c2, tw | (uint32_t)k, k0, k1);
+            float r1 = 1.0f - f01_from(a.x), r2 = 1.0f - f01_from(a.y);
+            float r3 = 1.0f - f01_from(a.z), r0 = f01_from(a.w);
+            float x2 = cospif(2.0f * r2);
+            lsq = -0.25f * prefactor * an * (logf(r1) + x2 * x2 * logf(r3));
+            if (k > max_iter)
+            {
+                S2<float> one;
+                one.e11 = mkc(1.0f, 0.0f);
+                one.e12 = mkc(0.0f, 0.0f);
+                return one;
+            }
+            if (r0 * r0 + lsq < 1.0f) break;
+        }
+        float x0 = 1.0f - 2.0f * lsq;
+        float ax = sqrtf(fmaxf(1.0f - x0 * x0, 0.0f));
+        U4 d = philox4x32(link, c1, c2, tw | 0xFFFFu, k0, k1);
+        float phi = f01_from(d.x);
+        float ct = 1.0f - 2.0f * f01_from(d.y);
+        float vn = ax * sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
+        float sp, cp;
+        sincospif(2.0f * phi, &sp, &cp);
+        S2<float> x, V;
+        x.e11 = mkc(x0, vn * cp);
+        x.e12 = mkc(vn * sp, ax * ct);
+        V.e11 = an * A.e11;
+        V.e12 = an * A.e12;
+        return s2_mul(x, s2_adj(V));
+    }
+};
+
+// HeatbathKernel::operator() (updates/heatbath.hpp:110-129) for one (mu, parity) sub-sweep
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_heatbath(Gauge<T, NR> U, Geom g, int mu, int par, T prefactor,
+                                                       uint64_t counter, uint32_t k0, uint32_t k1, int max_iter)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.vh) return;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> st = staple(U, g, par, i, c, mu);
+    M3<T> u = U.ld(mu, par, s);
+    M3<T> w = mul_nd(u, st);
+    const uint32_t link = (uint32_t)(4 * i + mu);
+#pragma unroll 1
+    for (int sg = 0; sg < 3; ++sg)
+    {
+        S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter);
+        embed_lmul(h, sg, u);
+        embed_lmul(h, sg, w);
+    }
+    gram_schmidt(u);
+    U.st(mu, par, s, u);
+}
+
+// ---------------------------------------------------------------- gradient flow
+// One fused RK3 stage (smearing/gradient_flow.hpp:120-168, :265-332): for every link
+//   Z   <- c_old Z + c_new Algebra(st U^dag)   (CalculateZ / UpdateZ)
+//   U'  <- exp(c_exp Z) U, Gram-Schmidt          (UpdateFields)
+// reading U from Uin and writing Uout (ping-pong), so all staples see the pre-stage field
+// exactly as the reference's separate Z and field sweeps do.
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
+                                                         T c_old, T c_new, T c_exp, int read_z, int write_z)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int mu = t / g.V, x = t - mu * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> u = Uin.ld(mu, par, s);
+    M3<T> st = staple(Uin, g, par, i, c, mu);
+    A8<T> a = algebra8(mul_nd(st, u));
+    A8<T> z;
+    if (read_z)
+    {
+        A8<T> zo = Z.ld(mu, par, s);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z.a[k] = c_old * zo.a[k] + c_new * a.a[k];
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z.a[k] = c_new * a.a[k];
+    }
+    if (write_z) Z.st(mu, par, s, z);
+    M3<T> un = mul(exp_ah(unpack_ah(z), c_exp), u);
+    gram_schmidt(un);
+    Uout.st(mu, par, s, un);
+}
+
+// ---------------------------------------------------------------- stout smearing
+// StoutSmearing4D (smearing/stout_smearing.hpp:29-57): U' = exp(rho Algebra(st U^dag)) U, Gram-Schmidt
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int mu = t / g.V, x = t - mu * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> u = Uin.ld(mu, par, s);
+    M3<T> st = staple(Uin, g, par, i, c, mu);
+    M3<T> un = mul(exp_ah(unpack_ah(algebra8(mul_nd(st, u))), rho), u);
+    gram_schmidt(un);
+    Uout.st(mu, par, s, un);
+}
+
+// ---------------------------------------------------------------- clover observables
+// Four-leaf clover C_{mu nu}(x) (observables/clover.hpp:94-152, plaquette.hpp:82-114)
+template <typename T, int NR>
+LT_D M3<T> clover_leaves(const Gauge<T, NR>& U, const Geom& g, int par, int i, const int c[4], int mu, int nu)
+{
+    const int op = par ^ 1;
+    const int dmu_p = step_up(g, mu, c[mu]), dmu_m = step_dn(g, mu, c[mu]);
+    const int dnu_p = step_up(g, nu, c[nu]), dnu_m = step_dn(g, nu, c[nu]);
+    const int s = i >> 1;
+    const M3<T> umu = U.ld(mu, par, s), unu = U.ld(nu, par, s);
+    const int imd = i + dmu_m, ind = i + dnu_m;
+    // I:   U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
+    M3<T> leaf = mul_nd(mul(umu, U.ld(nu, op, (i + dmu_p) >> 1)), mul(unu, U.ld(mu, op, (i + dnu_p) >> 1)));
+    // II:  U_nu(x) U_mu(x-mu+nu)^dag U_nu(x-mu)^dag U_mu(x-mu)
+    M3<T> umu_md = U.ld(mu, op, imd >> 1);
+    acc(leaf, mul(mul_nd(unu, U.ld(mu, par, (imd + dnu_p) >> 1)), mul_dn(U.ld(nu, op, imd >> 1), umu_md)));
+    // III: U_mu(x-mu)^dag U_nu(x-mu-nu)^dag U_mu(x-mu-nu) U_nu(x-nu)
+    const int imdnd = imd + dnu_m;
+    acc(leaf, mul(mul_dd(umu_md, U.ld(nu, par, imdnd >> 1)), mul(U.ld(mu, par, imdnd >> 1), U.ld(nu, op, ind >> 1))));
+    // IV:  U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu) U_mu(x)^dag
+    acc(leaf, mul_nd(mul(mul_dn(U.ld(nu, op, ind >> 1), U.ld(mu, op, ind >> 1)), U.ld(nu, par, (ind + dmu_p) >> 1)), umu));
+    return leaf;
+}
+
+// Per-site clover charge density q(x) = ReTr(F01 F23 - F02 F13 + F03 F12), F = C - C^dag
+// (observables/topological_charge.hpp:97-200) and energy density
+// e(x) = sum_{mu<nu} ReTr(F~^2), F~ = Traceless(-i/8 (C - C^dag))
+// (observables/field_strength_tensor.hpp:28-66, :107-134, :154-175).
+template <typename T, int NR>
+__global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> U, Geom g, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    Kahan kq, ke;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.V; x += gridDim.x * blockDim.x)
+    {
+        int par = x >= g.vh, s = x - par * g.vh;
+        int c[4];
+        int i = site_coords(g, par, s, c);
+        double q = 0.0, e = 0.0;
+        const int pairs[3][4] = { { 0, 1, 2, 3 }, { 0, 2, 1, 3 }, { 0, 3, 1, 2 } };
+#pragma unroll 1
+        for (int p = 0; p < 3; ++p)
+        {
+            M3<T> ca = clover_leaves(U, g, par, i, c, pairs[p][0], pairs[p][1]);
+            M3<T> cb = clover_leaves(U, g, par, i, c, pairs[p][2], pairs[p][3]);
+            M3<T> fa = ca - adj(ca), fb = cb - adj(cb);
+            double t = (double)retr_mul(fa, fb);
+            q += p == 1 ? -t : t;
+            // energy: F~ = -i/8 F made traceless; ReTr(F~^2) = sum |F~_ij|^2 (Hermitian)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const M3<T>& f = h == 0 ? fa : fb;
+                double tr3 = ((double)f.e[0][0].i + (double)f.e[1][1].i + (double)f.e[2][2].i) / 3.0;
+                double acc2 = 0.0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                {
+                    double d = (double)f.e[a][a].i - tr3;
+                    acc2 += d * d;
+#pragma unroll
+                    for (int b = 0; b < 3; ++b)
+                        if (a != b) acc2 += (double)norm2(f.e[a][b]);
+                }
+                e += acc2 * (1.0 / 64.0);
+            }
+        }
+        kq.add(q);
+        ke.add(e);
+    }
+    double rq = block_sum(kq.s - kq.c, sh);
+    double re = block_sum(ke.s - ke.c, sh);
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = rq;
+        partials[gridDim.x + blockIdx.x] = re;
+    }
+}
+
+// ---------------------------------------------------------------- HMC
+// HMC momentum kick P += eps * (beta/6 Algebra(st U^dag) + F)  (updates/hmc_gauge.hpp:450-464,
+// updates/hmc_metadynamics.hpp:441-459).  With P = null the force itself is written to F_out.
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_momenta(Gauge<T, NR> U, Alg<T> P, Alg<T> F, Geom g, T coef, T eps, int use_f)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int mu = t / g.V, x = t - mu * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> st = staple(U, g, par, i, c, mu);
+    A8<T> a = algebra8(mul_nd(st, U.ld(mu, par, s)));
+    A8<T> p = P.ld(mu, par, s);
+    if (use_f)
+    {
+        A8<T> f = F.ld(mu, par, s);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) p.a[k] += eps * (coef * a.a[k] + f.a[k]);
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) p.a[k] += eps * coef * a.a[k];
+    }
+    P.st(mu, par, s, p);
+}
+
+// U <- exp(eps P) U, Gram-Schmidt (updates/hmc_gauge.hpp:505-523)
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_fields(Gauge<T, NR> U, Alg<T> P, int nlink, T eps)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nlink) return;
+    int vh = U.vh;
+    int plane = t / vh, s = t - plane * vh;
+    int mu = plane >> 1, par = plane & 1;
+    M3<T> un = mul(exp_ah(unpack_ah(P.ld(mu, par, s)), eps), U.ld(mu, par, s));
+    gram_schmidt(un);
+    U.st(mu, par, s, un);
+}
+
+// RandomMomentum (updates/hmc_gauge.hpp:400-428): P = 1/2 i phi_a lambda_a with eight
+// Box-Muller Gaussians from Philox calls j = 0..3 of tag TAG_MOMENTA.
+template <typename T>
+__global__ void k_random_momenta(Alg<T> P, Geom g, uint64_t counter, uint32_t k0, uint32_t k1)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int plane = t / g.vh, s = t - plane * g.vh;
+    int mu = plane >> 1, par = plane & 1;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    const uint32_t link = (uint32_t)(4 * i + mu);
+    double phi[8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        U4 w = philox4x32(link, (uint32_t)counter, (uint32_t)(counter >> 32), (TAG_MOMENTA << 24) | (uint32_t)j, k0, k1);
+        double u1 = u01_from(w.x, w.y), u2 = u01_from(w.z, w.w);
+        double r = sqrt(-2.0 * log(1.0 - u1));
+        double sp, cp;
+        sincospi(2.0 * u2, &sp, &cp);
+        phi[2 * j] = r * cp;
+        phi[2 * j + 1] = r * sp;
+    }
+    const double is3 = 0.57735026918962576451;
+    A8<T> a;
+    a.a[0] = (T)(0.5 * (phi[2] + phi[7] * is3));
+    a.a[1] = (T)(0.5 * (-phi[2] + phi[7] * is3));
+    a.a[2] = (T)(0.5 * phi[1]);
+    a.a[3] = (T)(0.5 * phi[0]);
+    a.a[4] = (T)(0.5 * phi[4]);
+    a.a[5] = (T)(0.5 * phi[3]);
+    a.a[6] = (T)(0.5 * phi[6]);
+    a.a[7] = (T)(0.5 * phi[5]);
+    P.st(mu, par, s, a);
+}
+
+// Kinetic energy -sum ReTr(P^2) (updates/hmc_gauge.hpp:525-541) = sum_ij |P_ij|^2
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_kinetic(Alg<T> P, int nlink, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    Kahan k;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nlink; t += gridDim.x * blockDim.x)
+    {
+        int vh = P.vh;
+        int plane = t / vh, s = t - plane * vh;
+        A8<T> a = P.ld(plane >> 1, plane & 1, s);
+        double a0 = a.a[0], a1 = a.a[1], a2 = a0 + a1;
+        double off = 0.0;
+#pragma unroll
+        for (int j = 2; j < 8; ++j) off += (double)a.a[j] * (double)a.a[j];
+        k.add(a0 * a0 + a1 * a1 + a2 * a2 + 2.0 * off);
+    }
+    double r = block_sum(k.s - k.c, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
+// ---------------------------------------------------------------- MetaD force chain
+// R_{mu nu}(x) = C_{mu nu}(x) - C_{mu nu}(x)^dag for the six planes (observables/clover.hpp:94-152,
+// :256-262)
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_clover_R(Gauge<T, NR> U, Clov<T> R, Geom g)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6 * g.V) return;
+    int pl = t / g.V, x = t - pl * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    const int pm[6] = { 0, 0, 0, 1, 1, 2 }, pn[6] = { 1, 2, 3, 2, 3, 3 };
+    M3<T> cl = clover_leaves(U, g, par, i, c, pm[pl], pn[pl]);
+    R.st(pl, par, s, cl - adj(cl));
+}
+
+// CloverDerivativeComponent (observables/clover.hpp:238-276)
+template <typename T, int NR>
+LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const Geom& g, int par, int i,
+                                  const int c[4], int mu, int nu, int rho, int sigma)
+{
+    const int op = par ^ 1;
+    const int dmu = step_up(g, mu, c[mu]);
+    const int imu = i + dmu, inu = i + step_up(g, nu, c[nu]), ind = i + step_dn(g, nu, c[nu]);
+    // x+mu+nu and x+mu-nu share the nu offsets of x (coordinate c[nu] unchanged by the mu step)
+    const int imunu = inu + dmu, imund = ind + dmu;
+    const M3<T> u_s_nu = U.ld(nu, par, i >> 1);
+    const M3<T> u_mup_nu = U.ld(nu, op, imu >> 1);
+    const M3<T> u_nup_mu = U.ld(mu, op, inu >> 1);
+    const M3<T> u_mupnud_nu = U.ld(nu, par, imund >> 1);
+    const M3<T> u_nud_mu = U.ld(mu, op, ind >> 1);
+    const M3<T> u_nud_nu = U.ld(nu, op, ind >> 1);
+    const M3<T> R_s = R.ld(rho, sigma, par, i >> 1);
+    const M3<T> R_mup = R.ld(rho, sigma, op, imu >> 1);
+    M3<T> tmp1 = mul_nd(u_mup_nu, u_nup_mu);          // U(x+mu,nu) U(x+nu,mu)^dag
+    M3<T> tmp2 = mul_dd(u_nup_mu, u_s_nu);            // U(x+nu,mu)^dag U(x,nu)^dag
+    M3<T> tmp3 = mul_dd(u_mupnud_nu, u_nud_mu);       // U(x+mu-nu,nu)^dag U(x-nu,mu)^dag
+    M3<T> tmp4 = mul_dn(u_nud_mu, u_nud_nu);          // U(x-nu,mu)^dag U(x-nu,nu)
+    M3<T> r = mul(tmp1, mul_dn(u_s_nu, R_s) + mul_nd(R.ld(rho, sigma, op, inu >> 1), u_s_nu));
+    acc(r, mul(mul(u_mup_nu, R.ld(rho, sigma, par, imunu >> 1)) + mul(R_mup, u_mup_nu), tmp2));
+    r = r - mul(tmp3, mul(u_nud_nu, R_s) + mul(R.ld(rho, sigma, op, ind >> 1), u_nud_nu));
+    r = r - mul(mul_dn(u_mupnud_nu, R.ld(rho, sigma, par, imund >> 1)) + mul_nd(R_mup, u_mupnud_nu), tmp4);
+    return r;
+}
+
+// CloverDerivative (observables/clover.hpp:279-321) times `scale` (dV/dQ):
+// Sigma_n = scale * (-2/(512 pi^2)) Algebra(U_mu(x) sum_eps-terms)
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_clover_deriv(Gauge<T, NR> U, Clov<T> R, Alg<T> out, Geom g, T scale)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int mu = t / g.V, x = t - mu * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    // the three epsilon-tensor terms (sign, nu, rho, sigma) of each direction
+    const int tab[4][3][4] = {
+        { { +1, 1, 2, 3 }, { -1, 2, 1, 3 }, { +1, 3, 1, 2 } },
+        { { -1, 0, 2, 3 }, { +1, 2, 0, 3 }, { -1, 3, 0, 2 } },
+        { { +1, 0, 1, 3 }, { -1, 1, 0, 3 }, { +1, 3, 0, 1 } },
+        { { -1, 0, 1, 2 }, { +1, 1, 0, 2 }, { -1, 2, 0, 1 } } };
+    M3<T> d = zero3<T>();
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k)
+    {
+        M3<T> comp = clover_deriv_component(U, R, g, par, i, c, mu, tab[mu][k][1], tab[mu][k][2], tab[mu][k][3]);
+        d = tab[mu][k][0] > 0 ? d + comp : d - comp;
+    }
+    d = mul(U.ld(mu, par, s), d);
+    A8<T> a = algebra8(d);
+    const T pref = (T)(-2.0 / (512.0 * kPi * kPi)) * scale;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a.a[k] *= pref;
+    out.st(mu, par, s, a);
+}
+
+// First half of StoutForceRecursion (smearing/stout_smearing.hpp:152-175) with CalculateLambda
+// (:122-150): for level k-1 field U and level k field Up, Sigma' = Up^dag Sigma,
+// Lambda = TracelessHermitian(tr(B1 U Sigma') Q + tr(B2 U Sigma') Q^2 + f1 U Sigma' + f2 (Q U Sigma' + U Sigma' Q)),
+// with Q = -i rho Algebra(st U^dag); the exponential constants are recomputed from U here
+// rather than stored during the forward smearing.  Also writes the link-local part of the
+// recursion, Tloc = Sigma' exp(iQ) + i rho st^dag Lambda.
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_stout_lambda(Gauge<T, NR> U, Gauge<T, NR> Up, Alg<T> Sigma, Alg<T> Lam,
+                                                           Full<T> Tloc, Geom g, T rho)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int mu = t / g.V, x = t - mu * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> u = U.ld(mu, par, s);
+    M3<T> sp = mul_dn(Up.ld(mu, par, s), unpack_ah(Sigma.ld(mu, par, s)));
+    M3<T> st = staple(U, g, par, i, c, mu);
+    M3<T> C = unpack_ah(algebra8(mul_nd(st, u)));
+    M3<T> Q;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) Q.e[a][b] = mkc<T>(rho * C.e[a][b].i, -rho * C.e[a][b].r);
+    M3<T> Q2 = mul(Q, Q);
+    ExpScalars e = exp_scalars(Q, Q2);
+    ExpDerivScalars d = exp_deriv_scalars(e);
+    M3<T> tmp = mul(u, sp);
+    M3<T> Qt = mul(Q, tmp), tQ = mul(tmp, Q);
+    // tr(B_j tmp) = b_j0 tr(tmp) + b_j1 tr(Q tmp) + b_j2 tr(Q^2 tmp)
+    cx<double> tr0 = cvt<double>(trace(tmp)), tr1 = cvt<double>(trace(Qt)), tr2 = cvt<double>(tr_mul(Q2, tmp));
+    cx<T> t1 = cvt<T>(d.b10 * tr0 + d.b11 * tr1 + d.b12 * tr2);
+    cx<T> t2 = cvt<T>(d.b20 * tr0 + d.b21 * tr1 + d.b22 * tr2);
+    cx<T> f1 = cvt<T>(d.f1), f2 = cvt<T>(d.f2);
+    M3<T> lam;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            lam.e[a][b] = t1 * Q.e[a][b] + t2 * Q2.e[a][b] + f1 * tmp.e[a][b] + f2 * (Qt.e[a][b] + tQ.e[a][b]);
+    A8<T> l8 = traceless_herm8(lam);
+    Lam.st(mu, par, s, l8);
+    M3<T> ex = exp_from(e, Q, Q2);
+    M3<T> loc = mul(sp, ex);
+    M3<T> sl = mul_dn(st, unpack_h(l8));   // st^dag Lambda
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) loc.e[a][b] = loc.e[a][b] + rho * timesi(sl.e[a][b]);
+    Tloc.st(mu, par, s, loc);
+}
+
+// Second half of StoutForceRecursion (smearing/stout_smearing.hpp:177-230):
+// Sigma_{k-1} = Algebra(U (Tloc - i rho sum_{nu != mu} [six-term neighbour sum of U and Lambda]))
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Alg<T> Lam, Full<T> Tloc, Alg<T> Sigma,
+                                                              Geom g, T rho)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * g.V) return;
+    int mu = t / g.V, x = t - mu * g.V;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    const int op = par ^ 1;
+    const int dmu = step_up(g, mu, c[mu]);
+    const int imu = i + dmu;
+    M3<T> fs = zero3<T>();
+#pragma unroll 1
+    for (int nu = 0; nu < 4; ++nu)
+    {
+        if (nu == mu) continue;
+        const int inu = i + step_up(g, nu, c[nu]), ind = i + step_dn(g, nu, c[nu]);
+        const int imund = ind + dmu;
+        const M3<T> u_s_nu = U.ld(nu, par, i >> 1);
+        const M3<T> u_nud_mu = U.ld(mu, op, ind >> 1);
+        const M3<T> u_mupnud_nu = U.ld(nu, par, imund >> 1);
+        M3<T> tmp1 = mul_nd(U.ld(nu, op, imu >> 1), U.ld(mu, op, inu >> 1));
+        M3<T> tmp2 = mul_dn(u_nud_mu, unpack_h(Lam.ld(mu, op, ind >> 1)) - unpack_h(Lam.ld(nu, op, ind >> 1)));
+        // rows 1 and 6 of eq. C6 in arXiv:2307.04742
+        acc(fs, mul(tmp1, mul_dn(u_s_nu, unpack_h(Lam.ld(nu, par, i >> 1)))
+                          + mul_nd(unpack_h(Lam.ld(mu, op, inu >> 1)), u_s_nu)));
+        // rows 2, 3 and 4
+        acc(fs, mul(mul_dn(u_mupnud_nu, tmp2 + mul_nd(unpack_h(Lam.ld(nu, par, imund >> 1)), u_nud_mu)),
+                    U.ld(nu, op, ind >> 1)));
+        // row 5
+        fs = fs - mul_nd(mul(unpack_h(Lam.ld(nu, op, imu >> 1)), tmp1), u_s_nu);
+    }
+    M3<T> loc = Tloc.ld(mu, par, s);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) loc.e[a][b] = loc.e[a][b] - rho * timesi(fs.e[a][b]);
+    Sigma.st(mu, par, s, algebra8(mul(U.ld(mu, par, s), loc)));
+}
+
+} // namespace lt

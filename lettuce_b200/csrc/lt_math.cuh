@@ -1,0 +1,587 @@
+// SU(3)/SU(2) arithmetic for the B200 kernels: 3x3 complex matrices in registers,
+// Cabibbo-Marinari SU(2) subgroups, Gram-Schmidt reunitarisation, the Cayley-Hamilton
+// exponential and its Morningstar-Peardon derivative coefficients, and the Philox4x32-10
+// counter-based generator.  Everything is templated on the link arithmetic type T (float or
+// double); the scalar coefficient chain of the exponential always runs in double.
+//
+// Reference semantics (timo-eichhorn/Lettuce, LettuceGauge/...):
+//   Algebra / TracelessHermitian      math/su3.hpp:423-448
+//   GramSchmidt / RestoreLastRow      math/su3.hpp:362-394
+//   Extract0x / Embed0x / SU2_comp    math/su2.hpp:21-174
+//   ExpConstants / SU3::exp           math/su3_exp.hpp:204-283, :419-432
+//   ExpDerivativeConstants (r, b, B)  math/su3_exp.hpp:121-201, :389-415
+#pragma once
+#include <cstdint>
+#include <cfloat>
+#include <cuda_runtime.h>
+
+#define LT_HD __host__ __device__ __forceinline__
+#define LT_D __device__ __forceinline__
+
+namespace lt {
+
+template <typename T> struct __align__(2 * sizeof(T)) cx { T r, i; };
+
+template <typename T> LT_HD cx<T> mkc(T r, T i) { cx<T> c; c.r = r; c.i = i; return c; }
+template <typename T> LT_HD cx<T> operator+(cx<T> a, cx<T> b) { return mkc<T>(a.r + b.r, a.i + b.i); }
+template <typename T> LT_HD cx<T> operator-(cx<T> a, cx<T> b) { return mkc<T>(a.r - b.r, a.i - b.i); }
+template <typename T> LT_HD cx<T> operator-(cx<T> a) { return mkc<T>(-a.r, -a.i); }
+template <typename T> LT_HD cx<T> operator*(cx<T> a, cx<T> b) { return mkc<T>(a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r); }
+template <typename T> LT_HD cx<T> operator*(T s, cx<T> a) { return mkc<T>(s * a.r, s * a.i); }
+template <typename T> LT_HD cx<T> conj(cx<T> a) { return mkc<T>(a.r, -a.i); }
+// a * conj(b)
+template <typename T> LT_HD cx<T> mulc(cx<T> a, cx<T> b) { return mkc<T>(a.r * b.r + a.i * b.i, a.i * b.r - a.r * b.i); }
+// i * a
+template <typename T> LT_HD cx<T> timesi(cx<T> a) { return mkc<T>(-a.i, a.r); }
+template <typename T> LT_HD T norm2(cx<T> a) { return a.r * a.r + a.i * a.i; }
+template <typename To, typename From> LT_HD cx<To> cvt(cx<From> a) { return mkc<To>((To)a.r, (To)a.i); }
+
+template <typename T> struct M3 { cx<T> e[3][3]; };
+
+template <typename T> LT_HD M3<T> zero3()
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.e[i][j] = mkc<T>(0, 0);
+    return r;
+}
+
+template <typename T> LT_HD M3<T> unit3()
+{
+    M3<T> r = zero3<T>();
+    r.e[0][0].r = r.e[1][1].r = r.e[2][2].r = 1;
+    return r;
+}
+
+// A * B
+template <typename T> LT_HD M3<T> mul(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            T re = a.e[i][0].r * b.e[0][j].r - a.e[i][0].i * b.e[0][j].i;
+            T im = a.e[i][0].r * b.e[0][j].i + a.e[i][0].i * b.e[0][j].r;
+#pragma unroll
+            for (int k = 1; k < 3; ++k)
+            {
+                re += a.e[i][k].r * b.e[k][j].r - a.e[i][k].i * b.e[k][j].i;
+                im += a.e[i][k].r * b.e[k][j].i + a.e[i][k].i * b.e[k][j].r;
+            }
+            r.e[i][j] = mkc<T>(re, im);
+        }
+    return r;
+}
+
+// A * B^dagger
+template <typename T> LT_HD M3<T> mul_nd(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            T re = a.e[i][0].r * b.e[j][0].r + a.e[i][0].i * b.e[j][0].i;
+            T im = a.e[i][0].i * b.e[j][0].r - a.e[i][0].r * b.e[j][0].i;
+#pragma unroll
+            for (int k = 1; k < 3; ++k)
+            {
+                re += a.e[i][k].r * b.e[j][k].r + a.e[i][k].i * b.e[j][k].i;
+                im += a.e[i][k].i * b.e[j][k].r - a.e[i][k].r * b.e[j][k].i;
+            }
+            r.e[i][j] = mkc<T>(re, im);
+        }
+    return r;
+}
+
+// A^dagger * B
+template <typename T> LT_HD M3<T> mul_dn(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            T re = a.e[0][i].r * b.e[0][j].r + a.e[0][i].i * b.e[0][j].i;
+            T im = a.e[0][i].r * b.e[0][j].i - a.e[0][i].i * b.e[0][j].r;
+#pragma unroll
+            for (int k = 1; k < 3; ++k)
+            {
+                re += a.e[k][i].r * b.e[k][j].r + a.e[k][i].i * b.e[k][j].i;
+                im += a.e[k][i].r * b.e[k][j].i - a.e[k][i].i * b.e[k][j].r;
+            }
+            r.e[i][j] = mkc<T>(re, im);
+        }
+    return r;
+}
+
+// A^dagger * B^dagger = (B A)^dagger
+template <typename T> LT_HD M3<T> mul_dd(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            cx<T> acc = conj(a.e[0][i]) * conj(b.e[j][0]);
+#pragma unroll
+            for (int k = 1; k < 3; ++k) acc = acc + conj(a.e[k][i]) * conj(b.e[j][k]);
+            r.e[i][j] = acc;
+        }
+    return r;
+}
+
+template <typename T> LT_HD M3<T> adj(const M3<T>& a)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.e[i][j] = conj(a.e[j][i]);
+    return r;
+}
+
+template <typename T> LT_HD void acc(M3<T>& a, const M3<T>& b)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.e[i][j] = a.e[i][j] + b.e[i][j];
+}
+
+template <typename T> LT_HD M3<T> operator+(M3<T> a, const M3<T>& b) { acc(a, b); return a; }
+template <typename T> LT_HD M3<T> operator-(M3<T> a, const M3<T>& b)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.e[i][j] = a.e[i][j] - b.e[i][j];
+    return a;
+}
+template <typename T> LT_HD M3<T> operator*(T s, M3<T> a)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.e[i][j] = s * a.e[i][j];
+    return a;
+}
+template <typename T> LT_HD M3<T> operator*(cx<T> s, M3<T> a)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.e[i][j] = s * a.e[i][j];
+    return a;
+}
+
+template <typename T> LT_HD cx<T> trace(const M3<T>& a) { return a.e[0][0] + a.e[1][1] + a.e[2][2]; }
+
+// Re tr(A B) without forming the product
+template <typename T> LT_HD T retr_mul(const M3<T>& a, const M3<T>& b)
+{
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s += a.e[i][k].r * b.e[k][i].r - a.e[i][k].i * b.e[k][i].i;
+    return s;
+}
+
+// Re tr(A B^dag) = sum_ij Re(A_ij conj(B_ij))
+template <typename T> LT_HD T retr_nd(const M3<T>& a, const M3<T>& b)
+{
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) s += a.e[i][j].r * b.e[i][j].r + a.e[i][j].i * b.e[i][j].i;
+    return s;
+}
+
+// tr(A B) without forming the product
+template <typename T> LT_HD cx<T> tr_mul(const M3<T>& a, const M3<T>& b)
+{
+    cx<T> s = mkc<T>(0, 0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s = s + a.e[i][k] * b.e[k][i];
+    return s;
+}
+
+template <typename To, typename From> LT_HD M3<To> cvt(const M3<From>& a)
+{
+    M3<To> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.e[i][j] = cvt<To>(a.e[i][j]);
+    return r;
+}
+
+// ---------------------------------------------------------------- algebra fields
+// A traceless anti-Hermitian matrix X kept as 8 reals:
+//   X00 = i a0, X11 = i a1, X22 = -i (a0 + a1), X01 = a2 + i a3, X02 = a4 + i a5, X12 = a6 + i a7.
+template <typename T> struct A8 { T a[8]; };
+
+// Algebra(M) = (M - M^dag)/2 - tr(M - M^dag)/6 (math/su3.hpp:423-426), packed
+template <typename T> LT_HD A8<T> algebra8(const M3<T>& m)
+{
+    A8<T> x;
+    T d0 = m.e[0][0].i, d1 = m.e[1][1].i, d2 = m.e[2][2].i;
+    T t = (d0 + d1 + d2) * (T)(1.0 / 3.0);
+    x.a[0] = d0 - t;
+    x.a[1] = d1 - t;
+    x.a[2] = (T)0.5 * (m.e[0][1].r - m.e[1][0].r);
+    x.a[3] = (T)0.5 * (m.e[0][1].i + m.e[1][0].i);
+    x.a[4] = (T)0.5 * (m.e[0][2].r - m.e[2][0].r);
+    x.a[5] = (T)0.5 * (m.e[0][2].i + m.e[2][0].i);
+    x.a[6] = (T)0.5 * (m.e[1][2].r - m.e[2][1].r);
+    x.a[7] = (T)0.5 * (m.e[1][2].i + m.e[2][1].i);
+    return x;
+}
+
+template <typename T> LT_HD M3<T> unpack_ah(const A8<T>& x)
+{
+    M3<T> m;
+    m.e[0][0] = mkc<T>(0, x.a[0]);
+    m.e[1][1] = mkc<T>(0, x.a[1]);
+    m.e[2][2] = mkc<T>(0, -(x.a[0] + x.a[1]));
+    m.e[0][1] = mkc<T>(x.a[2], x.a[3]);
+    m.e[0][2] = mkc<T>(x.a[4], x.a[5]);
+    m.e[1][2] = mkc<T>(x.a[6], x.a[7]);
+    m.e[1][0] = mkc<T>(-x.a[2], x.a[3]);
+    m.e[2][0] = mkc<T>(-x.a[4], x.a[5]);
+    m.e[2][1] = mkc<T>(-x.a[6], x.a[7]);
+    return m;
+}
+
+// Hermitian traceless H kept as 8 reals: H00 = h0, H11 = h1, H22 = -(h0+h1), H01 = h2 + i h3, ...
+// TracelessHermitian(M) = (M + M^dag)/2 - tr(M + M^dag)/6 (math/su3.hpp:445-448), packed
+template <typename T> LT_HD A8<T> traceless_herm8(const M3<T>& m)
+{
+    A8<T> x;
+    T d0 = m.e[0][0].r, d1 = m.e[1][1].r, d2 = m.e[2][2].r;
+    T t = (d0 + d1 + d2) * (T)(1.0 / 3.0);
+    x.a[0] = d0 - t;
+    x.a[1] = d1 - t;
+    x.a[2] = (T)0.5 * (m.e[0][1].r + m.e[1][0].r);
+    x.a[3] = (T)0.5 * (m.e[0][1].i - m.e[1][0].i);
+    x.a[4] = (T)0.5 * (m.e[0][2].r + m.e[2][0].r);
+    x.a[5] = (T)0.5 * (m.e[0][2].i - m.e[2][0].i);
+    x.a[6] = (T)0.5 * (m.e[1][2].r + m.e[2][1].r);
+    x.a[7] = (T)0.5 * (m.e[1][2].i - m.e[2][1].i);
+    return x;
+}
+
+template <typename T> LT_HD M3<T> unpack_h(const A8<T>& x)
+{
+    M3<T> m;
+    m.e[0][0] = mkc<T>(x.a[0], 0);
+    m.e[1][1] = mkc<T>(x.a[1], 0);
+    m.e[2][2] = mkc<T>(-(x.a[0] + x.a[1]), 0);
+    m.e[0][1] = mkc<T>(x.a[2], x.a[3]);
+    m.e[0][2] = mkc<T>(x.a[4], x.a[5]);
+    m.e[1][2] = mkc<T>(x.a[6], x.a[7]);
+    m.e[1][0] = mkc<T>(x.a[2], -x.a[3]);
+    m.e[2][0] = mkc<T>(x.a[4], -x.a[5]);
+    m.e[2][1] = mkc<T>(x.a[6], -x.a[7]);
+    return m;
+}
+
+// ---------------------------------------------------------------- reunitarisation
+// RestoreLastRow (math/su3.hpp:362-367): row 2 = conj(row 0 x row 1)
+template <typename T> LT_HD void restore_last_row(M3<T>& a)
+{
+    a.e[2][0] = conj(a.e[0][1] * a.e[1][2] - a.e[0][2] * a.e[1][1]);
+    a.e[2][1] = conj(a.e[0][2] * a.e[1][0] - a.e[0][0] * a.e[1][2]);
+    a.e[2][2] = conj(a.e[0][0] * a.e[1][1] - a.e[0][1] * a.e[1][0]);
+}
+
+template <typename T> LT_D T rsqrt_t(T x);
+template <> LT_D double rsqrt_t<double>(double x) { return 1.0 / sqrt(x); }
+template <> LT_D float rsqrt_t<float>(float x) { return 1.0f / sqrtf(x); }
+
+// GramSchmidt (math/su3.hpp:370-394)
+template <typename T> LT_D void gram_schmidt(M3<T>& a)
+{
+    T n0 = rsqrt_t<T>(norm2(a.e[0][0]) + norm2(a.e[0][1]) + norm2(a.e[0][2]));
+#pragma unroll
+    for (int n = 0; n < 3; ++n) a.e[0][n] = n0 * a.e[0][n];
+    cx<T> psi = mulc(a.e[1][0], a.e[0][0]) + mulc(a.e[1][1], a.e[0][1]) + mulc(a.e[1][2], a.e[0][2]);
+#pragma unroll
+    for (int n = 0; n < 3; ++n) a.e[1][n] = a.e[1][n] - psi * a.e[0][n];
+    T n1 = rsqrt_t<T>(norm2(a.e[1][0]) + norm2(a.e[1][1]) + norm2(a.e[1][2]));
+#pragma unroll
+    for (int n = 0; n < 3; ++n) a.e[1][n] = n1 * a.e[1][n];
+    restore_last_row(a);
+}
+
+// ---------------------------------------------------------------- SU(2) subgroups
+template <typename T> struct S2 { cx<T> e11, e12; };
+
+template <typename T> LT_HD S2<T> s2_mul(const S2<T>& a, const S2<T>& b)
+{
+    S2<T> r;
+    r.e11 = a.e11 * b.e11 - mulc(a.e12, b.e12);
+    r.e12 = a.e11 * b.e12 + mulc(a.e12, b.e11);
+    return r;
+}
+template <typename T> LT_HD S2<T> s2_adj(const S2<T>& a) { S2<T> r; r.e11 = conj(a.e11); r.e12 = -a.e12; return r; }
+template <typename T> LT_HD T s2_det(const S2<T>& a) { return norm2(a.e11) + norm2(a.e12); }
+
+// Subgroup g in {0: (0,1), 1: (0,2), 2: (1,2)} as (row a, row b)
+LT_HD int sg_a(int g) { return g == 2 ? 1 : 0; }
+LT_HD int sg_b(int g) { return g == 0 ? 1 : 2; }
+
+// Extract0x (math/su2.hpp:151-174)
+template <typename T> LT_HD S2<T> extract(const M3<T>& w, int g)
+{
+    const int a = sg_a(g), b = sg_b(g);
+    S2<T> r;
+    r.e11 = (T)0.5 * (w.e[a][a] + conj(w.e[b][b]));
+    r.e12 = (T)0.5 * (w.e[a][b] - conj(w.e[b][a]));
+    return r;
+}
+
+// Embed0x(m) * X (math/su2.hpp:118-146): mixes rows a and b of X
+template <typename T> LT_HD void embed_lmul(const S2<T>& m, int g, M3<T>& x)
+{
+    const int a = sg_a(g), b = sg_b(g);
+#pragma unroll
+    for (int n = 0; n < 3; ++n)
+    {
+        cx<T> xa = x.e[a][n], xb = x.e[b][n];
+        x.e[a][n] = m.e11 * xa + m.e12 * xb;
+        x.e[b][n] = conj(m.e11) * xb - conj(m.e12) * xa;
+    }
+}
+
+// ---------------------------------------------------------------- Cayley-Hamilton exp
+// xi_0(w) = sin(w)/w and xi_1(w) = cos(w)/w^2 - sin(w)/w^3 with the double-precision Taylor
+// switches of ExpTaylorBounds<double> (math/su3_exp.hpp:38-82)
+LT_D double xi0(double w)
+{
+    if (fabs(w) <= 0.05)
+    {
+        double w2 = w * w;
+        return 1.0 - 1.0 / 6.0 * w2 * (1.0 - 1.0 / 20.0 * w2 * (1.0 - 1.0 / 42.0 * w2));
+    }
+    return sin(w) / w;
+}
+
+LT_D double xi1(double w)
+{
+    if (fabs(w) <= 0.115)
+    {
+        double w2 = w * w;
+        return -1.0 / 3.0 + 1.0 / 30.0 * w2 * (1.0 - 1.0 / 28.0 * w2 * (1.0 - 1.0 / 54.0 * w2));
+    }
+    double s, c;
+    sincos(w, &s, &c);
+    return c / (w * w) - s / (w * w * w);
+}
+
+// Scalar part of ExpConstants (math/su3_exp.hpp:204-283) for a traceless Hermitian Q.
+struct ExpScalars
+{
+    double u, w, u2, w2, c0max, denom;
+    int signflip;
+    cx<double> emiu, e2iu, cosw, ixi0, h0, h1, h2;
+};
+
+template <typename T> LT_D ExpScalars exp_scalars(const M3<T>& Q, const M3<T>& Q2)
+{
+    ExpScalars e;
+    // c0 = det Q = tr(Q^3)/3 and c1 = tr(Q^2)/2, accumulated in double
+    double c0s = 0.0, c1 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            c0s += (double)Q.e[i][k].r * (double)Q2.e[k][i].r - (double)Q.e[i][k].i * (double)Q2.e[k][i].i;
+        }
+    c0s *= 1.0 / 3.0;
+    c1 = 0.5 * ((double)Q2.e[0][0].r + (double)Q2.e[1][1].r + (double)Q2.e[2][2].r);
+    double c0 = fabs(c0s);
+    double c13 = c1 / 3.0;
+    e.c0max = 2.0 * c13 * sqrt(c13);
+    e.signflip = c0s < 0.0;
+    double theta = acos(fmin(c0 / e.c0max, 1.0));
+    double st3, ct3;
+    sincos(theta / 3.0, &st3, &ct3);
+    e.u = sqrt(c13) * ct3;
+    e.w = sqrt(c1) * st3;
+    e.u2 = e.u * e.u;
+    e.w2 = e.w * e.w;
+    double su, cu;
+    sincos(e.u, &su, &cu);
+    e.emiu = mkc<double>(cu, -su);
+    // exp(2iu) = conj(exp(-iu)^2)
+    e.e2iu = conj(e.emiu * e.emiu);
+    e.cosw = mkc<double>(cos(e.w), 0.0);
+    e.ixi0 = mkc<double>(0.0, xi0(e.w));
+    if (e.c0max < DBL_MIN)
+    {
+        e.denom = 1.0;
+        e.h0 = mkc<double>(1.0, 0.0);
+        e.h1 = mkc<double>(0.0, 0.0);
+        e.h2 = mkc<double>(0.0, 0.0);
+        return e;
+    }
+    const double u = e.u, u2 = e.u2, w2 = e.w2;
+    e.denom = 1.0 / (9.0 * u2 - w2);
+    cx<double> h0 = (u2 - w2) * e.e2iu + e.emiu * ((8.0 * u2) * e.cosw + (2.0 * u * (3.0 * u2 + w2)) * e.ixi0);
+    cx<double> h1 = (2.0 * u) * e.e2iu - e.emiu * ((2.0 * u) * e.cosw - (3.0 * u2 - w2) * e.ixi0);
+    cx<double> h2 = e.e2iu - e.emiu * (e.cosw + (3.0 * u) * e.ixi0);
+    if (e.signflip)
+    {
+        h0 = conj(h0);
+        h1 = -conj(h1);
+        h2 = conj(h2);
+    }
+    e.h0 = h0;
+    e.h1 = h1;
+    e.h2 = h2;
+    return e;
+}
+
+// exp(iQ) = denom (h0 + h1 Q + h2 Q^2) (math/su3_exp.hpp:419-432)
+template <typename T> LT_D M3<T> exp_from(const ExpScalars& e, const M3<T>& Q, const M3<T>& Q2)
+{
+    cx<T> f0 = cvt<T>(e.denom * e.h0), f1 = cvt<T>(e.denom * e.h1), f2 = cvt<T>(e.denom * e.h2);
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.e[i][j] = f1 * Q.e[i][j] + f2 * Q2.e[i][j];
+    r.e[0][0] = r.e[0][0] + f0;
+    r.e[1][1] = r.e[1][1] + f0;
+    r.e[2][2] = r.e[2][2] + f0;
+    return r;
+}
+
+// exp(c X) for X traceless anti-Hermitian: SU3::exp(-i c X) (gradient_flow.hpp:276,
+// hmc_gauge.hpp:516, stout_smearing.hpp:52)
+template <typename T> LT_D M3<T> exp_ah(const M3<T>& X, T c)
+{
+    // Q = -i c X is Hermitian traceless
+    M3<T> Q;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Q.e[i][j] = mkc<T>(c * X.e[i][j].i, -c * X.e[i][j].r);
+    M3<T> Q2 = mul(Q, Q);
+    ExpScalars e = exp_scalars(Q, Q2);
+    return exp_from(e, Q, Q2);
+}
+
+// f1, f2 and B_1, B_2 of ExpDerivativeConstants (math/su3_exp.hpp:121-201, :389-415)
+struct ExpDerivScalars
+{
+    cx<double> f1, f2, b10, b11, b12, b20, b21, b22;
+};
+
+LT_D ExpDerivScalars exp_deriv_scalars(const ExpScalars& e)
+{
+    ExpDerivScalars d;
+    const double u = e.u, u2 = e.u2, w2 = e.w2;
+    const cx<double> x0 = mkc<double>(xi0(e.w), 0.0), x1 = mkc<double>(xi1(e.w), 0.0);
+    const cx<double> I1 = mkc<double>(0.0, 1.0);
+    const cx<double> one = mkc<double>(1.0, 0.0);
+    cx<double> f0 = e.denom * e.h0, f1 = e.denom * e.h1, f2 = e.denom * e.h2;
+    const cx<double> emiu = e.emiu, e2iu = e.e2iu, cosw = e.cosw, ix0 = e.ixi0;
+    cx<double> r10 = 2.0 * (mkc<double>(u, u2 - w2) * e2iu)
+                   + 2.0 * (emiu * ((4.0 * u) * (mkc<double>(2.0, -u) * cosw)
+                                    + ix0 * mkc<double>(9.0 * u2 + w2, -u * (3.0 * u2 + w2))));
+    cx<double> r11 = 2.0 * (mkc<double>(1.0, 2.0 * u) * e2iu)
+                   + emiu * ((-2.0) * (mkc<double>(1.0, -u) * cosw) + ix0 * mkc<double>(6.0 * u, w2 - 3.0 * u2));
+    cx<double> r12 = 2.0 * (I1 * e2iu) + I1 * (emiu * (cosw - 3.0 * (mkc<double>(1.0, -u) * x0)));
+    cx<double> r20 = (-2.0) * e2iu
+                   + ((2.0 * u) * I1) * (emiu * (cosw + mkc<double>(1.0, 4.0 * u) * x0 + (3.0 * u2) * x1));
+    cx<double> r21 = -(I1 * (emiu * (cosw + mkc<double>(1.0, 2.0 * u) * x0 - (3.0 * u2) * x1)));
+    cx<double> r22 = emiu * (x0 - ((3.0 * u) * I1) * x1);
+    (void)one;
+    d.f1 = f1;
+    d.f2 = f2;
+    if (e.c0max < DBL_MIN)
+    {
+        d.b10 = d.b11 = d.b12 = d.b20 = d.b21 = d.b22 = mkc<double>(0.0, 0.0);
+        return d;
+    }
+    double bd = 9.0 * u2 - w2;
+    bd *= 2.0 * bd;
+    bd = 1.0 / bd;
+    const double k1 = 3.0 * u2 - w2, k2 = 2.0 * (15.0 * u2 + w2);
+    if (e.signflip)
+    {
+        d.b10 = bd * conj((2.0 * u) * r10 + k1 * r20 - k2 * conj(f0));
+        d.b11 = (-bd) * conj((2.0 * u) * r11 + k1 * r21 + k2 * conj(f1));
+        d.b12 = bd * conj((2.0 * u) * r12 + k1 * r22 - k2 * conj(f2));
+        d.b20 = (-bd) * conj(r10 - (3.0 * u) * r20 - (24.0 * u) * conj(f0));
+        d.b21 = bd * conj(r11 - (3.0 * u) * r21 + (24.0 * u) * conj(f1));
+        d.b22 = (-bd) * conj(r12 - (3.0 * u) * r22 - (24.0 * u) * conj(f2));
+    }
+    else
+    {
+        d.b10 = bd * ((2.0 * u) * r10 + k1 * r20 - k2 * f0);
+        d.b11 = bd * ((2.0 * u) * r11 + k1 * r21 - k2 * f1);
+        d.b12 = bd * ((2.0 * u) * r12 + k1 * r22 - k2 * f2);
+        d.b20 = bd * (r10 - (3.0 * u) * r20 - (24.0 * u) * f0);
+        d.b21 = bd * (r11 - (3.0 * u) * r21 - (24.0 * u) * f1);
+        d.b22 = bd * (r12 - (3.0 * u) * r22 - (24.0 * u) * f2);
+    }
+    return d;
+}
+
+// ---------------------------------------------------------------- Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11).
+struct U4 { uint32_t x, y, z, w; };
+
+LT_HD U4 philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r)
+    {
+#ifdef __CUDA_ARCH__
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c1 = lo1;
+        c3 = lo0;
+        c0 = n0;
+        c2 = n2;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    U4 o;
+    o.x = c0; o.y = c1; o.z = c2; o.w = c3;
+    return o;
+}
+
+// Stream tags (word 3 of the counter, bits 24..31)
+enum : uint32_t { TAG_HEATBATH = 1, TAG_MOMENTA = 2, TAG_ACCEPT = 3, TAG_HAAR = 4 };
+
+LT_HD double u01_from(uint32_t hi, uint32_t lo)
+{
+    return (double)((((uint64_t)hi << 32) | lo) >> 11) * 0x1.0p-53;
+}
+
+LT_HD float f01_from(uint32_t w) { return (float)(w >> 8) * 0x1.0p-24f; }
+
+} // namespace lt

@@ -1,0 +1,43 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TESTS = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(TESTS, "golden")
+for p in (ROOT, TESTS):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA path through the C ABI")
+    config.addinivalue_line("markers", "slow: longer statistical checks")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from ltref import Oracle
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def golden4():
+    return dict(np.load(os.path.join(GOLDEN, "ref_4x4x4x4.npz")))
+
+
+@pytest.fixture(scope="session")
+def golden_odd():
+    return dict(np.load(os.path.join(GOLDEN, "ref_4x6x8x10.npz")))
+
+
+@pytest.fixture(scope="session")
+def golden_bias():
+    return dict(np.load(os.path.join(GOLDEN, "ref_bias.npz")))
+
+
+@pytest.fixture(scope="session")
+def golden_chain():
+    return dict(np.load(os.path.join(GOLDEN, "ref_chain_8x8x8x8.npz")))

@@ -1,0 +1,171 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own code.
+
+Runs the compiled reference harness (oracle/ref_harness.cpp built by oracle/build_ref.py
+against the reference headers) on seeded inputs and stores inputs, sampled output links and
+full-field checksums.  Needs the reference checkout (it builds the harness); the fixtures it
+writes are committed so the tests never need the reference at run time.
+
+Usage: python tests/golden/gen_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from ltref import Reference, haar_links_numpy  # noqa: E402
+
+BETA = 6.0
+N_SAMPLE = 64
+
+
+def sample_links(V: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(4 * V, size=N_SAMPLE, replace=False))
+
+
+def checksums(field: np.ndarray) -> np.ndarray:
+    """Size-independent summary of a full field: sum, sum of squares, index-weighted sum."""
+    f = field.reshape(-1)
+    w = np.arange(f.size, dtype=np.float64) % 97.0
+    return np.array([f.sum(), (f * f).sum(), (w * f).sum()])
+
+
+def take(field: np.ndarray, links: np.ndarray) -> np.ndarray:
+    return field.reshape(-1, 18)[links]
+
+
+def random_momenta(V: int, seed: int) -> np.ndarray:
+    """Traceless anti-Hermitian momenta from numpy Gaussians (input data only)."""
+    rng = np.random.default_rng(seed)
+    phi = rng.standard_normal((V * 4, 8))
+    s3 = np.sqrt(3.0)
+    A = np.zeros((V * 4, 3, 3), dtype=np.complex128)
+    A[:, 0, 0] = 1j * (phi[:, 2] + phi[:, 7] / s3)
+    A[:, 0, 1] = phi[:, 1] + 1j * phi[:, 0]
+    A[:, 0, 2] = phi[:, 4] + 1j * phi[:, 3]
+    A[:, 1, 0] = -phi[:, 1] + 1j * phi[:, 0]
+    A[:, 1, 1] = 1j * (-phi[:, 2] + phi[:, 7] / s3)
+    A[:, 1, 2] = phi[:, 6] + 1j * phi[:, 5]
+    A[:, 2, 0] = -phi[:, 4] + 1j * phi[:, 3]
+    A[:, 2, 1] = -phi[:, 6] + 1j * phi[:, 5]
+    A[:, 2, 2] = 1j * (-2.0 * phi[:, 7] / s3)
+    A *= 0.5
+    out = np.empty((V, 4, 3, 3, 2))
+    out[..., 0] = A.real.reshape(V, 4, 3, 3)
+    out[..., 1] = A.imag.reshape(V, 4, 3, 3)
+    return out
+
+
+def hermitian_inputs(n: int, seed: int) -> np.ndarray:
+    """Traceless Hermitian matrices spanning the exponential's branches: generic, small
+    (Taylor branch of xi_0), negative determinant (sign flip) and exactly degenerate (zero)."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, 3, 3, 2))
+    for k in range(n):
+        M = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+        H = 0.5 * (M + M.conj().T)
+        H -= np.trace(H) / 3.0 * np.eye(3)
+        scale = [1.0, 0.01, 1e-4, 2.0][k % 4]
+        H *= scale
+        if k % 8 == 7:
+            H = -H
+        if k == n - 1:
+            H[:] = 0.0
+        out[k, ..., 0] = H.real
+        out[k, ..., 1] = H.imag
+    return out
+
+
+def gen_case(ext, seed: int, full: bool) -> dict:
+    ref = Reference(ext)
+    V = int(np.prod(ext))
+    U = haar_links_numpy(ext, seed)
+    links = sample_links(V, seed + 100)
+    d = {"ext": np.array(ext, dtype=np.int32), "seed": np.array(seed), "U": U, "links": links,
+         "plaq": np.array(ref.plaquette_sum(U)), "action": np.array(ref.wilson_action(U, BETA)),
+         "Q": np.array(ref.topcharge(U)), "E": np.array(ref.energy(U))}
+    S = ref.staples(U)
+    d["staples"], d["staples_ck"] = take(S, links), checksums(S)
+    O = ref.overrelax(U, 1)
+    d["or1"], d["or1_ck"] = take(O, links), checksums(O)
+    d["or1_plaq"] = np.array(ref.plaquette_sum(O))
+    F = ref.flow_rk3(U, 0.01, 10)
+    d["flow10"], d["flow10_ck"] = take(F, links), checksums(F)
+    p, q, e = ref.flow_rk3_measure(U, 0.01, 2, 5)
+    d["flowm_plaq"], d["flowm_q"], d["flowm_e"] = p, q, e
+    St = ref.stout(U, 0.12, 4)
+    d["stout4"], d["stout4_ck"] = take(St, links), checksums(St)
+    G = ref.gauge_force(U, BETA)
+    d["gforce"], d["gforce_ck"] = take(G, links), checksums(G)
+    if full:
+        D = ref.clover_derivative(U)
+        d["cderiv"], d["cderiv_ck"] = take(D, links), checksums(D)
+        M, qm = ref.metad_force(U, 0.12, 1.0)
+        d["metad"], d["metad_ck"], d["metad_q"] = take(M, links), checksums(M), np.array(qm)
+        d["metad_nstout"] = np.array(ref.lib.ref_n_smear_meta())
+        P = random_momenta(V, seed + 7)
+        d["P"] = P
+        U2, P2, ho, hn = ref.omf2(U, P, BETA, 1.0, 10)
+        d["omf2_U"], d["omf2_P"], d["omf2_h"] = take(U2, links), take(P2, links), np.array([ho, hn])
+        U3, P3, ho3, hn3 = ref.metad_omf2(U, P, BETA, 1.0, 4, 0.12, 0.5)
+        d["momf2_U"], d["momf2_P"], d["momf2_h"] = take(U3, links), take(P3, links), np.array([ho3, hn3])
+        Hm = hermitian_inputs(64, seed + 3)
+        d["exp_in"], d["exp_out"] = Hm, ref.su3_exp(Hm.reshape(-1)).reshape(Hm.shape)
+    return d
+
+
+def gen_bias() -> dict:
+    import ctypes as C  # noqa: F401
+    ref = Reference((4, 4, 4, 4))
+    rng = np.random.default_rng(11)
+    deposits = np.concatenate([rng.normal(0.0, 1.5, 40), [7.99, -8.5, 9.0]])
+    probes = np.concatenate([np.linspace(-9.0, 9.0, 181), [-8.0, 8.0, 7.99, -7.995]])
+    out = {}
+    for sym in (0, 1):
+        pot, der = np.empty(probes.size), np.empty(probes.size)
+        ref.lib.ref_bias_probe(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0, deposits, deposits.size, sym,
+                               probes, probes.size, pot, der)
+        out[f"pot{sym}"], out[f"der{sym}"] = pot, der
+    out["deposits"], out["probes"] = deposits, probes
+    return out
+
+
+def gen_chain() -> dict:
+    """Reference heatbath + overrelaxation chain at 8^4, beta = 6: plaquette history."""
+    ext = (8, 8, 8, 8)
+    ref = Reference(ext)
+    ref.lib.ref_reset_prng()
+    U = haar_links_numpy(ext, 5)
+    U, p_therm = ref.hb_or_chain(U, BETA, 200, 1, 4)
+    U, p = ref.hb_or_chain(U, BETA, 1000, 1, 4)
+    V = int(np.prod(ext))
+    return {"plaq_norm_therm": p_therm / V / 18.0, "plaq_norm": p / V / 18.0, "beta": np.array(BETA)}
+
+
+def main() -> int:
+    import subprocess
+    root = os.path.dirname(os.path.dirname(HERE))
+    subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "4x4x4x4",
+                    "4x6x8x10", "8x8x8x8"], check=True)
+    np.savez_compressed(os.path.join(HERE, "ref_4x4x4x4.npz"), **gen_case((4, 4, 4, 4), 1, True))
+    b = gen_case((4, 6, 8, 10), 2, False)
+    del b["U"]   # regenerated from numpy's seeded generator; checksum kept
+    U = haar_links_numpy((4, 6, 8, 10), 2)
+    b["U_ck"] = checksums(U)
+    np.savez_compressed(os.path.join(HERE, "ref_4x6x8x10.npz"), **b)
+    np.savez_compressed(os.path.join(HERE, "ref_bias.npz"), **gen_bias())
+    np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

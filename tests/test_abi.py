@@ -1,0 +1,101 @@
+"""CPU checks of the drop-in boundary: the C-ABI library loads, exports every symbol the
+header declares, and its host-side parts (Haar start, bias potential, argument checks)
+behave like the reference.  No compute call reaches a GPU here."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import lettuce_b200 as lt
+from lettuce_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_built_in_tree():
+    assert os.path.exists(_lib.LIB_PATH)
+    assert os.path.dirname(_lib.LIB_PATH) == os.path.join(ROOT, "lettuce_b200")
+
+
+def test_exports_every_declared_symbol():
+    declared = lt.declared_symbols()
+    assert len(declared) >= 40
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    missing = [s for s in declared if s not in exported]
+    assert not missing, missing
+    assert set(declared) <= set(_lib.SIGNATURES), set(declared) - set(_lib.SIGNATURES)
+
+
+def test_kernels_are_sm100a():
+    out = subprocess.run(["cuobjdump", "--list-elf", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_version():
+    assert lt.lib().lt_version() >= 100
+
+
+def test_haar_links_are_su3_and_seeded():
+    ext = (4, 4, 4, 6)
+    U = lt.haar_links(ext, 5)
+    M = (U[..., 0] + 1j * U[..., 1]).reshape(-1, 3, 3)
+    assert np.abs(np.einsum("nij,nkj->nik", M, M.conj()) - np.eye(3)).max() < 1e-13
+    assert np.abs(np.linalg.det(M) - 1).max() < 1e-13
+    assert np.array_equal(U, lt.haar_links(ext, 5))
+    assert not np.array_equal(U, lt.haar_links(ext, 6))
+    # Haar moments: <|U_ij|^2> = 1/3, <Re tr U> = 0
+    assert np.mean(np.abs(M) ** 2) == pytest.approx(1 / 3, abs=0.01)
+    assert abs(np.mean(np.trace(M, axis1=1, axis2=2).real)) < 0.05
+
+
+def test_haar_rejects_odd_extent():
+    out = np.empty((4 * 4 * 4 * 5, 4, 3, 3, 2))
+    code = lt.lib().lt_haar_links(np.array([4, 4, 4, 5], dtype=np.int32), C.c_uint64(1), out)
+    assert code == _lib.LT_ERR_ARG
+    assert b"even" in lt.lib().lt_last_error()
+
+
+def test_create_rejects_bad_extents_without_device():
+    with pytest.raises(lt.LettuceError) as e:
+        lt.GaugeField((4, 4, 3, 4))
+    assert e.value.code == _lib.LT_ERR_ARG
+    h = C.c_void_p()
+    assert lt.lib().lt_create(np.array([4, 4, 4, 4], dtype=np.int32), 7, C.byref(h)) == _lib.LT_ERR_ARG
+    assert not h.value
+
+
+def test_null_handles_are_errors():
+    v = C.c_double()
+    assert lt.lib().lt_plaquette_sum(None, C.byref(v)) == _lib.LT_ERR_ARG
+    assert lt.lib().lt_destroy(None) == _lib.LT_OK
+
+
+def test_bias_matches_reference_fixture(golden_bias):
+    g = golden_bias
+    for sym in (0, 1):
+        b = lt.MetaBiasPotential(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0)
+        for cv in g["deposits"]:
+            (b.UpdatePotentialSymmetric if sym else b.UpdatePotential)(cv)
+        pot = np.array([b.ReturnPotential(p) for p in g["probes"]])
+        der = np.array([b.ReturnDerivative(p) for p in g["probes"]])
+        np.testing.assert_allclose(pot, g[f"pot{sym}"], rtol=1e-13, atol=1e-13)
+        np.testing.assert_allclose(der, g[f"der{sym}"], rtol=1e-10, atol=1e-10)
+
+
+def test_bias_constructor_throws_like_reference():
+    with pytest.raises(ValueError, match="CV_min < CV_max"):
+        lt.MetaBiasPotential(1.0, -1.0, 800, 0.05, 0.08, 10, 1000)
+    with pytest.raises(ValueError, match="bin_number > 0"):
+        lt.MetaBiasPotential(-1.0, 1.0, 0, 0.05, 0.08, 10, 1000)
+
+
+def test_bias_generate_and_grid():
+    b = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 10, 1000)
+    b.GeneratePotentialFrom(lambda cv: 0.5 * cv)
+    assert b.ReturnDerivative(0.123) == pytest.approx(0.5, rel=1e-12)
+    assert b.grid().shape == (801,)
+    assert b.ReturnPotential(9.0) == pytest.approx(4.0 + 1000.0, rel=1e-12)

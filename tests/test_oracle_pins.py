@@ -1,0 +1,151 @@
+"""Pin the C restatement (oracle/lt_oracle.c) against the reference itself.
+
+Every oracle function is compared with the golden fixtures generated from the reference's
+own code (tests/golden/gen_golden.py) and, where the reference harness is built here, with
+the reference run live on fresh inputs.  Tolerance: 1e-12 relative to the field's largest
+entry (FP64 on both sides; the only differences are summation order and libm rounding).
+"""
+import numpy as np
+import pytest
+
+from ltref import Reference, haar_links_numpy, ref_available, rel_err
+
+TOL = 1e-12
+
+
+def links_of(field, idx):
+    return field.reshape(-1, 18)[idx]
+
+
+def checksums(field):
+    f = field.reshape(-1)
+    w = np.arange(f.size, dtype=np.float64) % 97.0
+    return np.array([f.sum(), (f * f).sum(), (w * f).sum()])
+
+
+def close_ck(a, b, tol=1e-10):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.all(np.abs(a - b) <= tol * np.maximum(1.0, np.abs(b)))
+
+
+class TestGolden4:
+    """4^4 fixture: Haar start, every function of the path."""
+
+    def test_scalars(self, oracle, golden4):
+        g, ext, U = golden4, golden4["ext"], golden4["U"]
+        assert oracle.plaquette_sum(ext, U) == pytest.approx(float(g["plaq"]), rel=TOL)
+        assert oracle.wilson_action(ext, U, 6.0) == pytest.approx(float(g["action"]), rel=TOL)
+        assert oracle.topcharge(ext, U) == pytest.approx(float(g["Q"]), rel=1e-11, abs=1e-14)
+        assert oracle.energy(ext, U) == pytest.approx(float(g["E"]), rel=TOL)
+
+    def test_staples(self, oracle, golden4):
+        g = golden4
+        S = oracle.staples(g["ext"], g["U"])
+        assert rel_err(links_of(S, g["links"]), g["staples"]) < TOL
+        assert close_ck(checksums(S), g["staples_ck"])
+
+    def test_overrelaxation_sweep(self, oracle, golden4):
+        g = golden4
+        O = oracle.overrelax(g["ext"], g["U"], 1)
+        # a hot (Haar) start has nearly singular SU(2) projections; 1e-10 there
+        assert rel_err(links_of(O, g["links"]), g["or1"]) < 1e-10
+        assert oracle.plaquette_sum(g["ext"], O) == pytest.approx(float(g["or1_plaq"]), rel=1e-11)
+
+    def test_flow_rk3(self, oracle, golden4):
+        g = golden4
+        F = oracle.flow_rk3(g["ext"], g["U"], 0.01, 10)
+        assert rel_err(links_of(F, g["links"]), g["flow10"]) < TOL
+        assert close_ck(checksums(F), g["flow10_ck"])
+
+    def test_stout(self, oracle, golden4):
+        g = golden4
+        S = oracle.stout(g["ext"], g["U"], 0.12, 4)
+        assert rel_err(links_of(S, g["links"]), g["stout4"]) < TOL
+
+    def test_gauge_force(self, oracle, golden4):
+        g = golden4
+        F = oracle.gauge_force(g["ext"], g["U"], 6.0)
+        assert rel_err(links_of(F, g["links"]), g["gforce"]) < TOL
+
+    def test_clover_derivative(self, oracle, golden4):
+        g = golden4
+        D = oracle.clover_derivative(g["ext"], g["U"])
+        assert rel_err(links_of(D, g["links"]), g["cderiv"]) < TOL
+
+    def test_metad_force(self, oracle, golden4):
+        g = golden4
+        n = int(g["metad_nstout"])
+        M, q = oracle.metad_force(g["ext"], g["U"], 0.12, n, 1.0)
+        assert rel_err(links_of(M, g["links"]), g["metad"]) < 1e-11
+        assert q == pytest.approx(float(g["metad_q"]), rel=1e-11)
+
+    def test_omf2(self, oracle, golden4):
+        g = golden4
+        U2, P2, ho, hn = oracle.omf2(g["ext"], g["U"], g["P"], 6.0, 1.0, 10)
+        assert rel_err(links_of(U2, g["links"]), g["omf2_U"]) < 1e-11
+        assert rel_err(links_of(P2, g["links"]), g["omf2_P"]) < 1e-11
+        assert ho == pytest.approx(g["omf2_h"][0], rel=TOL)
+        assert hn == pytest.approx(g["omf2_h"][1], rel=TOL)
+
+    def test_su3_exp(self, oracle, golden4):
+        g = golden4
+        out = oracle.su3_exp(g["exp_in"].reshape(-1)).reshape(g["exp_out"].shape)
+        assert np.max(np.abs(out - g["exp_out"])) < 1e-13
+
+
+class TestGoldenOdd:
+    """4x6x8x10: uneven extents, numpy-seeded Haar start regenerated from the seed."""
+
+    def test_input_regenerates(self, golden_odd):
+        U = haar_links_numpy((4, 6, 8, 10), int(golden_odd["seed"]))
+        assert close_ck(checksums(U), golden_odd["U_ck"], 1e-12)
+
+    def test_functions(self, oracle, golden_odd):
+        g = golden_odd
+        ext = g["ext"]
+        U = haar_links_numpy(tuple(ext), int(g["seed"]))
+        assert oracle.plaquette_sum(ext, U) == pytest.approx(float(g["plaq"]), rel=TOL)
+        assert oracle.topcharge(ext, U) == pytest.approx(float(g["Q"]), rel=1e-10, abs=1e-13)
+        assert oracle.energy(ext, U) == pytest.approx(float(g["E"]), rel=TOL)
+        assert rel_err(links_of(oracle.staples(ext, U), g["links"]), g["staples"]) < TOL
+        assert rel_err(links_of(oracle.flow_rk3(ext, U, 0.01, 10), g["links"]), g["flow10"]) < TOL
+        assert rel_err(links_of(oracle.stout(ext, U, 0.12, 4), g["links"]), g["stout4"]) < TOL
+        assert rel_err(links_of(oracle.gauge_force(ext, U, 6.0), g["links"]), g["gforce"]) < TOL
+        assert rel_err(links_of(oracle.overrelax(ext, U, 1), g["links"]), g["or1"]) < 1e-10
+
+
+def test_bias_potential(oracle, golden_bias):
+    """MetaBiasPotential deposits, interpolation, walls and derivative."""
+    g = golden_bias
+    for sym in (0, 1):
+        b = oracle.lib.or_bias_create(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0)
+        for cv in g["deposits"]:
+            if sym:
+                oracle.lib.or_bias_update_symmetric(b, cv)
+            else:
+                oracle.lib.or_bias_update(b, cv)
+        pot = np.array([oracle.lib.or_bias_potential(b, p) for p in g["probes"]])
+        der = np.array([oracle.lib.or_bias_derivative(b, p) for p in g["probes"]])
+        oracle.lib.or_bias_destroy(b)
+        np.testing.assert_allclose(pot, g[f"pot{sym}"], rtol=1e-13, atol=1e-13)
+        np.testing.assert_allclose(der, g[f"der{sym}"], rtol=1e-10, atol=1e-10)
+
+
+def test_bias_rejects_bad_range(oracle):
+    assert not oracle.lib.or_bias_create(1.0, -1.0, 800, 0.05, 0.08, 10.0, 1000.0)
+    assert not oracle.lib.or_bias_create(-1.0, 1.0, 0, 0.05, 0.08, 10.0, 1000.0)
+
+
+@pytest.mark.skipif(not ref_available((8, 8, 8, 8)), reason="reference harness not built here")
+class TestLiveReference:
+    """Oracle vs the reference on fresh inputs (8^4, thermalised by 20 reference heatbath sweeps)."""
+
+    def test_observables_and_flow(self, oracle):
+        ext = (8, 8, 8, 8)
+        ref = Reference(ext)
+        U = haar_links_numpy(ext, 77)
+        U, _ = ref.hb_or_chain(U, 6.0, 20, 1, 0)
+        assert oracle.plaquette_sum(ext, U) == pytest.approx(ref.plaquette_sum(U), rel=TOL)
+        assert oracle.topcharge(ext, U) == pytest.approx(ref.topcharge(U), rel=1e-10, abs=1e-12)
+        assert rel_err(oracle.overrelax(ext, U, 1), ref.overrelax(U, 1)) < TOL
+        assert rel_err(oracle.flow_rk3(ext, U, 0.01, 3), ref.flow_rk3(U, 0.01, 3)) < TOL
