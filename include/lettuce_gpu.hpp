@@ -1,0 +1,323 @@
+// lettuce_gpu.hpp -- C++20 drop-in header over the lettuce_b200 C ABI.
+//
+// Keeps the call surface of the CPU reference timo-eichhorn/Lettuce (LettuceGauge/...) so
+// that SU3_main.cpp-style host code recompiles against the B200 path with only its includes
+// changed.  Differences that cannot be hidden:
+//   * lattice extents are constructor arguments, not compile-time constants
+//     (defines.hpp:34-37), and beta is passed to the action instead of a global (:52);
+//   * a per-link functor cannot cross to the device, so Iterator::Checkerboard is
+//     overloaded for the update kernels and runs a whole sweep per call
+//     (iterators/iterators.hpp:65-87);
+//   * random numbers come from counter-based Philox streams (seed + counter) instead of
+//     one pcg64 per link (random/prng_wrapper.hpp:43-114).
+// A non-OK status from the C ABI throws lettuce_gpu::Error (the reference exits or
+// throws std::invalid_argument on the corresponding misuse).
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "lettuce_b200.h"
+
+namespace lettuce_gpu
+{
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void check(int code)
+{
+    if (code != LT_OK) throw Error(code, lt_last_error());
+}
+
+// GaugeField4D (lattice.hpp:87-394)
+class GaugeField
+{
+public:
+    explicit GaugeField(std::array<int, 4> ext, int prec = LT_PREC_FP64) : ext_(ext)
+    {
+        check(lt_create(ext.data(), prec, &h_));
+    }
+    GaugeField(const GaugeField& o) : ext_(o.ext_)
+    {
+        int prec;
+        check(lt_get_extents(o.h_, nullptr, &prec));
+        check(lt_create(ext_.data(), prec, &h_));
+        check(lt_copy(h_, o.h_));
+    }
+    GaugeField& operator=(const GaugeField& o)
+    {
+        if (this != &o) check(lt_copy(h_, o.h_));
+        return *this;
+    }
+    GaugeField(GaugeField&& o) noexcept : ext_(o.ext_), h_(std::exchange(o.h_, nullptr)) {}
+    ~GaugeField() { lt_destroy(h_); }
+
+    void SetToIdentity() { check(lt_set_identity(h_)); }
+    void SetToHaarRandom(std::uint64_t seed) { check(lt_set_haar_random(h_, seed)); }
+    std::size_t Volume() const { return (std::size_t)ext_[0] * ext_[1] * ext_[2] * ext_[3]; }
+    int Length(int d) const { return ext_[d]; }
+    std::array<int, 4> Shape() const { return ext_; }
+
+    // Whole field in the reference layout double[V][4][3][3][2]
+    void Upload(const std::vector<double>& links) { check(lt_upload_links(h_, links.data())); }
+    std::vector<double> Download() const
+    {
+        std::vector<double> v(Volume() * 72);
+        check(lt_download_links(h_, v.data()));
+        return v;
+    }
+    // operator()(link_coord) as explicit get/set of 18 doubles
+    std::array<double, 18> GetLink(std::int64_t site, int mu) const
+    {
+        std::array<double, 18> m;
+        check(lt_get_link(h_, site, mu, m.data()));
+        return m;
+    }
+    void SetLink(std::int64_t site, int mu, const std::array<double, 18>& m) { check(lt_set_link(h_, site, mu, m.data())); }
+
+    friend void Swap(GaugeField& a, GaugeField& b) { check(lt_swap(a.h_, b.h_)); }
+    lt_lattice* handle() const { return h_; }
+
+private:
+    std::array<int, 4> ext_;
+    lt_lattice* h_ = nullptr;
+};
+
+// observables/plaquette.hpp:26-43
+inline double PlaquetteSum(const GaugeField& U)
+{
+    double v;
+    check(lt_plaquette_sum(U.handle(), &v));
+    return v;
+}
+
+// observables/topological_charge.hpp:97-200
+inline double TopChargeClover(const GaugeField& U)
+{
+    double v;
+    check(lt_topcharge_clover(U.handle(), &v));
+    return v;
+}
+
+// EnergyDensity::Clover of the traceless clover field strength (field_strength_tensor.hpp:154-175)
+inline double EnergyDensityClover(const GaugeField& U)
+{
+    double v;
+    check(lt_energy_clover(U.handle(), &v));
+    return v;
+}
+
+namespace GaugeAction
+{
+// Rectangular<1> with (c_plaq, c_rect) = (1, 0) (actions/gauge/rectangular_action.hpp:23-294)
+struct Wilson
+{
+    double beta = 6.0;
+    void SetBeta(double b) { beta = b; }
+    double GetBeta() const { return beta; }
+    double Action(const GaugeField& U) const
+    {
+        double v;
+        check(lt_wilson_action(U.handle(), beta, &v));
+        return v;
+    }
+    double ActionNormalized(const GaugeField& U) const { return Action(U) / (6.0 * beta * (double)U.Volume()); }
+};
+inline Wilson WilsonAction;
+} // namespace GaugeAction
+
+// HeatbathKernel (updates/heatbath.hpp:30-130); beta fixed at construction (:40)
+struct HeatbathKernel
+{
+    GaugeField& U;
+    double beta;
+    std::uint64_t seed, counter;
+    HeatbathKernel(GaugeField& U_in, const GaugeAction::Wilson& action, std::uint64_t seed_in = 1,
+                   std::uint64_t counter_in = 0)
+        : U(U_in), beta(action.GetBeta()), seed(seed_in), counter(counter_in)
+    {
+    }
+};
+
+// OverrelaxationSubgroupKernel (updates/overrelaxation.hpp:68-117)
+struct OverrelaxationSubgroupKernel
+{
+    GaugeField& U;
+    OverrelaxationSubgroupKernel(GaugeField& U_in, const GaugeAction::Wilson&) : U(U_in) {}
+};
+
+namespace Iterator
+{
+// Iterator::Checkerboard (iterators/iterators.hpp:65-87): whole sweeps per call
+inline void Checkerboard(HeatbathKernel& k, int n_sweep = 1)
+{
+    check(lt_heatbath_sweeps(k.U.handle(), k.beta, n_sweep, k.seed, &k.counter));
+}
+inline void Checkerboard(OverrelaxationSubgroupKernel& k, int n_sweep = 1)
+{
+    check(lt_overrelax_sweeps(k.U.handle(), n_sweep));
+}
+// The 4-sublattice variant (:141-169) visits the same links; on the device both are the
+// same even/odd launch sequence.
+inline void Checkerboard4(HeatbathKernel& k, int n_sweep = 1) { Checkerboard(k, n_sweep); }
+inline void Checkerboard4(OverrelaxationSubgroupKernel& k, int n_sweep = 1) { Checkerboard(k, n_sweep); }
+} // namespace Iterator
+
+namespace Integrators::GradientFlow
+{
+struct RK3   // smearing/gradient_flow.hpp:120-168
+{
+    static std::string ReturnName() { return "RK3"; }
+};
+} // namespace Integrators::GradientFlow
+
+// GradientFlowKernel (smearing/gradient_flow.hpp:252-367) with the RK3 integrator
+template <typename IntegratorT = Integrators::GradientFlow::RK3, typename ActionT = GaugeAction::Wilson>
+struct GradientFlowKernel
+{
+    const GaugeField& U_unflowed;
+    GaugeField& U_flowed;
+    double epsilon;
+    GradientFlowKernel(const GaugeField& in, GaugeField& out, IntegratorT&, ActionT&, double eps)
+        : U_unflowed(in), U_flowed(out), epsilon(eps)
+    {
+    }
+    void operator()(int n_step) const { check(lt_flow_rk3(U_unflowed.handle(), U_flowed.handle(), epsilon, n_step)); }
+    void Resume(int n_step) const { check(lt_flow_rk3(U_flowed.handle(), U_flowed.handle(), epsilon, n_step)); }
+    void SetEpsilon(double e) { epsilon = e; }
+    double GetEpsilon() const { return epsilon; }
+    std::string ReturnIntegratorName() const { return IntegratorT::ReturnName(); }
+};
+
+// StoutSmearing4D (smearing/stout_smearing.hpp:29-57)
+inline void StoutSmearing4D(const GaugeField& in, GaugeField& out, double smear_param = 0.12)
+{
+    check(lt_stout(in.handle(), out.handle(), smear_param, 1));
+}
+
+// MetaBiasPotential (actions/bias_potential/metadynamics.hpp:29-507)
+class MetaBiasPotential
+{
+public:
+    MetaBiasPotential(double CV_min, double CV_max, int bin_number, double weight, double width,
+                      double well_tempered_parameter, double threshold_weight)
+    {
+        if (lt_bias_create(CV_min, CV_max, bin_number, weight, width, well_tempered_parameter, threshold_weight, &b_)
+            != LT_OK)
+            throw std::invalid_argument(lt_last_error());
+    }
+    MetaBiasPotential(const MetaBiasPotential&) = delete;
+    MetaBiasPotential& operator=(const MetaBiasPotential&) = delete;
+    ~MetaBiasPotential() { lt_bias_destroy(b_); }
+    void UpdatePotential(double cv) { check(lt_bias_update(b_, &cv, 1, 0)); }
+    void UpdatePotentialSymmetric(double cv) { check(lt_bias_update(b_, &cv, 1, 1)); }
+    void UpdatePotentialSymmetric(const std::vector<double>& cv)
+    {
+        check(lt_bias_update(b_, cv.data(), (int)cv.size(), 1));
+    }
+    double ReturnPotential(double cv) const
+    {
+        double v;
+        check(lt_bias_potential(b_, cv, &v));
+        return v;
+    }
+    double ReturnDerivative(double cv) const
+    {
+        double v;
+        check(lt_bias_derivative(b_, cv, &v));
+        return v;
+    }
+    lt_bias* handle() const { return b_; }
+
+private:
+    lt_bias* b_ = nullptr;
+};
+
+struct RunStatistics   // defines.hpp:93-106 (the fields this path fills)
+{
+    double delta_H_hmc = 0.0;
+    std::uint64_t acceptances_hmc = 0;
+    std::uint64_t acceptances_metadynamics_hmc = 0;
+};
+
+namespace Integrators::HMC
+{
+struct OMF_2   // updates/hmc_gauge.hpp:155-190
+{
+    static constexpr int NumberOfMomentumUpdates(int n_step) { return n_step > 0 ? 2 * n_step + 1 : 0; }
+};
+} // namespace Integrators::HMC
+
+namespace GaugeUpdates
+{
+// HMCKernel (updates/hmc_gauge.hpp:381-600) with OMF_2; U_copy and Momentum live on the device
+struct HMCKernel
+{
+    GaugeField& U;
+    GaugeAction::Wilson& Action;
+    RunStatistics& statistics;
+    double trajectory_length;
+    std::uint64_t seed, counter;
+    HMCKernel(GaugeField& U_in, Integrators::HMC::OMF_2&, GaugeAction::Wilson& action, RunStatistics& stats,
+              double tau = 1.0, std::uint64_t seed_in = 1, std::uint64_t counter_in = 0)
+        : U(U_in), Action(action), statistics(stats), trajectory_length(tau), seed(seed_in), counter(counter_in)
+    {
+    }
+    bool operator()(int n_step, bool metropolis_step)
+    {
+        double dH;
+        int acc;
+        check(lt_hmc_trajectory(U.handle(), Action.GetBeta(), trajectory_length, n_step, seed, &counter,
+                                metropolis_step ? 1 : 0, &dH, &acc));
+        statistics.delta_H_hmc = dH;
+        statistics.acceptances_hmc += (std::uint64_t)acc;
+        return acc != 0;
+    }
+};
+
+// HMCMetaDKernel (updates/hmc_metadynamics.hpp:264-675) with OMF_2
+struct HMCMetaDKernel
+{
+    GaugeField& U;
+    MetaBiasPotential& Metapotential;
+    GaugeAction::Wilson& Action;
+    RunStatistics& statistics;
+    double trajectory_length, rho_stout_cv;
+    int n_smear_meta;
+    std::uint64_t seed, counter;
+    double cv_current = 0.0;
+    HMCMetaDKernel(GaugeField& U_in, MetaBiasPotential& bias, Integrators::HMC::OMF_2&, GaugeAction::Wilson& action,
+                   RunStatistics& stats, double tau, double rho, int n_smear = 4, std::uint64_t seed_in = 1,
+                   std::uint64_t counter_in = 0)
+        : U(U_in), Metapotential(bias), Action(action), statistics(stats), trajectory_length(tau), rho_stout_cv(rho),
+          n_smear_meta(n_smear), seed(seed_in), counter(counter_in)
+    {
+    }
+    bool operator()(int n_step, bool metropolis_step)
+    {
+        double dH, cv;
+        int acc;
+        check(lt_metad_hmc_trajectory(U.handle(), Metapotential.handle(), Action.GetBeta(), trajectory_length, n_step,
+                                      rho_stout_cv, n_smear_meta, seed, &counter, metropolis_step ? 1 : 0, &dH, &acc,
+                                      &cv));
+        statistics.delta_H_hmc = dH;
+        statistics.acceptances_metadynamics_hmc += (std::uint64_t)acc;
+        cv_current = cv;
+        return acc != 0;
+    }
+    double MetaCharge() const
+    {
+        double q;
+        check(lt_metad_charge(U.handle(), rho_stout_cv, n_smear_meta, &q));
+        return q;
+    }
+};
+} // namespace GaugeUpdates
+} // namespace lettuce_gpu

@@ -1,0 +1,53 @@
+// A host program written against the reference's call surface (as SU3_main.cpp uses it),
+// compiled against include/lettuce_gpu.hpp instead of the reference headers.  Prints one
+// line per measurement; tests/test_dropin.py compiles it (CPU) and runs it (GPU).
+#include <cstdio>
+#include <cstdlib>
+
+#include "lettuce_gpu.hpp"
+
+using namespace lettuce_gpu;
+
+int main(int argc, char** argv)
+{
+    const int L = argc > 1 ? std::atoi(argv[1]) : 8;
+    GaugeField Gluon({L, L, L, L});
+    GaugeField Gluonsmeared1({L, L, L, L});
+    Gluon.SetToHaarRandom(2024);
+
+    auto& SimulatedAction = GaugeAction::WilsonAction;
+    SimulatedAction.SetBeta(6.0);
+    HeatbathKernel Heatbath(Gluon, SimulatedAction, 7);
+    OverrelaxationSubgroupKernel OverrelaxationSubgroup(Gluon, SimulatedAction);
+    for (int n = 0; n < 20; ++n)
+    {
+        Iterator::Checkerboard4(Heatbath, 1);
+        Iterator::Checkerboard4(OverrelaxationSubgroup, 4);
+    }
+    std::printf("plaquette %.15f\n", PlaquetteSum(Gluon) / Gluon.Volume() / 18.0);
+    std::printf("action %.12f\n", SimulatedAction.Action(Gluon));
+
+    Integrators::GradientFlow::RK3 rk3;
+    GradientFlowKernel Flow(Gluon, Gluonsmeared1, rk3, SimulatedAction, 0.01);
+    Flow(10);
+    for (int m = 0; m < 3; ++m)
+    {
+        Flow.Resume(10);
+        std::printf("flow t=%.2f Q %.12f E %.12f\n", 0.1 * (m + 2), TopChargeClover(Gluonsmeared1),
+                    EnergyDensityClover(Gluonsmeared1));
+    }
+
+    MetaBiasPotential TopBiasPotential(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0);
+    RunStatistics statistics;
+    Integrators::HMC::OMF_2 omf2;
+    GaugeUpdates::HMCMetaDKernel HMC_MetaD(Gluon, TopBiasPotential, omf2, SimulatedAction, statistics, 1.0, 0.12, 4, 99);
+    for (int n = 0; n < 3; ++n)
+    {
+        bool acc = HMC_MetaD(10, true);
+        std::printf("metad dH %.10f accepted %d cv %.10f\n", statistics.delta_H_hmc, acc ? 1 : 0, HMC_MetaD.cv_current);
+    }
+    GaugeField copy(Gluon);
+    Swap(copy, Gluonsmeared1);
+    std::printf("copy plaquette %.15f\n", PlaquetteSum(Gluonsmeared1) / Gluon.Volume() / 18.0);
+    return 0;
+}
