@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--size", type=int, default=32)
     ap.add_argument("--prec", choices=["fp32_12", "fp32", "fp64"], default="fp32_12")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 / flow / e2e / CPU side measurements")
+    ap.add_argument("--workload", choices=["sweeps", "flow", "metad"], default="sweeps",
+                    help="sweeps: the headline; flow / metad: secondary rates (and ncu targets)")
     return ap.parse_args()
 
 
@@ -188,6 +190,44 @@ def run_reference(a):
     return 0
 
 
+# ---------------------------------------------------------------------------- secondary workloads
+def run_secondary(a, lt, torch, ext, links, timed, barrier, max_over_ranks, world, rank, dist):
+    """flow: one RK3 step (eps = 0.01) per step, flow steps/s.
+    metad: one metadynamics force evaluation (4 stout steps rho = 0.12, clover Q, adjoint
+    chain) per step, force evaluations/s."""
+    G = lt.GaugeField(ext, a.prec)
+    G.upload(links)
+    lt.UpdateSweeps(G, BETA, 5, 1, 4, SEED + rank)
+    if a.workload == "flow":
+        H = lt.GaugeField(ext, a.prec)
+        flow = lt.GradientFlowKernel(G, H, lt.RK3, None, FLOW_EPS)
+        flow(1)
+        step = lambda: flow.Resume(1)   # noqa: E731
+        unit, launches_per_step, handle = "flow steps/s", 3, H
+    else:
+        bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 10, 1000)
+        k = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(BETA), 1.0, 0.12, 4)
+        step = lambda: k.CalculateTopologicalForce(dvdq=1.0, download=False)   # noqa: E731
+        unit, launches_per_step, handle = "force evaluations/s", 4 + 2 + 2 * 4 + 3, G
+    for _ in range(max(a.warmup, 3)):
+        step()
+    barrier()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(timed(handle, lambda: [step() for _ in range(a.steps)], 1))
+    line = {"metric": f"{unit} at {ext[0]}^4", "value": world * a.steps / (ms / 1000.0), "unit": unit,
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if a.prec != "fp64" else "f64", "data": "synthetic: seeded Haar-random SU(3) start",
+            "config": {"workload": f"{a.workload} at {ext[0]}^4, {a.prec} links", "lattice": list(ext),
+                       "storage": a.prec}, "gpu_launches": a.steps * launches_per_step}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 # ---------------------------------------------------------------------------- our arm
 def main():
     a = parse()
@@ -239,6 +279,9 @@ def main():
 
     def sweep_round(G):
         counter["c"] = lt.UpdateSweeps(G, BETA, 1, N_HB, N_OR, SEED + rank, counter["c"])
+
+    if a.workload != "sweeps":
+        return run_secondary(a, lt, torch, ext, links, timed, barrier, max_over_ranks, world, rank, dist)
 
     # ---- headline: FP32-bulk sweeps
     G = lt.GaugeField(ext, a.prec)

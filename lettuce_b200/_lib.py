@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liblettuce_b200.so")
+LIB_PATH = os.environ.get("LETTUCE_B200_LIB", os.path.join(HERE, "liblettuce_b200.so"))
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "lettuce_b200.h")
 
 LT_OK, LT_ERR_ARG, LT_ERR_CUDA, LT_ERR_NOMEM, LT_ERR_STATE, LT_ERR_NUMERIC = range(6)

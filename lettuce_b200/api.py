@@ -369,14 +369,16 @@ class HMCMetaDKernel(HMCKernel):
     def MetaCharge(self) -> float:
         return _out1(lib().lt_metad_charge, self.U.handle, self.rho, self.n_smear)
 
-    def CalculateTopologicalForce(self, dvdq: float | None = None) -> tuple[np.ndarray, float]:
-        """dV/dQ * dQ_smeared/dU on the thin links; dV/dQ from the bias unless given."""
+    def CalculateTopologicalForce(self, dvdq: float | None = None, download: bool = True):
+        """dV/dQ * dQ_smeared/dU on the thin links; dV/dQ from the bias unless given.
+        Returns (force in the reference layout or None when download is False, Q_smeared)."""
         q = C.c_double()
         if dvdq is None:
-            check(lib().lt_metad_force(self.U.handle, self.rho, self.n_smear, 0.0, None, C.byref(q)))
+            check(lib().lt_metad_charge(self.U.handle, self.rho, self.n_smear, C.byref(q)))
             dvdq = self.bias.ReturnDerivative(q.value)
-        out = np.empty((self.U.Volume(), 4, 3, 3, 2))
-        check(lib().lt_metad_force(self.U.handle, self.rho, self.n_smear, float(dvdq), out.ctypes.data, C.byref(q)))
+        out = np.empty((self.U.Volume(), 4, 3, 3, 2)) if download else None
+        check(lib().lt_metad_force(self.U.handle, self.rho, self.n_smear, float(dvdq),
+                                   out.ctypes.data if download else None, C.byref(q)))
         return out, q.value
 
     def Integrate(self, n_step: int) -> tuple[float, float]:

@@ -82,6 +82,19 @@ template <typename T, int NR> struct Gauge
         return m;
     }
 
+    // Rows 0 and 1 only (row 2 is not rebuilt for two-row storage)
+    LT_D M3<T> ld_rows(int mu, int par, int s) const
+    {
+        if (NR == 3) return ld(mu, par, s);
+        M3<T> m;
+        const cx<T>* q = p + plane(mu, par, 0) + s;
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) m.e[r][j] = q[(size_t)(3 * r + j) * vh];
+        return m;
+    }
+
     LT_D void st(int mu, int par, int s, const M3<T>& m) const
     {
         cx<T>* q = p + plane(mu, par, 0) + s;

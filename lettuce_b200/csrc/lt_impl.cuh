@@ -55,7 +55,7 @@ public:
     }
     void staples_aos(const Ctx& c, const void* U, double* aos) const override
     {
-        k_staple_aos<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), c.g, aos);
+        k_staple_aos<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(gauge(U, c.g), c.g, aos);
     }
 
     void plaquette(const Ctx& c, const void* U, int slot) const override
@@ -90,18 +90,18 @@ public:
     void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new, double c_exp,
                     int read_z, int write_z) const override
     {
-        k_flow_stage<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+        k_flow_stage<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
             gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z, write_z);
     }
     void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
     {
-        k_stout<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(Uin, c.g), gauge(Uout, c.g),
+        k_stout<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(gauge(Uin, c.g), gauge(Uout, c.g),
                                                                                   c.g, (T)rho);
     }
 
     void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const override
     {
-        k_momenta<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+        k_momenta<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
             gauge(U, c.g), alg(P, c.g), alg(F, c.g), c.g, (T)coef, (T)eps, F != nullptr);
     }
     void fields(const Ctx& c, void* U, const void* P, double eps) const override
@@ -121,19 +121,19 @@ public:
     }
     void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const override
     {
-        k_clover_deriv<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+        k_clover_deriv<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
             gauge(U, c.g), clov(R, c.g), alg(out, c.g), c.g, (T)scale);
     }
     void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam, void* Tloc,
                       double rho) const override
     {
-        k_stout_lambda<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+        k_stout_lambda<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
             gauge(U, c.g), gauge(Up, c.g), alg(Sigma, c.g), alg(Lam, c.g), full(Tloc, c.g), c.g, (T)rho);
     }
     void stout_recursion(const Ctx& c, const void* U, const void* Lam, const void* Tloc, void* Sigma,
                          double rho) const override
     {
-        k_stout_recursion<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(
+        k_stout_recursion<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
             gauge(U, c.g), alg(Lam, c.g), full(Tloc, c.g), alg(Sigma, c.g), c.g, (T)rho);
     }
 };

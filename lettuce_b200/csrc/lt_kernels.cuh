@@ -9,6 +9,24 @@ namespace lt {
 
 constexpr int kThreads = 128;
 constexpr int kRedThreads = 256;
+
+// Minimum resident blocks per SM requested from ptxas for the hot kernels (caps registers
+// per thread); tuned per arithmetic type on B200, overridable at build time.
+#ifndef LT_MINB_SWEEP_F32
+#define LT_MINB_SWEEP_F32 1
+#endif
+#ifndef LT_MINB_SWEEP_F64
+#define LT_MINB_SWEEP_F64 1
+#endif
+#ifndef LT_MINB_LINK_F32
+#define LT_MINB_LINK_F32 1
+#endif
+#ifndef LT_MINB_LINK_F64
+#define LT_MINB_LINK_F64 1
+#endif
+template <typename T> struct MinBlocks;
+template <> struct MinBlocks<float> { static constexpr int sweep = LT_MINB_SWEEP_F32, link = LT_MINB_LINK_F32; };
+template <> struct MinBlocks<double> { static constexpr int sweep = LT_MINB_SWEEP_F64, link = LT_MINB_LINK_F64; };
 constexpr double kPi = 3.14159265358979323846;
 
 // ---------------------------------------------------------------- reductions
@@ -52,6 +70,18 @@ __global__ void k_reduce_final(const double* __restrict__ partials, int nblk, do
     if (threadIdx.x == 0) out[blockIdx.x] = r;
 }
 
+// Link-parallel stencil kernels: a block of 128 threads covers the four directions of 32
+// consecutive sites (warp w = direction w), so every plane load of a warp is coalesced and
+// the neighbour links of a site block are shared through L1/L2 by all four directions.
+constexpr int kSitesPerBlock = 32;
+
+LT_D bool link_of_thread(const Geom& g, int& mu, int& x)
+{
+    mu = threadIdx.x >> 5;
+    x = blockIdx.x * kSitesPerBlock + (threadIdx.x & 31);
+    return x < g.V;
+}
+
 // ---------------------------------------------------------------- staple
 // Rectangular<1>::StaplePlaq (actions/gauge/rectangular_action.hpp:104-184):
 //   sum_{nu != mu} U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag + U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu)
@@ -69,8 +99,26 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
         if (nu == mu) continue;
         const int inu = i + step_up(g, nu, c[nu]);
         const int ind = i + step_dn(g, nu, c[nu]);
-        M3<T> up = mul_nd(mul(U.ld(nu, par, i >> 1), U.ld(mu, op, inu >> 1)), U.ld(nu, op, imu >> 1));
-        M3<T> dn = mul(mul_dn(U.ld(nu, op, ind >> 1), U.ld(mu, op, ind >> 1)), U.ld(nu, par, (ind + dmu) >> 1));
+        M3<T> up, dn;
+#ifdef LT_STAPLE_FULL_PRODUCTS
+        if (false)
+#else
+        if (NR == 2)
+#endif
+        {
+            // Two-row storage: each three-link path is an SU(3) matrix, so only its first two
+            // rows are multiplied out and the third is rebuilt (RestoreLastRow), which also
+            // spares the reconstruction of the leading factor of the upper path.
+            up = mul_nd_rows(mul_rows(U.ld_rows(nu, par, i >> 1), U.ld(mu, op, inu >> 1)), U.ld(nu, op, imu >> 1));
+            restore_last_row(up);
+            dn = mul_rows(mul_dn_rows(U.ld(nu, op, ind >> 1), U.ld(mu, op, ind >> 1)), U.ld(nu, par, (ind + dmu) >> 1));
+            restore_last_row(dn);
+        }
+        else
+        {
+            up = mul_nd(mul(U.ld(nu, par, i >> 1), U.ld(mu, op, inu >> 1)), U.ld(nu, op, imu >> 1));
+            dn = mul(mul_dn(U.ld(nu, op, ind >> 1), U.ld(mu, op, ind >> 1)), U.ld(nu, par, (ind + dmu) >> 1));
+        }
         acc = acc + (up + dn);
     }
     return acc;
@@ -239,9 +287,8 @@ __global__ void __launch_bounds__(kRedThreads) k_plaquette(Gauge<T, NR> U, Geom 
 template <typename T, int NR>
 __global__ void k_staple_aos(Gauge<T, NR> U, Geom g, double* __restrict__ aos)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * g.V) return;
-    int mu = t / g.V, x = t - mu * g.V;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
@@ -268,7 +315,7 @@ template <typename T> LT_D S2<T> or_su2(const S2<T>& A)
 }
 
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
+__global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.vh) return;
@@ -382,7 +429,7 @@ template <> struct HB<float>
 
 // HeatbathKernel::operator() (updates/heatbath.hpp:110-129) for one (mu, parity) sub-sweep
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads) k_heatbath(Gauge<T, NR> U, Geom g, int mu, int par, T prefactor,
+__global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_heatbath(Gauge<T, NR> U, Geom g, int mu, int par, T prefactor,
                                                        uint64_t counter, uint32_t k0, uint32_t k1, int max_iter)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -393,12 +440,13 @@ __global__ void __launch_bounds__(kThreads) k_heatbath(Gauge<T, NR> U, Geom g, i
     M3<T> u = U.ld(mu, par, s);
     M3<T> w = mul_nd(u, st);
     const uint32_t link = (uint32_t)(4 * i + mu);
-#pragma unroll 1
+    // unrolled so that the subgroup rows are compile-time indices (keeps u and w in registers)
+#pragma unroll
     for (int sg = 0; sg < 3; ++sg)
     {
         S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter);
         embed_lmul(h, sg, u);
-        embed_lmul(h, sg, w);
+        if (sg < 2) embed_lmul(h, sg, w);
     }
     gram_schmidt(u);
     U.st(mu, par, s, u);
@@ -411,12 +459,11 @@ __global__ void __launch_bounds__(kThreads) k_heatbath(Gauge<T, NR> U, Geom g, i
 // reading U from Uin and writing Uout (ping-pong), so all staples see the pre-stage field
 // exactly as the reference's separate Z and field sweeps do.
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
+__global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
                                                          T c_old, T c_new, T c_exp, int read_z, int write_z)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * g.V) return;
-    int mu = t / g.V, x = t - mu * g.V;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
@@ -444,11 +491,10 @@ __global__ void __launch_bounds__(kThreads) k_flow_stage(Gauge<T, NR> Uin, Gauge
 // ---------------------------------------------------------------- stout smearing
 // StoutSmearing4D (smearing/stout_smearing.hpp:29-57): U' = exp(rho Algebra(st U^dag)) U, Gram-Schmidt
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho)
+__global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * g.V) return;
-    int mu = t / g.V, x = t - mu * g.V;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
@@ -542,11 +588,10 @@ __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> U, Geom
 // HMC momentum kick P += eps * (beta/6 Algebra(st U^dag) + F)  (updates/hmc_gauge.hpp:450-464,
 // updates/hmc_metadynamics.hpp:441-459).  With P = null the force itself is written to F_out.
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads) k_momenta(Gauge<T, NR> U, Alg<T> P, Alg<T> F, Geom g, T coef, T eps, int use_f)
+__global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_momenta(Gauge<T, NR> U, Alg<T> P, Alg<T> F, Geom g, T coef, T eps, int use_f)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * g.V) return;
-    int mu = t / g.V, x = t - mu * g.V;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
@@ -690,9 +735,8 @@ LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const
 template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads) k_clover_deriv(Gauge<T, NR> U, Clov<T> R, Alg<T> out, Geom g, T scale)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * g.V) return;
-    int mu = t / g.V, x = t - mu * g.V;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
@@ -727,9 +771,8 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads) k_stout_lambda(Gauge<T, NR> U, Gauge<T, NR> Up, Alg<T> Sigma, Alg<T> Lam,
                                                            Full<T> Tloc, Geom g, T rho)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * g.V) return;
-    int mu = t / g.V, x = t - mu * g.V;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
@@ -776,9 +819,8 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Alg<T> Lam, Full<T> Tloc, Alg<T> Sigma,
                                                               Geom g, T rho)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 4 * g.V) return;
-    int mu = t / g.V, x = t - mu * g.V;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);

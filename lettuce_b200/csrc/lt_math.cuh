@@ -138,6 +138,71 @@ template <typename T> LT_HD M3<T> mul_dd(const M3<T>& a, const M3<T>& b)
     return r;
 }
 
+// Rows 0 and 1 only of A * B, A * B^dagger and A^dagger * B (row 2 of the result is left
+// unset); used where the product is an SU(3) matrix whose third row is rebuilt afterwards.
+template <typename T> LT_HD M3<T> mul_rows(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            T re = a.e[i][0].r * b.e[0][j].r - a.e[i][0].i * b.e[0][j].i;
+            T im = a.e[i][0].r * b.e[0][j].i + a.e[i][0].i * b.e[0][j].r;
+#pragma unroll
+            for (int k = 1; k < 3; ++k)
+            {
+                re += a.e[i][k].r * b.e[k][j].r - a.e[i][k].i * b.e[k][j].i;
+                im += a.e[i][k].r * b.e[k][j].i + a.e[i][k].i * b.e[k][j].r;
+            }
+            r.e[i][j] = mkc<T>(re, im);
+        }
+    return r;
+}
+
+template <typename T> LT_HD M3<T> mul_nd_rows(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            T re = a.e[i][0].r * b.e[j][0].r + a.e[i][0].i * b.e[j][0].i;
+            T im = a.e[i][0].i * b.e[j][0].r - a.e[i][0].r * b.e[j][0].i;
+#pragma unroll
+            for (int k = 1; k < 3; ++k)
+            {
+                re += a.e[i][k].r * b.e[j][k].r + a.e[i][k].i * b.e[j][k].i;
+                im += a.e[i][k].i * b.e[j][k].r - a.e[i][k].r * b.e[j][k].i;
+            }
+            r.e[i][j] = mkc<T>(re, im);
+        }
+    return r;
+}
+
+template <typename T> LT_HD M3<T> mul_dn_rows(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            T re = a.e[0][i].r * b.e[0][j].r + a.e[0][i].i * b.e[0][j].i;
+            T im = a.e[0][i].r * b.e[0][j].i - a.e[0][i].i * b.e[0][j].r;
+#pragma unroll
+            for (int k = 1; k < 3; ++k)
+            {
+                re += a.e[k][i].r * b.e[k][j].r + a.e[k][i].i * b.e[k][j].i;
+                im += a.e[k][i].r * b.e[k][j].i - a.e[k][i].i * b.e[k][j].r;
+            }
+            r.e[i][j] = mkc<T>(re, im);
+        }
+    return r;
+}
+
 template <typename T> LT_HD M3<T> adj(const M3<T>& a)
 {
     M3<T> r;
@@ -470,8 +535,38 @@ template <typename T> LT_D M3<T> exp_from(const ExpScalars& e, const M3<T>& Q, c
     return r;
 }
 
+// exp(iQ) = f0 + f1 Q + f2 Q^2 from the power series of exp reduced with Cayley-Hamilton,
+// Q^3 = c1 Q + c0 (c0 = det Q = tr Q^3 / 3, c1 = tr Q^2 / 2): with Q^n = a_n + b_n Q + c_n Q^2,
+// (a, b, c)_{n+1} = (c_n c0, a_n + c_n c1, b_n).  Valid when the spectral radius bound
+// sqrt(2 c1) is at most 1; N terms then leave a truncation error below 1/(N+1)!.
+// Same exponential as the closed form of SU3::exp (math/su3_exp.hpp:419-432) to rounding,
+// without its acos/sincos chain.
+template <int N> LT_D void exp_series(double c0, double c1, cx<double>& f0, cx<double>& f1, cx<double>& f2)
+{
+    double a = 1.0, b = 0.0, c = 0.0;   // scaled: (a_n, b_n, c_n) / n!
+    double f0r = 0.0, f0i = 0.0, f1r = 0.0, f1i = 0.0, f2r = 0.0, f2i = 0.0;
+#pragma unroll
+    for (int n = 0; n <= N; ++n)
+    {
+        // i^n = 1, i, -1, -i
+        const int ph = n & 3;
+        const double sr = ph == 0 ? 1.0 : (ph == 2 ? -1.0 : 0.0);
+        const double si = ph == 1 ? 1.0 : (ph == 3 ? -1.0 : 0.0);
+        f0r += sr * a; f0i += si * a;
+        f1r += sr * b; f1i += si * b;
+        f2r += sr * c; f2i += si * c;
+        const double inv = 1.0 / (double)(n + 1);
+        const double na = c * c0 * inv, nb = (a + c * c1) * inv, nc = b * inv;
+        a = na; b = nb; c = nc;
+    }
+    f0 = mkc(f0r, f0i);
+    f1 = mkc(f1r, f1i);
+    f2 = mkc(f2r, f2i);
+}
+
 // exp(c X) for X traceless anti-Hermitian: SU3::exp(-i c X) (gradient_flow.hpp:276,
-// hmc_gauge.hpp:516, stout_smearing.hpp:52)
+// hmc_gauge.hpp:516, stout_smearing.hpp:52).  Small arguments (every flow and HMC step)
+// take the Cayley-Hamilton-reduced series; larger ones the closed form of ExpConstants.
 template <typename T> LT_D M3<T> exp_ah(const M3<T>& X, T c)
 {
     // Q = -i c X is Hermitian traceless
@@ -481,6 +576,31 @@ template <typename T> LT_D M3<T> exp_ah(const M3<T>& X, T c)
 #pragma unroll
         for (int j = 0; j < 3; ++j) Q.e[i][j] = mkc<T>(c * X.e[i][j].i, -c * X.e[i][j].r);
     M3<T> Q2 = mul(Q, Q);
+    double c1 = 0.5 * ((double)Q2.e[0][0].r + (double)Q2.e[1][1].r + (double)Q2.e[2][2].r);
+    if (2.0 * c1 <= 1.0)
+    {
+        double c0 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                c0 += (double)Q.e[i][k].r * (double)Q2.e[k][i].r - (double)Q.e[i][k].i * (double)Q2.e[k][i].i;
+        c0 *= 1.0 / 3.0;
+        cx<double> f0, f1, f2;
+        // 1/19! = 8e-18 (FP64 links); 1/12! = 2e-9 (FP32 links)
+        if (sizeof(T) == 8) exp_series<18>(c0, c1, f0, f1, f2);
+        else exp_series<11>(c0, c1, f0, f1, f2);
+        const cx<T> g0 = cvt<T>(f0), g1 = cvt<T>(f1), g2 = cvt<T>(f2);
+        M3<T> r;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) r.e[i][j] = g1 * Q.e[i][j] + g2 * Q2.e[i][j];
+        r.e[0][0] = r.e[0][0] + g0;
+        r.e[1][1] = r.e[1][1] + g0;
+        r.e[2][2] = r.e[2][2] + g0;
+        return r;
+    }
     ExpScalars e = exp_scalars(Q, Q2);
     return exp_from(e, Q, Q2);
 }
