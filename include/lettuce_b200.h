@@ -108,6 +108,31 @@ int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, u
 int lt_update_sweeps(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed,
                      uint64_t* counter);
 
+/* ---- ensembles: independent chains and tempering streams ------------------------------ */
+typedef struct lt_ensemble lt_ensemble;
+/* n lattices (any even extents, one storage format) advanced together, lattice k at
+ * coupling betas[k] with the heatbath stream keyed seed + k.  The reference runs one lattice
+ * per process; this packs many into each launch (see lt_ensemble_sweeps). */
+int lt_ensemble_create(lt_lattice* const* lattices, const double* betas, int n, uint64_t seed, lt_ensemble** out);
+int lt_ensemble_destroy(lt_ensemble* e);
+/* n_sweep rounds of (n_hb heatbath + n_or overrelaxation) sweeps on every lattice, one
+ * launch per (mu, parity) sub-sweep covering all lattices, the round captured once as a
+ * CUDA graph and replayed.  reverse != 0 runs the round's sub-sweeps in reverse order (for
+ * a reversible mixture of both orders).  *counter advances by n_sweep * n_hb as in
+ * lt_heatbath_sweeps. */
+int lt_ensemble_sweeps(lt_ensemble* e, int n_sweep, int n_hb, int n_or, int reverse, uint64_t* counter);
+/* Time 64-, 128- and 256-thread blocks for the batched heatbath and overrelaxation on a
+ * scratch copy of the links (the chains are not advanced) and keep the fastest. */
+int lt_ensemble_autotune(lt_ensemble* e, int* threads_hb, int* threads_or);
+/* Fix the block sizes (64, 128 or 256 threads). */
+int lt_ensemble_set_block(lt_ensemble* e, int threads_hb, int threads_or);
+/* Tempering exchange between streams a and b sampling exp(-S - scale V(Q)) with CVs q_a, q_b
+ * (generalises MetadynamicsTemperingKernel::operator(), updates/tempering.hpp:51-72):
+ * accepted when u <= exp(-dE), dE = (scale_a - scale_b)(V(q_b) - V(q_a)); on acceptance the
+ * link storage of a and b is swapped (lt_swap). */
+int lt_tempering_swap(lt_lattice* a, lt_lattice* b, const lt_bias* bias, double scale_a, double scale_b, double q_a,
+                      double q_b, double u, int* accepted, double* dE_out);
+
 /* ---- smearing ------------------------------------------------------------------------ */
 /* GradientFlowKernel<RK3>::operator() (smearing/gradient_flow.hpp:120-168, :339-345):
  * out = in flowed by n_step RK3 steps of size eps.  in == out continues in place
@@ -117,6 +142,14 @@ int lt_flow_rk3(lt_lattice* in, lt_lattice* out, double eps, int n_step);
  * density after steps every, 2*every, ..., n_meas*every (SU3_main.cpp:150-163). */
 int lt_flow_rk3_measure(lt_lattice* in, lt_lattice* out, double eps, int n_meas, int every,
                         double* plaq_out, double* q_out, double* e_out);
+/* Scale setting: flow `in` into `out` (RK3, step eps) until t^2 E(t) reaches `target`
+ * (0.3 defines t0), E the clover energy density measured after every step as the driver
+ * measures it (SU3_main.cpp:128-141).  t0 is linearly interpolated between the two steps
+ * around the crossing; q_out (may be NULL) receives Q at the last step taken.  Fails with
+ * LT_ERR_STATE if the target is not reached within max_steps.  No counterpart in the
+ * reference (it measures at fixed flow times only). */
+int lt_flow_t0(lt_lattice* in, lt_lattice* out, double eps, double target, int max_steps, double* t0_out,
+               double* q_out);
 /* n steps of StoutSmearing4D (smearing/stout_smearing.hpp:29-57); in == out allowed. */
 int lt_stout(lt_lattice* in, lt_lattice* out, double rho, int n);
 

@@ -51,8 +51,15 @@ SIGNATURES = {
     "lt_overrelax_sweeps": (_i, [_vp, _i]),
     "lt_heatbath_sweeps": (_i, [_vp, _d, _i, _u64, _pu64]),
     "lt_update_sweeps": (_i, [_vp, _d, _i, _i, _i, _u64, _pu64]),
+    "lt_ensemble_create": (_i, [_vp, _dp, _i, _u64, C.POINTER(_vp)]),
+    "lt_ensemble_destroy": (_i, [_vp]),
+    "lt_ensemble_sweeps": (_i, [_vp, _i, _i, _i, _i, _pu64]),
+    "lt_ensemble_autotune": (_i, [_vp, _pi, _pi]),
+    "lt_ensemble_set_block": (_i, [_vp, _i, _i]),
+    "lt_tempering_swap": (_i, [_vp, _vp, _vp, _d, _d, _d, _d, _d, _pi, _pd]),
     "lt_flow_rk3": (_i, [_vp, _vp, _d, _i]),
     "lt_flow_rk3_measure": (_i, [_vp, _vp, _d, _i, _i, _vp, _vp, _vp]),
+    "lt_flow_t0": (_i, [_vp, _vp, _d, _d, _i, _pd, _pd]),
     "lt_stout": (_i, [_vp, _vp, _d, _i]),
     "lt_gauge_force": (_i, [_vp, _d, _dp]),
     "lt_set_momenta": (_i, [_vp, _dp]),

@@ -239,6 +239,13 @@ class GradientFlowKernel:
                                         int(every), p.ctypes.data, q.ctypes.data, e.ctypes.data))
         return p, q, e
 
+    def FlowToT0(self, target: float = 0.3, max_steps: int = 100000) -> tuple[float, float]:
+        """Flow U_unflowed into U_flowed until t^2 E = target; returns (t0, Q at the last step)."""
+        t0, q = C.c_double(), C.c_double()
+        check(lib().lt_flow_t0(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, float(target),
+                               int(max_steps), C.byref(t0), C.byref(q)))
+        return t0.value, q.value
+
     def SetEpsilon(self, eps: float) -> None:
         self.epsilon = float(eps)
 
@@ -388,6 +395,48 @@ class HMCMetaDKernel(HMCKernel):
         return ho.value, hn.value
 
 
+class Ensemble:
+    """Lattices of any even extents (one storage format) advanced together: one launch per
+    (mu, parity) sub-sweep over all of them, rounds replayed as CUDA graphs."""
+
+    def __init__(self, lattices, betas, seed: int = 1):
+        self.lattices = list(lattices)
+        arr = (C.c_void_p * len(self.lattices))(*[g.handle.value for g in self.lattices])
+        b = np.ascontiguousarray(betas, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib().lt_ensemble_create(C.cast(arr, C.c_void_p), b, len(self.lattices), C.c_uint64(seed), C.byref(h)))
+        self._h = h
+        self.counter = C.c_uint64(0)
+
+    def __del__(self):
+        try:
+            if self._h.value:
+                lib().lt_ensemble_destroy(self._h)
+        except Exception:
+            pass
+
+    def sweeps(self, n_sweep: int, n_hb: int = 1, n_or: int = 4, reverse: bool = False) -> None:
+        check(lib().lt_ensemble_sweeps(self._h, int(n_sweep), int(n_hb), int(n_or), int(bool(reverse)),
+                                       C.byref(self.counter)))
+
+    def autotune(self) -> tuple[int, int]:
+        a, b = C.c_int(), C.c_int()
+        check(lib().lt_ensemble_autotune(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_block(self, threads_hb: int, threads_or: int) -> None:
+        check(lib().lt_ensemble_set_block(self._h, int(threads_hb), int(threads_or)))
+
+
+def TemperingSwap(a: GaugeField, b: GaugeField, bias: MetaBiasPotential, scale_a: float, scale_b: float,
+                  q_a: float, q_b: float, u: float) -> tuple[bool, float]:
+    """Generalised MetadynamicsTemperingKernel swap (updates/tempering.hpp:51-72)."""
+    acc, dE = C.c_int(), C.c_double()
+    check(lib().lt_tempering_swap(a.handle, b.handle, bias.handle, float(scale_a), float(scale_b), float(q_a),
+                                  float(q_b), float(u), C.byref(acc), C.byref(dE)))
+    return bool(acc.value), dE.value
+
+
 def CloverDerivative(U: GaugeField) -> np.ndarray:
     """CloverDerivative for every link (observables/clover.hpp:279-321)."""
     out = np.empty((U.Volume(), 4, 3, 3, 2))
@@ -398,4 +447,5 @@ def CloverDerivative(U: GaugeField) -> np.ndarray:
 __all__ = ["GaugeField", "Swap", "haar_links", "PlaquetteSum", "TopChargeClover", "EnergyDensityClover",
            "CloverObservables", "Staples", "WilsonAction", "HeatbathKernel", "OverrelaxationSubgroupKernel",
            "Iterator", "UpdateSweeps", "RK3", "GradientFlowKernel", "StoutSmearing4D", "StoutSmearingN",
-           "MetaBiasPotential", "HMCKernel", "HMCMetaDKernel", "CloverDerivative", "LettuceError"]
+           "MetaBiasPotential", "HMCKernel", "HMCMetaDKernel", "CloverDerivative", "LettuceError", "Ensemble",
+           "TemperingSwap"]

@@ -56,6 +56,12 @@ public:
     virtual void fields(const Ctx& c, void* U, const void* P, double eps) const = 0;
     virtual void random_momenta(const Ctx& c, void* P, uint64_t counter, uint64_t seed) const = 0;
 
+    // One (mu, parity) sub-sweep of heatbath (op 0) or overrelaxation (op 1) over a batch of
+    // lattices described by the device array desc (LatDesc[n_lat]); sel picks 64/128/256
+    // threads per block and n_blocks is the batch's block count for that size.
+    virtual void batch_sweep(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int sel, int op, int mu,
+                             int par, const uint64_t* counter, int max_iter) const = 0;
+
     virtual void clover_R(const Ctx& c, const void* U, void* R) const = 0;
     virtual void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const = 0;
     virtual void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam,

@@ -7,9 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "lettuce_b200.h"
-#include "lt_backend.h"
-#include "lt_host.h"
+#include "lt_handle.h"
 
 namespace lt {
 
@@ -21,7 +19,7 @@ int set_error(int code, const char* msg)
     return code;
 }
 
-static int cuda_error(cudaError_t e, const char* what)
+int cuda_error(cudaError_t e, const char* what)
 {
     std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
     g_last_error = m;
@@ -29,52 +27,6 @@ static int cuda_error(cudaError_t e, const char* what)
 }
 
 } // namespace lt
-
-#define LT_CK(call)                                                  \
-    do {                                                             \
-        cudaError_t e_ = (call);                                     \
-        if (e_ != cudaSuccess) return lt::cuda_error(e_, #call);     \
-    } while (0)
-
-#define LT_TRY(call)                                                 \
-    do {                                                             \
-        int r_ = (call);                                             \
-        if (r_ != LT_OK) return r_;                                  \
-    } while (0)
-
-struct lt_lattice
-{
-    int ext[4];
-    int prec;
-    int device;
-    lt::Geom g;
-    const lt::Backend* be;
-    cudaStream_t stream = nullptr;
-    void* U = nullptr;       // links
-    void* U2 = nullptr;      // ping-pong partner for flow / stout
-    void* Z = nullptr;       // flow Z (algebra)
-    void* P = nullptr;       // HMC momenta (algebra)
-    void* F = nullptr;       // metadynamics force / Sigma (algebra)
-    void* Ubak = nullptr;    // HMC backup of the links
-    void* R = nullptr;       // clover planes
-    void* Lam = nullptr;     // Lambda (algebra)
-    void* Tloc = nullptr;    // link-local recursion term (full matrix)
-    std::vector<void*> levels;   // smeared levels 1..n of the MetaD chain
-    double* partials = nullptr;
-    double* results = nullptr;
-    double* h_results = nullptr; // pinned
-    double* d_aos = nullptr;     // staging buffer for host transfers (reference layout)
-
-    lt::Ctx ctx() const
-    {
-        lt::Ctx c;
-        c.g = g;
-        c.stream = stream;
-        c.partials = partials;
-        c.results = results;
-        return c;
-    }
-};
 
 namespace {
 
@@ -604,6 +556,32 @@ int lt_flow_rk3_measure(lt_lattice* in, lt_lattice* out, double eps, int n_meas,
             LT_TRY(clover_q_e(out, out->U, q_out ? &q_out[m] : nullptr, e_out ? &e_out[m] : nullptr));
     }
     return LT_OK;
+}
+
+int lt_flow_t0(lt_lattice* in, lt_lattice* out, double eps, double target, int max_steps, double* t0_out,
+               double* q_out)
+{
+    LT_TRY(check_h(in, "lt_flow_t0"));
+    LT_TRY(check_h(out, "lt_flow_t0"));
+    if (!t0_out || !(eps > 0.0) || max_steps < 1) return lt::set_error(LT_ERR_ARG, "lt_flow_t0: bad arguments");
+    LT_TRY(lt_copy(out, in));
+    double t_prev = 0.0, y_prev = 0.0, q = 0.0, e = 0.0;
+    for (int k = 1; k <= max_steps; ++k)
+    {
+        LT_TRY(flow_steps(out, eps, 1));
+        LT_TRY(clover_q_e(out, out->U, &q, &e));
+        const double t = k * eps, y = t * t * e;
+        if (y >= target)
+        {
+            *t0_out = k == 1 ? t : t_prev + (target - y_prev) / (y - y_prev) * (t - t_prev);
+            if (q_out) *q_out = q;
+            return LT_OK;
+        }
+        t_prev = t;
+        y_prev = y;
+    }
+    if (q_out) *q_out = q;
+    return lt::set_error(LT_ERR_STATE, "lt_flow_t0: t^2 E did not reach the target within max_steps");
 }
 
 int lt_stout(lt_lattice* in, lt_lattice* out, double rho, int n)

@@ -1,0 +1,59 @@
+// The lattice handle behind the C ABI's opaque lt_lattice, shared by the translation units
+// that implement the ABI (lt_capi.cu, lt_ensemble.cu).
+#pragma once
+#include <vector>
+
+#include "lettuce_b200.h"
+#include "lt_backend.h"
+#include "lt_host.h"
+
+namespace lt {
+// Records a CUDA error as this thread's last error; returns LT_ERR_NOMEM or LT_ERR_CUDA.
+int cuda_error(cudaError_t e, const char* what);
+} // namespace lt
+
+#define LT_CK(call)                                                  \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return lt::cuda_error(e_, #call);     \
+    } while (0)
+
+#define LT_TRY(call)                                                 \
+    do {                                                             \
+        int r_ = (call);                                             \
+        if (r_ != LT_OK) return r_;                                  \
+    } while (0)
+
+struct lt_lattice
+{
+    int ext[4];
+    int prec;
+    int device;
+    lt::Geom g;
+    const lt::Backend* be;
+    cudaStream_t stream = nullptr;
+    void* U = nullptr;       // links
+    void* U2 = nullptr;      // ping-pong partner for flow / stout
+    void* Z = nullptr;       // flow Z (algebra)
+    void* P = nullptr;       // HMC momenta (algebra)
+    void* F = nullptr;       // metadynamics force / Sigma (algebra)
+    void* Ubak = nullptr;    // HMC backup of the links
+    void* R = nullptr;       // clover planes
+    void* Lam = nullptr;     // Lambda (algebra)
+    void* Tloc = nullptr;    // link-local recursion term (full matrix)
+    std::vector<void*> levels;   // smeared levels 1..n of the MetaD chain
+    double* partials = nullptr;
+    double* results = nullptr;
+    double* h_results = nullptr; // pinned
+    double* d_aos = nullptr;     // staging buffer for host transfers (reference layout)
+
+    lt::Ctx ctx() const
+    {
+        lt::Ctx c;
+        c.g = g;
+        c.stream = stream;
+        c.partials = partials;
+        c.results = results;
+        return c;
+    }
+};

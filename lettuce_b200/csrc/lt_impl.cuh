@@ -115,6 +115,25 @@ public:
                                                                                (uint32_t)seed, (uint32_t)(seed >> 32));
     }
 
+    template <int SEL>
+    static void batch_launch(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int op, int mu, int par,
+                             const uint64_t* counter, int max_iter)
+    {
+        const LatDesc* d = static_cast<const LatDesc*>(desc);
+        if (op == 0)
+            k_batch_sweep<T, NR, SEL, 0><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter);
+        else
+            k_batch_sweep<T, NR, SEL, 1><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter);
+    }
+
+    void batch_sweep(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int sel, int op, int mu, int par,
+                     const uint64_t* counter, int max_iter) const override
+    {
+        if (sel == 0) batch_launch<0>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
+        else if (sel == 1) batch_launch<1>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
+        else batch_launch<2>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
+    }
+
     void clover_R(const Ctx& c, const void* U, void* R) const override
     {
         k_clover_R<T, NR><<<nblocks(6LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), clov(R, c.g), c.g);

@@ -13,10 +13,10 @@ constexpr int kRedThreads = 256;
 // Minimum resident blocks per SM requested from ptxas for the hot kernels (caps registers
 // per thread); tuned per arithmetic type on B200, overridable at build time.
 #ifndef LT_MINB_SWEEP_F32
-#define LT_MINB_SWEEP_F32 1
+#define LT_MINB_SWEEP_F32 5
 #endif
 #ifndef LT_MINB_SWEEP_F64
-#define LT_MINB_SWEEP_F64 1
+#define LT_MINB_SWEEP_F64 3
 #endif
 #ifndef LT_MINB_LINK_F32
 #define LT_MINB_LINK_F32 1
@@ -315,10 +315,8 @@ template <typename T> LT_D S2<T> or_su2(const S2<T>& A)
 }
 
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
+LT_D void or_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= g.vh) return;
     int c[4];
     int i = site_coords(g, par, s, c);
     M3<T> st = staple(U, g, par, i, c, mu);
@@ -333,6 +331,14 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gau
     }
     gram_schmidt(u);
     U.st(mu, par, s, u);
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.vh) return;
+    or_update(U, g, mu, par, s);
 }
 
 // ---------------------------------------------------------------- heatbath
@@ -434,6 +440,13 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_heatbath(Gaug
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.vh) return;
+    hb_update(U, g, mu, par, s, prefactor, counter, k0, k1, max_iter);
+}
+
+template <typename T, int NR>
+LT_D void hb_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s, T prefactor, uint64_t counter,
+                    uint32_t k0, uint32_t k1, int max_iter)
+{
     int c[4];
     int i = site_coords(g, par, s, c);
     M3<T> st = staple(U, g, par, i, c, mu);
@@ -450,6 +463,64 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_heatbath(Gaug
     }
     gram_schmidt(u);
     U.st(mu, par, s, u);
+}
+
+// ---------------------------------------------------------------- batched sweeps
+// Many lattices of any even extents (one storage format) advanced by one launch per
+// (mu, parity) sub-sweep: each lattice owns a contiguous range of blocks, found by binary
+// search over the block offsets.  Small lattices (12^4 has 10,368 sites per parity) cannot
+// fill 148 SMs alone; packed together they do.
+struct LatDesc
+{
+    Geom g;
+    void* U;
+    double prefactor;   // 3 / beta of this lattice (heatbath.hpp:40)
+    uint32_t k0, k1;    // Philox key of this lattice
+    int blk_begin[3];   // first block of this lattice for blocks of 64, 128 and 256 threads
+};
+
+constexpr int kBatchBlocks[3] = { 64, 128, 256 };
+
+template <int SEL> LT_D int find_lattice(const LatDesc* __restrict__ d, int n, int b)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (d[mid].blk_begin[SEL] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Registers capped at the level tuned for the single-lattice sweeps (640 resident threads per
+// SM in FP32, 384 in FP64)
+template <typename T, int BLOCK> struct BatchMinBlocks
+{
+    static constexpr int value = (sizeof(T) == 4 ? 640 : 384) / BLOCK > 0 ? (sizeof(T) == 4 ? 640 : 384) / BLOCK : 1;
+};
+
+template <typename T, int NR, int SEL, int OP>   // OP: 0 heatbath, 1 overrelaxation
+__global__ void __launch_bounds__(kBatchBlocks[SEL], (BatchMinBlocks<T, kBatchBlocks[SEL]>::value))
+    k_batch_sweep(const LatDesc* __restrict__ d, int n, int mu, int par, const uint64_t* __restrict__ counter,
+                  int max_iter)
+{
+    constexpr int BLOCK = kBatchBlocks[SEL];
+    const int k = find_lattice<SEL>(d, n, blockIdx.x);
+    const Geom g = d[k].g;
+    const int s = (blockIdx.x - d[k].blk_begin[SEL]) * BLOCK + threadIdx.x;
+    if (s >= g.vh) return;
+    Gauge<T, NR> U;
+    U.p = (cx<T>*)d[k].U;
+    U.vh = g.vh;
+    if (OP == 0) hb_update(U, g, mu, par, s, (T)d[k].prefactor, *counter, d[k].k0, d[k].k1, max_iter);
+    else or_update(U, g, mu, par, s);
+}
+
+// Advances the device-side sweep counter (read by the heatbath inside captured graphs)
+template <int Unused = 0> __global__ void k_counter_add(uint64_t* c, uint64_t n)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *c += n;
 }
 
 // ---------------------------------------------------------------- gradient flow

@@ -55,153 +55,50 @@ template <typename T> LT_HD M3<T> unit3()
     return r;
 }
 
+// Matrix products with optional adjoints, (A^[dag] B^[dag])_ij, written as explicit FMA
+// chains: each complex term adds two fused multiply-adds to each running sum.  (A single
+// expression like `re += a*b - c*d` would cost a multiply, an FMA and an add per term,
+// since the compiler may not reassociate it.)  ROWS < 3 computes only the leading rows.
+template <bool DA, bool DB, int ROWS = 3, typename T> LT_HD M3<T> prod(const M3<T>& a, const M3<T>& b)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < ROWS; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            T re = 0, im = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                const T xr = DA ? a.e[k][i].r : a.e[i][k].r;
+                const T xi = DA ? -a.e[k][i].i : a.e[i][k].i;
+                const T yr = DB ? b.e[j][k].r : b.e[k][j].r;
+                const T yi = DB ? -b.e[j][k].i : b.e[k][j].i;
+                re += xr * yr;
+                re -= xi * yi;
+                im += xr * yi;
+                im += xi * yr;
+            }
+            r.e[i][j] = mkc<T>(re, im);
+        }
+    return r;
+}
+
 // A * B
-template <typename T> LT_HD M3<T> mul(const M3<T>& a, const M3<T>& b)
-{
-    M3<T> r;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            T re = a.e[i][0].r * b.e[0][j].r - a.e[i][0].i * b.e[0][j].i;
-            T im = a.e[i][0].r * b.e[0][j].i + a.e[i][0].i * b.e[0][j].r;
-#pragma unroll
-            for (int k = 1; k < 3; ++k)
-            {
-                re += a.e[i][k].r * b.e[k][j].r - a.e[i][k].i * b.e[k][j].i;
-                im += a.e[i][k].r * b.e[k][j].i + a.e[i][k].i * b.e[k][j].r;
-            }
-            r.e[i][j] = mkc<T>(re, im);
-        }
-    return r;
-}
-
+template <typename T> LT_HD M3<T> mul(const M3<T>& a, const M3<T>& b) { return prod<false, false>(a, b); }
 // A * B^dagger
-template <typename T> LT_HD M3<T> mul_nd(const M3<T>& a, const M3<T>& b)
-{
-    M3<T> r;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            T re = a.e[i][0].r * b.e[j][0].r + a.e[i][0].i * b.e[j][0].i;
-            T im = a.e[i][0].i * b.e[j][0].r - a.e[i][0].r * b.e[j][0].i;
-#pragma unroll
-            for (int k = 1; k < 3; ++k)
-            {
-                re += a.e[i][k].r * b.e[j][k].r + a.e[i][k].i * b.e[j][k].i;
-                im += a.e[i][k].i * b.e[j][k].r - a.e[i][k].r * b.e[j][k].i;
-            }
-            r.e[i][j] = mkc<T>(re, im);
-        }
-    return r;
-}
-
+template <typename T> LT_HD M3<T> mul_nd(const M3<T>& a, const M3<T>& b) { return prod<false, true>(a, b); }
 // A^dagger * B
-template <typename T> LT_HD M3<T> mul_dn(const M3<T>& a, const M3<T>& b)
-{
-    M3<T> r;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            T re = a.e[0][i].r * b.e[0][j].r + a.e[0][i].i * b.e[0][j].i;
-            T im = a.e[0][i].r * b.e[0][j].i - a.e[0][i].i * b.e[0][j].r;
-#pragma unroll
-            for (int k = 1; k < 3; ++k)
-            {
-                re += a.e[k][i].r * b.e[k][j].r + a.e[k][i].i * b.e[k][j].i;
-                im += a.e[k][i].r * b.e[k][j].i - a.e[k][i].i * b.e[k][j].r;
-            }
-            r.e[i][j] = mkc<T>(re, im);
-        }
-    return r;
-}
-
-// A^dagger * B^dagger = (B A)^dagger
-template <typename T> LT_HD M3<T> mul_dd(const M3<T>& a, const M3<T>& b)
-{
-    M3<T> r;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            cx<T> acc = conj(a.e[0][i]) * conj(b.e[j][0]);
-#pragma unroll
-            for (int k = 1; k < 3; ++k) acc = acc + conj(a.e[k][i]) * conj(b.e[j][k]);
-            r.e[i][j] = acc;
-        }
-    return r;
-}
+template <typename T> LT_HD M3<T> mul_dn(const M3<T>& a, const M3<T>& b) { return prod<true, false>(a, b); }
+// A^dagger * B^dagger
+template <typename T> LT_HD M3<T> mul_dd(const M3<T>& a, const M3<T>& b) { return prod<true, true>(a, b); }
 
 // Rows 0 and 1 only of A * B, A * B^dagger and A^dagger * B (row 2 of the result is left
 // unset); used where the product is an SU(3) matrix whose third row is rebuilt afterwards.
-template <typename T> LT_HD M3<T> mul_rows(const M3<T>& a, const M3<T>& b)
-{
-    M3<T> r;
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            T re = a.e[i][0].r * b.e[0][j].r - a.e[i][0].i * b.e[0][j].i;
-            T im = a.e[i][0].r * b.e[0][j].i + a.e[i][0].i * b.e[0][j].r;
-#pragma unroll
-            for (int k = 1; k < 3; ++k)
-            {
-                re += a.e[i][k].r * b.e[k][j].r - a.e[i][k].i * b.e[k][j].i;
-                im += a.e[i][k].r * b.e[k][j].i + a.e[i][k].i * b.e[k][j].r;
-            }
-            r.e[i][j] = mkc<T>(re, im);
-        }
-    return r;
-}
-
-template <typename T> LT_HD M3<T> mul_nd_rows(const M3<T>& a, const M3<T>& b)
-{
-    M3<T> r;
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            T re = a.e[i][0].r * b.e[j][0].r + a.e[i][0].i * b.e[j][0].i;
-            T im = a.e[i][0].i * b.e[j][0].r - a.e[i][0].r * b.e[j][0].i;
-#pragma unroll
-            for (int k = 1; k < 3; ++k)
-            {
-                re += a.e[i][k].r * b.e[j][k].r + a.e[i][k].i * b.e[j][k].i;
-                im += a.e[i][k].i * b.e[j][k].r - a.e[i][k].r * b.e[j][k].i;
-            }
-            r.e[i][j] = mkc<T>(re, im);
-        }
-    return r;
-}
-
-template <typename T> LT_HD M3<T> mul_dn_rows(const M3<T>& a, const M3<T>& b)
-{
-    M3<T> r;
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            T re = a.e[0][i].r * b.e[0][j].r + a.e[0][i].i * b.e[0][j].i;
-            T im = a.e[0][i].r * b.e[0][j].i - a.e[0][i].i * b.e[0][j].r;
-#pragma unroll
-            for (int k = 1; k < 3; ++k)
-            {
-                re += a.e[k][i].r * b.e[k][j].r + a.e[k][i].i * b.e[k][j].i;
-                im += a.e[k][i].r * b.e[k][j].i - a.e[k][i].i * b.e[k][j].r;
-            }
-            r.e[i][j] = mkc<T>(re, im);
-        }
-    return r;
-}
+template <typename T> LT_HD M3<T> mul_rows(const M3<T>& a, const M3<T>& b) { return prod<false, false, 2>(a, b); }
+template <typename T> LT_HD M3<T> mul_nd_rows(const M3<T>& a, const M3<T>& b) { return prod<false, true, 2>(a, b); }
+template <typename T> LT_HD M3<T> mul_dn_rows(const M3<T>& a, const M3<T>& b) { return prod<true, false, 2>(a, b); }
 
 template <typename T> LT_HD M3<T> adj(const M3<T>& a)
 {
@@ -256,7 +153,11 @@ template <typename T> LT_HD T retr_mul(const M3<T>& a, const M3<T>& b)
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) s += a.e[i][k].r * b.e[k][i].r - a.e[i][k].i * b.e[k][i].i;
+        for (int k = 0; k < 3; ++k)
+        {
+            s += a.e[i][k].r * b.e[k][i].r;
+            s -= a.e[i][k].i * b.e[k][i].i;
+        }
     return s;
 }
 
@@ -267,19 +168,29 @@ template <typename T> LT_HD T retr_nd(const M3<T>& a, const M3<T>& b)
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) s += a.e[i][j].r * b.e[i][j].r + a.e[i][j].i * b.e[i][j].i;
+        for (int j = 0; j < 3; ++j)
+        {
+            s += a.e[i][j].r * b.e[i][j].r;
+            s += a.e[i][j].i * b.e[i][j].i;
+        }
     return s;
 }
 
 // tr(A B) without forming the product
 template <typename T> LT_HD cx<T> tr_mul(const M3<T>& a, const M3<T>& b)
 {
-    cx<T> s = mkc<T>(0, 0);
+    T re = 0, im = 0;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) s = s + a.e[i][k] * b.e[k][i];
-    return s;
+        for (int k = 0; k < 3; ++k)
+        {
+            re += a.e[i][k].r * b.e[k][i].r;
+            re -= a.e[i][k].i * b.e[k][i].i;
+            im += a.e[i][k].r * b.e[k][i].i;
+            im += a.e[i][k].i * b.e[k][i].r;
+        }
+    return mkc<T>(re, im);
 }
 
 template <typename To, typename From> LT_HD M3<To> cvt(const M3<From>& a)
@@ -364,11 +275,39 @@ template <typename T> LT_HD M3<T> unpack_h(const A8<T>& x)
 
 // ---------------------------------------------------------------- reunitarisation
 // RestoreLastRow (math/su3.hpp:362-367): row 2 = conj(row 0 x row 1)
+// g1 a + g2 b as an FMA chain
+template <typename T> LT_HD cx<T> lincomb2(cx<T> g1, cx<T> a, cx<T> g2, cx<T> b)
+{
+    T re = g1.r * a.r;
+    re -= g1.i * a.i;
+    re += g2.r * b.r;
+    re -= g2.i * b.i;
+    T im = g1.r * a.i;
+    im += g1.i * a.r;
+    im += g2.r * b.i;
+    im += g2.i * b.r;
+    return mkc<T>(re, im);
+}
+
+// conj(p q - r s) as an FMA chain
+template <typename T> LT_HD cx<T> conj_cross(cx<T> p, cx<T> q, cx<T> r, cx<T> s)
+{
+    T re = p.r * q.r;
+    re -= p.i * q.i;
+    re -= r.r * s.r;
+    re += r.i * s.i;
+    T im = p.r * q.i;
+    im += p.i * q.r;
+    im -= r.r * s.i;
+    im -= r.i * s.r;
+    return mkc<T>(re, -im);
+}
+
 template <typename T> LT_HD void restore_last_row(M3<T>& a)
 {
-    a.e[2][0] = conj(a.e[0][1] * a.e[1][2] - a.e[0][2] * a.e[1][1]);
-    a.e[2][1] = conj(a.e[0][2] * a.e[1][0] - a.e[0][0] * a.e[1][2]);
-    a.e[2][2] = conj(a.e[0][0] * a.e[1][1] - a.e[0][1] * a.e[1][0]);
+    a.e[2][0] = conj_cross(a.e[0][1], a.e[1][2], a.e[0][2], a.e[1][1]);
+    a.e[2][1] = conj_cross(a.e[0][2], a.e[1][0], a.e[0][0], a.e[1][2]);
+    a.e[2][2] = conj_cross(a.e[0][0], a.e[1][1], a.e[0][1], a.e[1][0]);
 }
 
 template <typename T> LT_D T rsqrt_t(T x);
@@ -381,9 +320,25 @@ template <typename T> LT_D void gram_schmidt(M3<T>& a)
     T n0 = rsqrt_t<T>(norm2(a.e[0][0]) + norm2(a.e[0][1]) + norm2(a.e[0][2]));
 #pragma unroll
     for (int n = 0; n < 3; ++n) a.e[0][n] = n0 * a.e[0][n];
-    cx<T> psi = mulc(a.e[1][0], a.e[0][0]) + mulc(a.e[1][1], a.e[0][1]) + mulc(a.e[1][2], a.e[0][2]);
+    T pr = 0, pi = 0;   // psi = sum_n row1_n conj(row0_n)
 #pragma unroll
-    for (int n = 0; n < 3; ++n) a.e[1][n] = a.e[1][n] - psi * a.e[0][n];
+    for (int n = 0; n < 3; ++n)
+    {
+        pr += a.e[1][n].r * a.e[0][n].r;
+        pr += a.e[1][n].i * a.e[0][n].i;
+        pi += a.e[1][n].i * a.e[0][n].r;
+        pi -= a.e[1][n].r * a.e[0][n].i;
+    }
+#pragma unroll
+    for (int n = 0; n < 3; ++n)
+    {
+        T r = a.e[1][n].r, i = a.e[1][n].i;
+        r -= pr * a.e[0][n].r;
+        r += pi * a.e[0][n].i;
+        i -= pr * a.e[0][n].i;
+        i -= pi * a.e[0][n].r;
+        a.e[1][n] = mkc<T>(r, i);
+    }
     T n1 = rsqrt_t<T>(norm2(a.e[1][0]) + norm2(a.e[1][1]) + norm2(a.e[1][2]));
 #pragma unroll
     for (int n = 0; n < 3; ++n) a.e[1][n] = n1 * a.e[1][n];
@@ -424,9 +379,25 @@ template <typename T> LT_HD void embed_lmul(const S2<T>& m, int g, M3<T>& x)
 #pragma unroll
     for (int n = 0; n < 3; ++n)
     {
-        cx<T> xa = x.e[a][n], xb = x.e[b][n];
-        x.e[a][n] = m.e11 * xa + m.e12 * xb;
-        x.e[b][n] = conj(m.e11) * xb - conj(m.e12) * xa;
+        const cx<T> xa = x.e[a][n], xb = x.e[b][n];
+        // row a: e11 xa + e12 xb
+        T ar = m.e11.r * xa.r, ai = m.e11.r * xa.i;
+        ar -= m.e11.i * xa.i;
+        ai += m.e11.i * xa.r;
+        ar += m.e12.r * xb.r;
+        ai += m.e12.r * xb.i;
+        ar -= m.e12.i * xb.i;
+        ai += m.e12.i * xb.r;
+        // row b: conj(e11) xb - conj(e12) xa
+        T br = m.e11.r * xb.r, bi = m.e11.r * xb.i;
+        br += m.e11.i * xb.i;
+        bi -= m.e11.i * xb.r;
+        br -= m.e12.r * xa.r;
+        bi -= m.e12.r * xa.i;
+        br -= m.e12.i * xa.i;
+        bi += m.e12.i * xa.r;
+        x.e[a][n] = mkc<T>(ar, ai);
+        x.e[b][n] = mkc<T>(br, bi);
     }
 }
 
@@ -528,7 +499,7 @@ template <typename T> LT_D M3<T> exp_from(const ExpScalars& e, const M3<T>& Q, c
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) r.e[i][j] = f1 * Q.e[i][j] + f2 * Q2.e[i][j];
+        for (int j = 0; j < 3; ++j) r.e[i][j] = lincomb2(f1, Q.e[i][j], f2, Q2.e[i][j]);
     r.e[0][0] = r.e[0][0] + f0;
     r.e[1][1] = r.e[1][1] + f0;
     r.e[2][2] = r.e[2][2] + f0;
@@ -595,7 +566,7 @@ template <typename T> LT_D M3<T> exp_ah(const M3<T>& X, T c)
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) r.e[i][j] = g1 * Q.e[i][j] + g2 * Q2.e[i][j];
+            for (int j = 0; j < 3; ++j) r.e[i][j] = lincomb2(g1, Q.e[i][j], g2, Q2.e[i][j]);
         r.e[0][0] = r.e[0][0] + g0;
         r.e[1][1] = r.e[1][1] + g0;
         r.e[2][2] = r.e[2][2] + g0;

@@ -204,6 +204,15 @@ void ref_reset_prng()
     g_prng.reset();
 }
 
+// Reseed the per-link pcg64 streams (PRNG4D::SeedPRNG, random/prng_wrapper.hpp:154-157):
+// link i gets seed i + offset * (number of links), so chains with different offsets draw
+// independent streams (FIXED_SEED seeds link i with i, prng_wrapper.hpp:104-109).
+void ref_reseed(std::uint64_t offset)
+{
+    PRNG& p = prng();
+    for (std::size_t i = 0; i < kL; ++i) p.SeedPRNG(i, i + offset * kL);
+}
+
 // heatbath.hpp:30-130 driven by iterators.hpp:65-87; the per-link pcg64 streams persist
 // across calls until ref_reset_prng().
 void ref_hb_sweeps(double* links, double b, int n)

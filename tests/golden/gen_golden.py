@@ -136,23 +136,37 @@ def gen_bias() -> dict:
     return out
 
 
-def gen_chain() -> dict:
-    """Reference heatbath + overrelaxation chain at 8^4, beta = 6: plaquette history."""
+def gen_chain(n_chain: int = 4, n_therm: int = 300, n_meas: int = 2500) -> dict:
+    """Reference heatbath + overrelaxation chains at 8^4, beta = 6 (1 + 4 sweeps per round):
+    plaquette histories of n_chain chains with independent pcg64 streams and Haar starts."""
+    import ctypes as C
     ext = (8, 8, 8, 8)
     ref = Reference(ext)
-    ref.lib.ref_reset_prng()
-    U = haar_links_numpy(ext, 5)
-    U, p_therm = ref.hb_or_chain(U, BETA, 200, 1, 4)
-    U, p = ref.hb_or_chain(U, BETA, 1000, 1, 4)
+    ref.lib.ref_reseed.argtypes = [C.c_uint64]
     V = int(np.prod(ext))
-    return {"plaq_norm_therm": p_therm / V / 18.0, "plaq_norm": p / V / 18.0, "beta": np.array(BETA)}
+    hist = np.empty((n_chain, n_meas))
+    for c in range(n_chain):
+        ref.lib.ref_reset_prng()
+        ref.lib.ref_reseed(c + 1)
+        U = haar_links_numpy(ext, 5 + c)
+        U, _ = ref.hb_or_chain(U, BETA, n_therm, 1, 4)
+        U, p = ref.hb_or_chain(U, BETA, n_meas, 1, 4)
+        hist[c] = p / V / 18.0
+    return {"plaq_norm": hist, "n_therm": np.array(n_therm), "beta": np.array(BETA)}
 
 
 def main() -> int:
+    import argparse
     import subprocess
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", choices=["chain"], default=None, help="regenerate one fixture only")
+    a = ap.parse_args()
     root = os.path.dirname(os.path.dirname(HERE))
     subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "4x4x4x4",
                     "4x6x8x10", "8x8x8x8"], check=True)
+    if a.only == "chain":
+        np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
+        return 0
     np.savez_compressed(os.path.join(HERE, "ref_4x4x4x4.npz"), **gen_case((4, 4, 4, 4), 1, True))
     b = gen_case((4, 6, 8, 10), 2, False)
     del b["U"]   # regenerated from numpy's seeded generator; checksum kept

@@ -166,6 +166,24 @@ class TestSmearing:
         flow.Resume(5)
         assert rel_err(H.download().reshape(-1, 18)[golden4["links"]], golden4["flow10"]) < TOL
 
+    def test_flow_to_t0(self, therm8):
+        """t0 from t^2 E(t) = target: the step-by-step measurements (parity-checked above)
+        interpolated here must give the library's t0."""
+        ext = (8, 8, 8, 8)
+        eps, target = 0.02, 0.05
+        G, H = gpu(ext, therm8), lt.GaugeField(ext)
+        flow = lt.GradientFlowKernel(G, H, lt.RK3, None, eps)
+        t0, q = flow.FlowToT0(target, 2000)
+        n = int(np.ceil(t0 / eps)) + 1
+        _, _, e = flow.Measure(n, 1)
+        t = eps * np.arange(1, n + 1)
+        y = t * t * e
+        k = int(np.argmax(y >= target))
+        expect = t[k - 1] + (target - y[k - 1]) / (y[k] - y[k - 1]) * eps
+        assert t0 == pytest.approx(expect, rel=1e-12)
+        with pytest.raises(lt.LettuceError):
+            flow.FlowToT0(target, 2)
+
     def test_stout(self, oracle, golden4):
         ext = golden4["ext"]
         G, H = gpu(ext, golden4["U"]), lt.GaugeField(ext)
