@@ -95,6 +95,16 @@ int lt_energy_clover(lt_lattice* h, double* out);
 int lt_clover_observables(lt_lattice* h, double* q_out, double* e_out);
 /* WilsonAction::Staple for every link (rectangular_action.hpp:104-184), reference layout. */
 int lt_staples(lt_lattice* h, double* staples_out);
+/* Plaquette sum of a field that the caller already holds in device memory, in the reference
+ * layout double[V][4][3][3][2], written as one double to the caller's device pointer
+ * out_dev, on the caller's stream (NULL = default stream).  No counterpart in the reference:
+ * this entry point exists for callers that cannot allocate device memory at the call (code
+ * under stream capture, framework-managed memory pools, allocation-free timing loops).  It
+ * allocates nothing: its scratch is a fixed 128 KiB static device array (present on every
+ * GPU that loads the library), so volumes above 16,777,216 sites (64^4) are rejected with
+ * LT_ERR_ARG.  The first call on a device looks up that array's address (make it before
+ * any stream capture).  All calls share the array: calls that overlap on the GPU race. */
+int lt_plaquette_sum_noalloc(const double* links_dev, const int ext[4], double* out_dev, void* stream);
 
 /* ---- local updates: Iterator::Checkerboard (iterators/iterators.hpp:65-87) ------------- */
 /* n_sweep sweeps of OverrelaxationSubgroupKernel (updates/overrelaxation.hpp:68-117). */

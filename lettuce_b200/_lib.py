@@ -48,6 +48,7 @@ SIGNATURES = {
     "lt_energy_clover": (_i, [_vp, _pd]),
     "lt_clover_observables": (_i, [_vp, _pd, _pd]),
     "lt_staples": (_i, [_vp, _dp]),
+    "lt_plaquette_sum_noalloc": (_i, [_vp, _ip, _vp, _vp]),
     "lt_overrelax_sweeps": (_i, [_vp, _i]),
     "lt_heatbath_sweeps": (_i, [_vp, _d, _i, _u64, _pu64]),
     "lt_update_sweeps": (_i, [_vp, _d, _i, _i, _i, _u64, _pu64]),
