@@ -190,6 +190,67 @@ def run_reference(a):
     return 0
 
 
+# ---------------------------------------------------------------------------- secondary rates
+def secondary_rates(lt, torch, timed, prec):
+    """Rates of the other workloads, reported beside the headline:
+    * metadynamics force evaluations/s at 16^4 (4 stout steps rho = 0.12, FP32 links);
+    * tempering ensemble link updates/s: 8 streams of 12^4 plus 40 chains with extents drawn
+      from {8,...,16}^4, beta in [5.8, 6.2], one batched round (1 HB + 4 OR) per step;
+    * one 48^4 HMC trajectory (OMF2, tau = 1, 20 steps, FP32 links, FP64 dH)."""
+    import numpy as np
+    out = {}
+    try:
+        ext = (16,) * 4
+        G = lt.GaugeField(ext, "fp32")
+        G.SetToHaarRandom(3)
+        lt.UpdateSweeps(G, BETA, 5, 1, 4, SEED)
+        bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 10, 1000)
+        k = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(BETA), 1.0, 0.12, 4)
+        for _ in range(3):
+            k.CalculateTopologicalForce(dvdq=1.0, download=False)
+        ms = timed(G, lambda: k.CalculateTopologicalForce(dvdq=1.0, download=False), 10)
+        out["metad_force_evals_per_s_16^4_fp32"] = 10 / (ms / 1000.0)
+        del k, G
+    except Exception as e:   # report, never hide
+        out["metad_force_error"] = repr(e)
+    try:
+        rng = np.random.default_rng(4)
+        lats = [lt.GaugeField((12,) * 4, prec) for _ in range(8)]
+        betas = [BETA] * 8
+        for _ in range(40):
+            e = tuple(int(v) for v in rng.choice([8, 10, 12, 14, 16], 4))
+            lats.append(lt.GaugeField(e, prec))
+            betas.append(float(rng.uniform(5.8, 6.2)))
+        for j, g in enumerate(lats):
+            g.SetToHaarRandom(100 + j)
+        ens = lt.Ensemble(lats, betas, SEED)
+        out["ensemble_autotuned_threads"] = ens.autotune()
+        ens.sweeps(3, 1, 4)
+        n = 10
+        ms = timed(lats[0], lambda: ens.sweeps(n, 1, 4), 1)
+        upd = 5 * 4 * sum(g.Volume() for g in lats)
+        out["ensemble_link_updates_per_s"] = n * upd / (ms / 1000.0)
+        out["ensemble_lattices"] = len(lats)
+        del ens, lats
+    except Exception as e:
+        out["ensemble_error"] = repr(e)
+    try:
+        ext = (48,) * 4
+        G = lt.GaugeField(ext, "fp32")
+        G.SetToHaarRandom(5)
+        lt.UpdateSweeps(G, 6.3, 3, 1, 4, SEED)
+        hmc = lt.HMCKernel(G, lt.WilsonAction(6.3), 1.0, seed=7)
+        hmc(20, True)
+        t0 = time.perf_counter()
+        acc = hmc(20, True)
+        out["hmc_48^4_fp32_s_per_trajectory"] = time.perf_counter() - t0
+        out["hmc_48^4_dH"] = hmc.delta_H
+        del hmc, G
+    except Exception as e:
+        out["hmc_48_error"] = repr(e)
+    return out
+
+
 # ---------------------------------------------------------------------------- secondary workloads
 def run_secondary(a, lt, torch, ext, links, timed, barrier, max_over_ranks, world, rank, dist):
     """flow: one RK3 step (eps = 0.01) per step, flow steps/s.
@@ -376,6 +437,9 @@ def main():
         line["e2e"] = {"value": world * n_e2e * upd_per_step / dt, "unit": UNIT,
                        "h2d_bytes_per_step": int(therm.nbytes), "d2h_bytes_per_step": 8,
                        "path": "lt_upload_links + lt_update_sweeps + lt_plaquette_sum"}
+
+        # ---- the other configurations' rates (each bounded to a few seconds)
+        line["secondary"] = secondary_rates(lt, torch, timed, a.prec)
 
         # ---- CPU baseline on this host, rank 0, bounded sample
         if rank == 0:

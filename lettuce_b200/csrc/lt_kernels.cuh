@@ -24,9 +24,17 @@ constexpr int kRedThreads = 256;
 #ifndef LT_MINB_LINK_F64
 #define LT_MINB_LINK_F64 1
 #endif
+#ifndef LT_MINB_LINK_F32C
+#define LT_MINB_LINK_F32C 4
+#endif
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int sweep = LT_MINB_SWEEP_F32, link = LT_MINB_LINK_F32; };
 template <> struct MinBlocks<double> { static constexpr int sweep = LT_MINB_SWEEP_F64, link = LT_MINB_LINK_F64; };
+// link-parallel kernels: two-row FP32 storage has its own setting
+template <typename T, int NR> struct LinkMinBlocks
+{
+    static constexpr int value = (sizeof(T) == 4 && NR == 2) ? LT_MINB_LINK_F32C : MinBlocks<T>::link;
+};
 constexpr double kPi = 3.14159265358979323846;
 
 // ---------------------------------------------------------------- reductions
@@ -122,6 +130,23 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
         acc = acc + (up + dn);
     }
     return acc;
+}
+
+// exp(c X) U followed by GramSchmidt (gradient_flow.hpp:265-282, hmc_gauge.hpp:505-523,
+// stout_smearing.hpp:52-53).  With two-row storage only rows 0 and 1 are formed: the store
+// keeps only those and every load rebuilds the third.
+template <typename T, int NR> LT_D M3<T> exp_update(const M3<T>& X, T c, const M3<T>& u)
+{
+    const M3<T> e = exp_ah(X, c);
+    if (NR == 2)
+    {
+        M3<T> r = mul_rows(e, u);
+        gram_schmidt<T, false>(r);
+        return r;
+    }
+    M3<T> r = mul(e, u);
+    gram_schmidt(r);
+    return r;
 }
 
 // ---------------------------------------------------------------- layout conversion
@@ -266,15 +291,17 @@ __global__ void __launch_bounds__(kRedThreads) k_plaquette(Gauge<T, NR> U, Geom 
         for (int mu = 0; mu < 4; ++mu)
         {
             const int imu = i + step_up(g, mu, c[mu]);
-            M3<T> umu = U.ld(mu, par, s);
+            // products in FP64 whatever the storage: the action enters HMC's dH and the
+            // plaquette the FP32-vs-FP64 error budget, so only storage rounding remains
+            const M3<double> umu = cvt<double>(U.ld(mu, par, s));
 #pragma unroll
             for (int nu = mu + 1; nu < 4; ++nu)
             {
                 const int inu = i + step_up(g, nu, c[nu]);
                 // ReTr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag) = ReTr[(U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag]
-                M3<T> a = mul(umu, U.ld(nu, op, imu >> 1));
-                M3<T> b = mul(U.ld(nu, par, s), U.ld(mu, op, inu >> 1));
-                acc += (double)retr_nd(a, b);
+                M3<double> a = mul(umu, cvt<double>(U.ld(nu, op, imu >> 1)));
+                M3<double> b = mul(cvt<double>(U.ld(nu, par, s)), cvt<double>(U.ld(mu, op, inu >> 1)));
+                acc += retr_nd(a, b);
             }
         }
         k.add(acc);
@@ -530,7 +557,7 @@ template <int Unused = 0> __global__ void k_counter_add(uint64_t* c, uint64_t n)
 // reading U from Uin and writing Uout (ping-pong), so all staples see the pre-stage field
 // exactly as the reference's separate Z and field sweeps do.
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
+__global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
                                                          T c_old, T c_new, T c_exp, int read_z, int write_z)
 {
     int mu, x;
@@ -554,15 +581,13 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_flow_stage(Gau
         for (int k = 0; k < 8; ++k) z.a[k] = c_new * a.a[k];
     }
     if (write_z) Z.st(mu, par, s, z);
-    M3<T> un = mul(exp_ah(unpack_ah(z), c_exp), u);
-    gram_schmidt(un);
-    Uout.st(mu, par, s, un);
+    Uout.st(mu, par, s, exp_update<T, NR>(unpack_ah(z), c_exp, u));
 }
 
 // ---------------------------------------------------------------- stout smearing
 // StoutSmearing4D (smearing/stout_smearing.hpp:29-57): U' = exp(rho Algebra(st U^dag)) U, Gram-Schmidt
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho)
+__global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho)
 {
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
@@ -571,9 +596,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_stout(Gauge<T,
     int i = site_coords(g, par, s, c);
     M3<T> u = Uin.ld(mu, par, s);
     M3<T> st = staple(Uin, g, par, i, c, mu);
-    M3<T> un = mul(exp_ah(unpack_ah(algebra8(mul_nd(st, u))), rho), u);
-    gram_schmidt(un);
-    Uout.st(mu, par, s, un);
+    Uout.st(mu, par, s, exp_update<T, NR>(unpack_ah(algebra8(mul_nd(st, u))), rho, u));
 }
 
 // ---------------------------------------------------------------- clover observables
@@ -659,7 +682,7 @@ __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> U, Geom
 // HMC momentum kick P += eps * (beta/6 Algebra(st U^dag) + F)  (updates/hmc_gauge.hpp:450-464,
 // updates/hmc_metadynamics.hpp:441-459).  With P = null the force itself is written to F_out.
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T>::link) k_momenta(Gauge<T, NR> U, Alg<T> P, Alg<T> F, Geom g, T coef, T eps, int use_f)
+__global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_momenta(Gauge<T, NR> U, Alg<T> P, Alg<T> F, Geom g, T coef, T eps, int use_f)
 {
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
@@ -692,9 +715,7 @@ __global__ void __launch_bounds__(kThreads) k_fields(Gauge<T, NR> U, Alg<T> P, i
     int vh = U.vh;
     int plane = t / vh, s = t - plane * vh;
     int mu = plane >> 1, par = plane & 1;
-    M3<T> un = mul(exp_ah(unpack_ah(P.ld(mu, par, s)), eps), U.ld(mu, par, s));
-    gram_schmidt(un);
-    U.st(mu, par, s, un);
+    U.st(mu, par, s, exp_update<T, NR>(unpack_ah(P.ld(mu, par, s)), eps, U.ld(mu, par, s)));
 }
 
 // RandomMomentum (updates/hmc_gauge.hpp:400-428): P = 1/2 i phi_a lambda_a with eight

@@ -59,8 +59,74 @@ template <typename T> LT_HD M3<T> unit3()
 // chains: each complex term adds two fused multiply-adds to each running sum.  (A single
 // expression like `re += a*b - c*d` would cost a multiply, an FMA and an add per term,
 // since the compiler may not reassociate it.)  ROWS < 3 computes only the leading rows.
+#if defined(LT_FFMA2)
+// FP32 products on Blackwell's paired FP32 FMA (fma.rn.f32x2): a complex term
+// (re, im) += a * b is two paired FMAs, (a.r, a.r) * (b.r, b.i) + (-a.i, a.i) * (b.i, b.r),
+// in the same rounding order as the scalar chain below.
+LT_D unsigned long long pk2(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+LT_D void upk2(unsigned long long v, float& lo, float& hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+LT_D unsigned long long ffma2(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+template <bool DA, bool DB, int ROWS> LT_D M3<float> prod_f2(const M3<float>& a, const M3<float>& b)
+{
+    unsigned long long y[3][3], ys[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            const float yr = DB ? b.e[j][k].r : b.e[k][j].r;
+            const float yi = DB ? -b.e[j][k].i : b.e[k][j].i;
+            y[k][j] = pk2(yr, yi);
+            ys[k][j] = pk2(yi, yr);
+        }
+    M3<float> r;
+#pragma unroll
+    for (int i = 0; i < ROWS; ++i)
+    {
+        unsigned long long xr[3], xi[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            const float ar = DA ? a.e[k][i].r : a.e[i][k].r;
+            const float ai = DA ? -a.e[k][i].i : a.e[i][k].i;
+            xr[k] = pk2(ar, ar);
+            xi[k] = pk2(-ai, ai);
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            unsigned long long acc = 0ull;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                acc = ffma2(xr[k], y[k][j], acc);
+                acc = ffma2(xi[k], ys[k][j], acc);
+            }
+            upk2(acc, r.e[i][j].r, r.e[i][j].i);
+        }
+    }
+    return r;
+}
+#endif
+
 template <bool DA, bool DB, int ROWS = 3, typename T> LT_HD M3<T> prod(const M3<T>& a, const M3<T>& b)
 {
+#if defined(LT_FFMA2) && defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 4) return prod_f2<DA, DB, ROWS>(a, b);
+#endif
     M3<T> r;
 #pragma unroll
     for (int i = 0; i < ROWS; ++i)
@@ -314,8 +380,8 @@ template <typename T> LT_D T rsqrt_t(T x);
 template <> LT_D double rsqrt_t<double>(double x) { return 1.0 / sqrt(x); }
 template <> LT_D float rsqrt_t<float>(float x) { return 1.0f / sqrtf(x); }
 
-// GramSchmidt (math/su3.hpp:370-394)
-template <typename T> LT_D void gram_schmidt(M3<T>& a)
+// GramSchmidt (math/su3.hpp:370-394); RESTORE = false skips the third row (two-row storage)
+template <typename T, bool RESTORE = true> LT_D void gram_schmidt(M3<T>& a)
 {
     T n0 = rsqrt_t<T>(norm2(a.e[0][0]) + norm2(a.e[0][1]) + norm2(a.e[0][2]));
 #pragma unroll
@@ -342,7 +408,7 @@ template <typename T> LT_D void gram_schmidt(M3<T>& a)
     T n1 = rsqrt_t<T>(norm2(a.e[1][0]) + norm2(a.e[1][1]) + norm2(a.e[1][2]));
 #pragma unroll
     for (int n = 0; n < 3; ++n) a.e[1][n] = n1 * a.e[1][n];
-    restore_last_row(a);
+    if (RESTORE) restore_last_row(a);
 }
 
 // ---------------------------------------------------------------- SU(2) subgroups
@@ -512,22 +578,23 @@ template <typename T> LT_D M3<T> exp_from(const ExpScalars& e, const M3<T>& Q, c
 // sqrt(2 c1) is at most 1; N terms then leave a truncation error below 1/(N+1)!.
 // Same exponential as the closed form of SU3::exp (math/su3_exp.hpp:419-432) to rounding,
 // without its acos/sincos chain.
-template <int N> LT_D void exp_series(double c0, double c1, cx<double>& f0, cx<double>& f1, cx<double>& f2)
+template <int N, typename S> LT_D void exp_series(S c0, S c1, cx<S>& f0, cx<S>& f1, cx<S>& f2)
 {
-    double a = 1.0, b = 0.0, c = 0.0;   // scaled: (a_n, b_n, c_n) / n!
-    double f0r = 0.0, f0i = 0.0, f1r = 0.0, f1i = 0.0, f2r = 0.0, f2i = 0.0;
+    S a = 1, b = 0, c = 0;   // scaled: (a_n, b_n, c_n) / n!
+    S f0r = 0, f0i = 0, f1r = 0, f1i = 0, f2r = 0, f2i = 0;
 #pragma unroll
     for (int n = 0; n <= N; ++n)
     {
         // i^n = 1, i, -1, -i
-        const int ph = n & 3;
-        const double sr = ph == 0 ? 1.0 : (ph == 2 ? -1.0 : 0.0);
-        const double si = ph == 1 ? 1.0 : (ph == 3 ? -1.0 : 0.0);
-        f0r += sr * a; f0i += si * a;
-        f1r += sr * b; f1i += si * b;
-        f2r += sr * c; f2i += si * c;
-        const double inv = 1.0 / (double)(n + 1);
-        const double na = c * c0 * inv, nb = (a + c * c1) * inv, nc = b * inv;
+        switch (n & 3)
+        {
+            case 0: f0r += a; f1r += b; f2r += c; break;
+            case 1: f0i += a; f1i += b; f2i += c; break;
+            case 2: f0r -= a; f1r -= b; f2r -= c; break;
+            default: f0i -= a; f1i -= b; f2i -= c; break;
+        }
+        const S inv = (S)(1.0 / (double)(n + 1));
+        const S na = c * c0 * inv, nb = (a + c * c1) * inv, nc = b * inv;
         a = na; b = nb; c = nc;
     }
     f0 = mkc(f0r, f0i);
@@ -535,9 +602,35 @@ template <int N> LT_D void exp_series(double c0, double c1, cx<double>& f0, cx<d
     f2 = mkc(f2r, f2i);
 }
 
+// Q^2 of a Hermitian Q (upper triangle computed, lower mirrored)
+template <typename T> LT_D M3<T> herm_sq(const M3<T>& q)
+{
+    M3<T> r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = i; j < 3; ++j)
+        {
+            T re = 0, im = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                re += q.e[i][k].r * q.e[k][j].r;
+                re -= q.e[i][k].i * q.e[k][j].i;
+                im += q.e[i][k].r * q.e[k][j].i;
+                im += q.e[i][k].i * q.e[k][j].r;
+            }
+            r.e[i][j] = mkc<T>(re, i == j ? (T)0 : im);
+            if (j != i) r.e[j][i] = mkc<T>(re, -im);
+        }
+    return r;
+}
+
 // exp(c X) for X traceless anti-Hermitian: SU3::exp(-i c X) (gradient_flow.hpp:276,
 // hmc_gauge.hpp:516, stout_smearing.hpp:52).  Small arguments (every flow and HMC step)
-// take the Cayley-Hamilton-reduced series; larger ones the closed form of ExpConstants.
+// take the Cayley-Hamilton-reduced series in the link arithmetic type (19 terms in FP64:
+// 1/20! = 4e-19; 12 terms in FP32: 1/13! = 2e-10); larger ones the closed form of
+// ExpConstants with its scalar chain in FP64.
 template <typename T> LT_D M3<T> exp_ah(const M3<T>& X, T c)
 {
     // Q = -i c X is Hermitian traceless
@@ -546,22 +639,14 @@ template <typename T> LT_D M3<T> exp_ah(const M3<T>& X, T c)
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) Q.e[i][j] = mkc<T>(c * X.e[i][j].i, -c * X.e[i][j].r);
-    M3<T> Q2 = mul(Q, Q);
-    double c1 = 0.5 * ((double)Q2.e[0][0].r + (double)Q2.e[1][1].r + (double)Q2.e[2][2].r);
-    if (2.0 * c1 <= 1.0)
+    M3<T> Q2 = herm_sq(Q);
+    const T c1 = (T)0.5 * (Q2.e[0][0].r + Q2.e[1][1].r + Q2.e[2][2].r);
+    if (c1 <= (T)0.5)
     {
-        double c0 = 0.0;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                c0 += (double)Q.e[i][k].r * (double)Q2.e[k][i].r - (double)Q.e[i][k].i * (double)Q2.e[k][i].i;
-        c0 *= 1.0 / 3.0;
-        cx<double> f0, f1, f2;
-        // 1/19! = 8e-18 (FP64 links); 1/12! = 2e-9 (FP32 links)
-        if (sizeof(T) == 8) exp_series<18>(c0, c1, f0, f1, f2);
-        else exp_series<11>(c0, c1, f0, f1, f2);
-        const cx<T> g0 = cvt<T>(f0), g1 = cvt<T>(f1), g2 = cvt<T>(f2);
+        T c0 = retr_mul(Q, Q2) * (T)(1.0 / 3.0);
+        cx<T> g0, g1, g2;
+        if (sizeof(T) == 8) exp_series<18>(c0, c1, g0, g1, g2);
+        else exp_series<11>(c0, c1, g0, g1, g2);
         M3<T> r;
 #pragma unroll
         for (int i = 0; i < 3; ++i)

@@ -265,6 +265,31 @@ class TestMetaD:
         assert q == pytest.approx(qo, rel=1e-11, abs=1e-13)
         assert rel_err(F, Fo) < 1e-11
 
+    @pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("fp32", 1e-4)])
+    def test_metad_reversibility(self, therm8, prec, tol):
+        """ReversibilityTest of the MetaD kernel (updates/hmc_metadynamics.hpp:657-674)."""
+        G = gpu((8, 8, 8, 8), therm8, prec)
+        bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 10, 1000)
+        bias.GeneratePotentialFrom(lambda cv: 3.0 * np.sin(cv))
+        k = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(6.0), 1.0, 0.12, 4, seed=3)
+        k.RandomMomentum(0)
+        start = G.download()
+        ho, _ = k.Integrate(10)
+        k.SetMomenta(-k.GetMomenta())
+        _, hn = k.Integrate(10)
+        assert abs(hn - ho) < tol * abs(ho)
+        assert rel_err(G.download(), start) < (1e-9 if prec == "fp64" else 1e-4)
+
+    def test_metad_trajectories_accept_and_update_bias(self, therm8):
+        G = gpu((8, 8, 8, 8), therm8)
+        bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 10, 1000)
+        k = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(6.0), 1.0, 0.12, 4, seed=11)
+        acc = [k(10, True) for _ in range(4)]
+        assert sum(acc) >= 2
+        assert bias.grid().max() > 0.0   # the symmetric well-tempered deposits happened
+        assert np.allclose(bias.grid(), bias.grid()[::-1])   # symmetric updates
+        assert abs(k.cv) < 8
+
     def test_metad_omf2_against_reference(self, golden4):
         ext = golden4["ext"]
         G = gpu(ext, golden4["U"])

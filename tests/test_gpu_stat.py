@@ -101,13 +101,20 @@ def test_metad_force_finite_differences():
     k = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(6.0), 1.0, 0.12, 4)
     F, q0 = k.CalculateTopologicalForce(dvdq=1.0)
     F = F[..., 0] + 1j * F[..., 1]
+    # the same configuration on FP32 links (config 3 runs FP32 links with the FP64 bias)
+    links = G.download()
+    G32 = lt.GaugeField(ext, "fp32")
+    G32.upload(links)
+    k32 = lt.HMCMetaDKernel(G32, bias, lt.WilsonAction(6.0), 1.0, 0.12, 4)
+    F32, q32 = k32.CalculateTopologicalForce(dvdq=1.0)
+    F32 = F32[..., 0] + 1j * F32[..., 1]
+    assert q32 == pytest.approx(q0, abs=1e-5)
     rng = np.random.default_rng(7)
     h = 1e-4
-    worst_abs, worst_rel = 0.0, 0.0
+    worst = {"fp64": [0.0, 0.0], "fp32": [0.0, 0.0]}
     for link in rng.choice(4 * V, size=64, replace=False):
         site, mu = divmod(int(link), 4)
         U0 = G.get_link(site, mu)
-        adj = np.array([np.real(np.trace(GELL_MANN[a] @ (1j * F[site, mu]))) for a in range(8)])
         fd = np.empty(8)
         for a in range(8):
             G.set_link(site, mu, exp_lambda(a, h) @ U0)
@@ -116,6 +123,11 @@ def test_metad_force_finite_differences():
             qm = k.MetaCharge()
             fd[a] = 0.5 * (qp - qm) / h
         G.set_link(site, mu, U0)
-        worst_abs = max(worst_abs, np.abs(adj - fd).max())
-        worst_rel = max(worst_rel, np.abs(adj - fd).max() / max(np.abs(fd).max(), 1e-12))
-    assert worst_abs < 1e-6, (worst_abs, worst_rel)
+        for name, FF in (("fp64", F), ("fp32", F32)):
+            adj = np.array([np.real(np.trace(GELL_MANN[a] @ (1j * FF[site, mu]))) for a in range(8)])
+            d = np.abs(adj - fd).max()
+            worst[name][0] = max(worst[name][0], d)
+            worst[name][1] = max(worst[name][1], d / max(np.abs(fd).max(), 1e-12))
+    print("adjoint vs finite differences (max abs, max rel):", worst)
+    assert worst["fp64"][0] < 1e-6, worst
+    assert worst["fp32"][0] < 1e-6, worst
