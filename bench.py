@@ -29,13 +29,15 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from lettuce_b200 import bytes_model as bm  # noqa: E402
+
 METRIC = "link updates/s & flow steps/s at 32^4: FP32-bulk vs plain FP64 GPU, dP<=1e-6"
 UNIT = "link updates/s"
 BETA = 6.0
 SEED = 20251203
 N_HB, N_OR = 1, 4
 FLOW_EPS = 0.01
-BYTES_PER_LINK = {"fp64": 144, "fp32": 72, "fp32_12": 48}
+N_THERM = 100
 
 
 def parse():
@@ -58,6 +60,29 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def flow_roofline(torch, prec: str, volume: int, ms_step: float, ms_step64: float, hbm_peak: float) -> dict:
+    """RK3 flow step against both ceilings: algorithmic HBM bytes over the measured copy
+    bandwidth, and algorithmic flops over the nominal CUDA-core peak (SMs x lanes x 2 x the
+    measured maximum SM clock; 128 FP32 and 64 FP64 lanes per SM)."""
+    props = torch.cuda.get_device_properties(0)
+    mhz = 1965.0
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        mhz = float(json.load(open(p)).get("sm_max_mhz", mhz))
+    f32_peak = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+    f64_peak = f32_peak / 2
+    links = 4 * volume
+    out = {}
+    for name, pr, ms, fpk in (("bulk", prec, ms_step, f32_peak if prec != "fp64" else f64_peak),
+                              ("fp64", "fp64", ms_step64, f64_peak)):
+        gbs = bm.flow_step_bytes_per_link(pr) * links / (ms / 1000.0) / 1e9
+        tfl = bm.FLOPS["flow_step"] * links / (ms / 1000.0) / 1e12
+        out[name] = {"prec": pr, "ms_per_step": ms, "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak,
+                     "tflops": tfl, "alu_peak_tflops": fpk, "alu_frac": tfl / fpk}
+    out["alu_peak_source"] = "nominal CUDA-core peak at the measured max SM clock"
+    return out
 
 
 def ncu_traffic(kernel: str):
@@ -235,17 +260,32 @@ def secondary_rates(lt, torch, timed, prec):
     except Exception as e:
         out["ensemble_error"] = repr(e)
     try:
+        # 48^4 at beta = 6.3: Haar start, 200 rounds of 1 HB + 4 OR, two OMF2 trajectories
+        # (tau = 1, 20 steps, FP32 links, FP64 dH and accept), then Wilson flow to t0
+        # (t^2 E = 0.3) with clover Q and E at every step
         ext = (48,) * 4
         G = lt.GaugeField(ext, "fp32")
         G.SetToHaarRandom(5)
-        lt.UpdateSweeps(G, 6.3, 3, 1, 4, SEED)
+        t0 = time.perf_counter()
+        lt.UpdateSweeps(G, 6.3, 200, 1, 4, SEED)
+        G.synchronize()
+        out["hmc_48^4_therm_s_200_rounds"] = time.perf_counter() - t0
         hmc = lt.HMCKernel(G, lt.WilsonAction(6.3), 1.0, seed=7)
         hmc(20, True)
         t0 = time.perf_counter()
         acc = hmc(20, True)
         out["hmc_48^4_fp32_s_per_trajectory"] = time.perf_counter() - t0
-        out["hmc_48^4_dH"] = hmc.delta_H
-        del hmc, G
+        out["hmc_48^4_dH"] = [hmc.delta_H]
+        out["hmc_48^4_accepted"] = bool(acc)
+        del hmc
+        F = lt.GaugeField(ext, "fp32")
+        flow = lt.GradientFlowKernel(G, F, lt.RK3, None, FLOW_EPS)
+        t0 = time.perf_counter()
+        tt0, q = flow.FlowToT0(0.3)
+        out["flow_to_t0_48^4_s"] = time.perf_counter() - t0
+        out["t0_48^4_beta6.3"] = tt0
+        out["Q_at_t0_48^4"] = q
+        del F, G
     except Exception as e:
         out["hmc_48_error"] = repr(e)
     return out
@@ -365,8 +405,7 @@ def main():
     or_ms = timed(G, lambda: lt.Iterator.Checkerboard(lt.OverrelaxationSubgroupKernel(G), n_or), 1) / (8 * n_or)
     hb_ms = timed(G, lambda: lt.Iterator.Checkerboard(lt.HeatbathKernel(G, lt.WilsonAction(BETA), 5), 5), 1) / 40
     peak, peak_kind = peaks()
-    b = BYTES_PER_LINK[a.prec]
-    alg_bytes = 9 * b * (V // 2)                  # 9 link reads/writes per update, V/2 updates
+    alg_bytes = bm.sweep_launch_bytes(a.prec, V)   # 9 link reads/writes per update, V/2 updates
     achieved = alg_bytes / (or_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": ncu_traffic(f"k_overrelax<{a.prec}>"), "kernel": f"k_overrelax ({a.prec})",
@@ -382,25 +421,28 @@ def main():
             "config": {"workload": f"{a.size}^4 SU(3) Wilson beta={BETA}: {N_HB} heatbath + {N_OR} overrelaxation "
                                    f"sweeps per step, {a.prec} links",
                        "lattice": list(ext), "beta": BETA, "storage": a.prec,
-                       "l2": f"inputs larger than L2 ({G.Volume() * 4 * b / 1e6:.0f} MB of links per sweep)",
+                       "l2": f"inputs larger than L2 ({G.Volume() * 4 * bm.LINK_BYTES[a.prec] / 1e6:.0f} MB "
+                             "of links per sweep)",
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "clocks": clocks.summary(), "gpu_launches": launches}
 
     if not a.no_extras:
-        # ---- flow steps/s (FP32-bulk and FP64) and |dP| from identical configurations
+        # ---- 100 further rounds (the plain-vs-FP32 protocol's thermalisation), then the identical
+        # configuration flowed in FP32-bulk and in FP64 to t = 4, with P, Q and E at t = 1, 2, 3, 4
+        for _ in range(N_THERM):
+            sweep_round(G)
         therm = G.download()
         res = {}
+        n_flow = 10
         for prec in (a.prec, "fp64"):
             A, B = lt.GaugeField(ext, prec), lt.GaugeField(ext, prec)
             A.upload(therm)
             flow = lt.GradientFlowKernel(A, B, lt.RK3, None, FLOW_EPS)
             flow(2)
-            n_flow = 10
             t = timed(B, lambda: flow.Resume(n_flow), 1)
-            flow(100)                                   # t = 1.0 from the identical start
-            q, e = lt.CloverObservables(B)
-            res[prec] = {"flow_steps_per_s": n_flow / (t / 1000.0), "plaq_t1": lt.PlaquetteSum(B) / V / 18,
-                         "Q_t1": q, "E_t1": e}
+            p, q, e = flow.Measure(4, 100)
+            res[prec] = {"flow_steps_per_s": n_flow / (t / 1000.0), "flow_ms": t / n_flow,
+                         "plaq": p / V / 18, "Q": q, "E": e}
             # sweeps in this precision
             C = lt.GaugeField(ext, prec)
             C.upload(therm)
@@ -414,8 +456,17 @@ def main():
         line["fp32_over_fp64"] = {
             "link_updates": res[a.prec]["link_updates_per_s"] / res["fp64"]["link_updates_per_s"],
             "flow_steps": res[a.prec]["flow_steps_per_s"] / res["fp64"]["flow_steps_per_s"]}
-        line["dP_flow_t1"] = abs(res[a.prec]["plaq_t1"] - res["fp64"]["plaq_t1"])
-        line["dQ_flow_t1"] = abs(res[a.prec]["Q_t1"] - res["fp64"]["Q_t1"])
+        dP = [abs(x - y) for x, y in zip(res[a.prec]["plaq"], res["fp64"]["plaq"])]
+        dQ = [abs(x - y) for x, y in zip(res[a.prec]["Q"], res["fp64"]["Q"])]
+        line["flow_vs_fp64"] = {"t": [1.0, 2.0, 3.0, 4.0], "dP": dP, "dQ": dQ,
+                                "Q_fp64": [float(x) for x in res["fp64"]["Q"]],
+                                "t2E_fp64": [float(t * t * x) for t, x in zip((1, 2, 3, 4), res["fp64"]["E"])],
+                                "start": f"{N_THERM} further rounds after the timed steps"}
+        line["dP_flow_max"] = max(dP)
+        line["dQ_flow_max"] = max(dQ)
+        line["dP_flow_max_rel"] = max(d / abs(p) for d, p in zip(dP, res["fp64"]["plaq"]))
+        line["dQ_flow_max_rel"] = max(d / max(abs(q), 1.0) for d, q in zip(dQ, res["fp64"]["Q"]))
+        line["flow_roofline"] = flow_roofline(torch, a.prec, V, res[a.prec]["flow_ms"], res["fp64"]["flow_ms"], peak)
 
         # ---- e2e through the public API with host buffers: H2D of the step's links from pinned
         # memory, the sweep round, D2H of the plaquette

@@ -32,6 +32,7 @@ extern "C" {
 #define LT_ERR_NOMEM   3   /* device or host allocation failed                                */
 #define LT_ERR_STATE   4   /* operation not valid in the handle's current state              */
 #define LT_ERR_NUMERIC 5   /* non-finite value detected in a result                          */
+#define LT_ERR_IO      6   /* file cannot be opened, read or written, or has a malformed header */
 
 /* Storage format of the link field. */
 #define LT_PREC_FP64    0  /* 18 doubles per link (the reference's Matrix_SU3, defines.hpp:122)   */
@@ -79,6 +80,20 @@ int lt_set_haar_random(lt_lattice* h, uint64_t seed);
 int lt_synchronize(lt_lattice* h);
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 int lt_get_stream(const lt_lattice* h, void** stream_out);
+
+/* ---- status word ----------------------------------------------------------------------- */
+/* No counterpart in the reference, which has no error channel (its kernels are noexcept and
+ * the heatbath silently falls back to the unit matrix, updates/heatbath.hpp:72-76).  Each
+ * handle keeps a device status word; kernels set bits, the host reads them here. */
+#define LT_STATUS_NONFINITE 1u /* a link holds NaN or Inf (set by lt_check_links) */
+#define LT_STATUS_UNITARITY 2u /* a link has an entry of |U U^dag - 1| above 1e-4 (FP32) or 1e-10 (FP64) */
+#define LT_STATUS_HB_CAP 4u    /* a heatbath subgroup update hit the 10-retry cap and took the unit matrix */
+/* Reads the status word (synchronising the handle's stream); clear = 1 resets it to 0. */
+int lt_status_word(lt_lattice* h, uint32_t* word, int clear);
+/* Scans every link, sets LT_STATUS_NONFINITE / LT_STATUS_UNITARITY, and returns the largest
+ * entry of |U U^dag - 1| over the lattice (for FP32 storage: the reunitarisation error left
+ * by the Gram-Schmidt projection after every update). */
+int lt_check_links(lt_lattice* h, double* max_dev);
 
 /* ---- observables --------------------------------------------------------------------- */
 /* PlaquetteSum (observables/plaquette.hpp:26-43): sum over sites, mu<nu of ReTr P. */

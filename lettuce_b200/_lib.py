@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("LETTUCE_B200_LIB", os.path.join(HERE, "liblettuce_b200.so"))
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "lettuce_b200.h")
 
-LT_OK, LT_ERR_ARG, LT_ERR_CUDA, LT_ERR_NOMEM, LT_ERR_STATE, LT_ERR_NUMERIC = range(6)
+LT_OK, LT_ERR_ARG, LT_ERR_CUDA, LT_ERR_NOMEM, LT_ERR_STATE, LT_ERR_NUMERIC, LT_ERR_IO = range(7)
 PREC = {"fp64": 0, "fp32": 1, "fp32_12": 2}
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -42,6 +42,8 @@ SIGNATURES = {
     "lt_set_haar_random": (_i, [_vp, _u64]),
     "lt_synchronize": (_i, [_vp]),
     "lt_get_stream": (_i, [_vp, C.POINTER(_vp)]),
+    "lt_status_word": (_i, [_vp, C.POINTER(C.c_uint32), _i]),
+    "lt_check_links": (_i, [_vp, _pd]),
     "lt_plaquette_sum": (_i, [_vp, _pd]),
     "lt_wilson_action": (_i, [_vp, _d, _pd]),
     "lt_topcharge_clover": (_i, [_vp, _pd]),

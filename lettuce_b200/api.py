@@ -102,6 +102,18 @@ class GaugeField:
         check(lib().lt_get_stream(self._h, C.byref(s)))
         return int(s.value or 0)
 
+    def status_word(self, clear: bool = False) -> int:
+        """The device status word (STATUS_* bits); clear=True resets it."""
+        w = C.c_uint32()
+        check(lib().lt_status_word(self._h, C.byref(w), int(bool(clear))))
+        return w.value
+
+    def check_links(self) -> float:
+        """Largest entry of |U U^dag - 1| over all links; flags NaN/Inf and unitarity loss."""
+        d = C.c_double()
+        check(lib().lt_check_links(self._h, C.byref(d)))
+        return d.value
+
 
 def Swap(U1: GaugeField, U2: GaugeField) -> None:
     """Swap (lattice.hpp:238-246): exchanges the link storage."""
@@ -444,7 +456,10 @@ def CloverDerivative(U: GaugeField) -> np.ndarray:
     return out
 
 
-__all__ = ["GaugeField", "Swap", "haar_links", "PlaquetteSum", "TopChargeClover", "EnergyDensityClover",
+# Bits of GaugeField.status_word() (LT_STATUS_* of include/lettuce_b200.h)
+STATUS_NONFINITE, STATUS_UNITARITY, STATUS_HB_CAP = 1, 2, 4
+
+__all__ = ["STATUS_NONFINITE", "STATUS_UNITARITY", "STATUS_HB_CAP", "GaugeField", "Swap", "haar_links", "PlaquetteSum", "TopChargeClover", "EnergyDensityClover",
            "CloverObservables", "Staples", "WilsonAction", "HeatbathKernel", "OverrelaxationSubgroupKernel",
            "Iterator", "UpdateSweeps", "RK3", "GradientFlowKernel", "StoutSmearing4D", "StoutSmearingN",
            "MetaBiasPotential", "HMCKernel", "HMCMetaDKernel", "CloverDerivative", "LettuceError", "Ensemble",

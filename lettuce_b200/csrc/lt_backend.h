@@ -17,6 +17,7 @@ struct Ctx
     cudaStream_t stream;
     double* partials;   // kNumSlots * kRedBlocks doubles
     double* results;    // kNumSlots doubles
+    unsigned* status = nullptr;   // the handle's device status word (LT_STATUS_* bits)
 };
 
 constexpr int kNumSlots = 8;
@@ -44,6 +45,10 @@ public:
     virtual void plaquette(const Ctx& c, const void* U, int slot) const = 0;
     virtual void clover_obs(const Ctx& c, const void* U, int slot) const = 0;
     virtual void kinetic(const Ctx& c, const void* P, int slot) const = 0;
+
+    // link health: sets kStatusNonFinite / kStatusUnitarity (tolerance tol) in c.status and
+    // atomically maxes the float bits of the largest |U U^dag - 1| entry into *maxbits
+    virtual void check_links(const Ctx& c, const void* U, double tol, unsigned* maxbits) const = 0;
 
     virtual void overrelax(const Ctx& c, void* U, int mu, int par) const = 0;
     virtual void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter,

@@ -275,6 +275,9 @@ int lt_create(const int ext[4], int prec, lt_lattice** out)
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->partials, sizeof(double) * lt::kNumSlots * lt::kRedBlocks);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->results, sizeof(double) * lt::kNumSlots);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_results, sizeof(double) * lt::kNumSlots);
+    // status[0]: the status word; status[1]: scratch of lt_check_links; status[2]: of lt_load_bmw
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->status, 4 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->status, 0, 4 * sizeof(unsigned), h->stream);
     if (e != cudaSuccess)
     {
         int r = lt::cuda_error(e, "lt_create");
@@ -297,7 +300,8 @@ int lt_destroy(lt_lattice* h)
     if (!h) return LT_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void* bufs[] = { h->U, h->U2, h->Z, h->P, h->F, h->Ubak, h->R, h->Lam, h->Tloc, h->partials, h->results, h->d_aos };
+    void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,  h->R,
+                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status };
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (void* p : h->levels) cudaFree(p);
@@ -437,6 +441,39 @@ int lt_get_stream(const lt_lattice* h, void** stream_out)
     LT_TRY(check_h(h, "lt_get_stream"));
     if (!stream_out) return lt::set_error(LT_ERR_ARG, "lt_get_stream: null pointer");
     *stream_out = (void*)h->stream;
+    return LT_OK;
+}
+
+static_assert(LT_STATUS_NONFINITE == lt::kStatusNonFinite && LT_STATUS_UNITARITY == lt::kStatusUnitarity &&
+                  LT_STATUS_HB_CAP == lt::kStatusHbCap,
+              "status bits of the C ABI and the kernels differ");
+
+int lt_status_word(lt_lattice* h, uint32_t* word, int clear)
+{
+    LT_TRY(check_h(h, "lt_status_word"));
+    if (!word) return lt::set_error(LT_ERR_ARG, "lt_status_word: null pointer");
+    LT_CK(cudaMemcpyAsync(h->h_results, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    if (clear) LT_CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    unsigned w;
+    std::memcpy(&w, h->h_results, sizeof(w));
+    *word = w;
+    return LT_OK;
+}
+
+int lt_check_links(lt_lattice* h, double* max_dev)
+{
+    LT_TRY(check_h(h, "lt_check_links"));
+    unsigned* maxbits = h->status + 1;
+    LT_CK(cudaMemsetAsync(maxbits, 0, sizeof(unsigned), h->stream));
+    const double tol = h->be->real_bytes() == 8 ? 1e-10 : 1e-4;
+    h->be->check_links(h->ctx(), h->U, tol, maxbits);
+    LT_TRY(launched("lt_check_links"));
+    LT_CK(cudaMemcpyAsync(h->h_results, maxbits, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    float f;
+    std::memcpy(&f, h->h_results, sizeof(f));
+    if (max_dev) *max_dev = (double)f;
     return LT_OK;
 }
 

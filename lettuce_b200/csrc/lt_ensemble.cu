@@ -55,6 +55,7 @@ int refresh(lt_ensemble* e)
         d[k].g = h->g;
         d[k].U = h->U;
         d[k].prefactor = 3.0 / e->betas[k];
+        d[k].status = h->status;
         const uint64_t key = e->seed + (uint64_t)k;   // lattice k draws from the stream keyed seed + k
         d[k].k0 = (uint32_t)key;
         d[k].k1 = (uint32_t)(key >> 32);

@@ -23,6 +23,11 @@ namespace lt {
 // Reduction grid: 148 SMs x 8 blocks, fixed so that every reduction sums in the same order.
 constexpr int kRedBlocks = 1184;
 
+// Bits of a lattice handle's device status word (LT_STATUS_* of the C ABI)
+constexpr unsigned kStatusNonFinite = 1u;   // a link holds NaN or Inf
+constexpr unsigned kStatusUnitarity = 2u;   // max |U U^dag - 1| above the storage's tolerance
+constexpr unsigned kStatusHbCap = 4u;       // a heatbath subgroup update hit its iteration cap
+
 struct Geom
 {
     int n[4];       // Nt, Nx, Ny, Nz

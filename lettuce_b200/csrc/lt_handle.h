@@ -46,6 +46,7 @@ struct lt_lattice
     double* results = nullptr;
     double* h_results = nullptr; // pinned
     double* d_aos = nullptr;     // staging buffer for host transfers (reference layout)
+    unsigned* status = nullptr;  // device status word (lt_status_word) and scratch words
 
     lt::Ctx ctx() const
     {
@@ -54,6 +55,7 @@ struct lt_lattice
         c.stream = stream;
         c.partials = partials;
         c.results = results;
+        c.status = status;
         return c;
     }
 };

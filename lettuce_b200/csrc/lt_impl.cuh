@@ -7,6 +7,34 @@ namespace lt {
 
 inline int nblocks(long long n, int threads) { return (int)((n + threads - 1) / threads); }
 
+#ifndef LT_PDL
+#define LT_PDL 1
+#endif
+
+// Launch of a kernel that follows a dependent kernel on the same stream (sweeps, flow and
+// stout stages).  With LT_PDL the launch carries the programmatic stream-serialisation
+// attribute, so that its blocks are scheduled while the predecessor drains and wait in
+// pdl_wait() (lt_kernels.cuh) for its completion.
+template <typename... KArgs, typename... Args>
+inline void launch_chained(void (*k)(KArgs...), int grid, int block, cudaStream_t s, Args... args)
+{
+#if LT_PDL
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+#else
+    k<<<grid, block, 0, s>>>(static_cast<KArgs>(args)...);
+#endif
+}
+
 template <typename T, int NR> class BackendImpl final : public Backend
 {
     using G = Gauge<T, NR>;
@@ -79,24 +107,28 @@ public:
 
     void overrelax(const Ctx& c, void* U, int mu, int par) const override
     {
-        k_overrelax<T, NR><<<nblocks(c.g.vh, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), c.g, mu, par);
+        launch_chained(k_overrelax<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu, par);
     }
     void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter, uint64_t seed,
                   int max_iter) const override
     {
-        k_heatbath<T, NR><<<nblocks(c.g.vh, kThreads), kThreads, 0, c.stream>>>(
-            gauge(U, c.g), c.g, mu, par, (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter);
+        launch_chained(k_heatbath<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu, par,
+                       (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter, c.status);
+    }
+    void check_links(const Ctx& c, const void* U, double tol, unsigned* maxbits) const override
+    {
+        k_check_links<T, NR><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, tol, c.status, maxbits);
     }
     void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new, double c_exp,
                     int read_z, int write_z) const override
     {
-        k_flow_stage<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
-            gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z, write_z);
+        launch_chained(k_flow_stage<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
+                       gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z, write_z);
     }
     void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
     {
-        k_stout<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(gauge(Uin, c.g), gauge(Uout, c.g),
-                                                                                  c.g, (T)rho);
+        launch_chained(k_stout<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
+                       gauge(Uout, c.g), c.g, (T)rho);
     }
 
     void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const override

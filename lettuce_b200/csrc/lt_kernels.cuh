@@ -36,6 +36,15 @@ template <typename T, int NR> struct LinkMinBlocks
     static constexpr int value = (sizeof(T) == 4 && NR == 2) ? LT_MINB_LINK_F32C : MinBlocks<T>::link;
 };
 constexpr double kPi = 3.14159265358979323846;
+constexpr float kTwoPiF = 6.28318530717958648f;
+
+// Programmatic dependent launch (sm_90 and later): a kernel launched with the programmatic
+// stream-serialisation attribute may be scheduled while its predecessor on the stream still
+// drains, once every block of the predecessor has passed pdl_release(); it must pass
+// pdl_wait(), which returns when the predecessor has completed and its writes are visible,
+// before reading the predecessor's output.  Launched without the attribute, both are no-ops.
+LT_D void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+LT_D void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // ---------------------------------------------------------------- reductions
 // Kahan-compensated FP64 accumulation per thread, then a warp/block tree into one partial
@@ -310,6 +319,46 @@ __global__ void __launch_bounds__(kRedThreads) k_plaquette(Gauge<T, NR> U, Geom 
     if (threadIdx.x == 0) partials[blockIdx.x] = r;
 }
 
+// ---------------------------------------------------------------- link health
+// Scans every link: non-finite entries set kStatusNonFinite; the largest entry of
+// |U U^dag - 1| (products in FP64, third row rebuilt for two-row storage) goes to *maxbits as
+// the bits of a non-negative float (whose unsigned order is its numeric order), and a link
+// above tol sets kStatusUnitarity.
+template <typename T, int NR>
+__global__ void __launch_bounds__(kRedThreads) k_check_links(Gauge<T, NR> U, Geom g, double tol, unsigned* status,
+                                                              unsigned* maxbits)
+{
+    float dmax = 0.0f;
+    bool bad = false;
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < 4 * g.V; l += gridDim.x * blockDim.x)
+    {
+        const int pl = l / g.vh, s = l - pl * g.vh;
+        const M3<double> u = cvt<double>(U.ld(pl >> 1, pl & 1, s));
+        double d = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+            {
+                bad |= !isfinite(u.e[i][j].r) || !isfinite(u.e[i][j].i);
+                double re = i == j ? -1.0 : 0.0, im = 0.0;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    re += u.e[i][k].r * u.e[j][k].r + u.e[i][k].i * u.e[j][k].i;
+                    im += u.e[i][k].i * u.e[j][k].r - u.e[i][k].r * u.e[j][k].i;
+                }
+                d = fmax(d, fmax(fabs(re), fabs(im)));
+            }
+        if (d > tol) atomicOr(status, kStatusUnitarity);
+        dmax = fmaxf(dmax, (float)d);
+    }
+    if (bad) atomicOr(status, kStatusNonFinite);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxbits, __float_as_uint(dmax));
+}
+
 // ---------------------------------------------------------------- staple output (tests)
 template <typename T, int NR>
 __global__ void k_staple_aos(Gauge<T, NR> U, Geom g, double* __restrict__ aos)
@@ -341,13 +390,10 @@ template <typename T> LT_D S2<T> or_su2(const S2<T>& A)
     return s2_adj(s2_mul(V, V));
 }
 
-template <typename T, int NR>
-LT_D void or_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s)
+// The three subgroup reflections of u against its staple, then Gram-Schmidt (the third row
+// is not rebuilt for two-row storage, which does not keep it)
+template <typename T, int NR> LT_D void or_apply(M3<T>& u, const M3<T>& st)
 {
-    int c[4];
-    int i = site_coords(g, par, s, c);
-    M3<T> st = staple(U, g, par, i, c, mu);
-    M3<T> u = U.ld(mu, par, s);
     M3<T> w = mul_nd(u, st);   // U st^dag
 #pragma unroll
     for (int sg = 0; sg < 3; ++sg)
@@ -356,7 +402,17 @@ LT_D void or_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s
         embed_lmul(h, sg, u);
         if (sg < 2) embed_lmul(h, sg, w);
     }
-    gram_schmidt(u);
+    gram_schmidt<T, NR == 3>(u);
+}
+
+template <typename T, int NR>
+LT_D void or_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s)
+{
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    M3<T> st = staple(U, g, par, i, c, mu);
+    M3<T> u = U.ld(mu, par, s);
+    or_apply<T, NR>(u, st);
     U.st(mu, par, s, u);
 }
 
@@ -364,6 +420,8 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
+    pdl_release();
+    pdl_wait();
     if (s >= g.vh) return;
     or_update(U, g, mu, par, s);
 }
@@ -371,14 +429,15 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gau
 // ---------------------------------------------------------------- heatbath
 // HeatbathKernel::HeatbathSU2 (updates/heatbath.hpp:47-104): Kennedy-Pendleton /
 // Fabricius-Haan sampling of x0 with lambda^2 = -(prefactor/4)/sqrt(det A) (ln r1 + cos^2(2 pi r2) ln r3),
-// accept while r0^2 + lambda^2 < 1, at most max_iter+1 proposals, else the unit matrix.
+// accept while r0^2 + lambda^2 < 1, at most max_iter+1 proposals, else the unit matrix
+// (reported through `capped`; the kernel then sets kStatusHbCap in the handle's status word).
 // Random numbers: Philox4x32-10, counter {link, counter lo, counter hi, tag|subgroup|call}.
 template <typename T> struct HB;
 
 template <> struct HB<double>
 {
     LT_D static S2<double> su2(const S2<double>& A, double prefactor, uint32_t link, uint64_t counter,
-                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter)
+                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped)
     {
         double an = 1.0 / sqrt(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
@@ -394,6 +453,7 @@ template <> struct HB<double>
             lsq = -0.25 * prefactor * an * (log(r1) + x2 * x2 * log(r3));
             if (k > max_iter)
             {
+                capped = true;
                 S2<double> one;
                 one.e11 = mkc(1.0, 0.0);
                 one.e12 = mkc(0.0, 0.0);
@@ -418,10 +478,13 @@ template <> struct HB<double>
     }
 };
 
+// FP32: the special functions use the SFU approximations (__logf, __cosf, __sincosf, absolute
+// error about 1e-6 on these arguments), below the FP32 rounding of the rest of the update;
+// FP32 chains are validated statistically against the reference's chains.
 template <> struct HB<float>
 {
     LT_D static S2<float> su2(const S2<float>& A, float prefactor, uint32_t link, uint64_t counter,
-                               uint32_t sg, uint32_t k0, uint32_t k1, int max_iter)
+                               uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped)
     {
         float an = 1.0f / sqrtf(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
@@ -432,10 +495,11 @@ template <> struct HB<float>
             U4 a = philox4x32(link, c1, c2, tw | (uint32_t)k, k0, k1);
             float r1 = 1.0f - f01_from(a.x), r2 = 1.0f - f01_from(a.y);
             float r3 = 1.0f - f01_from(a.z), r0 = f01_from(a.w);
-            float x2 = cospif(2.0f * r2);
-            lsq = -0.25f * prefactor * an * (logf(r1) + x2 * x2 * logf(r3));
+            float x2 = __cosf(kTwoPiF * r2);
+            lsq = -0.25f * prefactor * an * (__logf(r1) + x2 * x2 * __logf(r3));
             if (k > max_iter)
             {
+                capped = true;
                 S2<float> one;
                 one.e11 = mkc(1.0f, 0.0f);
                 one.e12 = mkc(0.0f, 0.0f);
@@ -450,7 +514,7 @@ template <> struct HB<float>
         float ct = 1.0f - 2.0f * f01_from(d.y);
         float vn = ax * sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
         float sp, cp;
-        sincospif(2.0f * phi, &sp, &cp);
+        __sincosf(kTwoPiF * phi, &sp, &cp);
         S2<float> x, V;
         x.e11 = mkc(x0, vn * cp);
         x.e12 = mkc(vn * sp, ax * ct);
@@ -463,16 +527,19 @@ template <> struct HB<float>
 // HeatbathKernel::operator() (updates/heatbath.hpp:110-129) for one (mu, parity) sub-sweep
 template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_heatbath(Gauge<T, NR> U, Geom g, int mu, int par, T prefactor,
-                                                       uint64_t counter, uint32_t k0, uint32_t k1, int max_iter)
+                                                       uint64_t counter, uint32_t k0, uint32_t k1, int max_iter,
+                                                       unsigned* status)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
+    pdl_release();
+    pdl_wait();
     if (s >= g.vh) return;
-    hb_update(U, g, mu, par, s, prefactor, counter, k0, k1, max_iter);
+    hb_update(U, g, mu, par, s, prefactor, counter, k0, k1, max_iter, status);
 }
 
 template <typename T, int NR>
 LT_D void hb_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s, T prefactor, uint64_t counter,
-                    uint32_t k0, uint32_t k1, int max_iter)
+                    uint32_t k0, uint32_t k1, int max_iter, unsigned* status)
 {
     int c[4];
     int i = site_coords(g, par, s, c);
@@ -480,16 +547,18 @@ LT_D void hb_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s
     M3<T> u = U.ld(mu, par, s);
     M3<T> w = mul_nd(u, st);
     const uint32_t link = (uint32_t)(4 * i + mu);
+    bool capped = false;
     // unrolled so that the subgroup rows are compile-time indices (keeps u and w in registers)
 #pragma unroll
     for (int sg = 0; sg < 3; ++sg)
     {
-        S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter);
+        S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter, capped);
         embed_lmul(h, sg, u);
         if (sg < 2) embed_lmul(h, sg, w);
     }
-    gram_schmidt(u);
+    gram_schmidt<T, NR == 3>(u);
     U.st(mu, par, s, u);
+    if (capped && status) atomicOr(status, kStatusHbCap);
 }
 
 // ---------------------------------------------------------------- batched sweeps
@@ -504,6 +573,7 @@ struct LatDesc
     double prefactor;   // 3 / beta of this lattice (heatbath.hpp:40)
     uint32_t k0, k1;    // Philox key of this lattice
     int blk_begin[3];   // first block of this lattice for blocks of 64, 128 and 256 threads
+    unsigned* status;   // the lattice handle's status word
 };
 
 constexpr int kBatchBlocks[3] = { 64, 128, 256 };
@@ -540,7 +610,7 @@ __global__ void __launch_bounds__(kBatchBlocks[SEL], (BatchMinBlocks<T, kBatchBl
     Gauge<T, NR> U;
     U.p = (cx<T>*)d[k].U;
     U.vh = g.vh;
-    if (OP == 0) hb_update(U, g, mu, par, s, (T)d[k].prefactor, *counter, d[k].k0, d[k].k1, max_iter);
+    if (OP == 0) hb_update(U, g, mu, par, s, (T)d[k].prefactor, *counter, d[k].k0, d[k].k1, max_iter, d[k].status);
     else or_update(U, g, mu, par, s);
 }
 
@@ -560,6 +630,8 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
                                                          T c_old, T c_new, T c_exp, int read_z, int write_z)
 {
+    pdl_release();
+    pdl_wait();
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
@@ -589,6 +661,8 @@ __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_flo
 template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho)
 {
+    pdl_release();
+    pdl_wait();
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
@@ -600,20 +674,30 @@ __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_sto
 }
 
 // ---------------------------------------------------------------- clover observables
-// Four-leaf clover C_{mu nu}(x) (observables/clover.hpp:94-152, plaquette.hpp:82-114)
-template <typename T, int NR>
-LT_D M3<T> clover_leaves(const Gauge<T, NR>& U, const Geom& g, int par, int i, const int c[4], int mu, int nu)
+// Read-only view of a link field that widens every loaded link to FP64, so that measurements
+// (Q, E) run their products in FP64 whatever the storage.
+template <typename T, int NR> struct Widened
 {
+    Gauge<T, NR> U;
+    LT_D M3<double> ld(int mu, int par, int s) const { return cvt<double>(U.ld(mu, par, s)); }
+};
+
+// Four-leaf clover C_{mu nu}(x) (observables/clover.hpp:94-152, plaquette.hpp:82-114), in the
+// arithmetic type of the field view F (Gauge<T, NR> or Widened<T, NR>).
+template <typename F>
+LT_D auto clover_leaves(const F& U, const Geom& g, int par, int i, const int c[4], int mu, int nu)
+{
+    using M = decltype(U.ld(0, 0, 0));
     const int op = par ^ 1;
     const int dmu_p = step_up(g, mu, c[mu]), dmu_m = step_dn(g, mu, c[mu]);
     const int dnu_p = step_up(g, nu, c[nu]), dnu_m = step_dn(g, nu, c[nu]);
     const int s = i >> 1;
-    const M3<T> umu = U.ld(mu, par, s), unu = U.ld(nu, par, s);
+    const M umu = U.ld(mu, par, s), unu = U.ld(nu, par, s);
     const int imd = i + dmu_m, ind = i + dnu_m;
     // I:   U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
-    M3<T> leaf = mul_nd(mul(umu, U.ld(nu, op, (i + dmu_p) >> 1)), mul(unu, U.ld(mu, op, (i + dnu_p) >> 1)));
+    M leaf = mul_nd(mul(umu, U.ld(nu, op, (i + dmu_p) >> 1)), mul(unu, U.ld(mu, op, (i + dnu_p) >> 1)));
     // II:  U_nu(x) U_mu(x-mu+nu)^dag U_nu(x-mu)^dag U_mu(x-mu)
-    M3<T> umu_md = U.ld(mu, op, imd >> 1);
+    M umu_md = U.ld(mu, op, imd >> 1);
     acc(leaf, mul(mul_nd(unu, U.ld(mu, par, (imd + dnu_p) >> 1)), mul_dn(U.ld(nu, op, imd >> 1), umu_md)));
     // III: U_mu(x-mu)^dag U_nu(x-mu-nu)^dag U_mu(x-mu-nu) U_nu(x-nu)
     const int imdnd = imd + dnu_m;
@@ -627,10 +711,13 @@ LT_D M3<T> clover_leaves(const Gauge<T, NR>& U, const Geom& g, int par, int i, c
 // (observables/topological_charge.hpp:97-200) and energy density
 // e(x) = sum_{mu<nu} ReTr(F~^2), F~ = Traceless(-i/8 (C - C^dag))
 // (observables/field_strength_tensor.hpp:28-66, :107-134, :154-175).
+// Products run in FP64 for every storage: the cancellations in F = C - C^dag of a smooth
+// (flowed) field would otherwise lift FP32 rounding of the leaves into Q and E.
 template <typename T, int NR>
-__global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> U, Geom g, double* __restrict__ partials)
+__global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> Ust, Geom g, double* __restrict__ partials)
 {
     __shared__ double sh[32];
+    const Widened<T, NR> U{ Ust };
     Kahan kq, ke;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.V; x += gridDim.x * blockDim.x)
     {
@@ -642,16 +729,16 @@ __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> U, Geom
 #pragma unroll 1
         for (int p = 0; p < 3; ++p)
         {
-            M3<T> ca = clover_leaves(U, g, par, i, c, pairs[p][0], pairs[p][1]);
-            M3<T> cb = clover_leaves(U, g, par, i, c, pairs[p][2], pairs[p][3]);
-            M3<T> fa = ca - adj(ca), fb = cb - adj(cb);
+            M3<double> ca = clover_leaves(U, g, par, i, c, pairs[p][0], pairs[p][1]);
+            M3<double> cb = clover_leaves(U, g, par, i, c, pairs[p][2], pairs[p][3]);
+            M3<double> fa = ca - adj(ca), fb = cb - adj(cb);
             double t = (double)retr_mul(fa, fb);
             q += p == 1 ? -t : t;
             // energy: F~ = -i/8 F made traceless; ReTr(F~^2) = sum |F~_ij|^2 (Hermitian)
 #pragma unroll
             for (int h = 0; h < 2; ++h)
             {
-                const M3<T>& f = h == 0 ? fa : fb;
+                const M3<double>& f = h == 0 ? fa : fb;
                 double tr3 = ((double)f.e[0][0].i + (double)f.e[1][1].i + (double)f.e[2][2].i) / 3.0;
                 double acc2 = 0.0;
 #pragma unroll

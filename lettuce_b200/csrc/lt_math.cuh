@@ -59,74 +59,8 @@ template <typename T> LT_HD M3<T> unit3()
 // chains: each complex term adds two fused multiply-adds to each running sum.  (A single
 // expression like `re += a*b - c*d` would cost a multiply, an FMA and an add per term,
 // since the compiler may not reassociate it.)  ROWS < 3 computes only the leading rows.
-#if defined(LT_FFMA2)
-// FP32 products on Blackwell's paired FP32 FMA (fma.rn.f32x2): a complex term
-// (re, im) += a * b is two paired FMAs, (a.r, a.r) * (b.r, b.i) + (-a.i, a.i) * (b.i, b.r),
-// in the same rounding order as the scalar chain below.
-LT_D unsigned long long pk2(float lo, float hi)
-{
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-LT_D void upk2(unsigned long long v, float& lo, float& hi)
-{
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-LT_D unsigned long long ffma2(unsigned long long a, unsigned long long b, unsigned long long c)
-{
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-template <bool DA, bool DB, int ROWS> LT_D M3<float> prod_f2(const M3<float>& a, const M3<float>& b)
-{
-    unsigned long long y[3][3], ys[3][3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            const float yr = DB ? b.e[j][k].r : b.e[k][j].r;
-            const float yi = DB ? -b.e[j][k].i : b.e[k][j].i;
-            y[k][j] = pk2(yr, yi);
-            ys[k][j] = pk2(yi, yr);
-        }
-    M3<float> r;
-#pragma unroll
-    for (int i = 0; i < ROWS; ++i)
-    {
-        unsigned long long xr[3], xi[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-        {
-            const float ar = DA ? a.e[k][i].r : a.e[i][k].r;
-            const float ai = DA ? -a.e[k][i].i : a.e[i][k].i;
-            xr[k] = pk2(ar, ar);
-            xi[k] = pk2(-ai, ai);
-        }
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-        {
-            unsigned long long acc = 0ull;
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-            {
-                acc = ffma2(xr[k], y[k][j], acc);
-                acc = ffma2(xi[k], ys[k][j], acc);
-            }
-            upk2(acc, r.e[i][j].r, r.e[i][j].i);
-        }
-    }
-    return r;
-}
-#endif
-
 template <bool DA, bool DB, int ROWS = 3, typename T> LT_HD M3<T> prod(const M3<T>& a, const M3<T>& b)
 {
-#if defined(LT_FFMA2) && defined(__CUDA_ARCH__)
-    if constexpr (sizeof(T) == 4) return prod_f2<DA, DB, ROWS>(a, b);
-#endif
     M3<T> r;
 #pragma unroll
     for (int i = 0; i < ROWS; ++i)

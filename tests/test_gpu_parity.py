@@ -120,6 +120,14 @@ class TestLocalUpdates:
         lt.Iterator.Checkerboard(lt.OverrelaxationSubgroupKernel(G), 1)
         assert rel_err(G.download(), oracle.overrelax(ext, therm8, 1)) < TOL
 
+    @pytest.mark.parametrize("prec", ["fp32", "fp32_12"])
+    def test_overrelaxation_sweep_fp32(self, oracle, therm8, prec):
+        """FP32 storage and arithmetic against the FP64 oracle: one deterministic sweep."""
+        ext = (8, 8, 8, 8)
+        G = gpu(ext, therm8, prec)
+        lt.Iterator.Checkerboard(lt.OverrelaxationSubgroupKernel(G), 1)
+        assert rel_err(G.download(), oracle.overrelax(ext, therm8, 1)) < 1e-5
+
     def test_overrelaxation_conserves_action(self, therm8):
         G = gpu((8, 8, 8, 8), therm8)
         p0 = lt.PlaquetteSum(G)
