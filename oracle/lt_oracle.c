@@ -986,3 +986,113 @@ double or_bias_derivative(const or_bias* b, double cv)
     double h = 0.5 * b->bin_width;
     return b->bin_width_inv * (or_bias_potential(b, cv + h) - or_bias_potential(b, cv - h));
 }
+
+/* ---------------------------------------------------------------- BMW configuration files */
+/* Payload of the BMW format (IO/config_io/bmw_format.hpp:27-47, :294-394, :564-645): sites in
+ * t, z, y, x order (x fastest), per site the directions x, y, z, t (reference mu = 1, 2, 3, 0),
+ * per link the first two rows (full: all three), row-major, re then im, as big-endian doubles.
+ * Checksum_Adler64 (bmw_format.hpp:63-97) runs over the native 64-bit words of every site block
+ * of 4 * nw words: d0, d1 = high and low halves; A += d0 + d1; B += (2 + revi d0 + (revi - 1) d1)
+ * mod p with revi = (V - block) * 2 * (4 nw) - 2 * word, all in wrapping 64-bit arithmetic;
+ * final = ((B mod p) << 32) + (A + 1) mod p, p = 4294967291. */
+static const uint64_t ADLER64_PRIME = 4294967291ULL;
+
+static uint64_t bswap64(uint64_t v)
+{
+    uint64_t r = 0;
+    for (int k = 0; k < 8; ++k) r |= ((v >> (8 * k)) & 0xFFULL) << (8 * (7 - k));
+    return r;
+}
+
+static void adler64_block(const uint64_t* w, uint64_t block, uint64_t nblocks, int bs, uint64_t* A, uint64_t* B)
+{
+    uint64_t sa = 0, sb = 0;
+    uint64_t revi = (nblocks - block) * (uint64_t)(2 * bs);
+    for (int i = 0; i < bs; ++i)
+    {
+        uint64_t d0 = w[i] >> 32, d1 = w[i] & 0xFFFFFFFFULL;
+        sa += d0 + d1;
+        sb += (2 + revi * d0 + (revi - 1) * d1) % ADLER64_PRIME;
+        revi -= 2;
+    }
+    *A = (*A + sa) % ADLER64_PRIME;
+    *B = (*B + sb) % ADLER64_PRIME;
+}
+
+static uint64_t adler64_final(uint64_t A, uint64_t B)
+{
+    return ((B % ADLER64_PRIME) << 32) + (A + 1) % ADLER64_PRIME;
+}
+
+uint64_t or_bmw_encode(const int ext[4], const double* U, int full, unsigned char* payload)
+{
+    const int nw = full ? 18 : 12;
+    Geo g = geo(ext);
+    uint64_t A = 0, B = 0;
+    uint64_t buf[4 * 18];
+    const int Nt = ext[0], Nx = ext[1], Ny = ext[2], Nz = ext[3];
+    for (int t = 0; t < Nt; ++t)
+        for (int z = 0; z < Nz; ++z)
+            for (int y = 0; y < Ny; ++y)
+                for (int x = 0; x < Nx; ++x)
+                {
+                    const int c[4] = { t, x, y, z };
+                    const long s = site_of(&g, c);
+                    for (int dp = 0; dp < 4; ++dp)
+                    {
+                        const int mu = (dp + 1) % 4;
+                        memcpy(buf + dp * nw, U + 18 * (4 * s + mu), sizeof(double) * (size_t)nw);
+                    }
+                    const uint64_t block = (((uint64_t)t * Nz + z) * Ny + y) * Nx + x;
+                    adler64_block(buf, block, (uint64_t)g.V, 4 * nw, &A, &B);
+                    if (payload)
+                        for (int k = 0; k < 4 * nw; ++k)
+                        {
+                            uint64_t be = bswap64(buf[k]);
+                            memcpy(payload + (block * 4 * nw + (uint64_t)k) * 8, &be, 8);
+                        }
+                }
+    return adler64_final(A, B);
+}
+
+uint64_t or_bmw_decode(const int ext[4], const unsigned char* payload, int full, double* U)
+{
+    const int nw = full ? 18 : 12;
+    Geo g = geo(ext);
+    uint64_t A = 0, B = 0;
+    uint64_t buf[4 * 18];
+    const int Nt = ext[0], Nx = ext[1], Ny = ext[2], Nz = ext[3];
+    for (int t = 0; t < Nt; ++t)
+        for (int z = 0; z < Nz; ++z)
+            for (int y = 0; y < Ny; ++y)
+                for (int x = 0; x < Nx; ++x)
+                {
+                    const uint64_t block = (((uint64_t)t * Nz + z) * Ny + y) * Nx + x;
+                    for (int k = 0; k < 4 * nw; ++k)
+                    {
+                        uint64_t be;
+                        memcpy(&be, payload + (block * 4 * nw + (uint64_t)k) * 8, 8);
+                        buf[k] = bswap64(be);
+                    }
+                    adler64_block(buf, block, (uint64_t)g.V, 4 * nw, &A, &B);
+                    const int c[4] = { t, x, y, z };
+                    const long s = site_of(&g, c);
+                    for (int dp = 0; dp < 4; ++dp)
+                    {
+                        const int mu = (dp + 1) % 4;
+                        double* p = U + 18 * (4 * s + mu);
+                        memset(p, 0, sizeof(double) * 18);
+                        memcpy(p, buf + dp * nw, sizeof(double) * (size_t)nw);
+                        if (!full)
+                        {
+                            /* ReconstructMatBMW + SU3::Projection::RestoreLastRow (bmw_format.hpp:131-143, :247-250) */
+                            M3 m = ld(U, s, mu);
+                            m.m[2][0] = conj(m.m[0][1] * m.m[1][2] - m.m[0][2] * m.m[1][1]);
+                            m.m[2][1] = conj(m.m[0][2] * m.m[1][0] - m.m[0][0] * m.m[1][2]);
+                            m.m[2][2] = conj(m.m[0][0] * m.m[1][1] - m.m[0][1] * m.m[1][0]);
+                            st(U, s, mu, &m);
+                        }
+                    }
+                }
+    return adler64_final(A, B);
+}

@@ -54,6 +54,12 @@ void     or_bias_update_symmetric(or_bias* b, double cv);
 double   or_bias_potential(const or_bias* b, double cv);
 double   or_bias_derivative(const or_bias* b, double cv);
 
+/* BMW configuration payload and its Adler-64 checksum (IO/config_io/bmw_format.hpp:63-97,
+ * :131-394, :406-645); full = 1 for the 18-real #18BMW variant.  encode writes the payload when
+ * payload is not NULL; both return the checksum. */
+uint64_t or_bmw_encode(const int ext[4], const double* U, int full, unsigned char* payload);
+uint64_t or_bmw_decode(const int ext[4], const unsigned char* payload, int full, double* U);
+
 /* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) as used by the GPU streams */
 void or_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

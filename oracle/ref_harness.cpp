@@ -64,6 +64,7 @@
 #include "LettuceGauge/smearing/gradient_flow.hpp"
 #include "LettuceGauge/updates/heatbath.hpp"
 #include "LettuceGauge/updates/overrelaxation.hpp"
+#include "LettuceGauge/IO/config_io/bmw_format.hpp"
 // Only the two HMC headers are compiled with `private` mapped to `public` (they hold no
 // OpenMP `private(...)` clauses, which the mapping would break).
 #define private public
@@ -491,6 +492,25 @@ double ref_field_flow(double eps, int n)
     GradientFlowKernel Flow(*g_field, *g_flowed, rk3, GaugeAction::WilsonAction, eps);
     Flow(n);
     return PlaquetteSum(*g_flowed);
+}
+
+// SaveConfigBMW / SaveConfigBMWFull (IO/config_io/bmw_format.hpp:294-394, :564-645) of the
+// given links to `path` (overwriting); returns 1 on success
+int ref_save_bmw(const double* links, const char* path, int full)
+{
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    return (full ? SaveConfigBMWFull(*U, path, true) : SaveConfigBMW(*U, path, true)) ? 1 : 0;
+}
+
+// LoadConfigBMW / LoadConfigBMWFull (bmw_format.hpp:153-290, :425-560) of `path` into
+// links_out; returns 1 when the reference accepts the file (its links pass IsGroupElement)
+int ref_load_bmw(const char* path, int full, double* links_out)
+{
+    auto U = std::make_unique<GaugeField>();
+    const bool ok = full ? LoadConfigBMWFull(*U, path) : LoadConfigBMW(*U, path);
+    store(*U, links_out);
+    return ok ? 1 : 0;
 }
 
 // SU3::exp (su3_exp.hpp:419-425) of n traceless Hermitian matrices (18 doubles each)

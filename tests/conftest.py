@@ -39,5 +39,12 @@ def golden_bias():
 
 
 @pytest.fixture(scope="session")
+def golden_bmw():
+    d = dict(np.load(os.path.join(GOLDEN, "ref_bmw.npz")))
+    d["two_row_file"] = os.path.join(GOLDEN, "ref_2x4x6x8.bmw")
+    return d
+
+
+@pytest.fixture(scope="session")
 def golden_chain():
     return dict(np.load(os.path.join(GOLDEN, "ref_chain_8x8x8x8.npz")))

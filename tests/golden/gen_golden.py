@@ -155,17 +155,46 @@ def gen_chain(n_chain: int = 4, n_therm: int = 300, n_meas: int = 2500) -> dict:
     return {"plaq_norm": hist, "n_therm": np.array(n_therm), "beta": np.array(BETA)}
 
 
+BMW_EXT = (2, 4, 6, 8)
+BMW_SEED = 11
+
+
+def gen_bmw() -> dict:
+    """The reference's SaveConfigBMW / SaveConfigBMWFull output for a seeded Haar field on
+    uneven extents: the two-row file is committed whole, the 18-real one by its digest."""
+    import hashlib
+    U = haar_links_numpy(BMW_EXT, BMW_SEED)
+    ref = Reference(BMW_EXT)
+    out = {"ext": np.array(BMW_EXT), "seed": np.array(BMW_SEED)}
+    for full, name in ((False, "ref_2x4x6x8.bmw"), (True, "ref_2x4x6x8.18bmw")):
+        path = os.path.join(HERE, name)
+        assert ref.save_bmw(U, path, full)
+        data = open(path, "rb").read()
+        key = "full" if full else "two_row"
+        out[f"sha256_{key}"] = np.array(hashlib.sha256(data).hexdigest())
+        out[f"checksum_{key}"] = np.array(data[:4096].split(b"\n")[0].split()[-1].decode())
+        ok, loaded = ref.load_bmw(path, full)
+        assert ok
+        out[f"loaded_ck_{key}"] = checksums(loaded)
+        if full:
+            os.remove(path)
+    return out
+
+
 def main() -> int:
     import argparse
     import subprocess
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["chain"], default=None, help="regenerate one fixture only")
+    ap.add_argument("--only", choices=["chain", "bmw"], default=None, help="regenerate one fixture only")
     a = ap.parse_args()
     root = os.path.dirname(os.path.dirname(HERE))
     subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "4x4x4x4",
-                    "4x6x8x10", "8x8x8x8"], check=True)
+                    "4x6x8x10", "8x8x8x8", "2x4x6x8"], check=True)
     if a.only == "chain":
         np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
+        return 0
+    if a.only == "bmw":
+        np.savez_compressed(os.path.join(HERE, "ref_bmw.npz"), **gen_bmw())
         return 0
     np.savez_compressed(os.path.join(HERE, "ref_4x4x4x4.npz"), **gen_case((4, 4, 4, 4), 1, True))
     b = gen_case((4, 6, 8, 10), 2, False)
@@ -175,6 +204,7 @@ def main() -> int:
     np.savez_compressed(os.path.join(HERE, "ref_4x6x8x10.npz"), **b)
     np.savez_compressed(os.path.join(HERE, "ref_bias.npz"), **gen_bias())
     np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
+    np.savez_compressed(os.path.join(HERE, "ref_bmw.npz"), **gen_bmw())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

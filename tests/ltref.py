@@ -61,6 +61,8 @@ class Oracle:
             "or_bias_update_symmetric": (None, [C.c_void_p, d]),
             "or_bias_potential": (d, [C.c_void_p, d]),
             "or_bias_derivative": (d, [C.c_void_p, d]),
+            "or_bmw_encode": (u64, [_ip, _dp, i, C.c_void_p]),
+            "or_bmw_decode": (u64, [_ip, C.c_void_p, i, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -145,6 +147,22 @@ class Oracle:
         self.lib.or_random_momenta(self._e(ext), P, seed, counter)
         return P
 
+    def bmw_encode(self, ext, U, full):
+        """(Adler-64 checksum, BMW payload bytes) of a field in the reference layout."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        V = int(np.prod(ext))
+        payload = np.empty(V * 4 * (18 if full else 12) * 8, dtype=np.uint8)
+        ck = self.lib.or_bmw_encode(self._e(ext), U, int(full), payload.ctypes.data)
+        return ck, payload.tobytes()
+
+    def bmw_decode(self, ext, payload, full):
+        """(Adler-64 checksum, links) of a BMW payload."""
+        V = int(np.prod(ext))
+        buf = np.frombuffer(payload, dtype=np.uint8).copy()
+        U = np.empty((V, 4, 3, 3, 2))
+        ck = self.lib.or_bmw_decode(self._e(ext), buf.ctypes.data, int(full), U)
+        return ck, U
+
     def kinetic(self, ext, P):
         return self.lib.or_kinetic(self._e(ext), P)
 
@@ -186,6 +204,8 @@ class Reference:
                 "ref_metad_omf2": (None, [_dp, _dp, d, d, i, d, d, C.POINTER(d), C.POINTER(d)]),
                 "ref_bias_probe": (None, [d, d, i, d, d, d, d, _dp, i, i, _dp, i, _dp, _dp]),
                 "ref_su3_exp": (None, [_dp, _dp, i]),
+                "ref_save_bmw": (i, [_dp, C.c_char_p, i]),
+                "ref_load_bmw": (i, [C.c_char_p, i, _dp]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(lib, name)
@@ -273,6 +293,25 @@ class Reference:
         out = np.empty_like(Q)
         self.lib.ref_su3_exp(Q, out, Q.size // 18)
         return out
+
+    def save_bmw(self, U, path, full):
+        return bool(self.lib.ref_save_bmw(np.ascontiguousarray(U, dtype=np.float64), str(path).encode(), int(full)))
+
+    def load_bmw(self, path, full):
+        V = int(np.prod(self.ext))
+        out = np.empty((V, 4, 3, 3, 2))
+        ok = bool(self.lib.ref_load_bmw(str(path).encode(), int(full), out))
+        return ok, out
+
+
+def bmw_header(ext, checksum: int, full: bool) -> bytes:
+    """The 4096-byte header SaveConfigBMW / SaveConfigBMWFull write (bmw_format.hpp:346-363)."""
+    h = bytearray(b"\n" * 4096)
+    line = f"{'#18BMW' if full else '#BMW'} {ext[1]} {ext[2]} {ext[3]} {ext[0]} {checksum:x}\n".encode()
+    tail = b"\nGenerated with Lettuce\n\0"
+    h[:len(line)] = line
+    h[len(line):len(line) + len(tail)] = tail
+    return bytes(h)
 
 
 def haar_links_numpy(ext, seed):

@@ -149,3 +149,46 @@ class TestLiveReference:
         assert oracle.topcharge(ext, U) == pytest.approx(ref.topcharge(U), rel=1e-10, abs=1e-12)
         assert rel_err(oracle.overrelax(ext, U, 1), ref.overrelax(U, 1)) < TOL
         assert rel_err(oracle.flow_rk3(ext, U, 0.01, 3), ref.flow_rk3(U, 0.01, 3)) < TOL
+
+
+class TestBMW:
+    """BMW configuration files (IO/config_io/bmw_format.hpp): the oracle's payload and
+    Adler-64 checksum against files written by the reference's SaveConfigBMW(Full)."""
+
+    def test_oracle_reproduces_reference_files(self, oracle, golden_bmw):
+        import hashlib
+        from ltref import bmw_header
+        ext = tuple(int(e) for e in golden_bmw["ext"])
+        U = haar_links_numpy(ext, int(golden_bmw["seed"]))
+        for full, key in ((False, "two_row"), (True, "full")):
+            ck, payload = oracle.bmw_encode(ext, U, full)
+            assert f"{ck:x}" == str(golden_bmw[f"checksum_{key}"])
+            data = bmw_header(ext, ck, full) + payload
+            assert hashlib.sha256(data).hexdigest() == str(golden_bmw[f"sha256_{key}"])
+
+    def test_oracle_decodes_reference_file(self, oracle, golden_bmw):
+        ext = tuple(int(e) for e in golden_bmw["ext"])
+        data = open(golden_bmw["two_row_file"], "rb").read()
+        ck, U = oracle.bmw_decode(ext, data[4096:], False)
+        assert f"{ck:x}" == data[:4096].split(b"\n")[0].split()[-1].decode()
+        assert np.array_equal(checksums(U), golden_bmw["loaded_ck_two_row"])
+        U0 = haar_links_numpy(ext, int(golden_bmw["seed"]))
+        assert np.abs(U - U0).max() < 1e-15
+
+    @pytest.mark.skipif(not ref_available((4, 6, 8, 10)), reason="reference harness not built")
+    def test_live_reference_save_and_load(self, oracle, tmp_path):
+        import hashlib
+        from ltref import bmw_header
+        ext = (4, 6, 8, 10)
+        ref = Reference(ext)
+        U = haar_links_numpy(ext, 23)
+        for full in (False, True):
+            path = tmp_path / f"c{int(full)}.bmw"
+            assert ref.save_bmw(U, path, full)
+            data = path.read_bytes()
+            ck, payload = oracle.bmw_encode(ext, U, full)
+            assert hashlib.sha256(bmw_header(ext, ck, full) + payload).digest() == hashlib.sha256(data).digest()
+            ok, loaded = ref.load_bmw(path, full)
+            assert ok
+            _, mine = oracle.bmw_decode(ext, data[4096:], full)
+            assert np.array_equal(mine, loaded)
