@@ -260,6 +260,32 @@ def secondary_rates(lt, torch, timed, prec):
     except Exception as e:
         out["ensemble_error"] = repr(e)
     try:
+        # BMW configuration files at 32^4: the device pack + Adler-64 pass alone (links read
+        # once, payload written once), and a two-row file saved and loaded through the C ABI
+        # (device pass + PCIe + file system)
+        import tempfile
+        ext = (32,) * 4
+        G = lt.GaugeField(ext, prec)
+        G.SetToHaarRandom(11)
+        G.bmw_checksum()
+        n = 10
+        ms = timed(G, lambda: G.bmw_checksum(), n) / n
+        out["bmw_checksum_call_ms_32^4"] = ms
+        out["bmw_checksum_link_gbs"] = 4 * G.Volume() * bm.LINK_BYTES[prec] / (ms / 1000.0) / 1e9
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "cfg.bmw")
+            t0 = time.perf_counter()
+            G.save_bmw(path, overwrite=True)
+            out["bmw_save_s_32^4"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            ok, grp = G.load_bmw(path)
+            out["bmw_load_s_32^4"] = time.perf_counter() - t0
+            out["bmw_file_mb"] = os.path.getsize(path) / 1e6
+            out["bmw_roundtrip_ok"] = bool(ok and grp)
+        del G
+    except Exception as e:
+        out["bmw_error"] = repr(e)
+    try:
         # 48^4 at beta = 6.3: Haar start, 200 rounds of 1 HB + 4 OR, two OMF2 trajectories
         # (tau = 1, 20 steps, FP32 links, FP64 dH and accept), then Wilson flow to t0
         # (t^2 E = 0.3) with clover Q and E at every step

@@ -95,6 +95,27 @@ int lt_status_word(lt_lattice* h, uint32_t* word, int clear);
  * by the Gram-Schmidt projection after every update). */
 int lt_check_links(lt_lattice* h, double* max_dev);
 
+/* ---- configuration files: the BMW format (IO/config_io/bmw_format.hpp) ------------------ */
+/* full = 0: "#BMW" files with the first two rows of each link; full = 1: "#18BMW" files with
+ * all three rows.  A 4096-byte ASCII header "#BMW Nx Ny Nz Nt <checksum>" is followed by the
+ * links in t, z, y, x order, directions x, y, z, t, as big-endian doubles; the checksum is
+ * Checksum_Adler64 (:63-118) of the link data.  The device packs the records and computes the
+ * checksum; the host writes the bytes. */
+/* SaveConfigBMW / SaveConfigBMWFull (:294-394, :564-645).  Fails with LT_ERR_IO when the file
+ * exists and overwrite = 0 (the reference returns false).  checksum_hex (17 bytes, may be
+ * NULL) receives the header's checksum string. */
+int lt_save_bmw(lt_lattice* h, const char* path, int full, int overwrite, char* checksum_hex);
+/* LoadConfigBMW / LoadConfigBMWFull (:153-290, :425-560): reads the links (two-row files get
+ * their third row from RestoreLastRow, su3.hpp:362-367, in the reference's rounding).
+ * *checksum_ok = 1 when the recomputed checksum string equals the header's (the reference
+ * only prints the comparison); *in_group = 1 when every link passes SU3::Tests::IsGroupElement
+ * (su3.hpp:568-595, tolerance 1e-6), the reference's return value.  LT_ERR_IO for a missing
+ * file, a malformed header or a short file; LT_ERR_ARG when the shape differs from the handle's. */
+int lt_load_bmw(lt_lattice* h, const char* path, int full, int* checksum_ok, int* in_group);
+/* Checksum_Adler64 of the handle's links as a BMW file would hold them, without file IO.
+ * No counterpart in the reference (which computes it only inside save and load). */
+int lt_bmw_checksum(lt_lattice* h, int full, uint64_t* checksum);
+
 /* ---- observables --------------------------------------------------------------------- */
 /* PlaquetteSum (observables/plaquette.hpp:26-43): sum over sites, mu<nu of ReTr P. */
 int lt_plaquette_sum(lt_lattice* h, double* out);

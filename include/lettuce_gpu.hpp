@@ -16,6 +16,8 @@
 
 #include <array>
 #include <cstdint>
+#include <filesystem>
+#include <fstream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -133,7 +135,11 @@ struct Wilson
 inline Wilson WilsonAction;
 } // namespace GaugeAction
 
-// HeatbathKernel (updates/heatbath.hpp:30-130); beta fixed at construction (:40)
+// HeatbathKernel (updates/heatbath.hpp:30-130); beta fixed at construction (:40).  Its random
+// stream is (seed, counter) of Philox4x32-10, so SaveState / LoadState (the PRNG's checkpoint
+// calls in the reference, random/prng_wrapper.hpp:268-279) write and read those two numbers;
+// the second file, the reference's normal-distribution state, has no counterpart and is
+// written as a marker only.
 struct HeatbathKernel
 {
     GaugeField& U;
@@ -143,6 +149,24 @@ struct HeatbathKernel
                    std::uint64_t counter_in = 0)
         : U(U_in), beta(action.GetBeta()), seed(seed_in), counter(counter_in)
     {
+    }
+    bool SaveState(const std::filesystem::path& state, const std::filesystem::path& normal, bool overwrite = false) const
+    {
+        if (!overwrite && (std::filesystem::exists(state) || std::filesystem::exists(normal))) return false;
+        std::ofstream s(state, std::ios::trunc), n(normal, std::ios::trunc);
+        s << "philox4x32-10 " << seed << ' ' << counter << '\n';
+        n << "counter-based stream: no distribution state\n";
+        return static_cast<bool>(s) && static_cast<bool>(n);
+    }
+    bool LoadState(const std::filesystem::path& state, const std::filesystem::path&)
+    {
+        std::ifstream s(state);
+        std::string tag;
+        std::uint64_t sd = 0, ct = 0;
+        if (!(s >> tag >> sd >> ct) || tag != "philox4x32-10") return false;
+        seed = sd;
+        counter = ct;
+        return true;
     }
 };
 
@@ -201,6 +225,122 @@ inline void StoutSmearing4D(const GaugeField& in, GaugeField& out, double smear_
 {
     check(lt_stout(in.handle(), out.handle(), smear_param, 1));
 }
+
+// Configuration files in the BMW format (IO/config_io/bmw_format.hpp): the reference's
+// signatures and return values (false for a missing or malformed file, a shape mismatch or an
+// existing file without overwrite; loading returns whether every link is an SU(3) element).
+// LoadConfigBMWChecked also returns what the reference only prints: whether the recomputed
+// Adler-64 checksum equals the header's (no counterpart in the reference).
+inline bool LoadConfigBMWChecked(GaugeField& U, const std::string& filename, bool full, bool& checksum_ok)
+{
+    int ok = 0, in_group = 0;
+    const int r = lt_load_bmw(U.handle(), filename.c_str(), full ? 1 : 0, &ok, &in_group);
+    checksum_ok = false;
+    if (r == LT_ERR_IO || r == LT_ERR_ARG) return false;
+    check(r);
+    checksum_ok = ok != 0;
+    return in_group != 0;
+}
+
+namespace detail
+{
+inline bool save_bmw(const GaugeField& U, const std::string& filename, bool overwrite, int full)
+{
+    const int r = lt_save_bmw(U.handle(), filename.c_str(), full, overwrite ? 1 : 0, nullptr);
+    if (r == LT_ERR_IO) return false;
+    check(r);
+    return true;
+}
+} // namespace detail
+
+// SaveConfigBMW (:294-394) / LoadConfigBMW (:153-290): first two rows per link, "#BMW" header
+inline bool SaveConfigBMW(const GaugeField& U, const std::string& filename, const bool overwrite = false)
+{
+    return detail::save_bmw(U, filename, overwrite, 0);
+}
+inline bool LoadConfigBMW(GaugeField& U, const std::string& filename)
+{
+    bool checksum_ok;
+    return LoadConfigBMWChecked(U, filename, false, checksum_ok);
+}
+// SaveConfigBMWFull (:564-645) / LoadConfigBMWFull (:425-560): all three rows, "#18BMW" header
+inline bool SaveConfigBMWFull(const GaugeField& U, const std::string& filename, const bool overwrite = false)
+{
+    return detail::save_bmw(U, filename, overwrite, 1);
+}
+inline bool LoadConfigBMWFull(GaugeField& U, const std::string& filename)
+{
+    bool checksum_ok;
+    return LoadConfigBMWChecked(U, filename, true, checksum_ok);
+}
+
+// CheckpointManager (IO/config_io/checkpoint_manager.hpp:12-161): rotating checkpoint copies in
+// backup1..backup<n-1> subdirectories; the save / load functions are passed in as in the
+// reference (for example SaveConfigBMWFull and LoadConfigBMWFull), the PRNG is any object with
+// SaveState / LoadState (HeatbathKernel above)
+struct CheckpointManager
+{
+private:
+    std::filesystem::path checkpoint_directory;
+
+public:
+    const int n_checkpoint_files;
+
+    CheckpointManager(const std::filesystem::path& dir, const int n_files, const bool create_subdirectories)
+        : checkpoint_directory(dir), n_checkpoint_files(n_files)
+    {
+        if (create_subdirectories) CreateSubdirectories();
+    }
+    std::filesystem::path CheckpointDirectory() const { return checkpoint_directory; }
+    void CheckpointDirectory(const std::filesystem::path& dir) { checkpoint_directory = dir; }
+    std::string ReturnBackupSubdirectory(const int counter) const
+    {
+        return counter == 0 ? std::string() : "backup" + std::to_string(counter);
+    }
+    void CreateSubdirectories() const
+    {
+        std::error_code err;
+        for (int k = 1; k < n_checkpoint_files; ++k)
+            std::filesystem::create_directories(checkpoint_directory / ReturnBackupSubdirectory(k), err);
+    }
+    void RotateFiles(const std::filesystem::path& current, const std::filesystem::path& old, const bool copy_file = true) const
+    {
+        if (!std::filesystem::exists(current)) return;
+        std::error_code err;
+        if (copy_file) std::filesystem::copy_file(current, old, std::filesystem::copy_options::overwrite_existing, err);
+        else std::filesystem::rename(current, old, err);
+    }
+    template <typename FuncT>
+    void AlternatingConfigCheckpoints(FuncT&& SaveFunction, const GaugeField& U, const std::string& filename_config) const
+    {
+        for (int k = n_checkpoint_files - 1; k > 0; --k)
+            RotateFiles(checkpoint_directory / ReturnBackupSubdirectory(k - 1) / filename_config,
+                        checkpoint_directory / ReturnBackupSubdirectory(k) / filename_config, k != 1);
+        SaveFunction(U, (checkpoint_directory / filename_config).string(), true);
+    }
+    template <typename FuncT, typename prngT>
+    void AlternatingCheckpoints(FuncT&& SaveFunction, prngT& prng, const GaugeField& U, const std::string& filename_config,
+                                const std::string& filename_prng, const std::string& filename_normal_distribution) const
+    {
+        for (int k = n_checkpoint_files - 1; k > 0; --k)
+        {
+            const auto old_dir = checkpoint_directory / ReturnBackupSubdirectory(k);
+            const auto cur_dir = checkpoint_directory / ReturnBackupSubdirectory(k - 1);
+            RotateFiles(cur_dir / filename_config, old_dir / filename_config, k != 1);
+            RotateFiles(cur_dir / filename_prng, old_dir / filename_prng, k != 1);
+            RotateFiles(cur_dir / filename_normal_distribution, old_dir / filename_normal_distribution, k != 1);
+        }
+        SaveFunction(U, (checkpoint_directory / filename_config).string(), true);
+        prng.SaveState(checkpoint_directory / filename_prng, checkpoint_directory / filename_normal_distribution, true);
+    }
+    template <typename FuncT, typename prngT>
+    void LoadCheckpoint(FuncT&& LoadFunction, prngT& prng, GaugeField& U, const std::string& filename_config,
+                        const std::string& filename_prng, const std::string& filename_normal_distribution) const
+    {
+        LoadFunction(U, (checkpoint_directory / filename_config).string());
+        prng.LoadState(checkpoint_directory / filename_prng, checkpoint_directory / filename_normal_distribution);
+    }
+};
 
 // MetaBiasPotential (actions/bias_potential/metadynamics.hpp:29-507)
 class MetaBiasPotential

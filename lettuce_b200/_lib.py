@@ -44,6 +44,9 @@ SIGNATURES = {
     "lt_get_stream": (_i, [_vp, C.POINTER(_vp)]),
     "lt_status_word": (_i, [_vp, C.POINTER(C.c_uint32), _i]),
     "lt_check_links": (_i, [_vp, _pd]),
+    "lt_save_bmw": (_i, [_vp, C.c_char_p, _i, _i, C.c_char_p]),
+    "lt_load_bmw": (_i, [_vp, C.c_char_p, _i, _pi, _pi]),
+    "lt_bmw_checksum": (_i, [_vp, _i, _pu64]),
     "lt_plaquette_sum": (_i, [_vp, _pd]),
     "lt_wilson_action": (_i, [_vp, _d, _pd]),
     "lt_topcharge_clover": (_i, [_vp, _pd]),

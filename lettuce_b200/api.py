@@ -7,6 +7,7 @@ reference layout, numpy float64 arrays of shape [V, 4, 3, 3, 2].
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -107,6 +108,26 @@ class GaugeField:
         w = C.c_uint32()
         check(lib().lt_status_word(self._h, C.byref(w), int(bool(clear))))
         return w.value
+
+    def save_bmw(self, path, full: bool = False, overwrite: bool = False) -> str:
+        """SaveConfigBMW / SaveConfigBMWFull (IO/config_io/bmw_format.hpp:294-394, :564-645);
+        returns the header's checksum string."""
+        buf = C.create_string_buffer(17)
+        check(lib().lt_save_bmw(self._h, os.fsencode(path), int(bool(full)), int(bool(overwrite)), buf))
+        return buf.value.decode()
+
+    def load_bmw(self, path, full: bool = False) -> tuple[bool, bool]:
+        """LoadConfigBMW / LoadConfigBMWFull (bmw_format.hpp:153-290, :425-560); returns
+        (checksum matches the header, every link passes IsGroupElement)."""
+        ok, grp = C.c_int(), C.c_int()
+        check(lib().lt_load_bmw(self._h, os.fsencode(path), int(bool(full)), C.byref(ok), C.byref(grp)))
+        return bool(ok.value), bool(grp.value)
+
+    def bmw_checksum(self, full: bool = False) -> int:
+        """Checksum_Adler64 of the links as a BMW file would hold them."""
+        v = C.c_uint64()
+        check(lib().lt_bmw_checksum(self._h, int(bool(full)), C.byref(v)))
+        return v.value
 
     def check_links(self) -> float:
         """Largest entry of |U U^dag - 1| over all links; flags NaN/Inf and unitarity loss."""

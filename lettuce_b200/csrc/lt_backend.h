@@ -50,6 +50,13 @@ public:
     // atomically maxes the float bits of the largest |U U^dag - 1| entry into *maxbits
     virtual void check_links(const Ctx& c, const void* U, double tol, unsigned* maxbits) const = 0;
 
+    // BMW payload (full: 18 reals per link, else 12) to / from device memory; Adler-64 partial
+    // sums (A then B, kRedBlocks each) into partials; unpack sets bit 0 of *flags for a link
+    // that fails the reference's group-element test
+    virtual void bmw_pack(const Ctx& c, const void* U, int full, void* out, unsigned long long* partials) const = 0;
+    virtual void bmw_unpack(const Ctx& c, void* U, int full, const void* in, unsigned long long* partials,
+                            unsigned* flags) const = 0;
+
     virtual void overrelax(const Ctx& c, void* U, int mu, int par) const = 0;
     virtual void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter,
                           uint64_t seed, int max_iter) const = 0;

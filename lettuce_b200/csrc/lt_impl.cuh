@@ -119,6 +119,21 @@ public:
     {
         k_check_links<T, NR><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, tol, c.status, maxbits);
     }
+    void bmw_pack(const Ctx& c, const void* U, int full, void* out, unsigned long long* partials) const override
+    {
+        auto* o = static_cast<unsigned long long*>(out);
+        if (full) k_bmw_pack<T, NR, 18><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, o, partials);
+        else k_bmw_pack<T, NR, 12><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, o, partials);
+    }
+    void bmw_unpack(const Ctx& c, void* U, int full, const void* in, unsigned long long* partials,
+                    unsigned* flags) const override
+    {
+        auto* p = static_cast<const unsigned long long*>(in);
+        if (full)
+            k_bmw_unpack<T, NR, 18><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, p, partials, flags);
+        else
+            k_bmw_unpack<T, NR, 12><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, p, partials, flags);
+    }
     void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new, double c_exp,
                     int read_z, int write_z) const override
     {

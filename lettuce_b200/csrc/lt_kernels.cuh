@@ -319,6 +319,182 @@ __global__ void __launch_bounds__(kRedThreads) k_plaquette(Gauge<T, NR> U, Geom 
     if (threadIdx.x == 0) partials[blockIdx.x] = r;
 }
 
+// ---------------------------------------------------------------- BMW configuration files
+// Payload of the BMW format (IO/config_io/bmw_format.hpp:27-47): records in t, z, y, x order
+// (x fastest), per record the links of directions x, y, z, t (mu = 1, 2, 3, 0), per link NW =
+// 12 (first two rows) or 18 (#18BMW) doubles, row-major re/im, big-endian.  Checksum_Adler64
+// (bmw_format.hpp:63-97) over record b of 4 NW native 64-bit words w_k, d0/d1 = high/low halves:
+//   A_b = sum_k (d0 + d1),  B_b = sum_k (2 + r_k d0 + (r_k - 1) d1) mod p,
+//   r_k = (V - b) * 2 * 4 NW - 2 k  (wrapping 64-bit arithmetic), p = 4294967291;
+// A and B are sums over records mod p, so every record is summed independently and the
+// partial sums are reduced per block (A in partials[block], B in partials[nblk + block]).
+constexpr unsigned long long kAdler64Prime = 4294967291ULL;
+
+LT_D unsigned long long bswap64(unsigned long long v)
+{
+    const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+    return ((unsigned long long)__byte_perm(lo, 0, 0x0123) << 32) | __byte_perm(hi, 0, 0x0123);
+}
+
+// Record b -> (coordinates, full index) in the reference site order
+LT_D int bmw_site(const Geom& g, int b, int c[4])
+{
+    int r = b;
+    c[1] = r % g.n[1];
+    r /= g.n[1];
+    c[2] = r % g.n[2];
+    r /= g.n[2];
+    c[3] = r % g.n[3];
+    c[0] = r / g.n[3];
+    return ((c[0] * g.n[1] + c[1]) * g.n[2] + c[2]) * g.n[3] + c[3];
+}
+
+LT_D void adler_word(unsigned long long w, unsigned long long& revi, unsigned long long& sa, unsigned long long& sb)
+{
+    const unsigned long long d0 = w >> 32, d1 = w & 0xFFFFFFFFULL;
+    sa += d0 + d1;
+    sb += (2ULL + revi * d0 + (revi - 1ULL) * d1) % kAdler64Prime;
+    revi -= 2ULL;
+}
+
+LT_D void adler_block_store(unsigned long long sa, unsigned long long sb, unsigned long long* __restrict__ partials)
+{
+    __shared__ unsigned long long sh[2][32];
+    sa %= kAdler64Prime;
+    sb %= kAdler64Prime;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sb += __shfl_xor_sync(0xffffffffu, sb, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0)
+    {
+        sh[0][wid] = sa;
+        sh[1][wid] = sb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        unsigned long long a = 0, b = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+        {
+            a += sh[0][w];
+            b += sh[1][w];
+        }
+        partials[blockIdx.x] = a % kAdler64Prime;
+        partials[gridDim.x + blockIdx.x] = b % kAdler64Prime;
+    }
+}
+
+// Links -> big-endian payload (out may be null: checksum only)
+template <typename T, int NR, int NW>
+__global__ void __launch_bounds__(kRedThreads) k_bmw_pack(Gauge<T, NR> U, Geom g, unsigned long long* __restrict__ out,
+                                                           unsigned long long* __restrict__ partials)
+{
+    unsigned long long sa = 0, sb = 0;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.V; b += gridDim.x * blockDim.x)
+    {
+        int c[4];
+        const int i = bmw_site(g, b, c);
+        const int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+        unsigned long long revi = (unsigned long long)(g.V - b) * (unsigned long long)(8 * NW);
+        unsigned long long* o = out ? out + (size_t)b * 4 * NW : nullptr;
+#pragma unroll
+        for (int dp = 0; dp < 4; ++dp)
+        {
+            const M3<double> m = cvt<double>(U.ld((dp + 1) & 3, par, i >> 1));
+#pragma unroll
+            for (int k = 0; k < NW; ++k)
+            {
+                const cx<double> e = m.e[k / 6][(k % 6) / 2];
+                const unsigned long long w = (unsigned long long)__double_as_longlong((k & 1) ? e.i : e.r);
+                adler_word(w, revi, sa, sb);
+                if (o) o[dp * NW + k] = bswap64(w);
+            }
+        }
+    }
+    adler_block_store(sa, sb, partials);
+}
+
+// Reference complex arithmetic without contraction: RestoreLastRow (math/su3.hpp:362-367) as
+// the reference's loader evaluates it, row 2 = conj(row0 x row1), each product rounded
+LT_D cx<double> cmul_rn(cx<double> a, cx<double> b)
+{
+    return mkc<double>(__dsub_rn(__dmul_rn(a.r, b.r), __dmul_rn(a.i, b.i)),
+                       __dadd_rn(__dmul_rn(a.r, b.i), __dmul_rn(a.i, b.r)));
+}
+LT_D cx<double> conj_cross_rn(cx<double> p, cx<double> q, cx<double> r, cx<double> s)
+{
+    const cx<double> x = cmul_rn(p, q), y = cmul_rn(r, s);
+    return mkc<double>(__dsub_rn(x.r, y.r), -__dsub_rn(x.i, y.i));
+}
+
+// Big-endian payload -> links (third row rebuilt for NW = 12, in the reference's rounding);
+// a link failing SU3::Tests::IsGroupElement (su3.hpp:568-578: |1 - U^dag U|_F or |det U - 1|
+// above 1e-6) sets bit 0 of *flags.
+template <typename T, int NR, int NW>
+__global__ void __launch_bounds__(kRedThreads) k_bmw_unpack(Gauge<T, NR> U, Geom g, const unsigned long long* __restrict__ in,
+                                                             unsigned long long* __restrict__ partials, unsigned* flags)
+{
+    unsigned long long sa = 0, sb = 0;
+    bool bad = false;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.V; b += gridDim.x * blockDim.x)
+    {
+        int c[4];
+        const int i = bmw_site(g, b, c);
+        const int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+        unsigned long long revi = (unsigned long long)(g.V - b) * (unsigned long long)(8 * NW);
+        const unsigned long long* p = in + (size_t)b * 4 * NW;
+#pragma unroll
+        for (int dp = 0; dp < 4; ++dp)
+        {
+            M3<double> m = zero3<double>();
+#pragma unroll
+            for (int k = 0; k < NW; ++k)
+            {
+                const unsigned long long w = bswap64(p[dp * NW + k]);
+                adler_word(w, revi, sa, sb);
+                const double v = __longlong_as_double((long long)w);
+                cx<double>& e = m.e[k / 6][(k % 6) / 2];
+                if (k & 1) e.i = v;
+                else e.r = v;
+            }
+            if (NW == 12)
+            {
+                m.e[2][0] = conj_cross_rn(m.e[0][1], m.e[1][2], m.e[0][2], m.e[1][1]);
+                m.e[2][1] = conj_cross_rn(m.e[0][2], m.e[1][0], m.e[0][0], m.e[1][2]);
+                m.e[2][2] = conj_cross_rn(m.e[0][0], m.e[1][1], m.e[0][1], m.e[1][0]);
+            }
+            // IsGroupElement: Frobenius norm of 1 - U^dag U and |det U - 1|
+            double f2 = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb)
+                {
+                    double re = a == bb ? 1.0 : 0.0, im = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                    {
+                        re -= m.e[k][a].r * m.e[k][bb].r + m.e[k][a].i * m.e[k][bb].i;
+                        im -= m.e[k][a].r * m.e[k][bb].i - m.e[k][a].i * m.e[k][bb].r;
+                    }
+                    f2 += re * re + im * im;
+                }
+            const cx<double> det = m.e[0][0] * (m.e[1][1] * m.e[2][2] - m.e[1][2] * m.e[2][1])
+                                 - m.e[0][1] * (m.e[1][0] * m.e[2][2] - m.e[1][2] * m.e[2][0])
+                                 + m.e[0][2] * (m.e[1][0] * m.e[2][1] - m.e[1][1] * m.e[2][0]);
+            const double dr = det.r - 1.0;
+            bad |= !(f2 <= 1e-12) || !(dr * dr + det.i * det.i <= 1e-12);
+            U.st((dp + 1) & 3, par, i >> 1, cvt<T>(m));
+        }
+    }
+    if (bad) atomicOr(flags, 1u);
+    adler_block_store(sa, sb, partials);
+}
+
 // ---------------------------------------------------------------- link health
 // Scans every link: non-finite entries set kStatusNonFinite; the largest entry of
 // |U U^dag - 1| (products in FP64, third row rebuilt for two-row storage) goes to *maxbits as

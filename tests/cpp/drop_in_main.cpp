@@ -49,5 +49,25 @@ int main(int argc, char** argv)
     GaugeField copy(Gluon);
     Swap(copy, Gluonsmeared1);
     std::printf("copy plaquette %.15f\n", PlaquetteSum(Gluonsmeared1) / Gluon.Volume() / 18.0);
+
+    // checkpoints as the reference's driver writes them (CheckpointManager + BMW files)
+    if (argc > 2)
+    {
+        CheckpointManager checkpoints(argv[2], 3, true);
+        for (int k = 0; k < 3; ++k)
+        {
+            Iterator::Checkerboard4(Heatbath, 1);
+            checkpoints.AlternatingCheckpoints(SaveConfigBMWFull, Heatbath, Gluon, "config", "prng_state", "distribution_state");
+        }
+        GaugeField restored({L, L, L, L});
+        HeatbathKernel resumed(restored, SimulatedAction);
+        checkpoints.LoadCheckpoint(LoadConfigBMWFull, resumed, restored, "config", "prng_state", "distribution_state");
+        bool checksum_ok = false;
+        const bool in_group = LoadConfigBMWChecked(restored, (checkpoints.CheckpointDirectory() / "missing").string(),
+                                                   false, checksum_ok);
+        std::printf("checkpoint counter %llu restored plaquette %.15f original %.15f missing %d\n",
+                    (unsigned long long)resumed.counter, PlaquetteSum(restored) / Gluon.Volume() / 18.0,
+                    PlaquetteSum(Gluon) / Gluon.Volume() / 18.0, in_group ? 1 : 0);
+    }
     return 0;
 }

@@ -25,8 +25,9 @@ def test_dropin_compiles_and_links():
 
 
 @pytest.mark.gpu
-def test_dropin_runs_like_python_mirror():
-    out = subprocess.run([build_exe(), "8"], capture_output=True, text=True, check=True).stdout
+def test_dropin_runs_like_python_mirror(tmp_path):
+    out = subprocess.run([build_exe(), "8", str(tmp_path / "ckpt")], capture_output=True, text=True,
+                         check=True).stdout
     lines = dict((l.split()[0] + (l.split()[1] if l.startswith("flow") else ""), l) for l in out.splitlines())
     # the same sequence through the Python mirror
     G = lt.GaugeField((8, 8, 8, 8))
@@ -40,3 +41,10 @@ def test_dropin_runs_like_python_mirror():
     assert float(lines["plaquette"].split()[1]) == pytest.approx(p, rel=1e-14)
     assert 0.55 < p < 0.65
     assert "metad" in out and "copy" in out
+    # checkpoints: three rotations, restored field and Philox counter, a missing file rejected
+    ck = lines["checkpoint"].split()
+    assert int(ck[2]) == 20 + 3
+    assert float(ck[5]) == float(ck[7])
+    assert ck[9] == "0"
+    for sub in ("", "backup1", "backup2"):
+        assert (tmp_path / "ckpt" / sub / "config").exists()
