@@ -523,6 +523,47 @@ void or_flow_rk3(const int ext[4], const double* in, double* out, double eps, in
     free(Z);
 }
 
+/* Integrators::GradientFlow::Euler, RK2, RK3, RK3W7 (gradient_flow.hpp:31-56, :88-113,
+ * :114-140, :142-168): the same Z / field update steps with the integrators' coefficients.
+ * integrator: 0 Euler, 1 RK2, 2 RK3, 3 RK3W7 */
+void or_flow(const int ext[4], const double* in, double* out, double eps, int n_step, int integrator)
+{
+    if (integrator == 2)
+    {
+        or_flow_rk3(ext, in, out, eps, n_step);
+        return;
+    }
+    Geo g = geo(ext);
+    size_t n = (size_t)g.V * 4 * 18;
+    double* Z = (double*)calloc(n, sizeof(double));
+    if (out != in) memcpy(out, in, n * sizeof(double));
+    for (int k = 0; k < n_step; ++k)
+    {
+        if (integrator == 0)
+        {
+            flow_z(&g, out, Z, 0.0, eps);
+            flow_update(&g, out, Z, 1.0);
+        }
+        else if (integrator == 1)
+        {
+            flow_z(&g, out, Z, 0.0, eps);
+            flow_update(&g, out, Z, 0.5);
+            flow_z(&g, out, Z, -0.5, eps);
+            flow_update(&g, out, Z, 1.0);
+        }
+        else
+        {
+            flow_z(&g, out, Z, 0.0, eps);
+            flow_update(&g, out, Z, 1.0 / 3.0);
+            flow_z(&g, out, Z, -25.0 / 48.0, 15.0 / 16.0 * eps);
+            flow_update(&g, out, Z, 1.0);
+            flow_z(&g, out, Z, -17.0 / 25.0, 8.0 / 15.0 * eps);
+            flow_update(&g, out, Z, 1.0);
+        }
+    }
+    free(Z);
+}
+
 /* ---------------------------------------------------------------- stout smearing */
 /* StoutSmearing4D (stout_smearing.hpp:29-57) */
 static void stout_step(const Geo* g, const double* in, double* out, double rho)
@@ -1095,4 +1136,134 @@ uint64_t or_bmw_decode(const int ext[4], const unsigned char* payload, int full,
                     }
                 }
     return adler64_final(A, B);
+}
+
+/* ---------------------------------------------------------------- measurement bundle */
+/* The observables SU3_main.cpp:89-235 measures on every smearing level. */
+
+/* TopChargeCloverTimeslice and EnergyDensity::CloverTimeslice (topological_charge.hpp:338-364,
+ * field_strength_tensor.hpp:178-195) for every t: the densities of or_topcharge_clover and
+ * or_energy_clover summed over one timeslice, with their normalisations (sum over t = total). */
+void or_clover_timeslices(const int ext[4], const double* U, double* q_t, double* e_t)
+{
+    Geo g = geo(ext);
+    for (int t = 0; t < ext[0]; ++t) q_t[t] = e_t[t] = 0.0;
+    for (long s = 0; s < g.V; ++s)
+    {
+        int c[4];
+        coords(&g, s, c);
+        M3 F[4][4];
+        double e = 0.0;
+        for (int mu = 0; mu < 4; ++mu)
+            for (int nu = mu + 1; nu < 4; ++nu)
+            {
+                M3 cl = clover(&g, U, s, mu, nu);
+                F[mu][nu] = sub(cl, dag(cl));
+                M3 f = scl(-I / 4.0, scl(0.5, F[mu][nu]));
+                cd tt = tr(f) / 3.0;
+                for (int i = 0; i < 3; ++i) f.m[i][i] -= tt;
+                e += creal(tr(mul(f, f)));
+            }
+        double q = creal(tr(sub(add(mul(F[0][1], F[2][3]), mul(F[0][3], F[1][2])), mul(F[0][2], F[1][3]))));
+        q_t[c[0]] += -1.0 / (64.0 * 4.0 * PI * PI) * q;
+        e_t[c[0]] += e / (double)g.V;
+    }
+}
+
+/* TopChargePlaquette (topological_charge.hpp:366-416): F = -i (P - P^dag) from the forward
+ * plaquettes, Q = 1/(16 pi^2) sum Re tr(F01 F23 + F02 F31 + F03 F12) */
+double or_topcharge_plaquette(const int ext[4], const double* U)
+{
+    Geo g = geo(ext);
+    double q = 0.0;
+    for (long s = 0; s < g.V; ++s)
+    {
+        M3 F[4][4];
+        for (int mu = 0; mu < 4; ++mu)
+            for (int nu = mu + 1; nu < 4; ++nu)
+            {
+                M3 p = plaquette(&g, U, s, mu, nu);
+                F[mu][nu] = scl(-I, sub(p, dag(p)));
+                F[nu][mu] = scl(-1.0, F[mu][nu]);
+            }
+        q += creal(tr(add(add(mul(F[0][1], F[2][3]), mul(F[0][2], F[3][1])), mul(F[0][3], F[1][2]))));
+    }
+    return 1.0 / (16.0 * PI * PI) * q;
+}
+
+/* Rectangular<2>::Action (actions/gauge/rectangular_action.hpp:61-94) with the 1x2 and 2x1
+ * loops of wilson_loop.hpp:155-175 */
+double or_rect_action(const int ext[4], const double* U, double beta, double c_plaq, double c_rect)
+{
+    Geo g = geo(ext);
+    double sp = 0.0, sr = 0.0;
+    for (long s = 0; s < g.V; ++s)
+        for (int nu = 1; nu < 4; ++nu)
+            for (int mu = 0; mu < nu; ++mu)
+            {
+                sp += creal(tr(plaquette(&g, U, s, mu, nu)));
+                long smu = move(&g, s, mu, 1), snu = move(&g, s, nu, 1);
+                long smu_nu = move(&g, smu, nu, 1), snu2 = move(&g, snu, nu, 1), smu2 = move(&g, smu, mu, 1);
+                /* <1,2>: U_mu(x) U_nu(x+mu) U_nu(x+mu+nu) U_mu(x+2nu)^dag U_nu(x+nu)^dag U_nu(x)^dag */
+                M3 r12 = mul(mul(mul(mul(mul(ld(U, s, mu), ld(U, smu, nu)), ld(U, smu_nu, nu)), dag(ld(U, snu2, mu))),
+                                 dag(ld(U, snu, nu))), dag(ld(U, s, nu)));
+                /* <2,1>: U_mu(x) U_mu(x+mu) U_nu(x+2mu) U_mu(x+mu+nu)^dag U_mu(x+nu)^dag U_nu(x)^dag */
+                M3 r21 = mul(mul(mul(mul(mul(ld(U, s, mu), ld(U, smu, mu)), ld(U, smu2, nu)), dag(ld(U, smu_nu, mu))),
+                                 dag(ld(U, snu, mu))), dag(ld(U, s, nu)));
+                sr += creal(tr(r12)) + creal(tr(r21));
+            }
+    return beta * (c_plaq * (6.0 * g.V - sp / 3.0) + c_rect * (12.0 * g.V - sr / 3.0));
+}
+
+/* Line product C_mu(x) = U_mu(x) U_mu(x+mu) ... U_mu(x+(L-1)mu) */
+static M3 line(const Geo* g, const double* U, long s, int mu, int L)
+{
+    M3 r = ld(U, s, mu);
+    long t = s;
+    for (int k = 1; k < L; ++k)
+    {
+        t = move(g, t, mu, 1);
+        r = mul(r, ld(U, t, mu));
+    }
+    return r;
+}
+
+/* WilsonLoop<0, L, true> (observables/wilson_loop.hpp:63-124): square L x L loops in all six
+ * planes, 1 - sum Re tr(C_mu(x) C_nu(x+L mu) C_mu(x+L nu)^dag C_nu(x)^dag) / (6 * 3 * V) */
+double or_wilson_loop(const int ext[4], const double* U, int L)
+{
+    Geo g = geo(ext);
+    double w = 0.0;
+    for (long s = 0; s < g.V; ++s)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int nu = mu + 1; nu < 4; ++nu)
+            {
+                long smu = s, snu = s;
+                for (int k = 0; k < L; ++k)
+                {
+                    smu = move(&g, smu, mu, 1);
+                    snu = move(&g, snu, nu, 1);
+                }
+                M3 m = mul(mul(mul(line(&g, U, s, mu, L), line(&g, U, smu, nu, L)), dag(line(&g, U, snu, mu, L))),
+                           dag(line(&g, U, s, nu, L)));
+                w += creal(tr(m));
+            }
+    return 1.0 - w / (18.0 * (double)g.V);
+}
+
+/* PolyakovLoop (observables/polyakov_loop.hpp:32-49): the trace of the product of the t links
+ * over every spatial site, averaged over the spatial volume */
+void or_polyakov_loop(const int ext[4], const double* U, double* re, double* im)
+{
+    Geo g = geo(ext);
+    cd p = 0.0;
+    long vs = (long)ext[1] * ext[2] * ext[3];
+    for (long k = 0; k < vs; ++k)
+    {
+        M3 m = id3();
+        for (int t = 0; t < ext[0]; ++t) m = mul(m, ld(U, (long)t * vs + k, 0));
+        p += tr(m);
+    }
+    *re = creal(p) / (double)vs;
+    *im = cimag(p) / (double)vs;
 }

@@ -54,6 +54,16 @@ void     or_bias_update_symmetric(or_bias* b, double cv);
 double   or_bias_potential(const or_bias* b, double cv);
 double   or_bias_derivative(const or_bias* b, double cv);
 
+/* Flow with any of the reference's integrators: 0 Euler, 1 RK2, 2 RK3, 3 RK3W7 */
+void   or_flow(const int ext[4], const double* in, double* out, double eps, int n_step, int integrator);
+
+/* The measurement bundle of SU3_main.cpp:89-235 */
+void   or_clover_timeslices(const int ext[4], const double* U, double* q_t, double* e_t);
+double or_topcharge_plaquette(const int ext[4], const double* U);
+double or_rect_action(const int ext[4], const double* U, double beta, double c_plaq, double c_rect);
+double or_wilson_loop(const int ext[4], const double* U, int L);
+void   or_polyakov_loop(const int ext[4], const double* U, double* re, double* im);
+
 /* BMW configuration payload and its Adler-64 checksum (IO/config_io/bmw_format.hpp:63-97,
  * :131-394, :406-645); full = 1 for the 18-real #18BMW variant.  encode writes the payload when
  * payload is not NULL; both return the checksum. */
