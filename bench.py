@@ -286,6 +286,23 @@ def secondary_rates(lt, torch, timed, prec):
     except Exception as e:
         out["bmw_error"] = repr(e)
     try:
+        # the driver's measurement step at 32^4 (clover Q and E per timeslice, plaquette, plaquette
+        # charge, Symanzik action, Wilson loops L = 2, 4, 8, Polyakov loop) from the given storage,
+        # each observable a device pass plus a host read of its sums
+        ext = (32,) * 4
+        G = lt.GaugeField(ext, prec)
+        G.SetToHaarRandom(13)
+        lt.UpdateSweeps(G, BETA, 5, 1, 4, SEED)
+        lt.Measure(G, BETA)
+        n = 5
+        ms = timed(G, lambda: lt.Measure(G, BETA), n) / n
+        out["measure_bundle_ms_32^4"] = ms
+        out["wilson_loop_L8_ms_32^4"] = timed(G, lambda: lt.WilsonLoop(G, 8), n) / n
+        out["polyakov_loop_ms_32^4"] = timed(G, lambda: lt.PolyakovLoop(G), n) / n
+        del G
+    except Exception as e:
+        out["measure_error"] = repr(e)
+    try:
         # 48^4 at beta = 6.3: Haar start, 200 rounds of 1 HB + 4 OR, two OMF2 trajectories
         # (tau = 1, 20 steps, FP32 links, FP64 dH and accept), then Wilson flow to t0
         # (t^2 E = 0.3) with clover Q and E at every step

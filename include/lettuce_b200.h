@@ -129,6 +129,23 @@ int lt_topcharge_clover(lt_lattice* h, double* out);
 int lt_energy_clover(lt_lattice* h, double* out);
 /* Both of the above from one pass over the clover leaves. */
 int lt_clover_observables(lt_lattice* h, double* q_out, double* e_out);
+/* The measurement bundle of the reference driver (SU3_main.cpp:89-235).
+ * TopChargeCloverTimeslice and EnergyDensity::CloverTimeslice (topological_charge.hpp:338-364,
+ * field_strength_tensor.hpp:178-195) for every t = 0..Nt-1 (each array Nt doubles; either may
+ * be NULL); the timeslices sum to lt_topcharge_clover / lt_energy_clover. */
+int lt_clover_timeslices(lt_lattice* h, double* q_t, double* e_t);
+/* TopChargePlaquette (topological_charge.hpp:366-416). */
+int lt_topcharge_plaquette(lt_lattice* h, double* out);
+/* GaugeAction::Rectangular<2>::Action (actions/gauge/rectangular_action.hpp:61-94) with
+ * coefficients c_plaq, c_rect (the driver's Symanzik action: 5/3, -1/12); divide by 6 beta V
+ * for ActionNormalized. */
+int lt_rect_action(lt_lattice* h, double beta, double c_plaq, double c_rect, double* out);
+/* WilsonLoop (observables/wilson_loop.hpp:63-124): 1 - sum Re tr W_LxL / (18 V) over all sites
+ * and the six planes, for square L x L loops (the driver measures L = 2, 4, 8). */
+int lt_wilson_loop(lt_lattice* h, int L, double* out);
+/* PolyakovLoop (observables/polyakov_loop.hpp:32-49): mean over the spatial sites of the trace
+ * of the product of the links in direction t. */
+int lt_polyakov_loop(lt_lattice* h, double* re, double* im);
 /* WilsonAction::Staple for every link (rectangular_action.hpp:104-184), reference layout. */
 int lt_staples(lt_lattice* h, double* staples_out);
 /* Plaquette sum of a field that the caller already holds in device memory, in the reference
@@ -150,7 +167,7 @@ int lt_overrelax_sweeps(lt_lattice* h, int n_sweep);
  * *counter; *counter is advanced by n_sweep. */
 int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, uint64_t* counter);
 /* n_sweep rounds of (n_hb heatbath + n_or overrelaxation) sweeps, as the driver's update
- * loop (SU3_main.cpp:381-402); launched as one CUDA graph. */
+ * loop (SU3_main.cpp:381-402); 8 chained launches per sweep on the handle's stream. */
 int lt_update_sweeps(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed,
                      uint64_t* counter);
 
@@ -180,6 +197,14 @@ int lt_tempering_swap(lt_lattice* a, lt_lattice* b, const lt_bias* bias, double 
                       double q_b, double u, int* accepted, double* dE_out);
 
 /* ---- smearing ------------------------------------------------------------------------ */
+/* Integrators::GradientFlow (smearing/gradient_flow.hpp:31-168) */
+#define LT_FLOW_EULER 0  /* Euler (:31-56), the smoothing of the reference's measurement step */
+#define LT_FLOW_RK2   1  /* RK2 (:88-113) */
+#define LT_FLOW_RK3   2  /* RK3 (:114-140), Luscher's third-order scheme */
+#define LT_FLOW_RK3W7 3  /* RK3W7 (:142-168) */
+/* GradientFlowKernel (:252-367) with any of the integrators: out = in flowed by n_step steps
+ * of size eps (in == out continues a flow, as GradientFlowKernel::Resume). */
+int lt_flow(lt_lattice* in, lt_lattice* out, int integrator, double eps, int n_step);
 /* GradientFlowKernel<RK3>::operator() (smearing/gradient_flow.hpp:120-168, :339-345):
  * out = in flowed by n_step RK3 steps of size eps.  in == out continues in place
  * (GradientFlowKernel::Resume, :347-351). */

@@ -15,6 +15,7 @@
 #pragma once
 
 #include <array>
+#include <complex>
 #include <cstdint>
 #include <filesystem>
 #include <fstream>
@@ -133,7 +134,79 @@ struct Wilson
     double ActionNormalized(const GaugeField& U) const { return Action(U) / (6.0 * beta * (double)U.Volume()); }
 };
 inline Wilson WilsonAction;
+
+// Rectangular<2> (actions/gauge/rectangular_action.hpp:23-94): plaquettes weighted by c_plaq
+// and 1x2 plus 2x1 rectangles by c_rect; the tree-level Symanzik choice is (5/3, -1/12).
+template <int stencil_radius_>
+struct Rectangular
+{
+    static_assert(stencil_radius_ > 0 && stencil_radius_ <= 2, "Invalid stencil_radius!");
+    double beta = 6.0;
+    const double c_plaq = 1.0;
+    const double c_rect = 0.0;
+    Rectangular(double beta_in, double c_plaq_in, double c_rect_in) : beta(beta_in), c_plaq(c_plaq_in), c_rect(c_rect_in) {}
+    void SetBeta(double b) { beta = b; }
+    double GetBeta() const { return beta; }
+    double Action(const GaugeField& U) const
+    {
+        double v;
+        check(lt_rect_action(U.handle(), beta, c_plaq, c_rect, &v));
+        return v;
+    }
+    double ActionNormalized(const GaugeField& U) const { return Action(U) / (6.0 * beta * (double)U.Volume()); }
+};
 } // namespace GaugeAction
+
+// TopChargeCloverTimeslice (observables/topological_charge.hpp:233-364) and
+// EnergyDensity::CloverTimeslice (observables/field_strength_tensor.hpp:178-195): one launch
+// computes every timeslice; the vector forms return all of them.
+inline std::vector<double> TopChargeCloverTimeslices(const GaugeField& U)
+{
+    std::vector<double> q((size_t)U.Length(0));
+    check(lt_clover_timeslices(U.handle(), q.data(), nullptr));
+    return q;
+}
+inline double TopChargeCloverTimeslice(const GaugeField& U, int t) { return TopChargeCloverTimeslices(U).at((size_t)t); }
+
+namespace EnergyDensity
+{
+inline double Clover(const GaugeField& U) { return EnergyDensityClover(U); }
+inline std::vector<double> CloverTimeslices(const GaugeField& U)
+{
+    std::vector<double> e((size_t)U.Length(0));
+    check(lt_clover_timeslices(U.handle(), nullptr, e.data()));
+    return e;
+}
+inline double CloverTimeslice(const GaugeField& U, int t) { return CloverTimeslices(U).at((size_t)t); }
+} // namespace EnergyDensity
+
+// observables/topological_charge.hpp:366-416
+inline double TopChargePlaquette(const GaugeField& U)
+{
+    double v;
+    check(lt_topcharge_plaquette(U.handle(), &v));
+    return v;
+}
+
+// WilsonLoop<N_mu_start, N_mu_end, reset>(U, U_chain) (observables/wilson_loop.hpp:63-124):
+// 1 - sum Re tr W / (18 V) over the square N_mu_end x N_mu_end loops.  The device builds the
+// line products itself, so U_chain is accepted for the signature and left untouched.
+template <int N_mu_start, int N_mu_end, bool reset>
+double WilsonLoop(const GaugeField& U, GaugeField& /*U_chain*/)
+{
+    static_assert(N_mu_start >= 0 && N_mu_end >= 0, "The template parameters of WilsonLoop are not allowed to be negative!");
+    double v;
+    check(lt_wilson_loop(U.handle(), N_mu_end, &v));
+    return v;
+}
+
+// observables/polyakov_loop.hpp:32-49
+inline std::complex<double> PolyakovLoop(const GaugeField& U)
+{
+    double re, im;
+    check(lt_polyakov_loop(U.handle(), &re, &im));
+    return {re, im};
+}
 
 // HeatbathKernel (updates/heatbath.hpp:30-130); beta fixed at construction (:40).  Its random
 // stream is (seed, counter) of Philox4x32-10, so SaveState / LoadState (the PRNG's checkpoint
@@ -196,13 +269,29 @@ inline void Checkerboard4(OverrelaxationSubgroupKernel& k, int n_sweep = 1) { Ch
 
 namespace Integrators::GradientFlow
 {
+struct Euler   // smearing/gradient_flow.hpp:31-56
+{
+    static constexpr int ID = LT_FLOW_EULER;
+    static std::string ReturnName() { return "Euler/StoutSmearing"; }
+};
+struct RK2   // smearing/gradient_flow.hpp:89-118
+{
+    static constexpr int ID = LT_FLOW_RK2;
+    static std::string ReturnName() { return "RK2"; }
+};
 struct RK3   // smearing/gradient_flow.hpp:120-168
 {
+    static constexpr int ID = LT_FLOW_RK3;
     static std::string ReturnName() { return "RK3"; }
+};
+struct RK3W7   // smearing/gradient_flow.hpp:170-218
+{
+    static constexpr int ID = LT_FLOW_RK3W7;
+    static std::string ReturnName() { return "RK3W7"; }
 };
 } // namespace Integrators::GradientFlow
 
-// GradientFlowKernel (smearing/gradient_flow.hpp:252-367) with the RK3 integrator
+// GradientFlowKernel (smearing/gradient_flow.hpp:252-367) with any of the integrators above
 template <typename IntegratorT = Integrators::GradientFlow::RK3, typename ActionT = GaugeAction::Wilson>
 struct GradientFlowKernel
 {
@@ -213,8 +302,8 @@ struct GradientFlowKernel
         : U_unflowed(in), U_flowed(out), epsilon(eps)
     {
     }
-    void operator()(int n_step) const { check(lt_flow_rk3(U_unflowed.handle(), U_flowed.handle(), epsilon, n_step)); }
-    void Resume(int n_step) const { check(lt_flow_rk3(U_flowed.handle(), U_flowed.handle(), epsilon, n_step)); }
+    void operator()(int n_step) const { check(lt_flow(U_unflowed.handle(), U_flowed.handle(), IntegratorT::ID, epsilon, n_step)); }
+    void Resume(int n_step) const { check(lt_flow(U_flowed.handle(), U_flowed.handle(), IntegratorT::ID, epsilon, n_step)); }
     void SetEpsilon(double e) { epsilon = e; }
     double GetEpsilon() const { return epsilon; }
     std::string ReturnIntegratorName() const { return IntegratorT::ReturnName(); }

@@ -243,27 +243,65 @@ def UpdateSweeps(U: GaugeField, beta: float, n_sweep: int, n_hb: int, n_or: int,
     return c.value
 
 
+class Euler:
+    """Integrators::GradientFlow::Euler (smearing/gradient_flow.hpp:31-56)."""
+    ID = 0
+
+    @staticmethod
+    def ReturnName() -> str:
+        return "Euler/StoutSmearing"
+
+
+class RK2:
+    """Integrators::GradientFlow::RK2 (smearing/gradient_flow.hpp:89-118)."""
+    ID = 1
+
+    @staticmethod
+    def ReturnName() -> str:
+        return "RK2"
+
+
 class RK3:
     """Integrators::GradientFlow::RK3 (smearing/gradient_flow.hpp:120-168)."""
+    ID = 2
 
     @staticmethod
     def ReturnName() -> str:
         return "RK3"
 
 
+class RK3W7:
+    """Integrators::GradientFlow::RK3W7 (smearing/gradient_flow.hpp:170-218)."""
+    ID = 3
+
+    @staticmethod
+    def ReturnName() -> str:
+        return "RK3W7"
+
+
 class GradientFlowKernel:
-    """GradientFlowKernel (smearing/gradient_flow.hpp:252-367) with the RK3 integrator."""
+    """GradientFlowKernel (smearing/gradient_flow.hpp:252-367) with any of the integrators above."""
 
     def __init__(self, U_unflowed: GaugeField, U_flowed: GaugeField, integrator=RK3, action=None, epsilon: float = 0.01):
-        if integrator is not RK3:
-            raise ValueError("only the RK3 integrator is provided")
+        if integrator not in (Euler, RK2, RK3, RK3W7):
+            raise ValueError("integrator must be Euler, RK2, RK3 or RK3W7")
+        self.integrator = integrator
         self.U_unflowed, self.U_flowed, self.epsilon = U_unflowed, U_flowed, float(epsilon)
 
+    def _run(self, src: GaugeField, n_step: int) -> None:
+        if self.integrator is RK3:
+            check(lib().lt_flow_rk3(src.handle, self.U_flowed.handle, self.epsilon, int(n_step)))
+        else:
+            check(lib().lt_flow(src.handle, self.U_flowed.handle, self.integrator.ID, self.epsilon, int(n_step)))
+
     def __call__(self, n_step: int) -> None:
-        check(lib().lt_flow_rk3(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, int(n_step)))
+        self._run(self.U_unflowed, n_step)
 
     def Resume(self, n_step: int) -> None:
-        check(lib().lt_flow_rk3(self.U_flowed.handle, self.U_flowed.handle, self.epsilon, int(n_step)))
+        self._run(self.U_flowed, n_step)
+
+    def ReturnIntegratorName(self) -> str:
+        return self.integrator.ReturnName()
 
     def Measure(self, n_meas: int, every: int):
         """Flow from U_unflowed with (plaquette sum, Q, E) after every `every` steps."""
@@ -470,6 +508,87 @@ def TemperingSwap(a: GaugeField, b: GaugeField, bias: MetaBiasPotential, scale_a
     return bool(acc.value), dE.value
 
 
+# ---------------------------------------------------------------- measurement bundle
+def TopChargeCloverTimeslice(U: GaugeField) -> np.ndarray:
+    """TopChargeCloverTimeslice for every t (observables/topological_charge.hpp:338-364)."""
+    q = np.empty(U.ext[0])
+    check(lib().lt_clover_timeslices(U.handle, q.ctypes.data, None))
+    return q
+
+
+def EnergyDensityCloverTimeslice(U: GaugeField) -> np.ndarray:
+    """EnergyDensity::CloverTimeslice for every t (observables/field_strength_tensor.hpp:178-195)."""
+    e = np.empty(U.ext[0])
+    check(lib().lt_clover_timeslices(U.handle, None, e.ctypes.data))
+    return e
+
+
+def TopChargePlaquette(U: GaugeField) -> float:
+    """observables/topological_charge.hpp:366-416."""
+    return _out1(lib().lt_topcharge_plaquette, U.handle)
+
+
+class RectangularAction:
+    """GaugeAction::Rectangular<2> (actions/gauge/rectangular_action.hpp:23-94) with plaquette
+    and 1x2 coefficients; SymanzikAction(beta) is the driver's tree-level Symanzik choice."""
+
+    def __init__(self, beta: float, c_plaq: float, c_rect: float):
+        self.beta, self.c_plaq, self.c_rect = float(beta), float(c_plaq), float(c_rect)
+
+    def Action(self, U: GaugeField) -> float:
+        return _out1(lib().lt_rect_action, U.handle, self.beta, self.c_plaq, self.c_rect)
+
+    def ActionNormalized(self, U: GaugeField) -> float:
+        return self.Action(U) / (6.0 * self.beta * U.Volume())
+
+
+def SymanzikAction(beta: float) -> RectangularAction:
+    """Rectangular<2>(beta, 1 + 8/12, -1/12) as in SU3_main.cpp:115."""
+    return RectangularAction(beta, 1.0 + 8.0 / 12.0, -1.0 / 12.0)
+
+
+def WilsonLoop(U: GaugeField, L: int) -> float:
+    """Square L x L Wilson loops: 1 - sum Re tr W / (18 V) (observables/wilson_loop.hpp:63-124)."""
+    return _out1(lib().lt_wilson_loop, U.handle, int(L))
+
+
+def PolyakovLoop(U: GaugeField) -> complex:
+    """observables/polyakov_loop.hpp:32-49."""
+    re, im = C.c_double(), C.c_double()
+    check(lib().lt_polyakov_loop(U.handle, C.byref(re), C.byref(im)))
+    return complex(re.value, im.value)
+
+
+def Measure(U: GaugeField, beta: float) -> dict:
+    """The PerformMeasurements step of the reference driver (SU3_main.cpp:117-139) on one field,
+    with the normalisations of its output (:160-167)."""
+    V = U.Volume()
+    q_t, e_t = np.empty(U.ext[0]), np.empty(U.ext[0])
+    check(lib().lt_clover_timeslices(U.handle, q_t.ctypes.data, e_t.ctypes.data))
+    plaq = PlaquetteSum(U) / V
+    return {"Wilson_Action": 1.0 - plaq / 18.0, "Improved_Action": SymanzikAction(beta).ActionNormalized(U),
+            "Plaquette": plaq, "E_plaq": 36.0 - 2.0 * plaq, "E_clov": float(e_t.sum()), "E_clov_timeslice": e_t,
+            "Wilson_loop(L=2)": WilsonLoop(U, 2), "Wilson_loop(L=4)": WilsonLoop(U, 4),
+            "Wilson_loop(L=8)": WilsonLoop(U, 8), "Polyakov_loop": PolyakovLoop(U),
+            "TopChargeClov": float(q_t.sum()), "TopChargeClov_timeslice": q_t, "TopChargePlaq": TopChargePlaquette(U)}
+
+
+def Observables(U: GaugeField, beta: float, n_smear: int, smear_skip: int, epsilon: float) -> list:
+    """Observables (SU3_main.cpp:89-235): measurements on U and on n_smear levels of Euler
+    gradient flow, smear_skip steps of size epsilon apart; one dict per level."""
+    out = [Measure(U, beta)]
+    if n_smear > 0:
+        S = GaugeField(U.ext, U.prec)
+        flow = GradientFlowKernel(U, S, Euler, None, epsilon)
+        for k in range(1, n_smear + 1):
+            if k == 1:
+                flow(smear_skip)
+            else:
+                flow.Resume(smear_skip)
+            out.append(Measure(S, beta))
+    return out
+
+
 def CloverDerivative(U: GaugeField) -> np.ndarray:
     """CloverDerivative for every link (observables/clover.hpp:279-321)."""
     out = np.empty((U.Volume(), 4, 3, 3, 2))
@@ -484,4 +603,6 @@ __all__ = ["STATUS_NONFINITE", "STATUS_UNITARITY", "STATUS_HB_CAP", "GaugeField"
            "CloverObservables", "Staples", "WilsonAction", "HeatbathKernel", "OverrelaxationSubgroupKernel",
            "Iterator", "UpdateSweeps", "RK3", "GradientFlowKernel", "StoutSmearing4D", "StoutSmearingN",
            "MetaBiasPotential", "HMCKernel", "HMCMetaDKernel", "CloverDerivative", "LettuceError", "Ensemble",
-           "TemperingSwap"]
+           "TemperingSwap", "Euler", "RK2", "RK3W7", "TopChargeCloverTimeslice", "EnergyDensityCloverTimeslice",
+           "TopChargePlaquette", "RectangularAction", "SymanzikAction", "WilsonLoop", "PolyakovLoop", "Measure",
+           "Observables"]

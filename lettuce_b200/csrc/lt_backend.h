@@ -50,6 +50,18 @@ public:
     // atomically maxes the float bits of the largest |U U^dag - 1| entry into *maxbits
     virtual void check_links(const Ctx& c, const void* U, double tol, unsigned* maxbits) const = 0;
 
+    // measurement bundle (SU3_main.cpp:89-235): clover densities per timeslice into partials
+    // (q then e, nbx blocks per timeslice); plaquette, rectangle and plaquette-charge sums into
+    // results[slot..slot+2]; Polyakov loop re, im into results[slot..slot+1]; straight-line
+    // products of the links (full FP64 matrices) for square Wilson loops
+    virtual void clover_timeslices(const Ctx& c, const void* U, double* partials, int nbx) const = 0;
+    virtual void loops(const Ctx& c, const void* U, int slot) const = 0;
+    virtual void polyakov(const Ctx& c, const void* U, int slot) const = 0;
+    virtual void chain_init(const Ctx& c, const void* U, void* C) const = 0;
+    virtual void chain_extend(const Ctx& c, const void* Cin, const void* U, void* Cout, int L) const = 0;
+    virtual void chain_double(const Ctx& c, const void* Cin, void* Cout, int L) const = 0;
+    virtual void wilson_square(const Ctx& c, const void* C, int L, int slot) const = 0;
+
     // BMW payload (full: 18 reals per link, else 12) to / from device memory; Adler-64 partial
     // sums (A then B, kRedBlocks each) into partials; unpack sets bit 0 of *flags for a link
     // that fails the reference's group-element test

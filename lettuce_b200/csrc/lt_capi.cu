@@ -1,5 +1,6 @@
 // C ABI of the lattice handle: device memory, one stream per handle, and the sequencing
 // of kernels for sweeps, flow, stout smearing, HMC and the metadynamics force.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -79,21 +80,38 @@ int order_after(lt_lattice* dst, const lt_lattice* src)
 const double kPi = 3.14159265358979323846;
 
 // Integrators::GradientFlow::RK3 (smearing/gradient_flow.hpp:151-161): three fused stages
-int flow_steps(lt_lattice* h, double eps, int n_step)
+// Stages of the reference's flow integrators (smearing/gradient_flow.hpp:31-168), each one
+// fused Z update + exponential update: Z <- c_old Z + c_new eps Algebra(st U^dag),
+// U <- exp(c_exp Z) U
+struct FlowStage
 {
+    double c_old, c_new, c_exp;
+    int read_z, write_z;
+};
+constexpr FlowStage kEuler[] = { { 0.0, 1.0, 1.0, 0, 0 } };
+constexpr FlowStage kRK2[] = { { 0.0, 1.0, 0.5, 0, 1 }, { -0.5, 1.0, 1.0, 1, 0 } };
+constexpr FlowStage kRK3[] = { { 0.0, 1.0, 0.25, 0, 1 }, { -17.0 / 36.0, 8.0 / 9.0, 1.0, 1, 1 }, { -1.0, 3.0 / 4.0, 1.0, 1, 0 } };
+constexpr FlowStage kRK3W7[] = { { 0.0, 1.0, 1.0 / 3.0, 0, 1 },
+                                 { -25.0 / 48.0, 15.0 / 16.0, 1.0, 1, 1 },
+                                 { -17.0 / 25.0, 8.0 / 15.0, 1.0, 1, 0 } };
+
+int flow_steps(lt_lattice* h, double eps, int n_step, int integrator = LT_FLOW_RK3)
+{
+    const FlowStage* st = integrator == LT_FLOW_EULER ? kEuler
+                        : integrator == LT_FLOW_RK2   ? kRK2
+                        : integrator == LT_FLOW_RK3W7 ? kRK3W7 : kRK3;
+    const int ns = integrator == LT_FLOW_EULER ? 1 : integrator == LT_FLOW_RK2 ? 2 : 3;
     LT_TRY(ensure(h, &h->U2, h->be->gauge_bytes(h->g)));
-    LT_TRY(ensure(h, &h->Z, h->be->alg_bytes(h->g)));
+    if (ns > 1) LT_TRY(ensure(h, &h->Z, h->be->alg_bytes(h->g)));
     const lt::Ctx c = h->ctx();
     for (int k = 0; k < n_step; ++k)
-    {
-        h->be->flow_stage(c, h->U, h->U2, h->Z, 0.0, eps, 0.25, 0, 1);
-        std::swap(h->U, h->U2);
-        h->be->flow_stage(c, h->U, h->U2, h->Z, -17.0 / 36.0, 8.0 / 9.0 * eps, 1.0, 1, 1);
-        std::swap(h->U, h->U2);
-        h->be->flow_stage(c, h->U, h->U2, h->Z, -1.0, 3.0 / 4.0 * eps, 1.0, 1, 0);
-        std::swap(h->U, h->U2);
-    }
-    return launched("flow_rk3");
+        for (int j = 0; j < ns; ++j)
+        {
+            h->be->flow_stage(c, h->U, h->U2, h->Z, st[j].c_old, st[j].c_new * eps, st[j].c_exp, st[j].read_z,
+                              st[j].write_z);
+            std::swap(h->U, h->U2);
+        }
+    return launched("flow");
 }
 
 int stout_steps(lt_lattice* h, double rho, int n)
@@ -300,8 +318,8 @@ int lt_destroy(lt_lattice* h)
     if (!h) return LT_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,  h->R,
-                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status };
+    void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,  h->R,      h->chainA,
+                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB };
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (void* p : h->levels) cudaFree(p);
@@ -509,6 +527,101 @@ int lt_energy_clover(lt_lattice* h, double* out)
     return clover_q_e(h, h->U, nullptr, out);
 }
 
+int lt_clover_timeslices(lt_lattice* h, double* q_t, double* e_t)
+{
+    LT_TRY(check_h(h, "lt_clover_timeslices"));
+    if (!q_t && !e_t) return lt::set_error(LT_ERR_ARG, "lt_clover_timeslices: null pointers");
+    const int nt = h->g.n[0];
+    const int nbx = std::max(1, std::min(lt::kRedBlocks / nt, (h->g.V / nt + lt::kRedThreads - 1) / lt::kRedThreads));
+    h->be->clover_timeslices(h->ctx(), h->U, h->partials, nbx);
+    LT_TRY(launched("lt_clover_timeslices"));
+    std::vector<double> p((size_t)2 * nt * nbx);
+    LT_CK(cudaMemcpyAsync(p.data(), h->partials, sizeof(double) * p.size(), cudaMemcpyDeviceToHost, h->stream));
+    LT_CK(cudaStreamSynchronize(h->stream));
+    for (int t = 0; t < nt; ++t)
+    {
+        double sq = 0.0, cq = 0.0, se = 0.0, ce = 0.0;   // Kahan, fixed order
+        for (int b = 0; b < nbx; ++b)
+        {
+            double y = p[(size_t)t * nbx + b] - cq, s2 = sq + y;
+            cq = (s2 - sq) - y;
+            sq = s2;
+            y = p[(size_t)(nt + t) * nbx + b] - ce;
+            s2 = se + y;
+            ce = (s2 - se) - y;
+            se = s2;
+        }
+        if (q_t) q_t[t] = -1.0 / (64.0 * 4.0 * kPi * kPi) * sq;
+        if (e_t) e_t[t] = se / (double)h->g.V;
+    }
+    return LT_OK;
+}
+
+int lt_topcharge_plaquette(lt_lattice* h, double* out)
+{
+    LT_TRY(check_h(h, "lt_topcharge_plaquette"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_topcharge_plaquette: null pointer");
+    h->be->loops(h->ctx(), h->U, 4);
+    double r[3];
+    LT_TRY(fetch(h, 4, 3, r));
+    *out = 1.0 / (16.0 * kPi * kPi) * r[2];
+    return LT_OK;
+}
+
+int lt_rect_action(lt_lattice* h, double beta, double c_plaq, double c_rect, double* out)
+{
+    LT_TRY(check_h(h, "lt_rect_action"));
+    if (!out) return lt::set_error(LT_ERR_ARG, "lt_rect_action: null pointer");
+    h->be->loops(h->ctx(), h->U, 4);
+    double r[3];
+    LT_TRY(fetch(h, 4, 3, r));
+    const double V = (double)h->g.V;
+    *out = beta * (c_plaq * (6.0 * V - r[0] / 3.0) + c_rect * (12.0 * V - r[1] / 3.0));
+    return LT_OK;
+}
+
+int lt_wilson_loop(lt_lattice* h, int L, double* out)
+{
+    LT_TRY(check_h(h, "lt_wilson_loop"));
+    if (!out || L < 1) return lt::set_error(LT_ERR_ARG, "lt_wilson_loop: null pointer or L < 1");
+    const size_t bytes = (size_t)4 * h->g.V * 9 * 2 * sizeof(double);
+    LT_TRY(ensure(h, &h->chainA, bytes));
+    LT_TRY(ensure(h, &h->chainB, bytes));
+    const lt::Ctx c = h->ctx();
+    h->be->chain_init(c, h->U, h->chainA);
+    void *cur = h->chainA, *nxt = h->chainB;
+    if ((L & (L - 1)) == 0)
+        for (int len = 1; len < L; len *= 2)
+        {
+            h->be->chain_double(c, cur, nxt, len);
+            std::swap(cur, nxt);
+        }
+    else
+        for (int len = 1; len < L; ++len)
+        {
+            h->be->chain_extend(c, cur, h->U, nxt, len);
+            std::swap(cur, nxt);
+        }
+    h->be->wilson_square(c, cur, L, 0);
+    double w;
+    LT_TRY(fetch(h, 0, 1, &w));
+    *out = 1.0 - w / (18.0 * (double)h->g.V);
+    return LT_OK;
+}
+
+int lt_polyakov_loop(lt_lattice* h, double* re, double* im)
+{
+    LT_TRY(check_h(h, "lt_polyakov_loop"));
+    if (!re || !im) return lt::set_error(LT_ERR_ARG, "lt_polyakov_loop: null pointer");
+    h->be->polyakov(h->ctx(), h->U, 0);
+    double r[2];
+    LT_TRY(fetch(h, 0, 2, r));
+    const double vs = (double)(h->g.V / h->g.n[0]);
+    *re = r[0] / vs;
+    *im = r[1] / vs;
+    return LT_OK;
+}
+
 int lt_clover_observables(lt_lattice* h, double* q_out, double* e_out)
 {
     LT_TRY(check_h(h, "lt_clover_observables"));
@@ -576,6 +689,16 @@ int lt_flow_rk3(lt_lattice* in, lt_lattice* out, double eps, int n_step)
     if (n_step < 0) return lt::set_error(LT_ERR_ARG, "lt_flow_rk3: n_step < 0");
     LT_TRY(lt_copy(out, in));
     return flow_steps(out, eps, n_step);
+}
+
+int lt_flow(lt_lattice* in, lt_lattice* out, int integrator, double eps, int n_step)
+{
+    LT_TRY(check_h(in, "lt_flow"));
+    LT_TRY(check_h(out, "lt_flow"));
+    if (n_step < 0 || integrator < LT_FLOW_EULER || integrator > LT_FLOW_RK3W7)
+        return lt::set_error(LT_ERR_ARG, "lt_flow: n_step < 0 or unknown integrator");
+    LT_TRY(lt_copy(out, in));
+    return flow_steps(out, eps, n_step, integrator);
 }
 
 int lt_flow_rk3_measure(lt_lattice* in, lt_lattice* out, double eps, int n_meas, int every, double* plaq_out,

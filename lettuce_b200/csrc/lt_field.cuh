@@ -22,6 +22,7 @@ namespace lt {
 
 // Reduction grid: 148 SMs x 8 blocks, fixed so that every reduction sums in the same order.
 constexpr int kRedBlocks = 1184;
+constexpr int kRedThreads = 256;
 
 // Bits of a lattice handle's device status word (LT_STATUS_* of the C ABI)
 constexpr unsigned kStatusNonFinite = 1u;   // a link holds NaN or Inf

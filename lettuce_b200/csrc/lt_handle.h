@@ -47,6 +47,8 @@ struct lt_lattice
     double* h_results = nullptr; // pinned
     double* d_aos = nullptr;     // staging buffer for host transfers (reference layout)
     unsigned* status = nullptr;  // device status word (lt_status_word) and scratch words
+    void* chainA = nullptr;      // straight-line link products of lt_wilson_loop (FP64 full matrices)
+    void* chainB = nullptr;
 
     lt::Ctx ctx() const
     {

@@ -43,6 +43,7 @@ template <typename T, int NR> class BackendImpl final : public Backend
     static Alg<T> alg(const void* p, const Geom& g) { Alg<T> a; a.p = (T*)p; a.vh = g.vh; return a; }
     static Full<T> full(const void* p, const Geom& g) { Full<T> a; a.p = (cx<T>*)p; a.vh = g.vh; return a; }
     static Clov<T> clov(const void* p, const Geom& g) { Clov<T> a; a.p = (T*)p; a.vh = g.vh; return a; }
+    static Full<double> full64(const void* p, const Geom& g) { Full<double> a; a.p = (cx<double>*)p; a.vh = g.vh; return a; }
 
     static void finish(const Ctx& c, int slot, int nslot)
     {
@@ -118,6 +119,39 @@ public:
     void check_links(const Ctx& c, const void* U, double tol, unsigned* maxbits) const override
     {
         k_check_links<T, NR><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, tol, c.status, maxbits);
+    }
+    void clover_timeslices(const Ctx& c, const void* U, double* partials, int nbx) const override
+    {
+        k_clover_timeslice<T, NR><<<dim3(nbx, c.g.n[0]), kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, partials);
+    }
+    void loops(const Ctx& c, const void* U, int slot) const override
+    {
+        k_loops<T, NR><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 3);
+    }
+    void polyakov(const Ctx& c, const void* U, int slot) const override
+    {
+        k_polyakov<T, NR><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 2);
+    }
+    void chain_init(const Ctx& c, const void* U, void* C) const override
+    {
+        k_chain_init<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(gauge(U, c.g), full64(C, c.g), c.g);
+    }
+    void chain_extend(const Ctx& c, const void* Cin, const void* U, void* Cout, int L) const override
+    {
+        k_chain_extend<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(full64(Cin, c.g), gauge(U, c.g),
+                                                                                full64(Cout, c.g), c.g, L);
+    }
+    void chain_double(const Ctx& c, const void* Cin, void* Cout, int L) const override
+    {
+        k_chain_double<<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(full64(Cin, c.g), full64(Cout, c.g), c.g, L);
+    }
+    void wilson_square(const Ctx& c, const void* C, int L, int slot) const override
+    {
+        k_wilson_square<<<kRedBlocks, kRedThreads, 0, c.stream>>>(full64(C, c.g), c.g, L,
+                                                                   c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 1);
     }
     void bmw_pack(const Ctx& c, const void* U, int full, void* out, unsigned long long* partials) const override
     {

@@ -8,7 +8,6 @@
 namespace lt {
 
 constexpr int kThreads = 128;
-constexpr int kRedThreads = 256;
 
 // Minimum resident blocks per SM requested from ptxas for the hot kernels (caps registers
 // per thread); tuned per arithmetic type on B200, overridable at build time.
@@ -889,6 +888,43 @@ LT_D auto clover_leaves(const F& U, const Geom& g, int par, int i, const int c[4
 // (observables/field_strength_tensor.hpp:28-66, :107-134, :154-175).
 // Products run in FP64 for every storage: the cancellations in F = C - C^dag of a smooth
 // (flowed) field would otherwise lift FP32 rounding of the leaves into Q and E.
+// Unnormalised clover densities of one site: q = ReTr(F01 F23 - F02 F13 + F03 F12) and
+// e = sum_{mu<nu} ReTr(F~^2) with F = C - C^dag, F~ = Traceless(-i/8 F)
+template <typename T, int NR>
+LT_D void clover_densities(const Widened<T, NR>& U, const Geom& g, int par, int i, const int c[4], double& q, double& e)
+{
+    q = 0.0;
+    e = 0.0;
+    const int pairs[3][4] = { { 0, 1, 2, 3 }, { 0, 2, 1, 3 }, { 0, 3, 1, 2 } };
+#pragma unroll 1
+    for (int p = 0; p < 3; ++p)
+    {
+        M3<double> ca = clover_leaves(U, g, par, i, c, pairs[p][0], pairs[p][1]);
+        M3<double> cb = clover_leaves(U, g, par, i, c, pairs[p][2], pairs[p][3]);
+        M3<double> fa = ca - adj(ca), fb = cb - adj(cb);
+        double t = retr_mul(fa, fb);
+        q += p == 1 ? -t : t;
+        // energy: F~ = -i/8 F made traceless; ReTr(F~^2) = sum |F~_ij|^2 (Hermitian)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            const M3<double>& f = h == 0 ? fa : fb;
+            double tr3 = (f.e[0][0].i + f.e[1][1].i + f.e[2][2].i) / 3.0;
+            double acc2 = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+            {
+                double d = f.e[a][a].i - tr3;
+                acc2 += d * d;
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+                    if (a != b) acc2 += norm2(f.e[a][b]);
+            }
+            e += acc2 * (1.0 / 64.0);
+        }
+    }
+}
+
 template <typename T, int NR>
 __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> Ust, Geom g, double* __restrict__ partials)
 {
@@ -900,35 +936,8 @@ __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> Ust, Ge
         int par = x >= g.vh, s = x - par * g.vh;
         int c[4];
         int i = site_coords(g, par, s, c);
-        double q = 0.0, e = 0.0;
-        const int pairs[3][4] = { { 0, 1, 2, 3 }, { 0, 2, 1, 3 }, { 0, 3, 1, 2 } };
-#pragma unroll 1
-        for (int p = 0; p < 3; ++p)
-        {
-            M3<double> ca = clover_leaves(U, g, par, i, c, pairs[p][0], pairs[p][1]);
-            M3<double> cb = clover_leaves(U, g, par, i, c, pairs[p][2], pairs[p][3]);
-            M3<double> fa = ca - adj(ca), fb = cb - adj(cb);
-            double t = (double)retr_mul(fa, fb);
-            q += p == 1 ? -t : t;
-            // energy: F~ = -i/8 F made traceless; ReTr(F~^2) = sum |F~_ij|^2 (Hermitian)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-            {
-                const M3<double>& f = h == 0 ? fa : fb;
-                double tr3 = ((double)f.e[0][0].i + (double)f.e[1][1].i + (double)f.e[2][2].i) / 3.0;
-                double acc2 = 0.0;
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-                {
-                    double d = (double)f.e[a][a].i - tr3;
-                    acc2 += d * d;
-#pragma unroll
-                    for (int b = 0; b < 3; ++b)
-                        if (a != b) acc2 += (double)norm2(f.e[a][b]);
-                }
-                e += acc2 * (1.0 / 64.0);
-            }
-        }
+        double q, e;
+        clover_densities(U, g, par, i, c, q, e);
         kq.add(q);
         ke.add(e);
     }
@@ -938,6 +947,227 @@ __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> Ust, Ge
     {
         partials[blockIdx.x] = rq;
         partials[gridDim.x + blockIdx.x] = re;
+    }
+}
+
+// ---------------------------------------------------------------- measurement bundle
+// The observables of the reference driver's measurement step (SU3_main.cpp:89-235), all with
+// products in FP64 whatever the storage.
+
+// Coordinates and parity of the site with full index i
+LT_D int coords_of(const Geom& g, int i, int c[4])
+{
+    int r = i;
+    c[3] = r % g.n[3];
+    r /= g.n[3];
+    c[2] = r % g.n[2];
+    r /= g.n[2];
+    c[1] = r % g.n[1];
+    c[0] = r / g.n[1];
+    return (c[0] + c[1] + c[2] + c[3]) & 1;
+}
+
+// Full index of the site c moved by L steps along d (periodic)
+LT_D int shifted(const Geom& g, const int c[4], int d, int L)
+{
+    int cc[4] = { c[0], c[1], c[2], c[3] };
+    cc[d] = (cc[d] + L) % g.n[d];
+    return ((cc[0] * g.n[1] + cc[1]) * g.n[2] + cc[2]) * g.n[3] + cc[3];
+}
+
+// TopChargeCloverTimeslice / EnergyDensity::CloverTimeslice (topological_charge.hpp:338-364,
+// field_strength_tensor.hpp:178-195): block (bx, t) sums the clover densities of timeslice t;
+// partials[t * nbx + bx] (q) and partials[(Nt + t) * nbx + bx] (e)
+template <typename T, int NR>
+__global__ void __launch_bounds__(kRedThreads) k_clover_timeslice(Gauge<T, NR> Ust, Geom g, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    const Widened<T, NR> U{ Ust };
+    const int t = blockIdx.y, nbx = gridDim.x;
+    const int vs = g.V / g.n[0];
+    Kahan kq, ke;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < vs; k += nbx * blockDim.x)
+    {
+        const int i = t * vs + k;
+        int c[4];
+        const int par = coords_of(g, i, c);
+        double q, e;
+        clover_densities(U, g, par, i, c, q, e);
+        kq.add(q);
+        ke.add(e);
+    }
+    double rq = block_sum(kq.s - kq.c, sh);
+    double re = block_sum(ke.s - ke.c, sh);
+    if (threadIdx.x == 0)
+    {
+        partials[t * nbx + blockIdx.x] = rq;
+        partials[(g.n[0] + t) * nbx + blockIdx.x] = re;
+    }
+}
+
+// Per site over the six planes mu < nu: the plaquette traces (slot 0), the 1x2 and 2x1 loop
+// traces of Rectangular<2>::Action (slot 1; rectangular_action.hpp:61-94, wilson_loop.hpp:155-175)
+// and the plaquette charge density of TopChargePlaquette (slot 2; topological_charge.hpp:366-416)
+template <typename T, int NR>
+__global__ void __launch_bounds__(kRedThreads) k_loops(Gauge<T, NR> Ust, Geom g, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    const Widened<T, NR> U{ Ust };
+    Kahan kp, kr, kq;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x)
+    {
+        int c[4];
+        const int par = coords_of(g, i, c), op = par ^ 1;
+        M3<double> F[6];
+        double sp = 0.0, sr = 0.0;
+        int pl = 0;
+#pragma unroll 1
+        for (int mu = 0; mu < 4; ++mu)
+#pragma unroll 1
+            for (int nu = mu + 1; nu < 4; ++nu, ++pl)
+            {
+                const int imu = shifted(g, c, mu, 1), inu = shifted(g, c, nu, 1);
+                int cmu[4], cnu[4];
+                coords_of(g, imu, cmu);
+                coords_of(g, inu, cnu);
+                const int imunu = shifted(g, cmu, nu, 1), imu2 = shifted(g, cmu, mu, 1), inu2 = shifted(g, cnu, nu, 1);
+                const M3<double> umu = U.ld(mu, par, i >> 1), unu = U.ld(nu, par, i >> 1);
+                const M3<double> unu_mu = U.ld(nu, op, imu >> 1), umu_nu = U.ld(mu, op, inu >> 1);
+                // P = U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
+                const M3<double> a = mul(umu, unu_mu);
+                const M3<double> p = mul_nd(a, mul(unu, umu_nu));
+                sp += p.e[0][0].r + p.e[1][1].r + p.e[2][2].r;
+                F[pl] = p - adj(p);   // times -i below
+                // 1x2: U_mu(x) U_nu(x+mu) U_nu(x+mu+nu) U_mu(x+2nu)^dag U_nu(x+nu)^dag U_nu(x)^dag
+                const M3<double> r12 = mul_nd(mul(a, U.ld(nu, par, imunu >> 1)),
+                                              mul(mul(unu, U.ld(nu, op, inu >> 1)), U.ld(mu, par, inu2 >> 1)));
+                // 2x1: U_mu(x) U_mu(x+mu) U_nu(x+2mu) U_mu(x+mu+nu)^dag U_mu(x+nu)^dag U_nu(x)^dag
+                const M3<double> r21 = mul_nd(mul(mul(umu, U.ld(mu, op, imu >> 1)), U.ld(nu, par, imu2 >> 1)),
+                                              mul(mul(unu, umu_nu), U.ld(mu, par, imunu >> 1)));
+                sr += r12.e[0][0].r + r12.e[1][1].r + r12.e[2][2].r + r21.e[0][0].r + r21.e[1][1].r + r21.e[2][2].r;
+            }
+        // F_mu,nu = -i (P - P^dag); Re tr(F01 F23 + F02 F31 + F03 F12) with F31 = -F13 and
+        // (-i)^2 = -1: -(G01 G23 - G02 G13 + G03 G12) for G = P - P^dag (planes 01 02 03 12 13 23)
+        const double q = -(retr_mul(F[0], F[5]) - retr_mul(F[1], F[4]) + retr_mul(F[2], F[3]));
+        kp.add(sp);
+        kr.add(sr);
+        kq.add(q);
+    }
+    double a = block_sum(kp.s - kp.c, sh);
+    double b = block_sum(kr.s - kr.c, sh);
+    double d = block_sum(kq.s - kq.c, sh);
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = a;
+        partials[gridDim.x + blockIdx.x] = b;
+        partials[2 * gridDim.x + blockIdx.x] = d;
+    }
+}
+
+// Straight line products for WilsonLoop (observables/wilson_loop.hpp:63-124), kept as full
+// FP64 matrices C_mu(x) = U_mu(x) U_mu(x+mu) ... U_mu(x+(L-1)mu): init (L = 1), extension by one
+// link (L -> L+1) and doubling (L -> 2L)
+template <typename T, int NR>
+__global__ void k_chain_init(Gauge<T, NR> Ust, Full<double> C, Geom g)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    const int pl = l / g.vh, s = l - pl * g.vh;
+    C.st(pl >> 1, pl & 1, s, cvt<double>(Ust.ld(pl >> 1, pl & 1, s)));
+}
+
+template <typename T, int NR>
+__global__ void k_chain_extend(Full<double> Cin, Gauge<T, NR> Ust, Full<double> Cout, Geom g, int L)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    const int pl = l / g.vh, s = l - pl * g.vh, mu = pl >> 1, par = pl & 1;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    (void)i;
+    const int j = shifted(g, c, mu, L);
+    int cj[4];
+    const int pj = coords_of(g, j, cj);
+    Cout.st(mu, par, s, mul(Cin.ld(mu, par, s), cvt<double>(Ust.ld(mu, pj, j >> 1))));
+}
+
+template <int Unused = 0>
+__global__ void k_chain_double(Full<double> Cin, Full<double> Cout, Geom g, int L)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    const int pl = l / g.vh, s = l - pl * g.vh, mu = pl >> 1, par = pl & 1;
+    int c[4];
+    site_coords(g, par, s, c);
+    const int j = shifted(g, c, mu, L);
+    int cj[4];
+    const int pj = coords_of(g, j, cj);
+    Cout.st(mu, par, s, mul(Cin.ld(mu, par, s), Cin.ld(mu, pj, j >> 1)));
+}
+
+// sum over sites and mu < nu of Re tr(C_mu(x) C_nu(x+L mu) C_mu(x+L nu)^dag C_nu(x)^dag)
+template <int Unused = 0>
+__global__ void __launch_bounds__(kRedThreads) k_wilson_square(Full<double> C, Geom g, int L, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    Kahan k;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x)
+    {
+        int c[4];
+        const int par = coords_of(g, i, c);
+        double w = 0.0;
+#pragma unroll 1
+        for (int mu = 0; mu < 4; ++mu)
+        {
+            const M3<double> cmu = C.ld(mu, par, i >> 1);
+            const int jm = shifted(g, c, mu, L);
+            int cm[4];
+            const int pm = coords_of(g, jm, cm);
+#pragma unroll 1
+            for (int nu = mu + 1; nu < 4; ++nu)
+            {
+                const int jn = shifted(g, c, nu, L);
+                int cn[4];
+                const int pn = coords_of(g, jn, cn);
+                const M3<double> a = mul(cmu, C.ld(nu, pm, jm >> 1));
+                const M3<double> b = mul(C.ld(nu, par, i >> 1), C.ld(mu, pn, jn >> 1));
+                w += retr_nd(a, b);
+            }
+        }
+        k.add(w);
+    }
+    double r = block_sum(k.s - k.c, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
+// PolyakovLoop (observables/polyakov_loop.hpp:32-49): tr of the product of the Nt links in
+// direction t over every spatial site; re in slot 0, im in slot 1
+template <typename T, int NR>
+__global__ void __launch_bounds__(kRedThreads) k_polyakov(Gauge<T, NR> Ust, Geom g, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    const int vs = g.V / g.n[0];
+    Kahan kr, ki;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < vs; k += gridDim.x * blockDim.x)
+    {
+        M3<double> m = unit3<double>();
+        for (int t = 0; t < g.n[0]; ++t)
+        {
+            const int i = t * vs + k;
+            int c[4];
+            const int par = coords_of(g, i, c);
+            m = mul(m, cvt<double>(Ust.ld(0, par, i >> 1)));
+        }
+        const cx<double> tr = trace(m);
+        kr.add(tr.r);
+        ki.add(tr.i);
+    }
+    double a = block_sum(kr.s - kr.c, sh);
+    double b = block_sum(ki.s - ki.c, sh);
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = a;
+        partials[gridDim.x + blockIdx.x] = b;
     }
 }
 

@@ -60,6 +60,8 @@
 #include "LettuceGauge/observables/plaquette.hpp"
 #include "LettuceGauge/observables/field_strength_tensor.hpp"
 #include "LettuceGauge/observables/topological_charge.hpp"
+#include "LettuceGauge/observables/wilson_loop.hpp"
+#include "LettuceGauge/observables/polyakov_loop.hpp"
 #include "LettuceGauge/smearing/stout_smearing.hpp"
 #include "LettuceGauge/smearing/gradient_flow.hpp"
 #include "LettuceGauge/updates/heatbath.hpp"
@@ -492,6 +494,47 @@ double ref_field_flow(double eps, int n)
     GradientFlowKernel Flow(*g_field, *g_flowed, rk3, GaugeAction::WilsonAction, eps);
     Flow(n);
     return PlaquetteSum(*g_flowed);
+}
+
+// GradientFlowKernel with the Euler / RK2 / RK3 / RK3W7 integrator (gradient_flow.hpp:31-168)
+void ref_flow(const double* in, double* out, double eps, int n, int integrator)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto V = std::make_unique<GaugeField>();
+    auto F = std::make_unique<GaugeField>();
+    load(*U, in);
+    switch (integrator)
+    {
+        case 0: { Integrators::GradientFlow::Euler it(*F); GradientFlowKernel k(*U, *V, it, GaugeAction::WilsonAction, eps); k(n); break; }
+        case 1: { Integrators::GradientFlow::RK2 it(*F); GradientFlowKernel k(*U, *V, it, GaugeAction::WilsonAction, eps); k(n); break; }
+        case 2: { Integrators::GradientFlow::RK3 it(*F); GradientFlowKernel k(*U, *V, it, GaugeAction::WilsonAction, eps); k(n); break; }
+        default: { Integrators::GradientFlow::RK3W7 it(*F); GradientFlowKernel k(*U, *V, it, GaugeAction::WilsonAction, eps); k(n); break; }
+    }
+    store(*V, out);
+}
+
+// The measurement bundle of SU3_main.cpp:89-235 on one field: out = {Symanzik action
+// (normalised), TopChargePlaquette, W(L=2), W(L=4), W(L=8), Re P, Im P}; q_t, e_t = the
+// clover charge and energy per timeslice (Nt each)
+void ref_measure(const double* links, double b, double* out, double* q_t, double* e_t)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto chain = std::make_unique<GaugeField>();
+    auto F = std::make_unique<FullTensor>();
+    load(*U, links);
+    GaugeAction::Rectangular<2> Symanzik(b, 1.0 + 8.0 * 1.0 / 12.0, -1.0 / 12.0);
+    out[0] = Symanzik.ActionNormalized(*U);
+    out[1] = TopChargePlaquette(*U);
+    out[2] = WilsonLoop<0, 2, true>(*U, *chain);
+    out[3] = WilsonLoop<2, 4, false>(*U, *chain);
+    out[4] = WilsonLoop<4, 8, false>(*U, *chain);
+    const std::complex<double> P = PolyakovLoop(*U);
+    out[5] = std::real(P);
+    out[6] = std::imag(P);
+    FieldStrengthTensor::Clover(*U, *F);
+    for (int t = 0; t < Nt; ++t) q_t[t] = TopChargeCloverTimeslice(*F, t);
+    FieldStrengthTensor::MakeComponentsTraceless(*F);
+    for (int t = 0; t < Nt; ++t) e_t[t] = EnergyDensity::CloverTimeslice(*F, t);
 }
 
 // SaveConfigBMW / SaveConfigBMWFull (IO/config_io/bmw_format.hpp:294-394, :564-645) of the

@@ -46,5 +46,15 @@ def golden_bmw():
 
 
 @pytest.fixture(scope="session")
+def golden_measure(oracle):
+    """Reference measurement bundle and flow samples; "U" is the regenerated input."""
+    from ltref import haar_links_numpy
+    d = dict(np.load(os.path.join(GOLDEN, "ref_measure.npz")))
+    ext = tuple(int(e) for e in d["ext"])
+    d["U"] = oracle.heatbath(ext, haar_links_numpy(ext, 2), 6.0, 5, 17, 0)
+    return d
+
+
+@pytest.fixture(scope="session")
 def golden_chain():
     return dict(np.load(os.path.join(GOLDEN, "ref_chain_8x8x8x8.npz")))

@@ -27,6 +27,21 @@ int main(int argc, char** argv)
     std::printf("plaquette %.15f\n", PlaquetteSum(Gluon) / Gluon.Volume() / 18.0);
     std::printf("action %.12f\n", SimulatedAction.Action(Gluon));
 
+    // the measurement bundle of the reference driver (SU3_main.cpp:117-139)
+    GaugeAction::Rectangular<2> SymanzikAction(6.0, 1.0 + 8.0 / 12.0, -1.0 / 12.0);
+    GaugeField Gluonchain({L, L, L, L});
+    const std::complex<double> poly = PolyakovLoop(Gluon);
+    double q_sum = 0.0;
+    for (const double q : TopChargeCloverTimeslices(Gluon)) q_sum += q;
+    std::printf("bundle S %.15f W2 %.15f W4 %.15f P %.15f %.15f Qplaq %.15f Qt %.15f E0 %.15f\n",
+                SymanzikAction.ActionNormalized(Gluon), WilsonLoop<0, 2, true>(Gluon, Gluonchain),
+                WilsonLoop<2, 4, false>(Gluon, Gluonchain), poly.real(), poly.imag(), TopChargePlaquette(Gluon), q_sum,
+                EnergyDensity::CloverTimeslice(Gluon, 0));
+    Integrators::GradientFlow::Euler euler;
+    GradientFlowKernel EulerFlow(Gluon, Gluonchain, euler, SimulatedAction, 0.02);
+    EulerFlow(5);
+    std::printf("euler E %.15f\n", EnergyDensityClover(Gluonchain));
+
     Integrators::GradientFlow::RK3 rk3;
     GradientFlowKernel Flow(Gluon, Gluonsmeared1, rk3, SimulatedAction, 0.01);
     Flow(10);

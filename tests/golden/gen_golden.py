@@ -181,17 +181,40 @@ def gen_bmw() -> dict:
     return out
 
 
+def gen_measure() -> dict:
+    """The reference's measurement bundle (SU3_main.cpp:89-235) and its four flow integrators on
+    the 4x6x8x10 input (Haar seed 2) after 5 oracle heatbath sweeps (the tests regenerate it)."""
+    from ltref import Oracle
+    ext = (4, 6, 8, 10)
+    U = Oracle().heatbath(ext, haar_links_numpy(ext, 2), 6.0, 5, 17, 0)
+    ref = Reference(ext)
+    m = ref.measure(U, 6.0)
+    out = {"ext": np.array(ext), "U_ck": checksums(U)}
+    for k, v in m.items():
+        out[k] = np.array(v)
+    links = sample_links(int(np.prod(ext)), 5)
+    out["links"] = links
+    for integ in range(4):
+        F = ref.flow(U, 0.02, 5, integ)
+        out[f"flow{integ}"] = take(F, links)
+        out[f"flow{integ}_ck"] = checksums(F)
+    return out
+
+
 def main() -> int:
     import argparse
     import subprocess
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["chain", "bmw"], default=None, help="regenerate one fixture only")
+    ap.add_argument("--only", choices=["chain", "bmw", "measure"], default=None, help="regenerate one fixture only")
     a = ap.parse_args()
     root = os.path.dirname(os.path.dirname(HERE))
     subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "4x4x4x4",
                     "4x6x8x10", "8x8x8x8", "2x4x6x8"], check=True)
     if a.only == "chain":
         np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
+        return 0
+    if a.only == "measure":
+        np.savez_compressed(os.path.join(HERE, "ref_measure.npz"), **gen_measure())
         return 0
     if a.only == "bmw":
         np.savez_compressed(os.path.join(HERE, "ref_bmw.npz"), **gen_bmw())
@@ -205,6 +228,7 @@ def main() -> int:
     np.savez_compressed(os.path.join(HERE, "ref_bias.npz"), **gen_bias())
     np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
     np.savez_compressed(os.path.join(HERE, "ref_bmw.npz"), **gen_bmw())
+    np.savez_compressed(os.path.join(HERE, "ref_measure.npz"), **gen_measure())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -62,6 +62,12 @@ class Oracle:
             "or_bias_potential": (d, [C.c_void_p, d]),
             "or_bias_derivative": (d, [C.c_void_p, d]),
             "or_bmw_encode": (u64, [_ip, _dp, i, C.c_void_p]),
+            "or_flow": (None, [_ip, _dp, _dp, d, i, i]),
+            "or_clover_timeslices": (None, [_ip, _dp, _dp, _dp]),
+            "or_topcharge_plaquette": (d, [_ip, _dp]),
+            "or_rect_action": (d, [_ip, _dp, d, d, d]),
+            "or_wilson_loop": (d, [_ip, _dp, i]),
+            "or_polyakov_loop": (None, [_ip, _dp, C.POINTER(d), C.POINTER(d)]),
             "or_bmw_decode": (u64, [_ip, C.c_void_p, i, _dp]),
         }
         for name, (res, args) in sig.items():
@@ -147,6 +153,25 @@ class Oracle:
         self.lib.or_random_momenta(self._e(ext), P, seed, counter)
         return P
 
+    def flow(self, ext, U, eps, n, integrator):
+        out = np.empty_like(U)
+        self.lib.or_flow(self._e(ext), np.ascontiguousarray(U), out, eps, n, integrator)
+        return out
+
+    def measure(self, ext, U, beta=6.0):
+        """The bundle of SU3_main.cpp:89-235 on one field: dict of the observables."""
+        U = np.ascontiguousarray(U)
+        e = self._e(ext)
+        qt, et = np.empty(ext[0]), np.empty(ext[0])
+        self.lib.or_clover_timeslices(e, U, qt, et)
+        re, im = C.c_double(), C.c_double()
+        self.lib.or_polyakov_loop(e, U, C.byref(re), C.byref(im))
+        V = int(np.prod(ext))
+        return {"q_t": qt, "e_t": et, "Q_plaq": self.lib.or_topcharge_plaquette(e, U),
+                "S_improved": self.lib.or_rect_action(e, U, beta, 1 + 8 / 12, -1 / 12) / (6 * beta * V),
+                "W2": self.lib.or_wilson_loop(e, U, 2), "W4": self.lib.or_wilson_loop(e, U, 4),
+                "W8": self.lib.or_wilson_loop(e, U, 8), "P": complex(re.value, im.value)}
+
     def bmw_encode(self, ext, U, full):
         """(Adler-64 checksum, BMW payload bytes) of a field in the reference layout."""
         U = np.ascontiguousarray(U, dtype=np.float64)
@@ -205,6 +230,8 @@ class Reference:
                 "ref_bias_probe": (None, [d, d, i, d, d, d, d, _dp, i, i, _dp, i, _dp, _dp]),
                 "ref_su3_exp": (None, [_dp, _dp, i]),
                 "ref_save_bmw": (i, [_dp, C.c_char_p, i]),
+                "ref_flow": (None, [_dp, _dp, d, i, i]),
+                "ref_measure": (None, [_dp, d, _dp, _dp, _dp]),
                 "ref_load_bmw": (i, [C.c_char_p, i, _dp]),
             }
             for name, (res, args) in sig.items():
@@ -293,6 +320,17 @@ class Reference:
         out = np.empty_like(Q)
         self.lib.ref_su3_exp(Q, out, Q.size // 18)
         return out
+
+    def flow(self, U, eps, n, integrator):
+        out = np.empty_like(U)
+        self.lib.ref_flow(np.ascontiguousarray(U), out, eps, n, integrator)
+        return out
+
+    def measure(self, U, beta=6.0):
+        out, qt, et = np.empty(7), np.empty(self.ext[0]), np.empty(self.ext[0])
+        self.lib.ref_measure(np.ascontiguousarray(U), beta, out, qt, et)
+        return {"q_t": qt, "e_t": et, "S_improved": out[0], "Q_plaq": out[1], "W2": out[2], "W4": out[3],
+                "W8": out[4], "P": complex(out[5], out[6])}
 
     def save_bmw(self, U, path, full):
         return bool(self.lib.ref_save_bmw(np.ascontiguousarray(U, dtype=np.float64), str(path).encode(), int(full)))

@@ -41,6 +41,19 @@ def test_dropin_runs_like_python_mirror(tmp_path):
     assert float(lines["plaquette"].split()[1]) == pytest.approx(p, rel=1e-14)
     assert 0.55 < p < 0.65
     assert "metad" in out and "copy" in out
+    # measurement bundle and an Euler flow on the same thermalised field
+    b = lines["bundle"].split()
+    m = lt.Measure(G, 6.0)
+    assert float(b[2]) == pytest.approx(m["Improved_Action"], rel=1e-13)
+    assert float(b[4]) == pytest.approx(m["Wilson_loop(L=2)"], rel=1e-13)
+    assert float(b[6]) == pytest.approx(m["Wilson_loop(L=4)"], rel=1e-13)
+    assert complex(float(b[8]), float(b[9])) == pytest.approx(m["Polyakov_loop"], abs=1e-14)
+    assert float(b[11]) == pytest.approx(m["TopChargePlaq"], abs=1e-13)
+    assert float(b[13]) == pytest.approx(m["TopChargeClov"], abs=1e-13)
+    assert float(b[15]) == pytest.approx(m["E_clov_timeslice"][0], rel=1e-13)
+    F = lt.GaugeField((8, 8, 8, 8))
+    lt.GradientFlowKernel(G, F, lt.Euler, None, 0.02)(5)
+    assert float(lines["euler"].split()[2]) == pytest.approx(lt.EnergyDensityClover(F), rel=1e-13)
     # checkpoints: three rotations, restored field and Philox counter, a missing file rejected
     ck = lines["checkpoint"].split()
     assert int(ck[2]) == 20 + 3

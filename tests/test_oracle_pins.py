@@ -192,3 +192,36 @@ class TestBMW:
             assert ok
             _, mine = oracle.bmw_decode(ext, data[4096:], full)
             assert np.array_equal(mine, loaded)
+
+
+class TestMeasurementBundle:
+    """The observables of the reference driver's measurement step (SU3_main.cpp:89-235) and
+    the four flow integrators (smearing/gradient_flow.hpp:31-168), against the reference."""
+
+    def test_against_fixture(self, oracle, golden_measure):
+        g = golden_measure
+        ext = tuple(int(e) for e in g["ext"])
+        U = g["U"]
+        assert close_ck(checksums(U), g["U_ck"], 1e-12)
+        m = oracle.measure(ext, U, 6.0)
+        for k in ("Q_plaq", "S_improved", "W2", "W4", "W8"):
+            assert m[k] == pytest.approx(float(g[k]), rel=TOL, abs=1e-14), k
+        assert m["P"] == pytest.approx(complex(g["P"]), rel=TOL, abs=1e-14)
+        np.testing.assert_allclose(m["q_t"], g["q_t"], rtol=1e-10, atol=1e-14)
+        np.testing.assert_allclose(m["e_t"], g["e_t"], rtol=TOL)
+        assert m["q_t"].sum() == pytest.approx(oracle.topcharge(ext, U), rel=1e-12, abs=1e-14)
+        for integ in range(4):
+            F = oracle.flow(ext, U, 0.02, 5, integ)
+            assert rel_err(links_of(F, g["links"]), g[f"flow{integ}"]) < TOL, integ
+            assert close_ck(checksums(F), g[f"flow{integ}_ck"], 1e-11)
+
+    @pytest.mark.skipif(not ref_available((4, 4, 4, 4)), reason="reference harness not built")
+    def test_live_reference(self, oracle):
+        ext = (4, 4, 4, 4)
+        U = oracle.heatbath(ext, haar_links_numpy(ext, 8), 5.8, 4, 3, 0)
+        ref = Reference(ext).measure(U, 6.2)
+        mine = oracle.measure(ext, U, 6.2)
+        for k in ("Q_plaq", "S_improved", "W2", "W4", "W8", "P"):
+            assert mine[k] == pytest.approx(ref[k], rel=TOL, abs=1e-14), k
+        np.testing.assert_allclose(mine["q_t"], ref["q_t"], rtol=1e-10, atol=1e-14)
+        np.testing.assert_allclose(mine["e_t"], ref["e_t"], rtol=TOL)
