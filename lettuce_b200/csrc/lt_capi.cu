@@ -533,6 +533,8 @@ int lt_clover_timeslices(lt_lattice* h, double* q_t, double* e_t)
     if (!q_t && !e_t) return lt::set_error(LT_ERR_ARG, "lt_clover_timeslices: null pointers");
     const int nt = h->g.n[0];
     const int nbx = std::max(1, std::min(lt::kRedBlocks / nt, (h->g.V / nt + lt::kRedThreads - 1) / lt::kRedThreads));
+    if (2 * nt * nbx > lt::kNumSlots * lt::kRedBlocks)
+        return lt::set_error(LT_ERR_ARG, "lt_clover_timeslices: more timeslices than the partial-sum buffer holds");
     h->be->clover_timeslices(h->ctx(), h->U, h->partials, nbx);
     LT_TRY(launched("lt_clover_timeslices"));
     std::vector<double> p((size_t)2 * nt * nbx);

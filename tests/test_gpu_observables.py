@@ -83,7 +83,7 @@ class TestBundle:
         m = gpu_measure(G, 6.0)
         for k in ("S_improved", "W2", "W4", "W8", "Q_plaq"):
             assert abs(m[k]) < 1e-15, k
-        assert m["P"] == pytest.approx(1.0, abs=1e-15)
+        assert m["P"] == pytest.approx(3.0, abs=1e-15)   # tr 1 over the spatial volume, as the reference
         assert np.all(np.abs(m["q_t"]) < 1e-15) and np.all(np.abs(m["e_t"]) < 1e-15)
 
     def test_rectangular_coefficients(self, oracle, therm_odd):
