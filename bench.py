@@ -221,7 +221,7 @@ def secondary_rates(lt, torch, timed, prec):
     * metadynamics force evaluations/s at 16^4 (4 stout steps rho = 0.12, FP32 links);
     * tempering ensemble link updates/s: 8 streams of 12^4 plus 40 chains with extents drawn
       from {8,...,16}^4, beta in [5.8, 6.2], one batched round (1 HB + 4 OR) per step;
-    * one 48^4 HMC trajectory (OMF2, tau = 1, 20 steps, FP32 links, FP64 dH)."""
+    * one 48^4 HMC trajectory (OMF4, tau = 1, 20 steps, FP32 links, FP64 dH)."""
     import numpy as np
     out = {}
     try:
@@ -303,8 +303,9 @@ def secondary_rates(lt, torch, timed, prec):
     except Exception as e:
         out["measure_error"] = repr(e)
     try:
-        # 48^4 at beta = 6.3: Haar start, 200 rounds of 1 HB + 4 OR, two OMF2 trajectories
-        # (tau = 1, 20 steps, FP32 links, FP64 dH and accept), then Wilson flow to t0
+        # 48^4 at beta = 6.3: Haar start, 200 rounds of 1 HB + 4 OR, two OMF4 trajectories (the
+        # reference driver's integrator; tau = 1, 20 steps, FP32 links, FP64 dH and accept), then
+        # Wilson flow to t0
         # (t^2 E = 0.3) with clover Q and E at every step
         ext = (48,) * 4
         G = lt.GaugeField(ext, "fp32")
@@ -313,7 +314,7 @@ def secondary_rates(lt, torch, timed, prec):
         lt.UpdateSweeps(G, 6.3, 200, 1, 4, SEED)
         G.synchronize()
         out["hmc_48^4_therm_s_200_rounds"] = time.perf_counter() - t0
-        hmc = lt.HMCKernel(G, lt.WilsonAction(6.3), 1.0, seed=7)
+        hmc = lt.HMCKernel(G, lt.WilsonAction(6.3), 1.0, seed=7, integrator=lt.OMF_4)
         hmc(20, True)
         t0 = time.perf_counter()
         acc = hmc(20, True)

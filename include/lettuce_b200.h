@@ -261,6 +261,41 @@ int lt_metad_hmc_trajectory(lt_lattice* h, lt_bias* bias, double beta, double ta
                             int n_stout, uint64_t seed, uint64_t* counter, int metropolis, double* dH,
                             int* accepted, double* cv_out);
 
+/* ---- molecular-dynamics integrators (updates/hmc_gauge.hpp:19-377,
+ *      updates/hmc_metadynamics.hpp:26-238) and parity (updates/parity_update.hpp:22-47) ---- */
+#define LT_MD_LEAPFROG_SLOW          0   /* Integrators::HMC::Leapfrog_slow (hmc_gauge.hpp:21-44) */
+#define LT_MD_LEAPFROG               1   /* Leapfrog (:47-70) */
+#define LT_MD_OMF2_SLOW              2   /* OMF_2_slow (:121-151) */
+#define LT_MD_OMF2                   3   /* OMF_2 (:155-190) */
+#define LT_MD_OMF4_SLOW              4   /* OMF_4_slow (:195-237) */
+#define LT_MD_OMF4                   5   /* OMF_4 (:241-294), the reference driver's choice */
+#define LT_MD_LEAPFROG_FRICTION_SLOW 6   /* Leapfrog_friction_slow (:74-116), gauge action only */
+#define LT_MD_OMF4_FRICTION_SLOW     7   /* OMF_4_friction_slow (:298-376), gauge action only */
+#define LT_MD_LEAPFROG_OMF4          8   /* Leapfrog_OMF_4 (hmc_metadynamics.hpp:28-83), MetaD only */
+#define LT_MD_OMF2_OMF4_SLOW         9   /* OMF_2_OMF_4_slow (:85-143), MetaD only */
+#define LT_MD_OMF2_OMF4              10  /* OMF_2_OMF_4 (:145-237), MetaD only */
+/* Molecular dynamics with any integrator from the current links and momenta, with the bias
+ * force (bias != NULL: CV = clover Q after n_stout stout steps of rho) or the gauge action
+ * alone; H (+ V(CV)) before and after in h_old / h_new (either may be NULL).  The
+ * multiple-timescale integrators evaluate the bias force at the current links at each of
+ * their Metadynamics momentum updates (the reference's UpdateMetadynamicsMomenta adds the
+ * force it last stored). */
+int lt_md_integrate(lt_lattice* h, lt_bias* bias, int integrator, double beta, double tau, int n_step, double rho,
+                    int n_stout, double* h_old, double* h_new);
+/* HMCKernel::operator() (hmc_gauge.hpp:549-583) or, with a bias, HMCMetaDKernel::operator()
+ * (hmc_metadynamics.hpp:552-655) with any integrator: random momenta from Philox at
+ * *counter (advanced by 1), MD, Metropolis (if metropolis != 0), and under MetaD the
+ * symmetric bias update from the CVs recorded at the submeasurement kicks (the final CV for
+ * the multiple-timescale integrators, which record none). */
+int lt_md_trajectory(lt_lattice* h, lt_bias* bias, int integrator, double beta, double tau, int n_step, double rho,
+                     int n_stout, uint64_t seed, uint64_t* counter, int metropolis, double* dH, int* accepted,
+                     double* cv_out);
+/* ReverseMomenta (hmc_gauge.hpp:432-446): P <- -P, for reversibility tests. */
+int lt_reverse_momenta(lt_lattice* h);
+/* ParityUpdate (parity_update.hpp:22-47): the spatial reflection that maps Q to -Q and leaves
+ * the action unchanged, in place. */
+int lt_parity_update(lt_lattice* h);
+
 /* ---- bias potential: MetaBiasPotential (actions/bias_potential/metadynamics.hpp:29-507) -- */
 /* Constructor (:60-91); fails with LT_ERR_ARG where the reference throws (:70-77). */
 int lt_bias_create(double cv_min, double cv_max, int bin_number, double weight, double width,

@@ -476,26 +476,51 @@ struct RunStatistics   // defines.hpp:93-106 (the fields this path fills)
     std::uint64_t acceptances_metadynamics_hmc = 0;
 };
 
+// The integrators of updates/hmc_gauge.hpp:19-377 and updates/hmc_metadynamics.hpp:26-238;
+// ID selects the device program.  The friction variants run on HMCKernel only, the
+// multiple-timescale ones on HMCMetaDKernel only (as in the reference, whose HMCKernel has no
+// UpdateGaugeMomenta / UpdateMetadynamicsMomenta and whose HMCMetaDKernel no
+// UpdateMomentaFriction).
 namespace Integrators::HMC
 {
-struct OMF_2   // updates/hmc_gauge.hpp:155-190
-{
-    static constexpr int NumberOfMomentumUpdates(int n_step) { return n_step > 0 ? 2 * n_step + 1 : 0; }
-};
+#define LT_HMC_INTEGRATOR(NAME, ID_, GAUGE, METAD)                                        \
+    struct NAME                                                                            \
+    {                                                                                      \
+        static constexpr int ID = ID_;                                                     \
+        static constexpr bool gauge_kernel = GAUGE, metad_kernel = METAD;                  \
+    };
+LT_HMC_INTEGRATOR(Leapfrog_slow, LT_MD_LEAPFROG_SLOW, true, true)                 // hmc_gauge.hpp:21-44
+LT_HMC_INTEGRATOR(Leapfrog, LT_MD_LEAPFROG, true, true)                           // :47-70
+LT_HMC_INTEGRATOR(OMF_2_slow, LT_MD_OMF2_SLOW, true, true)                        // :121-151
+LT_HMC_INTEGRATOR(OMF_2, LT_MD_OMF2, true, true)                                  // :155-190
+LT_HMC_INTEGRATOR(OMF_4_slow, LT_MD_OMF4_SLOW, true, true)                        // :195-237
+LT_HMC_INTEGRATOR(OMF_4, LT_MD_OMF4, true, true)                                  // :241-294
+LT_HMC_INTEGRATOR(Leapfrog_friction_slow, LT_MD_LEAPFROG_FRICTION_SLOW, true, false)   // :74-116
+LT_HMC_INTEGRATOR(OMF_4_friction_slow, LT_MD_OMF4_FRICTION_SLOW, true, false)     // :298-376
+LT_HMC_INTEGRATOR(Leapfrog_OMF_4, LT_MD_LEAPFROG_OMF4, false, true)               // hmc_metadynamics.hpp:28-83
+LT_HMC_INTEGRATOR(OMF_2_OMF_4_slow, LT_MD_OMF2_OMF4_SLOW, false, true)            // :85-143
+LT_HMC_INTEGRATOR(OMF_2_OMF_4, LT_MD_OMF2_OMF4, false, true)                      // :145-237
+#undef LT_HMC_INTEGRATOR
 } // namespace Integrators::HMC
+
+// ParityUpdate (updates/parity_update.hpp:22-47); the copy lives on the device, so U_copy is
+// accepted for the signature and left untouched
+inline void ParityUpdate(GaugeField& U, GaugeField& /*U_copy*/) { check(lt_parity_update(U.handle())); }
 
 namespace GaugeUpdates
 {
-// HMCKernel (updates/hmc_gauge.hpp:381-600) with OMF_2; U_copy and Momentum live on the device
+// HMCKernel (updates/hmc_gauge.hpp:381-600); U_copy and Momentum live on the device
+template <typename IntegratorT>
 struct HMCKernel
 {
+    static_assert(IntegratorT::gauge_kernel, "this integrator needs the Metadynamics kernel");
     GaugeField& U;
     GaugeAction::Wilson& Action;
     RunStatistics& statistics;
     double trajectory_length;
     std::uint64_t seed, counter;
-    HMCKernel(GaugeField& U_in, Integrators::HMC::OMF_2&, GaugeAction::Wilson& action, RunStatistics& stats,
-              double tau = 1.0, std::uint64_t seed_in = 1, std::uint64_t counter_in = 0)
+    HMCKernel(GaugeField& U_in, IntegratorT&, GaugeAction::Wilson& action, RunStatistics& stats, double tau = 1.0,
+              std::uint64_t seed_in = 1, std::uint64_t counter_in = 0)
         : U(U_in), Action(action), statistics(stats), trajectory_length(tau), seed(seed_in), counter(counter_in)
     {
     }
@@ -503,17 +528,31 @@ struct HMCKernel
     {
         double dH;
         int acc;
-        check(lt_hmc_trajectory(U.handle(), Action.GetBeta(), trajectory_length, n_step, seed, &counter,
-                                metropolis_step ? 1 : 0, &dH, &acc));
+        check(lt_md_trajectory(U.handle(), nullptr, IntegratorT::ID, Action.GetBeta(), trajectory_length, n_step, 0.0,
+                               0, seed, &counter, metropolis_step ? 1 : 0, &dH, &acc, nullptr));
         statistics.delta_H_hmc = dH;
         statistics.acceptances_hmc += (std::uint64_t)acc;
         return acc != 0;
     }
+    // ReversibilityTest (:585-598): returns H after the forward-reverse-forward run minus H before
+    double ReversibilityTest(int n_step)
+    {
+        double ho, hn;
+        check(lt_random_momenta(U.handle(), seed, counter));
+        check(lt_md_integrate(U.handle(), nullptr, IntegratorT::ID, Action.GetBeta(), trajectory_length, n_step, 0.0, 0,
+                              &ho, nullptr));
+        check(lt_reverse_momenta(U.handle()));
+        check(lt_md_integrate(U.handle(), nullptr, IntegratorT::ID, Action.GetBeta(), trajectory_length, n_step, 0.0, 0,
+                              nullptr, &hn));
+        return hn - ho;
+    }
 };
 
-// HMCMetaDKernel (updates/hmc_metadynamics.hpp:264-675) with OMF_2
+// HMCMetaDKernel (updates/hmc_metadynamics.hpp:264-675)
+template <typename IntegratorT>
 struct HMCMetaDKernel
 {
+    static_assert(IntegratorT::metad_kernel, "this integrator needs the gauge-only kernel");
     GaugeField& U;
     MetaBiasPotential& Metapotential;
     GaugeAction::Wilson& Action;
@@ -522,7 +561,7 @@ struct HMCMetaDKernel
     int n_smear_meta;
     std::uint64_t seed, counter;
     double cv_current = 0.0;
-    HMCMetaDKernel(GaugeField& U_in, MetaBiasPotential& bias, Integrators::HMC::OMF_2&, GaugeAction::Wilson& action,
+    HMCMetaDKernel(GaugeField& U_in, MetaBiasPotential& bias, IntegratorT&, GaugeAction::Wilson& action,
                    RunStatistics& stats, double tau, double rho, int n_smear = 4, std::uint64_t seed_in = 1,
                    std::uint64_t counter_in = 0)
         : U(U_in), Metapotential(bias), Action(action), statistics(stats), trajectory_length(tau), rho_stout_cv(rho),
@@ -533,9 +572,9 @@ struct HMCMetaDKernel
     {
         double dH, cv;
         int acc;
-        check(lt_metad_hmc_trajectory(U.handle(), Metapotential.handle(), Action.GetBeta(), trajectory_length, n_step,
-                                      rho_stout_cv, n_smear_meta, seed, &counter, metropolis_step ? 1 : 0, &dH, &acc,
-                                      &cv));
+        check(lt_md_trajectory(U.handle(), Metapotential.handle(), IntegratorT::ID, Action.GetBeta(), trajectory_length,
+                               n_step, rho_stout_cv, n_smear_meta, seed, &counter, metropolis_step ? 1 : 0, &dH, &acc,
+                               &cv));
         statistics.delta_H_hmc = dH;
         statistics.acceptances_metadynamics_hmc += (std::uint64_t)acc;
         cv_current = cv;
@@ -546,6 +585,17 @@ struct HMCMetaDKernel
         double q;
         check(lt_metad_charge(U.handle(), rho_stout_cv, n_smear_meta, &q));
         return q;
+    }
+    double ReversibilityTest(int n_step)
+    {
+        double ho, hn;
+        check(lt_random_momenta(U.handle(), seed, counter));
+        check(lt_md_integrate(U.handle(), Metapotential.handle(), IntegratorT::ID, Action.GetBeta(), trajectory_length,
+                              n_step, rho_stout_cv, n_smear_meta, &ho, nullptr));
+        check(lt_reverse_momenta(U.handle()));
+        check(lt_md_integrate(U.handle(), Metapotential.handle(), IntegratorT::ID, Action.GetBeta(), trajectory_length,
+                              n_step, rho_stout_cv, n_smear_meta, nullptr, &hn));
+        return hn - ho;
     }
 };
 } // namespace GaugeUpdates

@@ -85,6 +85,10 @@ SIGNATURES = {
     "lt_metad_force": (_i, [_vp, _d, _i, _d, _vp, _pd]),
     "lt_metad_omf2": (_i, [_vp, _vp, _d, _d, _i, _d, _i, _pd, _pd]),
     "lt_metad_hmc_trajectory": (_i, [_vp, _vp, _d, _d, _i, _d, _i, _u64, _pu64, _i, _pd, _pi, _pd]),
+    "lt_md_integrate": (_i, [_vp, _vp, _i, _d, _d, _i, _d, _i, _pd, _pd]),
+    "lt_md_trajectory": (_i, [_vp, _vp, _i, _d, _d, _i, _d, _i, _u64, _pu64, _i, _pd, _pi, _pd]),
+    "lt_reverse_momenta": (_i, [_vp]),
+    "lt_parity_update": (_i, [_vp]),
     "lt_bias_create": (_i, [_d, _d, _i, _d, _d, _d, _d, C.POINTER(_vp)]),
     "lt_bias_destroy": (_i, [_vp]),
     "lt_bias_update": (_i, [_vp, _vp, _i, _i]),

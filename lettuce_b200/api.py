@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -388,22 +389,74 @@ class MetaBiasPotential:
         self.set_grid(np.array([fn(self._cv_min + i * self._bin_width) for i in range(n)], dtype=np.float64))
 
 
+class MDIntegrator:
+    """One integrator of Integrators::HMC (updates/hmc_gauge.hpp:19-377,
+    updates/hmc_metadynamics.hpp:26-238); ID is its LT_MD_* number in the C ABI.  gauge /
+    metad say which kernels accept it (the friction variants need UpdateMomentaFriction of
+    HMCKernel, the multiple-timescale ones UpdateGaugeMomenta / UpdateMetadynamicsMomenta of
+    HMCMetaDKernel)."""
+
+    def __init__(self, name: str, ID: int, gauge: bool = True, metad: bool = True):
+        self.name, self.ID, self.gauge, self.metad = name, ID, gauge, metad
+
+    def ReturnName(self) -> str:
+        return self.name
+
+    def __repr__(self) -> str:
+        return f"Integrators.HMC.{self.name}"
+
+
+Leapfrog_slow = MDIntegrator("Leapfrog_slow", 0)
+Leapfrog = MDIntegrator("Leapfrog", 1)
+OMF_2_slow = MDIntegrator("OMF_2_slow", 2)
+OMF_2 = MDIntegrator("OMF_2", 3)
+OMF_4_slow = MDIntegrator("OMF_4_slow", 4)
+OMF_4 = MDIntegrator("OMF_4", 5)
+Leapfrog_friction_slow = MDIntegrator("Leapfrog_friction_slow", 6, metad=False)
+OMF_4_friction_slow = MDIntegrator("OMF_4_friction_slow", 7, metad=False)
+Leapfrog_OMF_4 = MDIntegrator("Leapfrog_OMF_4", 8, gauge=False)
+OMF_2_OMF_4_slow = MDIntegrator("OMF_2_OMF_4_slow", 9, gauge=False)
+OMF_2_OMF_4 = MDIntegrator("OMF_2_OMF_4", 10, gauge=False)
+
+# Integrators::HMC / Integrators::GradientFlow as in the reference's namespaces
+Integrators = SimpleNamespace(
+    HMC=SimpleNamespace(**{i.name: i for i in (Leapfrog_slow, Leapfrog, OMF_2_slow, OMF_2, OMF_4_slow, OMF_4,
+                                               Leapfrog_friction_slow, OMF_4_friction_slow, Leapfrog_OMF_4,
+                                               OMF_2_OMF_4_slow, OMF_2_OMF_4)}),
+    GradientFlow=SimpleNamespace(Euler=Euler, RK2=RK2, RK3=RK3, RK3W7=RK3W7))
+
+
 class HMCKernel:
-    """GaugeUpdates::HMCKernel with Integrators::HMC::OMF_2 (updates/hmc_gauge.hpp:155-190,
-    :381-600)."""
+    """GaugeUpdates::HMCKernel (updates/hmc_gauge.hpp:381-600) with any gauge integrator
+    (OMF_2 by default; the reference driver uses OMF_4)."""
 
     def __init__(self, U: GaugeField, action: WilsonAction, trajectory_length: float = 1.0, seed: int = 1,
-                 counter: int = 0):
+                 counter: int = 0, integrator: MDIntegrator = OMF_2):
+        if not isinstance(integrator, MDIntegrator) or not integrator.gauge:
+            raise ValueError(f"{integrator!r} is not an integrator of HMCKernel")
         self.U, self.beta, self.tau, self.seed = U, action.GetBeta(), float(trajectory_length), int(seed)
         self.counter = C.c_uint64(counter)
+        self.integrator = integrator
         self.delta_H = 0.0
 
+    def _bias(self):
+        return None
+
+    def _rho_n(self):
+        return 0.0, 0
+
     def __call__(self, n_step: int, metropolis_step: bool = True) -> bool:
-        dH, acc = C.c_double(), C.c_int()
-        check(lib().lt_hmc_trajectory(self.U.handle, self.beta, self.tau, int(n_step), C.c_uint64(self.seed),
-                                      C.byref(self.counter), int(bool(metropolis_step)), C.byref(dH), C.byref(acc)))
+        dH, acc, cv = C.c_double(), C.c_int(), C.c_double()
+        rho, n = self._rho_n()
+        check(lib().lt_md_trajectory(self.U.handle, self._bias(), self.integrator.ID, self.beta, self.tau, int(n_step),
+                                     rho, n, C.c_uint64(self.seed), C.byref(self.counter), int(bool(metropolis_step)),
+                                     C.byref(dH), C.byref(acc), C.byref(cv)))
         self.delta_H = dH.value
+        self._after(cv.value)
         return bool(acc.value)
+
+    def _after(self, cv: float) -> None:
+        pass
 
     def SetMomenta(self, P: np.ndarray) -> None:
         check(lib().lt_set_momenta(self.U.handle, np.ascontiguousarray(P, dtype=np.float64).reshape(-1)))
@@ -416,33 +469,55 @@ class HMCKernel:
     def RandomMomentum(self, counter: int) -> None:
         check(lib().lt_random_momenta(self.U.handle, C.c_uint64(self.seed), C.c_uint64(counter)))
 
+    def ReverseMomenta(self) -> None:
+        check(lib().lt_reverse_momenta(self.U.handle))
+
     def Hamiltonian(self) -> float:
         return _out1(lib().lt_hamiltonian, self.U.handle, self.beta)
 
     def Integrate(self, n_step: int) -> tuple[float, float]:
-        """OMF_2 molecular dynamics only; returns (H_old, H_new)."""
+        """Molecular dynamics only, from the current links and momenta; returns (H_old, H_new)
+        (with + V(CV) under MetaD)."""
         ho, hn = C.c_double(), C.c_double()
-        check(lib().lt_omf2(self.U.handle, self.beta, self.tau, int(n_step), C.byref(ho), C.byref(hn)))
+        rho, n = self._rho_n()
+        check(lib().lt_md_integrate(self.U.handle, self._bias(), self.integrator.ID, self.beta, self.tau, int(n_step),
+                                    rho, n, C.byref(ho), C.byref(hn)))
         return ho.value, hn.value
+
+    def ReversibilityTest(self, n_step: int, counter: int = 0) -> tuple[float, float]:
+        """ReversibilityTest (hmc_gauge.hpp:585-598): random momenta, integrate, reverse the
+        momenta, integrate again; returns (H_old, H_new), which agree for a reversible
+        integrator.  The links end where they started."""
+        self.RandomMomentum(counter)
+        ho, _ = self.Integrate(n_step)
+        self.ReverseMomenta()
+        _, hn = self.Integrate(n_step)
+        return ho, hn
 
 
 class HMCMetaDKernel(HMCKernel):
-    """GaugeUpdates::HMCMetaDKernel (updates/hmc_metadynamics.hpp:264-675) with OMF_2, CV =
-    clover Q after n_smear_meta stout steps of parameter rho_stout_cv."""
+    """GaugeUpdates::HMCMetaDKernel (updates/hmc_metadynamics.hpp:264-675) with any of its
+    integrators (OMF_2 by default), CV = clover Q after n_smear_meta stout steps of parameter
+    rho_stout_cv."""
 
     def __init__(self, U: GaugeField, bias: MetaBiasPotential, action: WilsonAction, trajectory_length: float = 1.0,
-                 rho_stout_cv: float = 0.12, n_smear_meta: int = 4, seed: int = 1, counter: int = 0):
-        super().__init__(U, action, trajectory_length, seed, counter)
+                 rho_stout_cv: float = 0.12, n_smear_meta: int = 4, seed: int = 1, counter: int = 0,
+                 integrator: MDIntegrator = OMF_2):
+        if not isinstance(integrator, MDIntegrator) or not integrator.metad:
+            raise ValueError(f"{integrator!r} is not an integrator of HMCMetaDKernel")
+        HMCKernel.__init__(self, U, action, trajectory_length, seed, counter, OMF_2)
+        self.integrator = integrator
         self.bias, self.rho, self.n_smear = bias, float(rho_stout_cv), int(n_smear_meta)
         self.cv = 0.0
 
-    def __call__(self, n_step: int, metropolis_step: bool = True) -> bool:
-        dH, acc, cv = C.c_double(), C.c_int(), C.c_double()
-        check(lib().lt_metad_hmc_trajectory(self.U.handle, self.bias.handle, self.beta, self.tau, int(n_step), self.rho,
-                                            self.n_smear, C.c_uint64(self.seed), C.byref(self.counter),
-                                            int(bool(metropolis_step)), C.byref(dH), C.byref(acc), C.byref(cv)))
-        self.delta_H, self.cv = dH.value, cv.value
-        return bool(acc.value)
+    def _bias(self):
+        return self.bias.handle
+
+    def _rho_n(self):
+        return self.rho, self.n_smear
+
+    def _after(self, cv: float) -> None:
+        self.cv = cv
 
     def MetaCharge(self) -> float:
         return _out1(lib().lt_metad_charge, self.U.handle, self.rho, self.n_smear)
@@ -459,11 +534,11 @@ class HMCMetaDKernel(HMCKernel):
                                    out.ctypes.data if download else None, C.byref(q)))
         return out, q.value
 
-    def Integrate(self, n_step: int) -> tuple[float, float]:
-        ho, hn = C.c_double(), C.c_double()
-        check(lib().lt_metad_omf2(self.U.handle, self.bias.handle, self.beta, self.tau, int(n_step), self.rho,
-                                  self.n_smear, C.byref(ho), C.byref(hn)))
-        return ho.value, hn.value
+
+def ParityUpdate(U: GaugeField) -> None:
+    """ParityUpdate (updates/parity_update.hpp:22-47): the spatial reflection that maps Q to -Q
+    and leaves the action unchanged, in place."""
+    check(lib().lt_parity_update(U.handle))
 
 
 class Ensemble:
@@ -605,4 +680,6 @@ __all__ = ["STATUS_NONFINITE", "STATUS_UNITARITY", "STATUS_HB_CAP", "GaugeField"
            "MetaBiasPotential", "HMCKernel", "HMCMetaDKernel", "CloverDerivative", "LettuceError", "Ensemble",
            "TemperingSwap", "Euler", "RK2", "RK3W7", "TopChargeCloverTimeslice", "EnergyDensityCloverTimeslice",
            "TopChargePlaquette", "RectangularAction", "SymanzikAction", "WilsonLoop", "PolyakovLoop", "Measure",
-           "Observables"]
+           "Observables", "MDIntegrator", "Integrators", "Leapfrog_slow", "Leapfrog", "OMF_2_slow", "OMF_2",
+           "OMF_4_slow", "OMF_4", "Leapfrog_friction_slow", "OMF_4_friction_slow", "Leapfrog_OMF_4",
+           "OMF_2_OMF_4_slow", "OMF_2_OMF_4", "ParityUpdate"]

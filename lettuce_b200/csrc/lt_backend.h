@@ -79,6 +79,9 @@ public:
     virtual void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const = 0;
     virtual void fields(const Ctx& c, void* U, const void* P, double eps) const = 0;
     virtual void random_momenta(const Ctx& c, void* P, uint64_t counter, uint64_t seed) const = 0;
+    // P <- a P + b F on algebra fields (F may be null); the spatial parity reflection Uin -> Uout
+    virtual void alg_axpby(const Ctx& c, void* P, const void* F, double a, double b) const = 0;
+    virtual void parity(const Ctx& c, const void* Uin, void* Uout) const = 0;
 
     // One (mu, parity) sub-sweep of heatbath (op 0) or overrelaxation (op 1) over a batch of
     // lattices described by the device array desc (LatDesc[n_lat]); sel picks 64/128/256

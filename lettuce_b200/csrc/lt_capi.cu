@@ -79,7 +79,6 @@ int order_after(lt_lattice* dst, const lt_lattice* src)
 
 const double kPi = 3.14159265358979323846;
 
-// Integrators::GradientFlow::RK3 (smearing/gradient_flow.hpp:151-161): three fused stages
 // Stages of the reference's flow integrators (smearing/gradient_flow.hpp:31-168), each one
 // fused Z update + exponential update: Z <- c_old Z + c_new eps Algebra(st U^dag),
 // U <- exp(c_exp Z) U
@@ -205,16 +204,24 @@ struct MetaDParams
     std::vector<double>* samples;
 };
 
+// dV/dQ * dQ/dU into h->F at the current links (CalculateTopologicalForce,
+// updates/hmc_metadynamics.hpp:374-436); with submeasure the CV is recorded as the
+// reference's path samples are (:405-412)
+int metad_force_now(lt_lattice* h, const MetaDParams* md, bool submeasure)
+{
+    LT_TRY(metad_forward(h, md->rho, md->n_stout));
+    double q;
+    LT_TRY(clover_q_e(h, level(h, md->n_stout), &q, nullptr));
+    if (submeasure && md->samples) md->samples->push_back(q);
+    return metad_backward(h, md->rho, md->n_stout, md->bias->derivative(q));
+}
+
 int kick(lt_lattice* h, double beta, double eps, const MetaDParams* md, bool submeasure)
 {
     const void* F = nullptr;
     if (md)
     {
-        LT_TRY(metad_forward(h, md->rho, md->n_stout));
-        double q;
-        LT_TRY(clover_q_e(h, level(h, md->n_stout), &q, nullptr));
-        if (submeasure && md->samples) md->samples->push_back(q);
-        LT_TRY(metad_backward(h, md->rho, md->n_stout, md->bias->derivative(q)));
+        LT_TRY(metad_force_now(h, md, submeasure));
         F = h->F;
     }
     h->be->momenta(h->ctx(), h->U, h->P, F, beta / 6.0, eps);
@@ -227,25 +234,193 @@ int drift(lt_lattice* h, double eps)
     return launched("fields");
 }
 
+// One step of a molecular-dynamics program:
+//   KICK          UpdateMomenta: gauge force plus, under MetaD, the force at the current links
+//   KICK_GAUGE    UpdateGaugeMomenta (hmc_metadynamics.hpp:464-476)
+//   KICK_METAD    UpdateMetadynamicsMomenta (:478-491); the force is evaluated at the current
+//                 links first (the reference adds its stored ForceFatLink as it stands)
+//   FRICTION_PRE  UpdateMomentaFriction with friction_without_kick (hmc_gauge.hpp:469-484):
+//                 P <- e P + eps beta/6 Alg(st U^dag), e = exp(-friction eps)
+//   FRICTION_POST the other branch (:485-500): P <- e (P + eps beta/6 Alg(st U^dag))
+//   DRIFT         UpdateFields
+enum class Md : unsigned char { KICK, KICK_GAUGE, KICK_METAD, FRICTION_PRE, FRICTION_POST, DRIFT };
+struct MdOp
+{
+    Md kind;
+    double eps;
+    bool sub = false;        // record the CV (path samples)
+    double friction = 0.0;
+};
+
+// The integrators of updates/hmc_gauge.hpp:19-377 and updates/hmc_metadynamics.hpp:26-238 as
+// programs of the steps above; eps = tau / n_step.
+bool md_program(int integ, double tau, int n, std::vector<MdOp>& ops)
+{
+    ops.clear();
+    if (integ < LT_MD_LEAPFROG_SLOW || integ > LT_MD_OMF2_OMF4) return false;
+    if (n <= 0) return true;
+    const double e = tau / n;
+    auto K = [&](double x, bool sub = false) { ops.push_back({ Md::KICK, x, sub }); };
+    auto G = [&](double x) { ops.push_back({ Md::KICK_GAUGE, x }); };
+    auto M = [&](double x) { ops.push_back({ Md::KICK_METAD, x }); };
+    auto D = [&](double x) { ops.push_back({ Md::DRIFT, x }); };
+    auto FP = [&](double x, double f, bool pre) { ops.push_back({ pre ? Md::FRICTION_PRE : Md::FRICTION_POST, x, false, f }); };
+    // OMF2 (hep-lat/0505020) and OMF4 coefficients
+    const double l2 = 0.1931833275037836;
+    const double a4 = 0.08398315262876693, b4 = 0.2539785108410595, g4 = 0.6822365335719091,
+                 d4 = -0.03230286765269967;
+    const double m4 = 0.5 - g4 - a4, n4 = 1.0 - 2.0 * d4 - 2.0 * b4;
+    // one OMF4 step of the gauge part with kicks `kick` and the first / last kick left out
+    auto omf4_inner = [&](double s, auto kick) {
+        D(s * b4 * e); kick(s * g4 * e); D(s * d4 * e);
+        kick(s * m4 * e); D(s * n4 * e); kick(s * m4 * e);
+        D(s * d4 * e); kick(s * g4 * e); D(s * b4 * e);
+    };
+    auto kfull = [&](double x) { K(x); };
+    switch (integ)
+    {
+    case LT_MD_LEAPFROG_SLOW:   // hmc_gauge.hpp:21-44
+        for (int k = 0; k < n; ++k) { K(0.5 * e); D(e); K(0.5 * e, true); }
+        break;
+    case LT_MD_LEAPFROG:        // :47-70
+        K(0.5 * e);
+        for (int k = 0; k < n - 1; ++k) { D(e); K(e, true); }
+        D(e); K(0.5 * e, true);
+        break;
+    case LT_MD_OMF2_SLOW:       // :121-151
+        for (int k = 0; k < n; ++k) { K(l2 * e); D(0.5 * e); K((1.0 - 2.0 * l2) * e); D(0.5 * e); K(l2 * e, true); }
+        break;
+    case LT_MD_OMF2:            // :155-190
+        K(l2 * e); D(0.5 * e); K((1.0 - 2.0 * l2) * e); D(0.5 * e);
+        for (int k = 0; k < n - 1; ++k) { K(2.0 * l2 * e, true); D(0.5 * e); K((1.0 - 2.0 * l2) * e); D(0.5 * e); }
+        K(l2 * e, true);
+        break;
+    case LT_MD_OMF4_SLOW:       // :195-237
+        for (int k = 0; k < n; ++k) { K(a4 * e); omf4_inner(1.0, kfull); K(a4 * e, true); }
+        break;
+    case LT_MD_OMF4:            // :241-294
+        K(a4 * e); omf4_inner(1.0, kfull);
+        for (int k = 0; k < n - 1; ++k) { K(2.0 * a4 * e, true); omf4_inner(1.0, kfull); }
+        K(a4 * e, true);
+        break;
+    case LT_MD_LEAPFROG_FRICTION_SLOW:   // :74-116 (RAHMC, 2403.04607)
+    case LT_MD_OMF4_FRICTION_SLOW:       // :298-376
+    {
+        double f = 0.01;
+        const int half = n / 2;
+        auto step = [&](bool flip_mid) {
+            if (integ == LT_MD_LEAPFROG_FRICTION_SLOW)
+            {
+                FP(0.5 * e, f, true); D(e);
+                if (flip_mid) f = -f;
+                FP(0.5 * e, f, false);
+            }
+            else
+            {
+                FP(a4 * e, f, true); D(b4 * e); FP(g4 * e, f, true); D(d4 * e);
+                FP(m4 * e, f, true); D(n4 * e);
+                if (flip_mid) f = -f;
+                FP(m4 * e, f, false);
+                D(d4 * e); FP(g4 * e, f, false); D(b4 * e); FP(a4 * e, f, false);
+            }
+        };
+        for (int k = 0; k < half; ++k) step(false);
+        if (n % 2 != 0) step(true);
+        else f = -f;
+        for (int k = 0; k < half; ++k) step(false);
+        break;
+    }
+    case LT_MD_LEAPFROG_OMF4:   // hmc_metadynamics.hpp:28-83
+    {
+        auto kg = [&](double x) { G(x); };
+        M(0.5 * e);
+        for (int k = 0; k < n; ++k)
+        {
+            G(a4 * e); omf4_inner(1.0, kg); G(a4 * e);
+            M(k < n - 1 ? e : 0.5 * e);
+        }
+        break;
+    }
+    case LT_MD_OMF2_OMF4_SLOW:  // :85-143
+    {
+        auto kg = [&](double x) { G(x); };
+        for (int k = 0; k < n; ++k)
+        {
+            M(l2 * e);
+            G(a4 * e); omf4_inner(1.0, kg); G(a4 * e);
+            M((1.0 - 2.0 * l2) * e);
+            G(a4 * e); omf4_inner(1.0, kg); G(a4 * e);
+            M(l2 * e);
+        }
+        break;
+    }
+    case LT_MD_OMF2_OMF4:       // :145-237 (inner OMF4 at half steps)
+    {
+        auto kg = [&](double x) { G(x); };
+        M(l2 * e);
+        for (int k = 0; k < n; ++k)
+        {
+            G(0.5 * a4 * e); omf4_inner(0.5, kg); G(0.5 * a4 * e);
+            M((1.0 - 2.0 * l2) * e);
+            G(0.5 * a4 * e); omf4_inner(0.5, kg); G(0.5 * a4 * e);
+            M(k < n - 1 ? 2.0 * l2 * e : l2 * e);
+        }
+        break;
+    }
+    }
+    return true;
+}
+
+bool md_needs_bias(int integ) { return integ >= LT_MD_LEAPFROG_OMF4; }
+bool md_friction(int integ) { return integ == LT_MD_LEAPFROG_FRICTION_SLOW || integ == LT_MD_OMF4_FRICTION_SLOW; }
+
+int md_check(int integ, bool metad, const char* fn)
+{
+    if (integ < LT_MD_LEAPFROG_SLOW || integ > LT_MD_OMF2_OMF4)
+        return lt::set_error(LT_ERR_ARG, (std::string(fn) + ": unknown integrator").c_str());
+    if (md_needs_bias(integ) && !metad)
+        return lt::set_error(LT_ERR_ARG, (std::string(fn) + ": multiple-timescale integrators need a bias").c_str());
+    if (md_friction(integ) && metad)
+        return lt::set_error(LT_ERR_ARG, (std::string(fn) + ": friction integrators are gauge-only").c_str());
+    return LT_OK;
+}
+
+// Run a program on (h->U, h->P); md null for the gauge action alone
+int integrate(lt_lattice* h, double beta, const std::vector<MdOp>& ops, const MetaDParams* md)
+{
+    const lt::Ctx c = h->ctx();
+    for (const MdOp& op : ops)
+    {
+        switch (op.kind)
+        {
+        case Md::KICK: LT_TRY(kick(h, beta, op.eps, md, op.sub)); break;
+        case Md::KICK_GAUGE: LT_TRY(kick(h, beta, op.eps, nullptr, false)); break;
+        case Md::KICK_METAD:
+            LT_TRY(metad_force_now(h, md, op.sub));
+            h->be->alg_axpby(c, h->P, h->F, 1.0, op.eps);
+            LT_TRY(launched("metad momenta"));
+            break;
+        case Md::FRICTION_PRE:
+            h->be->alg_axpby(c, h->P, nullptr, std::exp(-op.friction * op.eps), 0.0);
+            LT_TRY(kick(h, beta, op.eps, nullptr, false));
+            break;
+        case Md::FRICTION_POST:
+            LT_TRY(kick(h, beta, op.eps, nullptr, false));
+            h->be->alg_axpby(c, h->P, nullptr, std::exp(-op.friction * op.eps), 0.0);
+            LT_TRY(launched("friction"));
+            break;
+        case Md::DRIFT: LT_TRY(drift(h, op.eps)); break;
+        }
+    }
+    return LT_OK;
+}
+
 // Integrators::HMC::OMF_2 (updates/hmc_gauge.hpp:155-190)
 int omf2(lt_lattice* h, double beta, double tau, int n_step, const MetaDParams* md)
 {
-    if (n_step <= 0) return LT_OK;
-    const double lam = 0.1931833275037836;
-    const double eps = tau / n_step;
-    const double a = lam * eps, b = 0.5 * eps, g = (1.0 - 2.0 * lam) * eps;
-    LT_TRY(kick(h, beta, a, md, false));
-    LT_TRY(drift(h, b));
-    LT_TRY(kick(h, beta, g, md, false));
-    LT_TRY(drift(h, b));
-    for (int k = 0; k < n_step - 1; ++k)
-    {
-        LT_TRY(kick(h, beta, 2.0 * a, md, true));
-        LT_TRY(drift(h, b));
-        LT_TRY(kick(h, beta, g, md, false));
-        LT_TRY(drift(h, b));
-    }
-    return kick(h, beta, a, md, true);
+    std::vector<MdOp> ops;
+    md_program(LT_MD_OMF2, tau, n_step, ops);
+    return integrate(h, beta, ops, md);
 }
 
 int metad_charge(lt_lattice* h, double rho, int n_stout, double* q)
@@ -828,27 +1003,25 @@ int lt_omf2(lt_lattice* h, double beta, double tau, int n_step, double* h_old, d
 int lt_hmc_trajectory(lt_lattice* h, double beta, double tau, int n_step, uint64_t seed, uint64_t* counter,
                       int metropolis, double* dH, int* accepted)
 {
-    LT_TRY(check_h(h, "lt_hmc_trajectory"));
-    if (!counter) return lt::set_error(LT_ERR_ARG, "lt_hmc_trajectory: null counter");
-    LT_TRY(ensure(h, &h->Ubak, h->be->gauge_bytes(h->g)));
-    LT_CK(cudaMemcpyAsync(h->Ubak, h->U, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
-    LT_TRY(lt_random_momenta(h, seed, *counter));
-    double ho, hn;
-    LT_TRY(hamiltonian(h, beta, &ho));
-    LT_TRY(omf2(h, beta, tau, n_step, nullptr));
-    LT_TRY(hamiltonian(h, beta, &hn));
-    const double d = hn - ho;
-    bool acc = true;
-    if (metropolis)
-    {
-        acc = accept_uniform(seed, *counter) <= std::exp(-d);
-        if (!acc) LT_CK(cudaMemcpyAsync(h->U, h->Ubak, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
-    }
-    ++*counter;
-    if (dH) *dH = d;
-    if (accepted) *accepted = acc ? 1 : 0;
-    if (!std::isfinite(d)) return lt::set_error(LT_ERR_NUMERIC, "lt_hmc_trajectory: non-finite dH");
-    return LT_OK;
+    return lt_md_trajectory(h, nullptr, LT_MD_OMF2, beta, tau, n_step, 0.0, 0, seed, counter, metropolis, dH, accepted,
+                            nullptr);
+}
+
+int lt_reverse_momenta(lt_lattice* h)
+{
+    LT_TRY(check_h(h, "lt_reverse_momenta"));
+    if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_reverse_momenta: no momenta set");
+    h->be->alg_axpby(h->ctx(), h->P, nullptr, -1.0, 0.0);
+    return launched("lt_reverse_momenta");
+}
+
+int lt_parity_update(lt_lattice* h)
+{
+    LT_TRY(check_h(h, "lt_parity_update"));
+    LT_TRY(ensure(h, &h->U2, h->be->gauge_bytes(h->g)));
+    h->be->parity(h->ctx(), h->U, h->U2);
+    std::swap(h->U, h->U2);
+    return launched("lt_parity_update");
 }
 
 // ---------------------------------------------------------------- metadynamics
@@ -896,24 +1069,7 @@ int lt_metad_omf2(lt_lattice* h, lt_bias* bias, double beta, double tau, int n_s
 {
     LT_TRY(check_h(h, "lt_metad_omf2"));
     if (!bias) return lt::set_error(LT_ERR_ARG, "lt_metad_omf2: null bias");
-    if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_metad_omf2: no momenta set");
-    auto* b = reinterpret_cast<lt::Bias*>(bias);
-    double q, hh;
-    if (h_old)
-    {
-        LT_TRY(metad_charge(h, rho, n_stout, &q));
-        LT_TRY(hamiltonian(h, beta, &hh));
-        *h_old = hh + b->potential(q);
-    }
-    MetaDParams md { b, rho, n_stout, nullptr };
-    LT_TRY(omf2(h, beta, tau, n_step, &md));
-    if (h_new)
-    {
-        LT_TRY(metad_charge(h, rho, n_stout, &q));
-        LT_TRY(hamiltonian(h, beta, &hh));
-        *h_new = hh + b->potential(q);
-    }
-    return LT_OK;
+    return lt_md_integrate(h, bias, LT_MD_OMF2, beta, tau, n_step, rho, n_stout, h_old, h_new);
 }
 
 int lt_metad_hmc_trajectory(lt_lattice* h, lt_bias* bias, double beta, double tau, int n_step, double rho,
@@ -921,49 +1077,94 @@ int lt_metad_hmc_trajectory(lt_lattice* h, lt_bias* bias, double beta, double ta
                             double* cv_out)
 {
     LT_TRY(check_h(h, "lt_metad_hmc_trajectory"));
-    if (!bias || !counter) return lt::set_error(LT_ERR_ARG, "lt_metad_hmc_trajectory: null argument");
+    if (!bias) return lt::set_error(LT_ERR_ARG, "lt_metad_hmc_trajectory: null bias");
+    return lt_md_trajectory(h, bias, LT_MD_OMF2, beta, tau, n_step, rho, n_stout, seed, counter, metropolis, dH,
+                            accepted, cv_out);
+}
+
+// H (+ V(CV) under MetaD) of the current links and momenta
+static int md_energy(lt_lattice* h, lt::Bias* b, double beta, double rho, int n_stout, double* e, double* cv)
+{
+    double hh;
+    if (b)
+    {
+        LT_TRY(metad_charge(h, rho, n_stout, cv));
+        LT_TRY(hamiltonian(h, beta, &hh));
+        *e = hh + b->potential(*cv);
+        return LT_OK;
+    }
+    LT_TRY(hamiltonian(h, beta, &hh));
+    *e = hh;
+    return LT_OK;
+}
+
+int lt_md_integrate(lt_lattice* h, lt_bias* bias, int integrator, double beta, double tau, int n_step, double rho,
+                    int n_stout, double* h_old, double* h_new)
+{
+    LT_TRY(check_h(h, "lt_md_integrate"));
+    if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_md_integrate: no momenta set");
+    if (bias && n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_md_integrate: n_stout < 0");
+    LT_TRY(md_check(integrator, bias != nullptr, "lt_md_integrate"));
+    auto* b = reinterpret_cast<lt::Bias*>(bias);
+    double cv;
+    if (h_old) LT_TRY(md_energy(h, b, beta, rho, n_stout, h_old, &cv));
+    std::vector<MdOp> ops;
+    md_program(integrator, tau, n_step, ops);
+    MetaDParams md { b, rho, n_stout, nullptr };
+    LT_TRY(integrate(h, beta, ops, b ? &md : nullptr));
+    if (h_new) LT_TRY(md_energy(h, b, beta, rho, n_stout, h_new, &cv));
+    return LT_OK;
+}
+
+int lt_md_trajectory(lt_lattice* h, lt_bias* bias, int integrator, double beta, double tau, int n_step, double rho,
+                     int n_stout, uint64_t seed, uint64_t* counter, int metropolis, double* dH, int* accepted,
+                     double* cv_out)
+{
+    LT_TRY(check_h(h, "lt_md_trajectory"));
+    if (!counter) return lt::set_error(LT_ERR_ARG, "lt_md_trajectory: null counter");
+    if (bias && n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_md_trajectory: n_stout < 0");
+    LT_TRY(md_check(integrator, bias != nullptr, "lt_md_trajectory"));
     auto* b = reinterpret_cast<lt::Bias*>(bias);
     LT_TRY(ensure(h, &h->Ubak, h->be->gauge_bytes(h->g)));
     LT_CK(cudaMemcpyAsync(h->Ubak, h->U, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
     LT_TRY(lt_random_momenta(h, seed, *counter));
-    double cv_old, cv_new, hh;
-    LT_TRY(metad_charge(h, rho, n_stout, &cv_old));
-    LT_TRY(hamiltonian(h, beta, &hh));
-    const double e_old = hh + b->potential(cv_old);
+    double cv_old = 0.0, cv_new = 0.0, e_old, e_new;
+    LT_TRY(md_energy(h, b, beta, rho, n_stout, &e_old, &cv_old));
     std::vector<double> samples;
     samples.reserve((size_t)n_step);
+    std::vector<MdOp> ops;
+    md_program(integrator, tau, n_step, ops);
     MetaDParams md { b, rho, n_stout, &samples };
-    LT_TRY(omf2(h, beta, tau, n_step, &md));
-    LT_TRY(metad_charge(h, rho, n_stout, &cv_new));
-    LT_TRY(hamiltonian(h, beta, &hh));
-    const double e_new = hh + b->potential(cv_new);
+    LT_TRY(integrate(h, beta, ops, b ? &md : nullptr));
+    LT_TRY(md_energy(h, b, beta, rho, n_stout, &e_new, &cv_new));
     const double d = e_new - e_old;
     bool acc = true;
     if (metropolis)
     {
         acc = accept_uniform(seed, *counter) <= std::exp(-d);
-        if (acc)
-            b->cv_current = cv_new;
-        else
-        {
-            b->cv_current = cv_old;
-            for (double& s : samples) s = cv_old;
-            LT_CK(cudaMemcpyAsync(h->U, h->Ubak, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
-        }
+        if (!acc) LT_CK(cudaMemcpyAsync(h->U, h->Ubak, h->be->gauge_bytes(h->g), cudaMemcpyDeviceToDevice, h->stream));
     }
-    else
-        b->cv_current = cv_new;
-    for (double s : samples)
+    if (b)
     {
-        b->update(s);
-        b->update(-s);
+        // the visited CVs (or, for the multiple-timescale integrators, which record none, the
+        // final CV) are deposited symmetrically; a rejected trajectory deposits CV_old
+        // (updates/hmc_metadynamics.hpp:583-626)
+        b->cv_current = acc ? cv_new : cv_old;
+        if (samples.empty()) samples.push_back(b->cv_current);
+        if (!acc)
+            for (double& s : samples) s = cv_old;
+        for (double s : samples)
+        {
+            b->update(s);
+            b->update(-s);
+        }
     }
     ++*counter;
     LT_CK(cudaStreamSynchronize(h->stream));
     if (dH) *dH = d;
     if (accepted) *accepted = acc ? 1 : 0;
-    if (cv_out) *cv_out = b->cv_current;
-    if (!std::isfinite(d)) return lt::set_error(LT_ERR_NUMERIC, "lt_metad_hmc_trajectory: non-finite dH");
+    if (cv_out) *cv_out = b ? b->cv_current : 0.0;
+    if (!std::isfinite(d)) return lt::set_error(LT_ERR_NUMERIC, "lt_md_trajectory: non-finite dH");
     return LT_OK;
 }
 

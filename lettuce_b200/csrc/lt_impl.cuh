@@ -1,5 +1,7 @@
 // Backend implementation for one storage format: launches the kernels of lt_kernels.cuh.
 #pragma once
+#include <algorithm>
+
 #include "lt_backend.h"
 #include "lt_kernels.cuh"
 
@@ -189,6 +191,16 @@ public:
     {
         k_fields<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), alg(P, c.g),
                                                                                    4 * c.g.V, (T)eps);
+    }
+    void alg_axpby(const Ctx& c, void* P, const void* F, double a, double b) const override
+    {
+        const size_t n = (size_t)4 * c.g.V * 8;
+        const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)kRedBlocks * 4);
+        k_alg_axpby<T><<<blocks, 256, 0, c.stream>>>(static_cast<T*>(P), static_cast<const T*>(F), n, (T)a, (T)b);
+    }
+    void parity(const Ctx& c, const void* Uin, void* Uout) const override
+    {
+        k_parity<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(Uin, c.g), gauge(Uout, c.g), c.g);
     }
     void random_momenta(const Ctx& c, void* P, uint64_t counter, uint64_t seed) const override
     {

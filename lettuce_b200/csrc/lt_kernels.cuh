@@ -1211,6 +1211,36 @@ __global__ void __launch_bounds__(kThreads) k_fields(Gauge<T, NR> U, Alg<T> P, i
     U.st(mu, par, s, exp_update<T, NR>(unpack_ah(P.ld(mu, par, s)), eps, U.ld(mu, par, s)));
 }
 
+// P <- a P + b F over the flat algebra field (n reals; F may be null): the Metadynamics
+// momentum update with a stored force (updates/hmc_metadynamics.hpp:478-491), ReverseMomenta
+// (updates/hmc_gauge.hpp:432-446) and the friction factor of UpdateMomentaFriction (:469-503)
+template <typename T>
+__global__ void k_alg_axpby(T* __restrict__ P, const T* __restrict__ F, size_t n, T a, T b)
+{
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+        P[k] = F ? a * P[k] + b * F[k] : a * P[k];
+}
+
+// ParityUpdate (updates/parity_update.hpp:22-47): the spatial reflection x -> -x - 1 (per
+// spatial extent), out of place.  Time links move with their sites; a spatial link U_i(x)
+// becomes the adjoint of the reflected link that ends at the reflected site.
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_parity(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    const int pl = l / g.vh, s = l - pl * g.vh, mu = pl >> 1, par = pl & 1;
+    int c[4];
+    site_coords(g, par, s, c);
+    int r[4] = { c[0], g.n[1] - c[1] - 1, g.n[2] - c[2] - 1, g.n[3] - c[3] - 1 };
+    if (mu > 0) r[mu] = (r[mu] - 1 + g.n[mu]) % g.n[mu];
+    const int j = ((r[0] * g.n[1] + r[1]) * g.n[2] + r[2]) * g.n[3] + r[3];
+    const int pj = (r[0] + r[1] + r[2] + r[3]) & 1;
+    const M3<T> m = Uin.ld(mu, pj, j >> 1);
+    Uout.st(mu, par, s, mu == 0 ? m : adj(m));
+}
+
 // RandomMomentum (updates/hmc_gauge.hpp:400-428): P = 1/2 i phi_a lambda_a with eight
 // Box-Muller Gaussians from Philox calls j = 0..3 of tag TAG_MOMENTA.
 template <typename T>

@@ -975,6 +975,238 @@ double or_metad_charge(const int ext[4], const double* U, double rho, int n_stou
     return q;
 }
 
+/* ---------------------------------------------------------------- MD integrators */
+/* The integrators of updates/hmc_gauge.hpp:19-377 and updates/hmc_metadynamics.hpp:26-238,
+ * driven through the five momentum/field updates below.  With metad != 0 the bias is linear,
+ * V(Q) = slope * Q, and its force slope * dQ_stout/dU is evaluated at the current links at
+ * every full or Metadynamics momentum update. */
+typedef struct
+{
+    const int* ext;
+    Geo g;
+    double *U, *P, *F, beta, rho, slope;
+    int metad, n_stout;
+} MdState;
+
+/* UpdateMomenta (hmc_gauge.hpp:450-464; hmc_metadynamics.hpp:441-459 under MetaD) */
+static void md_kick(MdState* s, double eps)
+{
+    if (s->metad) or_metad_force(s->ext, s->U, s->rho, s->n_stout, s->slope, s->F);
+    hmc_update_momenta(&s->g, s->U, s->P, s->beta, eps, s->metad ? s->F : NULL);
+}
+
+/* UpdateGaugeMomenta (hmc_metadynamics.hpp:464-476) */
+static void md_kick_gauge(MdState* s, double eps) { hmc_update_momenta(&s->g, s->U, s->P, s->beta, eps, NULL); }
+
+/* UpdateMetadynamicsMomenta (hmc_metadynamics.hpp:478-491) with the force at the current links */
+static void md_kick_metad(MdState* s, double eps)
+{
+    or_metad_force(s->ext, s->U, s->rho, s->n_stout, s->slope, s->F);
+    for (long x = 0; x < s->g.V; ++x)
+        for (int mu = 0; mu < 4; ++mu)
+        {
+            M3 p = add(ld(s->P, x, mu), scl(eps, ld(s->F, x, mu)));
+            st(s->P, x, mu, &p);
+        }
+}
+
+/* UpdateMomentaFriction (hmc_gauge.hpp:469-503) */
+static void md_friction(MdState* s, double eps, double fric, int without_kick)
+{
+    const double e = exp(-fric * eps);
+    for (long x = 0; x < s->g.V; ++x)
+        for (int mu = 0; mu < 4; ++mu)
+        {
+            M3 f = scl(eps * s->beta / 6.0, algebra(mul(staple(&s->g, s->U, x, mu), dag(ld(s->U, x, mu)))));
+            M3 p = without_kick ? add(scl(e, ld(s->P, x, mu)), f) : scl(e, add(ld(s->P, x, mu), f));
+            st(s->P, x, mu, &p);
+        }
+}
+
+static void md_drift(MdState* s, double eps) { hmc_update_fields(&s->g, s->U, s->P, eps); }
+
+static const double OMF2_L = 0.1931833275037836;
+static const double OMF4_A = 0.08398315262876693, OMF4_B = 0.2539785108410595, OMF4_G = 0.6822365335719091,
+                    OMF4_D = -0.03230286765269967;
+
+/* the middle of one OMF4 step (everything between its first and last momentum update) at
+ * step size e, kicks by UpdateGaugeMomenta (gauge_only) or UpdateMomenta */
+static void md_omf4_middle(MdState* s, double e, int gauge_only)
+{
+    const double mu = 0.5 - OMF4_G - OMF4_A, nu = 1.0 - 2.0 * OMF4_D - 2.0 * OMF4_B;
+    void (*k)(MdState*, double) = gauge_only ? md_kick_gauge : md_kick;
+    md_drift(s, OMF4_B * e);
+    k(s, OMF4_G * e);
+    md_drift(s, OMF4_D * e);
+    k(s, mu * e);
+    md_drift(s, nu * e);
+    k(s, mu * e);
+    md_drift(s, OMF4_D * e);
+    k(s, OMF4_G * e);
+    md_drift(s, OMF4_B * e);
+}
+
+static void md_friction_step(MdState* s, int omf4, double e, double* fric, int flip_mid)
+{
+    if (!omf4)
+    {
+        md_friction(s, 0.5 * e, *fric, 1);
+        md_drift(s, e);
+        if (flip_mid) *fric = -*fric;
+        md_friction(s, 0.5 * e, *fric, 0);
+        return;
+    }
+    const double mu = 0.5 - OMF4_G - OMF4_A, nu = 1.0 - 2.0 * OMF4_D - 2.0 * OMF4_B;
+    md_friction(s, OMF4_A * e, *fric, 1);
+    md_drift(s, OMF4_B * e);
+    md_friction(s, OMF4_G * e, *fric, 1);
+    md_drift(s, OMF4_D * e);
+    md_friction(s, mu * e, *fric, 1);
+    md_drift(s, nu * e);
+    if (flip_mid) *fric = -*fric;
+    md_friction(s, mu * e, *fric, 0);
+    md_drift(s, OMF4_D * e);
+    md_friction(s, OMF4_G * e, *fric, 0);
+    md_drift(s, OMF4_B * e);
+    md_friction(s, OMF4_A * e, *fric, 0);
+}
+
+static double md_energy(MdState* s)
+{
+    double h = or_wilson_action(s->ext, s->U, s->beta) + or_kinetic(s->ext, s->P);
+    if (s->metad) h += s->slope * or_metad_charge(s->ext, s->U, s->rho, s->n_stout);
+    return h;
+}
+
+void or_md_integrate(const int ext[4], double* U, double* P, double beta, double tau, int n, int integrator,
+                     int metad, double rho, int n_stout, double slope, double* h_old, double* h_new)
+{
+    MdState s;
+    s.ext = ext;
+    s.g = geo(ext);
+    s.U = U;
+    s.P = P;
+    s.F = (double*)malloc(sizeof(double) * (size_t)s.g.V * 72);
+    s.beta = beta;
+    s.rho = rho;
+    s.slope = slope;
+    s.metad = metad;
+    s.n_stout = n_stout;
+    *h_old = md_energy(&s);
+    const double e = n > 0 ? tau / n : 0.0;
+    const double l2 = OMF2_L, a4 = OMF4_A;
+    if (n > 0) switch (integrator)
+    {
+    case 0:   /* Leapfrog_slow (hmc_gauge.hpp:21-44) */
+        for (int k = 0; k < n; ++k) { md_kick(&s, 0.5 * e); md_drift(&s, e); md_kick(&s, 0.5 * e); }
+        break;
+    case 1:   /* Leapfrog (:47-70) */
+        md_kick(&s, 0.5 * e);
+        for (int k = 0; k < n - 1; ++k) { md_drift(&s, e); md_kick(&s, e); }
+        md_drift(&s, e);
+        md_kick(&s, 0.5 * e);
+        break;
+    case 2:   /* OMF_2_slow (:121-151) */
+        for (int k = 0; k < n; ++k)
+        {
+            md_kick(&s, l2 * e); md_drift(&s, 0.5 * e); md_kick(&s, (1.0 - 2.0 * l2) * e);
+            md_drift(&s, 0.5 * e); md_kick(&s, l2 * e);
+        }
+        break;
+    case 3:   /* OMF_2 (:155-190) */
+        md_kick(&s, l2 * e); md_drift(&s, 0.5 * e); md_kick(&s, (1.0 - 2.0 * l2) * e); md_drift(&s, 0.5 * e);
+        for (int k = 0; k < n - 1; ++k)
+        {
+            md_kick(&s, 2.0 * l2 * e); md_drift(&s, 0.5 * e); md_kick(&s, (1.0 - 2.0 * l2) * e);
+            md_drift(&s, 0.5 * e);
+        }
+        md_kick(&s, l2 * e);
+        break;
+    case 4:   /* OMF_4_slow (:195-237) */
+        for (int k = 0; k < n; ++k) { md_kick(&s, a4 * e); md_omf4_middle(&s, e, 0); md_kick(&s, a4 * e); }
+        break;
+    case 5:   /* OMF_4 (:241-294) */
+        md_kick(&s, a4 * e);
+        md_omf4_middle(&s, e, 0);
+        for (int k = 0; k < n - 1; ++k) { md_kick(&s, 2.0 * a4 * e); md_omf4_middle(&s, e, 0); }
+        md_kick(&s, a4 * e);
+        break;
+    case 6:   /* Leapfrog_friction_slow (:74-116) */
+    case 7:   /* OMF_4_friction_slow (:298-376) */
+    {
+        double fric = 0.01;
+        const int omf4 = integrator == 7, half = n / 2;
+        for (int k = 0; k < half; ++k) md_friction_step(&s, omf4, e, &fric, 0);
+        if (n % 2 != 0) md_friction_step(&s, omf4, e, &fric, 1);
+        else fric = -fric;
+        for (int k = 0; k < half; ++k) md_friction_step(&s, omf4, e, &fric, 0);
+        break;
+    }
+    case 8:   /* Leapfrog_OMF_4 (hmc_metadynamics.hpp:28-83) */
+        md_kick_metad(&s, 0.5 * e);
+        for (int k = 0; k < n; ++k)
+        {
+            md_kick_gauge(&s, a4 * e); md_omf4_middle(&s, e, 1); md_kick_gauge(&s, a4 * e);
+            md_kick_metad(&s, k < n - 1 ? e : 0.5 * e);
+        }
+        break;
+    case 9:   /* OMF_2_OMF_4_slow (:85-143) */
+        for (int k = 0; k < n; ++k)
+        {
+            md_kick_metad(&s, l2 * e);
+            md_kick_gauge(&s, a4 * e); md_omf4_middle(&s, e, 1); md_kick_gauge(&s, a4 * e);
+            md_kick_metad(&s, (1.0 - 2.0 * l2) * e);
+            md_kick_gauge(&s, a4 * e); md_omf4_middle(&s, e, 1); md_kick_gauge(&s, a4 * e);
+            md_kick_metad(&s, l2 * e);
+        }
+        break;
+    case 10:  /* OMF_2_OMF_4 (:145-237): the inner OMF4 at half steps */
+        md_kick_metad(&s, l2 * e);
+        for (int k = 0; k < n; ++k)
+        {
+            md_kick_gauge(&s, 0.5 * a4 * e); md_omf4_middle(&s, 0.5 * e, 1); md_kick_gauge(&s, 0.5 * a4 * e);
+            md_kick_metad(&s, (1.0 - 2.0 * l2) * e);
+            md_kick_gauge(&s, 0.5 * a4 * e); md_omf4_middle(&s, 0.5 * e, 1); md_kick_gauge(&s, 0.5 * a4 * e);
+            md_kick_metad(&s, k < n - 1 ? 2.0 * l2 * e : l2 * e);
+        }
+        break;
+    default:
+        break;
+    }
+    *h_new = md_energy(&s);
+    free(s.F);
+}
+
+/* ParityUpdate (updates/parity_update.hpp:22-47) */
+void or_parity_update(const int ext[4], double* U)
+{
+    Geo g = geo(ext);
+    size_t n = (size_t)g.V * 72;
+    double* c = (double*)malloc(n * sizeof(double));
+    memcpy(c, U, n * sizeof(double));
+    const int Nx = ext[1], Ny = ext[2], Nz = ext[3];
+    for (int t = 0; t < ext[0]; ++t)
+        for (int x = 0; x < Nx; ++x)
+            for (int y = 0; y < Ny; ++y)
+                for (int z = 0; z < Nz; ++z)
+                {
+                    const long site = (((long)t * Nx + x) * Ny + y) * Nz + z;
+                    const int rx = Nx - x - 1, ry = Ny - y - 1, rz = Nz - z - 1;
+                    const int rxm = (rx - 1 + Nx) % Nx, rym = (ry - 1 + Ny) % Ny, rzm = (rz - 1 + Nz) % Nz;
+#define SITE(tt, xx, yy, zz) ((((long)(tt) * Nx + (xx)) * Ny + (yy)) * Nz + (zz))
+                    M3 m0 = ld(c, SITE(t, rx, ry, rz), 0);
+                    M3 m1 = dag(ld(c, SITE(t, rxm, ry, rz), 1));
+                    M3 m2 = dag(ld(c, SITE(t, rx, rym, rz), 2));
+                    M3 m3 = dag(ld(c, SITE(t, rx, ry, rzm), 3));
+#undef SITE
+                    st(U, site, 0, &m0);
+                    st(U, site, 1, &m1);
+                    st(U, site, 2, &m2);
+                    st(U, site, 3, &m3);
+                }
+    free(c);
+}
+
 /* ---------------------------------------------------------------- bias potential */
 /* MetaBiasPotential (metadynamics.hpp:60-187), well-tempered deposits */
 or_bias* or_bias_create(double cv_min, double cv_max, int bins, double weight, double width, double wt, double thr)
@@ -1255,7 +1487,6 @@ double or_wilson_loop(const int ext[4], const double* U, int L)
  * over every spatial site, averaged over the spatial volume */
 void or_polyakov_loop(const int ext[4], const double* U, double* re, double* im)
 {
-    Geo g = geo(ext);
     cd p = 0.0;
     long vs = (long)ext[1] * ext[2] * ext[3];
     for (long k = 0; k < vs; ++k)

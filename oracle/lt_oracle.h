@@ -38,6 +38,10 @@ double or_metad_charge(const int ext[4], const double* U, double rho, int n_stou
 void   or_omf2(const int ext[4], double* U, double* P, double beta, double tau, int n_step,
                double* h_old, double* h_new);
 void   or_random_momenta(const int ext[4], double* P, uint64_t seed, uint64_t counter);
+/* any of the eleven MD integrators (ids as LT_MD_* of the C ABI); metad: linear bias slope*Q */
+void   or_md_integrate(const int ext[4], double* U, double* P, double beta, double tau, int n_step, int integrator,
+                       int metad, double rho, int n_stout, double slope, double* h_old, double* h_new);
+void   or_parity_update(const int ext[4], double* U);
 double or_kinetic(const int ext[4], const double* P);
 
 /* MetaBiasPotential (metadynamics.hpp:29-187) */

@@ -67,6 +67,7 @@
 #include "LettuceGauge/updates/heatbath.hpp"
 #include "LettuceGauge/updates/overrelaxation.hpp"
 #include "LettuceGauge/IO/config_io/bmw_format.hpp"
+#include "LettuceGauge/updates/parity_update.hpp"
 // Only the two HMC headers are compiled with `private` mapped to `public` (they hold no
 // OpenMP `private(...)` clauses, which the mapping would break).
 #define private public
@@ -134,6 +135,40 @@ std::unique_ptr<MetaBiasPotential> linear_bias(double slope)
     auto bias = std::make_unique<MetaBiasPotential>(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0);
     bias->GeneratePotentialFrom([slope](double cv) { return slope * cv; });
     return bias;
+}
+// The integrator hooks of HMCMetaDKernel with the Metadynamics momentum update preceded by
+// CalculateTopologicalForce on the current links, so that the multiple-timescale integrators
+// of hmc_metadynamics.hpp:26-238 apply the bias force of the field they are at (the kernel's
+// own UpdateMetadynamicsMomenta, :478-491, adds the force it last stored).
+template <typename KernelT>
+struct RefreshedMetaD
+{
+    KernelT& k;
+    void UpdateGaugeMomenta(const floatT e) { k.UpdateGaugeMomenta(e); }
+    void UpdateMetadynamicsMomenta(const floatT e)
+    {
+        k.CalculateTopologicalForce();
+        k.UpdateMetadynamicsMomenta(e);
+    }
+    void UpdateMomenta(const floatT e, const bool sub = false) { k.UpdateMomenta(e, sub); }
+    void UpdateFields(const floatT e) { k.UpdateFields(e); }
+};
+
+// Run integrator `id` (the LT_MD_* numbering of the C ABI) of the reference on `kernel`
+template <typename HMCFunctor>
+bool run_integrator(int id, HMCFunctor& kernel, double tau, int n)
+{
+    using namespace Integrators::HMC;
+    switch (id)
+    {
+    case 0: Leapfrog_slow{}(kernel, tau, n); return true;
+    case 1: Leapfrog{}(kernel, tau, n); return true;
+    case 2: OMF_2_slow{}(kernel, tau, n); return true;
+    case 3: OMF_2{}(kernel, tau, n); return true;
+    case 4: OMF_4_slow{}(kernel, tau, n); return true;
+    case 5: OMF_4{}(kernel, tau, n); return true;
+    default: return false;
+    }
 }
 } // namespace
 
@@ -554,6 +589,62 @@ int ref_load_bmw(const char* path, int full, double* links_out)
     const bool ok = full ? LoadConfigBMWFull(*U, path) : LoadConfigBMW(*U, path);
     store(*U, links_out);
     return ok ? 1 : 0;
+}
+
+// Deterministic molecular dynamics with any of the reference's integrators from given links
+// and momenta: HMCKernel (metad = 0; ids 0-7, the friction variants 6 and 7 included) or
+// HMCMetaDKernel under the linear bias slope * Q (metad = 1; ids 0-5 and the
+// multiple-timescale ids 8-10).  Returns 0 for a combination the reference does not offer.
+int ref_md_integrate(double* links, double* momenta, double b, double tau, int n_step, int id, int metad, double rho,
+                     double slope, double* h_old, double* h_new)
+{
+    set_beta(b);
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    load(*P, momenta);
+    RunStatistics stats;
+    Integrators::HMC::OMF_2 omf2;
+    bool ok = true;
+    if (!metad)
+    {
+        GaugeUpdates::HMCKernel hmc(*U, *Uc, *P, omf2, GaugeAction::WilsonAction, prng(), stats, std::cout, tau);
+        *h_old = hmc.Hamiltonian();
+        if (id == 6) Integrators::HMC::Leapfrog_friction_slow{}(hmc, tau, n_step);
+        else if (id == 7) Integrators::HMC::OMF_4_friction_slow{}(hmc, tau, n_step);
+        else ok = run_integrator(id, hmc, tau, n_step);
+        *h_new = hmc.Hamiltonian();
+    }
+    else
+    {
+        auto bias = linear_bias(slope);
+        auto data = std::make_unique<GaugeUpdates::HMCMetaDData>(n_smear_meta);
+        std::string log_path {"/dev/null"};
+        GaugeUpdates::HMCMetaDKernel kern(*U, *Uc, *P, *bias, *data, omf2, GaugeAction::WilsonAction, prng(), stats,
+                                          std::cout, log_path, tau, rho);
+        kern.cv_path_samples.clear();
+        *h_old = kern.Hamiltonian() + bias->ReturnPotential(kern.MetaCharge());
+        RefreshedMetaD<decltype(kern)> hooks {kern};
+        if (id == 8) Integrators::HMC::Leapfrog_OMF_4{}(hooks, tau, n_step);
+        else if (id == 9) Integrators::HMC::OMF_2_OMF_4_slow{}(hooks, tau, n_step);
+        else if (id == 10) Integrators::HMC::OMF_2_OMF_4{}(hooks, tau, n_step);
+        else ok = run_integrator(id, kern, tau, n_step);
+        *h_new = kern.Hamiltonian() + bias->ReturnPotential(kern.MetaCharge());
+    }
+    store(*U, links);
+    store(*P, momenta);
+    return ok ? 1 : 0;
+}
+
+// ParityUpdate (parity_update.hpp:22-47) in place
+void ref_parity_update(double* links)
+{
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    load(*U, links);
+    ParityUpdate(*U, *Uc);
+    store(*U, links);
 }
 
 // SU3::exp (su3_exp.hpp:419-425) of n traceless Hermitian matrices (18 doubles each)

@@ -56,5 +56,16 @@ def golden_measure(oracle):
 
 
 @pytest.fixture(scope="session")
+def golden_md(oracle):
+    """Reference MD integrators and parity update; "U" and "P" are the regenerated inputs."""
+    from ltref import haar_links_numpy
+    d = dict(np.load(os.path.join(GOLDEN, "ref_md.npz")))
+    ext = tuple(int(e) for e in d["ext"])
+    d["U"] = oracle.heatbath(ext, haar_links_numpy(ext, 2), 6.0, 5, 17, 0)
+    d["P"] = oracle.random_momenta(ext, 9, 0)
+    return d
+
+
+@pytest.fixture(scope="session")
 def golden_chain():
     return dict(np.load(os.path.join(GOLDEN, "ref_chain_8x8x8x8.npz")))

@@ -52,10 +52,19 @@ int main(int argc, char** argv)
                     EnergyDensityClover(Gluonsmeared1));
     }
 
+    // the reference driver's HMC integrator, OMF_4 (SU3_main.cpp:331), then a parity update (:527-531)
+    Integrators::HMC::OMF_4 omf4;
+    RunStatistics hmc_statistics;
+    GaugeUpdates::HMCKernel HMC(Gluon, omf4, SimulatedAction, hmc_statistics, 1.0, 5);
+    HMC(10, false);
+    const double q_before = TopChargeClover(Gluon);
+    ParityUpdate(Gluon, Gluonsmeared1);
+    std::printf("parity dH %.10f Q %.12f %.12f\n", hmc_statistics.delta_H_hmc, q_before, TopChargeClover(Gluon));
+
     MetaBiasPotential TopBiasPotential(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0);
     RunStatistics statistics;
-    Integrators::HMC::OMF_2 omf2;
-    GaugeUpdates::HMCMetaDKernel HMC_MetaD(Gluon, TopBiasPotential, omf2, SimulatedAction, statistics, 1.0, 0.12, 4, 99);
+    Integrators::HMC::OMF_2_OMF_4 omf2_omf4;
+    GaugeUpdates::HMCMetaDKernel HMC_MetaD(Gluon, TopBiasPotential, omf2_omf4, SimulatedAction, statistics, 1.0, 0.12, 4, 99);
     for (int n = 0; n < 3; ++n)
     {
         bool acc = HMC_MetaD(10, true);

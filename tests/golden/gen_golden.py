@@ -201,11 +201,39 @@ def gen_measure() -> dict:
     return out
 
 
+def gen_md() -> dict:
+    """The reference's eleven MD integrators (hmc_gauge.hpp:19-377, hmc_metadynamics.hpp:26-238;
+    ids as LT_MD_*) from the measurement fixture's links and Philox momenta (seed 9, counter
+    0), tau = 0.5 in 3 steps at beta = 6: gauge-only (ids 0-7) and under the linear bias
+    0.7 * Q with n_smear_meta stout steps of rho = 0.12 (ids 0-5, 8-10); and ParityUpdate."""
+    from ltref import Oracle
+    ext = (4, 6, 8, 10)
+    o = Oracle()
+    U = o.heatbath(ext, haar_links_numpy(ext, 2), 6.0, 5, 17, 0)
+    P = o.random_momenta(ext, 9, 0)
+    ref = Reference(ext)
+    links = sample_links(int(np.prod(ext)), 6)[:32]
+    out = {"ext": np.array(ext), "U_ck": checksums(U), "P_ck": checksums(P), "links": links,
+           "n_stout": np.array(ref.lib.ref_n_smear_meta()), "beta": np.array(6.0), "tau": np.array(0.5),
+           "n_step": np.array(3), "rho": np.array(0.12), "slope": np.array(0.7)}
+    cases = [(i, False) for i in range(8)] + [(i, True) for i in (0, 1, 2, 3, 4, 5, 8, 9, 10)]
+    for integ, metad in cases:
+        key = f"{'metad' if metad else 'gauge'}{integ}"
+        U2, P2, ho, hn = ref.md_integrate(U, P, 6.0, 0.5, 3, integ, metad, 0.12, 0.7)
+        out[key + "_U"], out[key + "_P"] = take(U2, links), take(P2, links)
+        out[key + "_ck"] = np.concatenate([checksums(U2), checksums(P2)])
+        out[key + "_h"] = np.array([ho, hn])
+    R = ref.parity_update(U)
+    out["parity_U"], out["parity_ck"] = take(R, links), checksums(R)
+    return out
+
+
 def main() -> int:
     import argparse
     import subprocess
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["chain", "bmw", "measure"], default=None, help="regenerate one fixture only")
+    ap.add_argument("--only", choices=["chain", "bmw", "measure", "md"], default=None,
+                    help="regenerate one fixture only")
     a = ap.parse_args()
     root = os.path.dirname(os.path.dirname(HERE))
     subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "4x4x4x4",
@@ -215,6 +243,9 @@ def main() -> int:
         return 0
     if a.only == "measure":
         np.savez_compressed(os.path.join(HERE, "ref_measure.npz"), **gen_measure())
+        return 0
+    if a.only == "md":
+        np.savez_compressed(os.path.join(HERE, "ref_md.npz"), **gen_md())
         return 0
     if a.only == "bmw":
         np.savez_compressed(os.path.join(HERE, "ref_bmw.npz"), **gen_bmw())
@@ -229,6 +260,7 @@ def main() -> int:
     np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
     np.savez_compressed(os.path.join(HERE, "ref_bmw.npz"), **gen_bmw())
     np.savez_compressed(os.path.join(HERE, "ref_measure.npz"), **gen_measure())
+    np.savez_compressed(os.path.join(HERE, "ref_md.npz"), **gen_md())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

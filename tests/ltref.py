@@ -69,6 +69,8 @@ class Oracle:
             "or_wilson_loop": (d, [_ip, _dp, i]),
             "or_polyakov_loop": (None, [_ip, _dp, C.POINTER(d), C.POINTER(d)]),
             "or_bmw_decode": (u64, [_ip, C.c_void_p, i, _dp]),
+            "or_md_integrate": (None, [_ip, _dp, _dp, d, d, i, i, i, d, i, d, C.POINTER(d), C.POINTER(d)]),
+            "or_parity_update": (None, [_ip, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -146,6 +148,20 @@ class Oracle:
         ho, hn = C.c_double(), C.c_double()
         self.lib.or_omf2(self._e(ext), U2, P2, beta, tau, n, C.byref(ho), C.byref(hn))
         return U2, P2, ho.value, hn.value
+
+    def md_integrate(self, ext, U, P, beta, tau, n, integrator, metad=False, rho=0.12, n_stout=0, slope=0.0):
+        """(U, P, H_old, H_new) after n steps of integrator (ids as LT_MD_*); MetaD with the
+        linear bias slope * Q."""
+        U2, P2 = np.ascontiguousarray(U).copy(), np.ascontiguousarray(P).copy()
+        ho, hn = C.c_double(), C.c_double()
+        self.lib.or_md_integrate(self._e(ext), U2, P2, beta, tau, n, integrator, int(metad), rho, n_stout, slope,
+                                 C.byref(ho), C.byref(hn))
+        return U2, P2, ho.value, hn.value
+
+    def parity_update(self, ext, U):
+        V = np.ascontiguousarray(U).copy()
+        self.lib.or_parity_update(self._e(ext), V)
+        return V
 
     def random_momenta(self, ext, seed, counter):
         V = int(np.prod(ext))
@@ -233,6 +249,8 @@ class Reference:
                 "ref_flow": (None, [_dp, _dp, d, i, i]),
                 "ref_measure": (None, [_dp, d, _dp, _dp, _dp]),
                 "ref_load_bmw": (i, [C.c_char_p, i, _dp]),
+                "ref_md_integrate": (i, [_dp, _dp, d, d, i, i, i, d, d, C.POINTER(d), C.POINTER(d)]),
+                "ref_parity_update": (None, [_dp]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(lib, name)
@@ -314,6 +332,22 @@ class Reference:
         ho, hn = C.c_double(), C.c_double()
         self.lib.ref_metad_omf2(U2, P2, beta, tau, n, rho, slope, C.byref(ho), C.byref(hn))
         return U2, P2, ho.value, hn.value
+
+    def md_integrate(self, U, P, beta, tau, n, integrator, metad=False, rho=0.12, slope=0.0):
+        """The reference's integrator `integrator` (LT_MD_* ids) on HMCKernel or, with metad,
+        HMCMetaDKernel under V(Q) = slope * Q (n_smear_meta stout steps of rho)."""
+        U2, P2 = np.ascontiguousarray(U).copy(), np.ascontiguousarray(P).copy()
+        ho, hn = C.c_double(), C.c_double()
+        ok = self.lib.ref_md_integrate(U2, P2, beta, tau, n, integrator, int(metad), rho, slope, C.byref(ho),
+                                       C.byref(hn))
+        if not ok:
+            raise ValueError("the reference has no such integrator/kernel combination")
+        return U2, P2, ho.value, hn.value
+
+    def parity_update(self, U):
+        V = np.ascontiguousarray(U).copy()
+        self.lib.ref_parity_update(V)
+        return V
 
     def su3_exp(self, Q):
         Q = np.ascontiguousarray(Q, dtype=np.float64)

@@ -41,6 +41,9 @@ def test_dropin_runs_like_python_mirror(tmp_path):
     assert float(lines["plaquette"].split()[1]) == pytest.approx(p, rel=1e-14)
     assert 0.55 < p < 0.65
     assert "metad" in out and "copy" in out
+    par = lines["parity"].split()
+    assert abs(float(par[2])) < 1.0   # OMF_4 at 10 steps conserves H well
+    assert float(par[5]) == pytest.approx(-float(par[4]), rel=1e-10, abs=1e-12)
     # measurement bundle and an Euler flow on the same thermalised field
     b = lines["bundle"].split()
     m = lt.Measure(G, 6.0)

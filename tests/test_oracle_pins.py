@@ -225,3 +225,70 @@ class TestMeasurementBundle:
             assert mine[k] == pytest.approx(ref[k], rel=TOL, abs=1e-14), k
         np.testing.assert_allclose(mine["q_t"], ref["q_t"], rtol=1e-10, atol=1e-14)
         np.testing.assert_allclose(mine["e_t"], ref["e_t"], rtol=TOL)
+
+
+MD_CASES = [(i, False) for i in range(8)] + [(i, True) for i in (0, 1, 2, 3, 4, 5, 8, 9, 10)]
+
+
+class TestMDIntegrators:
+    """The eleven MD integrators of the reference (hmc_gauge.hpp:19-377,
+    hmc_metadynamics.hpp:26-238) on HMCKernel and HMCMetaDKernel, and ParityUpdate
+    (parity_update.hpp:22-47), against the reference."""
+
+    @pytest.mark.parametrize("integ,metad", MD_CASES)
+    def test_against_fixture(self, oracle, golden_md, integ, metad):
+        g = golden_md
+        ext = tuple(int(e) for e in g["ext"])
+        assert close_ck(checksums(g["U"]), g["U_ck"], 1e-12) and close_ck(checksums(g["P"]), g["P_ck"], 1e-12)
+        U, P, ho, hn = oracle.md_integrate(ext, g["U"], g["P"], float(g["beta"]), float(g["tau"]), int(g["n_step"]),
+                                           integ, metad, float(g["rho"]), int(g["n_stout"]), float(g["slope"]))
+        key = f"{'metad' if metad else 'gauge'}{integ}"
+        assert rel_err(links_of(U, g["links"]), g[key + "_U"]) < 1e-12
+        assert rel_err(links_of(P, g["links"]), g[key + "_P"]) < 1e-12
+        assert close_ck(np.concatenate([checksums(U), checksums(P)]), g[key + "_ck"], 1e-11)
+        assert ho == pytest.approx(g[key + "_h"][0], rel=1e-13)
+        assert hn == pytest.approx(g[key + "_h"][1], rel=1e-13)
+
+    def test_parity_fixture(self, oracle, golden_md):
+        g = golden_md
+        ext = tuple(int(e) for e in g["ext"])
+        R = oracle.parity_update(ext, g["U"])
+        assert np.array_equal(links_of(R, g["links"]), g["parity_U"])
+        assert close_ck(checksums(R), g["parity_ck"], 0.0)
+        # action unchanged, clover charge flips sign
+        assert oracle.wilson_action(ext, R, 6.0) == pytest.approx(oracle.wilson_action(ext, g["U"], 6.0), rel=1e-14)
+        assert oracle.topcharge(ext, R) == pytest.approx(-oracle.topcharge(ext, g["U"]), rel=1e-10, abs=1e-13)
+
+    def test_orders(self, oracle):
+        """dH falls as eps^2 (OMF2, Leapfrog-OMF4, OMF2-OMF4) and eps^4 (OMF4); the reference's
+        OMF_2_OMF_4_slow runs its inner OMF4 at full steps, so the gauge part advances 2 tau and
+        dH does not fall."""
+        ext = (4, 4, 4, 4)
+        U = oracle.heatbath(ext, haar_links_numpy(ext, 2), 6.0, 5, 17, 0)
+        P = oracle.random_momenta(ext, 9, 0)
+
+        def ratio(integ, n, metad):
+            d = []
+            for k in (n, 2 * n):
+                _, _, ho, hn = oracle.md_integrate(ext, U, P, 6.0, 0.5, k, integ, metad, 0.12, 1, 0.7)
+                d.append(abs(hn - ho))
+            return d[0] / d[1]
+
+        assert 3.0 < ratio(3, 8, False) < 5.0
+        assert 12.0 < ratio(5, 4, False) < 24.0
+        assert 3.0 < ratio(8, 4, True) < 6.0
+        assert 3.0 < ratio(10, 4, True) < 6.0
+        assert ratio(9, 4, True) < 1.2
+
+    @pytest.mark.skipif(not ref_available((4, 6, 8, 10)), reason="reference harness not built")
+    def test_live_reference(self, oracle):
+        ext = (4, 6, 8, 10)
+        U = oracle.heatbath(ext, haar_links_numpy(ext, 9), 5.9, 3, 4, 0)
+        P = oracle.random_momenta(ext, 3, 1)
+        ref = Reference(ext)
+        for integ, metad in ((7, False), (5, True), (10, True)):
+            a = oracle.md_integrate(ext, U, P, 5.9, 0.4, 2, integ, metad, 0.1, int(ref.lib.ref_n_smear_meta()), -1.3)
+            b = ref.md_integrate(U, P, 5.9, 0.4, 2, integ, metad, 0.1, -1.3)
+            assert rel_err(a[0], b[0]) < 1e-12 and rel_err(a[1], b[1]) < 1e-12
+            assert a[3] == pytest.approx(b[3], rel=1e-13)
+        assert np.array_equal(oracle.parity_update(ext, U), ref.parity_update(U))
