@@ -159,6 +159,19 @@ int lt_staples(lt_lattice* h, double* staples_out);
  * any stream capture).  All calls share the array: calls that overlap on the GPU race. */
 int lt_plaquette_sum_noalloc(const double* links_dev, const int ext[4], double* out_dev, void* stream);
 
+/* ---- gauge action: GaugeAction::Rectangular (actions/gauge/rectangular_action.hpp) ------ */
+/* The handle's simulated action, used by lt_staples, the sweeps, the HMC force and
+ * Hamiltonian (lt_gauge_force, lt_hamiltonian, lt_omf2, lt_md_*, lt_hmc_trajectory and the
+ * MetaD variants) and the gradient flow (lt_flow*, lt_flow_t0).  stencil_radius 1:
+ * Rectangular<1>, whose staple is the plaquette staple and whose action is
+ * beta c_plaq (6V - sum ReTr P / 3) (the default, (1, 1.0, 0.0), is WilsonAction);
+ * 2: Rectangular<2>, staple c_plaq StaplePlaq + c_rect StapleRect (:187-246), action
+ * beta (c_plaq (6V - ReTr P/3) + c_rect (12V - ReTr R/3)).  The reference's named
+ * actions: LuescherWeisz (2, 1 + 8/12, -1/12), Iwasaki (2, 1 + 8 * 0.331, -0.331), DBW2
+ * (2, 1 + 8 * 1.4088, -1.4088) (:273-276).  Radius 2 needs the Checkerboard4 sweeps. */
+int lt_set_gauge_action(lt_lattice* h, int stencil_radius, double c_plaq, double c_rect);
+int lt_get_gauge_action(lt_lattice* h, int* stencil_radius, double* c_plaq, double* c_rect);
+
 /* ---- local updates: Iterator::Checkerboard (iterators/iterators.hpp:65-87) ------------- */
 /* n_sweep sweeps of OverrelaxationSubgroupKernel (updates/overrelaxation.hpp:68-117). */
 int lt_overrelax_sweeps(lt_lattice* h, int n_sweep);
@@ -170,6 +183,18 @@ int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, u
  * loop (SU3_main.cpp:381-402); 8 chained launches per sweep on the handle's stream. */
 int lt_update_sweeps(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed,
                      uint64_t* counter);
+/* The Wilson-action sweeps above refuse a radius-2 action (LT_ERR_ARG): the rectangle staple
+ * reaches links that a two-colour checkerboard updates together. */
+
+/* ---- local updates: Iterator::Checkerboard4 (iterators/iterators.hpp:141-166) ----------- */
+/* The same sweeps over Checkerboard4: per direction mu four sublattices
+ * (t + x + y + z + x_mu) mod 4 = 0..3, one launch each (16 per sweep), with the handle's
+ * action; every extent a multiple of 4 (else LT_ERR_ARG, where the reference exits).  The
+ * reference driver runs these with every action (SU3_main.cpp:361-362, :594-595). */
+int lt_overrelax_sweeps4(lt_lattice* h, int n_sweep);
+int lt_heatbath_sweeps4(lt_lattice* h, double beta, int n_sweep, uint64_t seed, uint64_t* counter);
+int lt_update_sweeps4(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed,
+                      uint64_t* counter);
 
 /* ---- ensembles: independent chains and tempering streams ------------------------------ */
 typedef struct lt_ensemble lt_ensemble;

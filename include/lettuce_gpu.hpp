@@ -119,43 +119,63 @@ inline double EnergyDensityClover(const GaugeField& U)
 
 namespace GaugeAction
 {
-// Rectangular<1> with (c_plaq, c_rect) = (1, 0) (actions/gauge/rectangular_action.hpp:23-294)
-struct Wilson
-{
-    double beta = 6.0;
-    void SetBeta(double b) { beta = b; }
-    double GetBeta() const { return beta; }
-    double Action(const GaugeField& U) const
-    {
-        double v;
-        check(lt_wilson_action(U.handle(), beta, &v));
-        return v;
-    }
-    double ActionNormalized(const GaugeField& U) const { return Action(U) / (6.0 * beta * (double)U.Volume()); }
-};
-inline Wilson WilsonAction;
-
-// Rectangular<2> (actions/gauge/rectangular_action.hpp:23-94): plaquettes weighted by c_plaq
-// and 1x2 plus 2x1 rectangles by c_rect; the tree-level Symanzik choice is (5/3, -1/12).
+// Rectangular<stencil_radius> (actions/gauge/rectangular_action.hpp:23-246): radius 1 is the
+// plaquette action (its staple is the plaquette staple whatever c_plaq), radius 2 adds the
+// 1x2 and 2x1 rectangles with weight c_rect.  Apply() makes it the action of a field's
+// device staples, sweeps, HMC force and Hamiltonian, and flow.
 template <int stencil_radius_>
 struct Rectangular
 {
     static_assert(stencil_radius_ > 0 && stencil_radius_ <= 2, "Invalid stencil_radius!");
+    static constexpr int stencil_radius = stencil_radius_;
     double beta = 6.0;
     const double c_plaq = 1.0;
     const double c_rect = 0.0;
     Rectangular(double beta_in, double c_plaq_in, double c_rect_in) : beta(beta_in), c_plaq(c_plaq_in), c_rect(c_rect_in) {}
+    Rectangular() = default;
     void SetBeta(double b) { beta = b; }
     double GetBeta() const { return beta; }
     double Action(const GaugeField& U) const
     {
         double v;
-        check(lt_rect_action(U.handle(), beta, c_plaq, c_rect, &v));
-        return v;
+        if constexpr (stencil_radius == 1)
+        {
+            check(lt_wilson_action(U.handle(), beta, &v));
+            return c_plaq * v;
+        }
+        else
+        {
+            check(lt_rect_action(U.handle(), beta, c_plaq, c_rect, &v));
+            return v;
+        }
     }
     double ActionNormalized(const GaugeField& U) const { return Action(U) / (6.0 * beta * (double)U.Volume()); }
+    void Apply(const GaugeField& U) const { check(lt_set_gauge_action(U.handle(), stencil_radius, c_plaq, c_rect)); }
 };
+using Wilson = Rectangular<1>;
+
+// The named actions of rectangular_action.hpp:273-276 (c_plaq = 1 - 8 c_rect)
+inline Rectangular<1> WilsonAction(6.0, 1.0, 0.0);
+inline Rectangular<2> LüscherWeiszAction(6.0, 1.0 + 8.0 * 1.0 / 12.0, -1.0 / 12.0);
+inline Rectangular<2>& LuescherWeiszAction = LüscherWeiszAction;
+inline Rectangular<2> IwasakiAction(6.0, 1.0 + 8.0 * 0.331, -0.331);
+inline Rectangular<2> DBW2Action(6.0, 1.0 + 8.0 * 1.4088, -1.4088);
 } // namespace GaugeAction
+
+// The action a kernel runs with: its device form and a view of its coupling, which the kernels
+// read at each call as the reference's kernels read their action
+struct ActionRef
+{
+    int radius;
+    double c_plaq, c_rect;
+    const double* beta;
+    template <int R>
+    ActionRef(const GaugeAction::Rectangular<R>& a) : radius(R), c_plaq(a.c_plaq), c_rect(a.c_rect), beta(&a.beta)
+    {
+    }
+    void Apply(const GaugeField& U) const { check(lt_set_gauge_action(U.handle(), radius, c_plaq, c_rect)); }
+    double GetBeta() const { return *beta; }
+};
 
 // TopChargeCloverTimeslice (observables/topological_charge.hpp:233-364) and
 // EnergyDensity::CloverTimeslice (observables/field_strength_tensor.hpp:178-195): one launch
@@ -216,11 +236,11 @@ inline std::complex<double> PolyakovLoop(const GaugeField& U)
 struct HeatbathKernel
 {
     GaugeField& U;
+    ActionRef action;
     double beta;
     std::uint64_t seed, counter;
-    HeatbathKernel(GaugeField& U_in, const GaugeAction::Wilson& action, std::uint64_t seed_in = 1,
-                   std::uint64_t counter_in = 0)
-        : U(U_in), beta(action.GetBeta()), seed(seed_in), counter(counter_in)
+    HeatbathKernel(GaugeField& U_in, ActionRef action_in, std::uint64_t seed_in = 1, std::uint64_t counter_in = 0)
+        : U(U_in), action(action_in), beta(action_in.GetBeta()), seed(seed_in), counter(counter_in)
     {
     }
     bool SaveState(const std::filesystem::path& state, const std::filesystem::path& normal, bool overwrite = false) const
@@ -247,24 +267,36 @@ struct HeatbathKernel
 struct OverrelaxationSubgroupKernel
 {
     GaugeField& U;
-    OverrelaxationSubgroupKernel(GaugeField& U_in, const GaugeAction::Wilson&) : U(U_in) {}
+    ActionRef action;
+    OverrelaxationSubgroupKernel(GaugeField& U_in, ActionRef action_in) : U(U_in), action(action_in) {}
 };
 
 namespace Iterator
 {
-// Iterator::Checkerboard (iterators/iterators.hpp:65-87): whole sweeps per call
+// Iterator::Checkerboard (iterators/iterators.hpp:65-87): whole sweeps per call; a radius-2
+// action throws (its rectangle staples reach links of the same colour)
 inline void Checkerboard(HeatbathKernel& k, int n_sweep = 1)
 {
+    k.action.Apply(k.U);
     check(lt_heatbath_sweeps(k.U.handle(), k.beta, n_sweep, k.seed, &k.counter));
 }
 inline void Checkerboard(OverrelaxationSubgroupKernel& k, int n_sweep = 1)
 {
+    k.action.Apply(k.U);
     check(lt_overrelax_sweeps(k.U.handle(), n_sweep));
 }
-// The 4-sublattice variant (:141-169) visits the same links; on the device both are the
-// same even/odd launch sequence.
-inline void Checkerboard4(HeatbathKernel& k, int n_sweep = 1) { Checkerboard(k, n_sweep); }
-inline void Checkerboard4(OverrelaxationSubgroupKernel& k, int n_sweep = 1) { Checkerboard(k, n_sweep); }
+// Iterator::Checkerboard4 (:141-166): four sublattices per direction, any action; every
+// extent a multiple of 4
+inline void Checkerboard4(HeatbathKernel& k, int n_sweep = 1)
+{
+    k.action.Apply(k.U);
+    check(lt_heatbath_sweeps4(k.U.handle(), k.beta, n_sweep, k.seed, &k.counter));
+}
+inline void Checkerboard4(OverrelaxationSubgroupKernel& k, int n_sweep = 1)
+{
+    k.action.Apply(k.U);
+    check(lt_overrelax_sweeps4(k.U.handle(), n_sweep));
+}
 } // namespace Iterator
 
 namespace Integrators::GradientFlow
@@ -292,18 +324,27 @@ struct RK3W7   // smearing/gradient_flow.hpp:170-218
 } // namespace Integrators::GradientFlow
 
 // GradientFlowKernel (smearing/gradient_flow.hpp:252-367) with any of the integrators above
-template <typename IntegratorT = Integrators::GradientFlow::RK3, typename ActionT = GaugeAction::Wilson>
+template <typename IntegratorT = Integrators::GradientFlow::RK3, typename ActionT = GaugeAction::Rectangular<1>>
 struct GradientFlowKernel
 {
     const GaugeField& U_unflowed;
     GaugeField& U_flowed;
+    ActionRef action;
     double epsilon;
-    GradientFlowKernel(const GaugeField& in, GaugeField& out, IntegratorT&, ActionT&, double eps)
-        : U_unflowed(in), U_flowed(out), epsilon(eps)
+    GradientFlowKernel(const GaugeField& in, GaugeField& out, IntegratorT&, ActionT& act, double eps)
+        : U_unflowed(in), U_flowed(out), action(act), epsilon(eps)
     {
     }
-    void operator()(int n_step) const { check(lt_flow(U_unflowed.handle(), U_flowed.handle(), IntegratorT::ID, epsilon, n_step)); }
-    void Resume(int n_step) const { check(lt_flow(U_flowed.handle(), U_flowed.handle(), IntegratorT::ID, epsilon, n_step)); }
+    void operator()(int n_step) const
+    {
+        action.Apply(U_flowed);
+        check(lt_flow(U_unflowed.handle(), U_flowed.handle(), IntegratorT::ID, epsilon, n_step));
+    }
+    void Resume(int n_step) const
+    {
+        action.Apply(U_flowed);
+        check(lt_flow(U_flowed.handle(), U_flowed.handle(), IntegratorT::ID, epsilon, n_step));
+    }
     void SetEpsilon(double e) { epsilon = e; }
     double GetEpsilon() const { return epsilon; }
     std::string ReturnIntegratorName() const { return IntegratorT::ReturnName(); }
@@ -515,11 +556,11 @@ struct HMCKernel
 {
     static_assert(IntegratorT::gauge_kernel, "this integrator needs the Metadynamics kernel");
     GaugeField& U;
-    GaugeAction::Wilson& Action;
+    ActionRef Action;
     RunStatistics& statistics;
     double trajectory_length;
     std::uint64_t seed, counter;
-    HMCKernel(GaugeField& U_in, IntegratorT&, GaugeAction::Wilson& action, RunStatistics& stats, double tau = 1.0,
+    HMCKernel(GaugeField& U_in, IntegratorT&, ActionRef action, RunStatistics& stats, double tau = 1.0,
               std::uint64_t seed_in = 1, std::uint64_t counter_in = 0)
         : U(U_in), Action(action), statistics(stats), trajectory_length(tau), seed(seed_in), counter(counter_in)
     {
@@ -528,6 +569,7 @@ struct HMCKernel
     {
         double dH;
         int acc;
+        Action.Apply(U);
         check(lt_md_trajectory(U.handle(), nullptr, IntegratorT::ID, Action.GetBeta(), trajectory_length, n_step, 0.0,
                                0, seed, &counter, metropolis_step ? 1 : 0, &dH, &acc, nullptr));
         statistics.delta_H_hmc = dH;
@@ -538,6 +580,7 @@ struct HMCKernel
     double ReversibilityTest(int n_step)
     {
         double ho, hn;
+        Action.Apply(U);
         check(lt_random_momenta(U.handle(), seed, counter));
         check(lt_md_integrate(U.handle(), nullptr, IntegratorT::ID, Action.GetBeta(), trajectory_length, n_step, 0.0, 0,
                               &ho, nullptr));
@@ -555,13 +598,13 @@ struct HMCMetaDKernel
     static_assert(IntegratorT::metad_kernel, "this integrator needs the gauge-only kernel");
     GaugeField& U;
     MetaBiasPotential& Metapotential;
-    GaugeAction::Wilson& Action;
+    ActionRef Action;
     RunStatistics& statistics;
     double trajectory_length, rho_stout_cv;
     int n_smear_meta;
     std::uint64_t seed, counter;
     double cv_current = 0.0;
-    HMCMetaDKernel(GaugeField& U_in, MetaBiasPotential& bias, IntegratorT&, GaugeAction::Wilson& action,
+    HMCMetaDKernel(GaugeField& U_in, MetaBiasPotential& bias, IntegratorT&, ActionRef action,
                    RunStatistics& stats, double tau, double rho, int n_smear = 4, std::uint64_t seed_in = 1,
                    std::uint64_t counter_in = 0)
         : U(U_in), Metapotential(bias), Action(action), statistics(stats), trajectory_length(tau), rho_stout_cv(rho),
@@ -572,6 +615,7 @@ struct HMCMetaDKernel
     {
         double dH, cv;
         int acc;
+        Action.Apply(U);
         check(lt_md_trajectory(U.handle(), Metapotential.handle(), IntegratorT::ID, Action.GetBeta(), trajectory_length,
                                n_step, rho_stout_cv, n_smear_meta, seed, &counter, metropolis_step ? 1 : 0, &dH, &acc,
                                &cv));
@@ -589,6 +633,7 @@ struct HMCMetaDKernel
     double ReversibilityTest(int n_step)
     {
         double ho, hn;
+        Action.Apply(U);
         check(lt_random_momenta(U.handle(), seed, counter));
         check(lt_md_integrate(U.handle(), Metapotential.handle(), IntegratorT::ID, Action.GetBeta(), trajectory_length,
                               n_step, rho_stout_cv, n_smear_meta, &ho, nullptr));

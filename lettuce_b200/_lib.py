@@ -57,6 +57,11 @@ SIGNATURES = {
     "lt_overrelax_sweeps": (_i, [_vp, _i]),
     "lt_heatbath_sweeps": (_i, [_vp, _d, _i, _u64, _pu64]),
     "lt_update_sweeps": (_i, [_vp, _d, _i, _i, _i, _u64, _pu64]),
+    "lt_overrelax_sweeps4": (_i, [_vp, _i]),
+    "lt_heatbath_sweeps4": (_i, [_vp, _d, _i, _u64, _pu64]),
+    "lt_update_sweeps4": (_i, [_vp, _d, _i, _i, _i, _u64, _pu64]),
+    "lt_set_gauge_action": (_i, [_vp, _i, _d, _d]),
+    "lt_get_gauge_action": (_i, [_vp, _pi, _pd, _pd]),
     "lt_ensemble_create": (_i, [_vp, _dp, _i, _u64, C.POINTER(_vp)]),
     "lt_ensemble_destroy": (_i, [_vp]),
     "lt_ensemble_sweeps": (_i, [_vp, _i, _i, _i, _i, _pu64]),

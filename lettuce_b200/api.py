@@ -172,17 +172,34 @@ def CloverObservables(U: GaugeField) -> tuple[float, float]:
 
 def Staples(U: GaugeField) -> np.ndarray:
     """WilsonAction::Staple for every link (actions/gauge/rectangular_action.hpp:104-184)."""
-    out = np.empty((U.Volume(), 4, 3, 3, 2))
-    check(lib().lt_staples(U.handle, out.reshape(-1)))
-    return out
+    return WilsonAction().Staple(U)
+
+
+def _set_action(U: GaugeField, action) -> None:
+    """Make `action` (None: the Wilson action) the gauge action of U's device staples, sweeps,
+    HMC force and Hamiltonian, and flow."""
+    if action is None:
+        check(lib().lt_set_gauge_action(U.handle, 1, 1.0, 0.0))
+    else:
+        check(lib().lt_set_gauge_action(U.handle, int(action.stencil_radius), float(action.c_plaq),
+                                        float(action.c_rect)))
 
 
 class WilsonAction:
     """GaugeAction::Rectangular<1> with (c_plaq, c_rect) = (1, 0)
     (actions/gauge/rectangular_action.hpp:23-294)."""
 
+    stencil_radius, c_plaq, c_rect = 1, 1.0, 0.0
+
     def __init__(self, beta: float = 6.0):
         self.beta = float(beta)
+
+    def Staple(self, U: GaugeField) -> np.ndarray:
+        """Rectangular<1>::Staple for every link (rectangular_action.hpp:104-184), reference layout."""
+        _set_action(U, self)
+        out = np.empty((U.Volume(), 4, 3, 3, 2))
+        check(lib().lt_staples(U.handle, out.reshape(-1)))
+        return out
 
     def SetBeta(self, beta: float) -> None:
         self.beta = float(beta)
@@ -198,6 +215,7 @@ class WilsonAction:
 
     def Force(self, U: GaugeField) -> np.ndarray:
         """beta/6 Algebra(st U^dag) per link (updates/hmc_gauge.hpp:450-464)."""
+        _set_action(U, self)
         out = np.empty((U.Volume(), 4, 3, 3, 2))
         check(lib().lt_gauge_force(U.handle, self.beta, out.reshape(-1)))
         return out
@@ -208,39 +226,66 @@ class HeatbathKernel:
     reference's cached prefactor 3/beta (:40); random numbers come from Philox streams keyed
     by `seed`, one counter value per sweep."""
 
-    def __init__(self, U: GaugeField, action: WilsonAction, seed: int = 1, counter: int = 0):
-        self.U, self.beta, self.seed = U, action.GetBeta(), int(seed)
+    def __init__(self, U: GaugeField, action=None, seed: int = 1, counter: int = 0):
+        self.action = action if action is not None else WilsonAction()
+        self.U, self.beta, self.seed = U, self.action.GetBeta(), int(seed)
         self.counter = C.c_uint64(counter)
 
     def sweeps(self, n: int) -> None:
+        _set_action(self.U, self.action)
         check(lib().lt_heatbath_sweeps(self.U.handle, self.beta, int(n), C.c_uint64(self.seed), C.byref(self.counter)))
+
+    def sweeps4(self, n: int) -> None:
+        _set_action(self.U, self.action)
+        check(lib().lt_heatbath_sweeps4(self.U.handle, self.beta, int(n), C.c_uint64(self.seed), C.byref(self.counter)))
 
 
 class OverrelaxationSubgroupKernel:
     """OverrelaxationSubgroupKernel (updates/overrelaxation.hpp:68-117)."""
 
-    def __init__(self, U: GaugeField, action: WilsonAction | None = None):
-        self.U = U
+    def __init__(self, U: GaugeField, action=None):
+        self.U, self.action = U, action
 
     def sweeps(self, n: int) -> None:
+        _set_action(self.U, self.action)
         check(lib().lt_overrelax_sweeps(self.U.handle, int(n)))
+
+    def sweeps4(self, n: int) -> None:
+        _set_action(self.U, self.action)
+        check(lib().lt_overrelax_sweeps4(self.U.handle, int(n)))
 
 
 class Iterator:
-    """Iterator::Checkerboard (iterators/iterators.hpp:65-87): a whole sweep (all mu and both
-    parities) is one call; a per-link functor cannot cross to the device."""
+    """Iterator::Checkerboard (iterators/iterators.hpp:65-87) and Checkerboard4 (:141-166): a
+    whole sweep is one call; a per-link functor cannot cross to the device.  Checkerboard
+    refuses radius-2 actions; Checkerboard4 needs every extent a multiple of 4."""
 
     @staticmethod
     def Checkerboard(kernel, n_sweep: int = 1) -> None:
         kernel.sweeps(n_sweep)
 
-    Checkerboard4 = Checkerboard
+    @staticmethod
+    def Checkerboard4(kernel, n_sweep: int = 1) -> None:
+        kernel.sweeps4(n_sweep)
 
 
 def UpdateSweeps(U: GaugeField, beta: float, n_sweep: int, n_hb: int, n_or: int, seed: int, counter: int = 0) -> int:
-    """n_sweep rounds of (n_hb heatbath + n_or overrelaxation); returns the next counter."""
+    """n_sweep rounds of (n_hb heatbath + n_or overrelaxation) with the Wilson action over
+    Iterator::Checkerboard; returns the next counter."""
+    _set_action(U, None)
     c = C.c_uint64(counter)
     check(lib().lt_update_sweeps(U.handle, float(beta), int(n_sweep), int(n_hb), int(n_or), C.c_uint64(seed), C.byref(c)))
+    return c.value
+
+
+def UpdateSweeps4(U: GaugeField, beta: float, n_sweep: int, n_hb: int, n_or: int, seed: int, counter: int = 0,
+                  action=None) -> int:
+    """The same rounds over Iterator::Checkerboard4 with any action (the reference driver's
+    update loop, SU3_main.cpp:361-362); returns the next counter."""
+    _set_action(U, action)
+    c = C.c_uint64(counter)
+    check(lib().lt_update_sweeps4(U.handle, float(beta), int(n_sweep), int(n_hb), int(n_or), C.c_uint64(seed),
+                                  C.byref(c)))
     return c.value
 
 
@@ -286,10 +331,11 @@ class GradientFlowKernel:
     def __init__(self, U_unflowed: GaugeField, U_flowed: GaugeField, integrator=RK3, action=None, epsilon: float = 0.01):
         if integrator not in (Euler, RK2, RK3, RK3W7):
             raise ValueError("integrator must be Euler, RK2, RK3 or RK3W7")
-        self.integrator = integrator
+        self.integrator, self.action = integrator, action
         self.U_unflowed, self.U_flowed, self.epsilon = U_unflowed, U_flowed, float(epsilon)
 
     def _run(self, src: GaugeField, n_step: int) -> None:
+        _set_action(self.U_flowed, self.action)
         if self.integrator is RK3:
             check(lib().lt_flow_rk3(src.handle, self.U_flowed.handle, self.epsilon, int(n_step)))
         else:
@@ -307,6 +353,7 @@ class GradientFlowKernel:
     def Measure(self, n_meas: int, every: int):
         """Flow from U_unflowed with (plaquette sum, Q, E) after every `every` steps."""
         p, q, e = np.empty(n_meas), np.empty(n_meas), np.empty(n_meas)
+        _set_action(self.U_flowed, self.action)
         check(lib().lt_flow_rk3_measure(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, int(n_meas),
                                         int(every), p.ctypes.data, q.ctypes.data, e.ctypes.data))
         return p, q, e
@@ -314,6 +361,7 @@ class GradientFlowKernel:
     def FlowToT0(self, target: float = 0.3, max_steps: int = 100000) -> tuple[float, float]:
         """Flow U_unflowed into U_flowed until t^2 E = target; returns (t0, Q at the last step)."""
         t0, q = C.c_double(), C.c_double()
+        _set_action(self.U_flowed, self.action)
         check(lib().lt_flow_t0(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, float(target),
                                int(max_steps), C.byref(t0), C.byref(q)))
         return t0.value, q.value
@@ -435,6 +483,7 @@ class HMCKernel:
         if not isinstance(integrator, MDIntegrator) or not integrator.gauge:
             raise ValueError(f"{integrator!r} is not an integrator of HMCKernel")
         self.U, self.beta, self.tau, self.seed = U, action.GetBeta(), float(trajectory_length), int(seed)
+        self.action = action
         self.counter = C.c_uint64(counter)
         self.integrator = integrator
         self.delta_H = 0.0
@@ -448,6 +497,7 @@ class HMCKernel:
     def __call__(self, n_step: int, metropolis_step: bool = True) -> bool:
         dH, acc, cv = C.c_double(), C.c_int(), C.c_double()
         rho, n = self._rho_n()
+        _set_action(self.U, self.action)
         check(lib().lt_md_trajectory(self.U.handle, self._bias(), self.integrator.ID, self.beta, self.tau, int(n_step),
                                      rho, n, C.c_uint64(self.seed), C.byref(self.counter), int(bool(metropolis_step)),
                                      C.byref(dH), C.byref(acc), C.byref(cv)))
@@ -473,6 +523,7 @@ class HMCKernel:
         check(lib().lt_reverse_momenta(self.U.handle))
 
     def Hamiltonian(self) -> float:
+        _set_action(self.U, self.action)
         return _out1(lib().lt_hamiltonian, self.U.handle, self.beta)
 
     def Integrate(self, n_step: int) -> tuple[float, float]:
@@ -480,6 +531,7 @@ class HMCKernel:
         (with + V(CV) under MetaD)."""
         ho, hn = C.c_double(), C.c_double()
         rho, n = self._rho_n()
+        _set_action(self.U, self.action)
         check(lib().lt_md_integrate(self.U.handle, self._bias(), self.integrator.ID, self.beta, self.tau, int(n_step),
                                     rho, n, C.byref(ho), C.byref(hn)))
         return ho.value, hn.value
@@ -604,11 +656,34 @@ def TopChargePlaquette(U: GaugeField) -> float:
 
 
 class RectangularAction:
-    """GaugeAction::Rectangular<2> (actions/gauge/rectangular_action.hpp:23-94) with plaquette
-    and 1x2 coefficients; SymanzikAction(beta) is the driver's tree-level Symanzik choice."""
+    """GaugeAction::Rectangular<2> (actions/gauge/rectangular_action.hpp:23-246) with plaquette
+    and 1x2 coefficients; SymanzikAction(beta) is the driver's tree-level Symanzik choice.
+    As the action of a kernel it selects the rectangle staples (sweeps over Checkerboard4)."""
+
+    stencil_radius = 2
 
     def __init__(self, beta: float, c_plaq: float, c_rect: float):
         self.beta, self.c_plaq, self.c_rect = float(beta), float(c_plaq), float(c_rect)
+
+    def SetBeta(self, beta: float) -> None:
+        self.beta = float(beta)
+
+    def GetBeta(self) -> float:
+        return self.beta
+
+    def Staple(self, U: GaugeField) -> np.ndarray:
+        """c_plaq StaplePlaq + c_rect StapleRect for every link (:187-246), reference layout."""
+        _set_action(U, self)
+        out = np.empty((U.Volume(), 4, 3, 3, 2))
+        check(lib().lt_staples(U.handle, out.reshape(-1)))
+        return out
+
+    def Force(self, U: GaugeField) -> np.ndarray:
+        """beta/6 Algebra(Staple U^dag) per link, the HMC momentum kick (hmc_gauge.hpp:450-464)."""
+        _set_action(U, self)
+        out = np.empty((U.Volume(), 4, 3, 3, 2))
+        check(lib().lt_gauge_force(U.handle, self.beta, out.reshape(-1)))
+        return out
 
     def Action(self, U: GaugeField) -> float:
         return _out1(lib().lt_rect_action, U.handle, self.beta, self.c_plaq, self.c_rect)
@@ -620,6 +695,21 @@ class RectangularAction:
 def SymanzikAction(beta: float) -> RectangularAction:
     """Rectangular<2>(beta, 1 + 8/12, -1/12) as in SU3_main.cpp:115."""
     return RectangularAction(beta, 1.0 + 8.0 / 12.0, -1.0 / 12.0)
+
+
+def LuescherWeiszAction(beta: float = 6.0) -> RectangularAction:
+    """GaugeAction::LüscherWeiszAction (rectangular_action.hpp:273): tree-level Symanzik."""
+    return RectangularAction(beta, 1.0 + 8.0 / 12.0, -1.0 / 12.0)
+
+
+def IwasakiAction(beta: float = 6.0) -> RectangularAction:
+    """GaugeAction::IwasakiAction (rectangular_action.hpp:274)."""
+    return RectangularAction(beta, 1.0 + 8.0 * 0.331, -0.331)
+
+
+def DBW2Action(beta: float = 6.0) -> RectangularAction:
+    """GaugeAction::DBW2Action (rectangular_action.hpp:275)."""
+    return RectangularAction(beta, 1.0 + 8.0 * 1.4088, -1.4088)
 
 
 def WilsonLoop(U: GaugeField, L: int) -> float:
@@ -682,4 +772,5 @@ __all__ = ["STATUS_NONFINITE", "STATUS_UNITARITY", "STATUS_HB_CAP", "GaugeField"
            "TopChargePlaquette", "RectangularAction", "SymanzikAction", "WilsonLoop", "PolyakovLoop", "Measure",
            "Observables", "MDIntegrator", "Integrators", "Leapfrog_slow", "Leapfrog", "OMF_2_slow", "OMF_2",
            "OMF_4_slow", "OMF_4", "Leapfrog_friction_slow", "OMF_4_friction_slow", "Leapfrog_OMF_4",
-           "OMF_2_OMF_4_slow", "OMF_2_OMF_4", "ParityUpdate"]
+           "OMF_2_OMF_4_slow", "OMF_2_OMF_4", "ParityUpdate", "LuescherWeiszAction", "IwasakiAction", "DBW2Action",
+           "UpdateSweeps4"]

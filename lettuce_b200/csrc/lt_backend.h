@@ -18,6 +18,10 @@ struct Ctx
     double* partials;   // kNumSlots * kRedBlocks doubles
     double* results;    // kNumSlots doubles
     unsigned* status = nullptr;   // the handle's device status word (LT_STATUS_* bits)
+    // the handle's gauge action: Rectangular<2> (rect = 1: c_plaq StaplePlaq + c_rect StapleRect)
+    // or Rectangular<1> (rect = 0: the plaquette staple)
+    int rect = 0;
+    double cp = 1.0, cr = 0.0;
 };
 
 constexpr int kNumSlots = 8;
@@ -70,6 +74,10 @@ public:
                             unsigned* flags) const = 0;
 
     virtual void overrelax(const Ctx& c, void* U, int mu, int par) const = 0;
+    // one (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the context's action:
+    // heatbath (op 0, Philox counter/seed as heatbath()) or overrelaxation (op 1)
+    virtual void sweep4(const Ctx& c, void* U, int op, int mu, int sub, double prefactor, uint64_t counter,
+                        uint64_t seed, int max_iter) const = 0;
     virtual void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter,
                           uint64_t seed, int max_iter) const = 0;
     virtual void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new,

@@ -183,14 +183,26 @@ int metad_backward(lt_lattice* h, double rho, int n_stout, double dvdq)
     return launched("metad_backward");
 }
 
+// Action(U) of the handle's gauge action (rectangular_action.hpp:61-94) + (-sum ReTr P^2)
 int hamiltonian(lt_lattice* h, double beta, double* out)
 {
     const lt::Ctx c = h->ctx();
+    const double V = (double)h->g.V;
+    if (h->act_radius == 2)
+    {
+        h->be->loops(c, h->U, 4);
+        h->be->kinetic(c, h->P, 1);
+        double r[3], k;
+        LT_TRY(fetch(h, 4, 3, r));
+        LT_TRY(fetch(h, 1, 1, &k));
+        *out = beta * (h->act_cp * (6.0 * V - r[0] / 3.0) + h->act_cr * (12.0 * V - r[1] / 3.0)) + k;
+        return LT_OK;
+    }
     h->be->plaquette(c, h->U, 0);
     h->be->kinetic(c, h->P, 1);
     double r[2];
     LT_TRY(fetch(h, 0, 2, r));
-    *out = beta * (6.0 * (double)h->g.V - r[0] / 3.0) + r[1];
+    *out = beta * h->act_cp * (6.0 * V - r[0] / 3.0) + r[1];
     return LT_OK;
 }
 
@@ -819,10 +831,32 @@ int lt_staples(lt_lattice* h, double* staples_out)
 }
 
 // ---------------------------------------------------------------- local updates
+int lt_set_gauge_action(lt_lattice* h, int stencil_radius, double c_plaq, double c_rect)
+{
+    LT_TRY(check_h(h, "lt_set_gauge_action"));
+    if ((stencil_radius != 1 && stencil_radius != 2) || !std::isfinite(c_plaq) || !std::isfinite(c_rect))
+        return lt::set_error(LT_ERR_ARG, "lt_set_gauge_action: stencil radius 1 or 2 and finite coefficients");
+    h->act_radius = stencil_radius;
+    h->act_cp = c_plaq;
+    h->act_cr = stencil_radius == 2 ? c_rect : 0.0;
+    return LT_OK;
+}
+
+int lt_get_gauge_action(lt_lattice* h, int* stencil_radius, double* c_plaq, double* c_rect)
+{
+    LT_TRY(check_h(h, "lt_get_gauge_action"));
+    if (stencil_radius) *stencil_radius = h->act_radius;
+    if (c_plaq) *c_plaq = h->act_cp;
+    if (c_rect) *c_rect = h->act_cr;
+    return LT_OK;
+}
+
 int lt_overrelax_sweeps(lt_lattice* h, int n_sweep)
 {
     LT_TRY(check_h(h, "lt_overrelax_sweeps"));
     if (n_sweep < 0) return lt::set_error(LT_ERR_ARG, "lt_overrelax_sweeps: n_sweep < 0");
+    if (h->act_radius == 2)
+        return lt::set_error(LT_ERR_ARG, "lt_overrelax_sweeps: a rectangular action needs Checkerboard4 (lt_overrelax_sweeps4)");
     const lt::Ctx c = h->ctx();
     for (int s = 0; s < n_sweep; ++s)
         for (int mu = 0; mu < 4; ++mu)
@@ -835,6 +869,8 @@ int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, u
     LT_TRY(check_h(h, "lt_heatbath_sweeps"));
     if (n_sweep < 0 || !counter || !(beta > 0.0))
         return lt::set_error(LT_ERR_ARG, "lt_heatbath_sweeps: bad arguments");
+    if (h->act_radius == 2)
+        return lt::set_error(LT_ERR_ARG, "lt_heatbath_sweeps: a rectangular action needs Checkerboard4 (lt_heatbath_sweeps4)");
     const lt::Ctx c = h->ctx();
     for (int s = 0; s < n_sweep; ++s)
     {
@@ -854,6 +890,55 @@ int lt_update_sweeps(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or
     {
         LT_TRY(lt_heatbath_sweeps(h, beta, n_hb, seed, counter));
         LT_TRY(lt_overrelax_sweeps(h, n_or));
+    }
+    return LT_OK;
+}
+
+static int check_cb4(const lt_lattice* h, const char* fn)
+{
+    for (int d = 0; d < 4; ++d)
+        if (h->ext[d] % 4 != 0)
+            return lt::set_error(LT_ERR_ARG, (std::string(fn) + ": Checkerboard4 needs every extent a multiple of 4").c_str());
+    return LT_OK;
+}
+
+int lt_overrelax_sweeps4(lt_lattice* h, int n_sweep)
+{
+    LT_TRY(check_h(h, "lt_overrelax_sweeps4"));
+    if (n_sweep < 0) return lt::set_error(LT_ERR_ARG, "lt_overrelax_sweeps4: n_sweep < 0");
+    LT_TRY(check_cb4(h, "lt_overrelax_sweeps4"));
+    const lt::Ctx c = h->ctx();
+    for (int s = 0; s < n_sweep; ++s)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int sub = 0; sub < 4; ++sub) h->be->sweep4(c, h->U, 1, mu, sub, 0.0, 0, 0, 0);
+    return launched("lt_overrelax_sweeps4");
+}
+
+int lt_heatbath_sweeps4(lt_lattice* h, double beta, int n_sweep, uint64_t seed, uint64_t* counter)
+{
+    LT_TRY(check_h(h, "lt_heatbath_sweeps4"));
+    if (n_sweep < 0 || !counter || !(beta > 0.0))
+        return lt::set_error(LT_ERR_ARG, "lt_heatbath_sweeps4: bad arguments");
+    LT_TRY(check_cb4(h, "lt_heatbath_sweeps4"));
+    const lt::Ctx c = h->ctx();
+    for (int s = 0; s < n_sweep; ++s)
+    {
+        for (int mu = 0; mu < 4; ++mu)
+            for (int sub = 0; sub < 4; ++sub) h->be->sweep4(c, h->U, 0, mu, sub, 3.0 / beta, *counter, seed, 10);
+        ++*counter;
+    }
+    return launched("lt_heatbath_sweeps4");
+}
+
+int lt_update_sweeps4(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed, uint64_t* counter)
+{
+    LT_TRY(check_h(h, "lt_update_sweeps4"));
+    if (n_sweep < 0 || n_hb < 0 || n_or < 0 || !counter || !(beta > 0.0))
+        return lt::set_error(LT_ERR_ARG, "lt_update_sweeps4: bad arguments");
+    for (int s = 0; s < n_sweep; ++s)
+    {
+        LT_TRY(lt_heatbath_sweeps4(h, beta, n_hb, seed, counter));
+        LT_TRY(lt_overrelax_sweeps4(h, n_or));
     }
     return LT_OK;
 }

@@ -171,6 +171,8 @@ int lt_ensemble_create(lt_lattice* const* lattices, const double* betas, int n, 
     for (int k = 0; k < n; ++k)
     {
         if (!lattices[k]) return lt::set_error(LT_ERR_ARG, "lt_ensemble_create: null lattice");
+        if (lattices[k]->act_radius != 1)
+            return lt::set_error(LT_ERR_ARG, "lt_ensemble_create: ensembles run the Wilson action (radius 1)");
         if (lattices[k]->prec != lattices[0]->prec)
             return lt::set_error(LT_ERR_ARG, "lt_ensemble_create: all lattices need the same storage format");
         if (!(betas[k] > 0.0)) return lt::set_error(LT_ERR_ARG, "lt_ensemble_create: beta must be positive");

@@ -49,6 +49,10 @@ struct lt_lattice
     unsigned* status = nullptr;  // device status word (lt_status_word) and scratch words
     void* chainA = nullptr;      // straight-line link products of lt_wilson_loop (FP64 full matrices)
     void* chainB = nullptr;
+    // gauge action of staples, sweeps, HMC forces / Hamiltonian and flow (lt_set_gauge_action):
+    // stencil radius 1 (Wilson, the default) or 2 (plaquettes and 1x2 rectangles)
+    int act_radius = 1;
+    double act_cp = 1.0, act_cr = 0.0;
 
     lt::Ctx ctx() const
     {
@@ -58,6 +62,9 @@ struct lt_lattice
         c.partials = partials;
         c.results = results;
         c.status = status;
+        c.rect = act_radius == 2;
+        c.cp = act_cp;
+        c.cr = act_cr;
         return c;
     }
 };

@@ -86,7 +86,8 @@ public:
     }
     void staples_aos(const Ctx& c, const void* U, double* aos) const override
     {
-        k_staple_aos<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(gauge(U, c.g), c.g, aos);
+        auto k = c.rect ? k_staple_aos<T, NR, true> : k_staple_aos<T, NR, false>;
+        k<<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(gauge(U, c.g), c.g, aos, (T)c.cp, (T)c.cr);
     }
 
     void plaquette(const Ctx& c, const void* U, int slot) const override
@@ -173,8 +174,9 @@ public:
     void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new, double c_exp,
                     int read_z, int write_z) const override
     {
-        launch_chained(k_flow_stage<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
-                       gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z, write_z);
+        launch_chained(c.rect ? k_flow_stage<T, NR, true> : k_flow_stage<T, NR, false>, nblocks(c.g.V, kSitesPerBlock),
+                       4 * kSitesPerBlock, c.stream, gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old,
+                       (T)c_new, (T)c_exp, read_z, write_z, (T)c.cp, (T)c.cr);
     }
     void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
     {
@@ -184,13 +186,26 @@ public:
 
     void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const override
     {
-        k_momenta<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
-            gauge(U, c.g), alg(P, c.g), alg(F, c.g), c.g, (T)coef, (T)eps, F != nullptr);
+        auto k = c.rect ? k_momenta<T, NR, true> : k_momenta<T, NR, false>;
+        k<<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
+            gauge(U, c.g), alg(P, c.g), alg(F, c.g), c.g, (T)coef, (T)eps, F != nullptr, (T)c.cp, (T)c.cr);
     }
     void fields(const Ctx& c, void* U, const void* P, double eps) const override
     {
         k_fields<T, NR><<<nblocks(4LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), alg(P, c.g),
                                                                                    4 * c.g.V, (T)eps);
+    }
+    void sweep4(const Ctx& c, void* U, int op, int mu, int sub, double prefactor, uint64_t counter, uint64_t seed,
+                int max_iter) const override
+    {
+        const int nb = nblocks(c.g.V / 4, kThreads);
+        if (op == 0)
+            launch_chained(c.rect ? k_heatbath4<T, NR, true> : k_heatbath4<T, NR, false>, nb, kThreads, c.stream,
+                           gauge(U, c.g), c.g, mu, sub, (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32),
+                           max_iter, c.status, (T)c.cp, (T)c.cr);
+        else
+            launch_chained(c.rect ? k_overrelax4<T, NR, true> : k_overrelax4<T, NR, false>, nb, kThreads, c.stream,
+                           gauge(U, c.g), c.g, mu, sub, (T)c.cp, (T)c.cr);
     }
     void alg_axpby(const Ctx& c, void* P, const void* F, double a, double b) const override
     {

@@ -534,16 +534,109 @@ __global__ void __launch_bounds__(kRedThreads) k_check_links(Gauge<T, NR> U, Geo
     if ((threadIdx.x & 31) == 0) atomicMax(maxbits, __float_as_uint(dmax));
 }
 
-// ---------------------------------------------------------------- staple output (tests)
+// ---------------------------------------------------------------- rectangular actions
+// Full index of x + dm mu + dn nu (periodic) for the site x with coordinates c
+LT_D int site_at(const Geom& g, const int c[4], int mu, int dm, int nu, int dn)
+{
+    int cc[4] = { c[0], c[1], c[2], c[3] };
+    cc[mu] += dm;
+    cc[mu] += cc[mu] < 0 ? g.n[mu] : cc[mu] >= g.n[mu] ? -g.n[mu] : 0;
+    cc[nu] += dn;
+    cc[nu] += cc[nu] < 0 ? g.n[nu] : cc[nu] >= g.n[nu] ? -g.n[nu] : 0;
+    return ((cc[0] * g.n[1] + cc[1]) * g.n[2] + cc[2]) * g.n[3] + cc[3];
+}
+
+// Rectangular<2>::StapleRect (actions/gauge/rectangular_action.hpp:187-233): for each
+// nu = mu+1, mu+2, mu+3 (mod 4), the 1x2 loops orthogonal to the link (up and down) and the
+// 2x1 loops along it that start at x and at x - mu, each with U_mu(x) removed.
 template <typename T, int NR>
-__global__ void k_staple_aos(Gauge<T, NR> U, Geom g, double* __restrict__ aos)
+LT_D M3<T> staple_rect(const Gauge<T, NR>& U, const Geom& g, int par, const int c[4], int mu)
+{
+    // link U_d at x + dm mu + dn nu
+    auto L = [&](int d, int nu, int dm, int dn) -> M3<T> {
+        const int j = site_at(g, c, mu, dm, nu, dn);
+        return U.ld(d, par ^ ((dm + dn) & 1), j >> 1);
+    };
+    M3<T> st = zero3<T>();
+#pragma unroll 1
+    for (int off = 1; off < 4; ++off)
+    {
+        const int nu = (mu + off) & 3;
+        // orthogonal: U_nu(x) U_nu(x+nu) U_mu(x+2nu) U_nu(x+mu+nu)^dag U_nu(x+mu)^dag
+        //           + U_nu(x-nu)^dag U_nu(x-2nu)^dag U_mu(x-2nu) U_nu(x+mu-2nu) U_nu(x+mu-nu)
+        const M3<T> o_up = mul_nd(mul_nd(mul(mul(L(nu, nu, 0, 0), L(nu, nu, 0, 1)), L(mu, nu, 0, 2)), L(nu, nu, 1, 1)),
+                                  L(nu, nu, 1, 0));
+        const M3<T> o_dn = mul(mul(mul(mul_dd(L(nu, nu, 0, -1), L(nu, nu, 0, -2)), L(mu, nu, 0, -2)), L(nu, nu, 1, -2)),
+                               L(nu, nu, 1, -1));
+        acc(st, o_up + o_dn);
+        // along the link from x: [U_nu(x) U_mu(x+nu) U_mu(x+mu+nu) U_nu(x+2mu)^dag
+        //                        + U_nu(x-nu)^dag U_mu(x-nu) U_mu(x+mu-nu) U_nu(x+2mu-nu)] U_mu(x+mu)^dag
+        const M3<T> f_up = mul_nd(mul(mul(L(nu, nu, 0, 0), L(mu, nu, 0, 1)), L(mu, nu, 1, 1)), L(nu, nu, 2, 0));
+        const M3<T> f_dn = mul(mul(mul_dn(L(nu, nu, 0, -1), L(mu, nu, 0, -1)), L(mu, nu, 1, -1)), L(nu, nu, 2, -1));
+        acc(st, mul_nd(f_up + f_dn, L(mu, nu, 1, 0)));
+        // along the link from x - mu: U_mu(x-mu)^dag [U_nu(x-mu) U_mu(x-mu+nu) U_mu(x+nu) U_nu(x+mu)^dag
+        //                        + U_nu(x-mu-nu)^dag U_mu(x-mu-nu) U_mu(x-nu) U_nu(x+mu-nu)]
+        const M3<T> b_up = mul_nd(mul(mul(L(nu, nu, -1, 0), L(mu, nu, -1, 1)), L(mu, nu, 0, 1)), L(nu, nu, 1, 0));
+        const M3<T> b_dn = mul(mul(mul_dn(L(nu, nu, -1, -1), L(mu, nu, -1, -1)), L(mu, nu, 0, -1)), L(nu, nu, 1, -1));
+        acc(st, mul_dn(L(mu, nu, -1, 0), b_up + b_dn));
+    }
+    return st;
+}
+
+// The handle's gauge action on the device: Rectangular<1> (the plaquette staple alone, whatever
+// c_plaq) or Rectangular<2> (c_plaq StaplePlaq + c_rect StapleRect; rectangular_action.hpp:236-246)
+template <bool RECT, typename T, int NR>
+LT_D M3<T> action_staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const int c[4], int mu, T cp, T cr)
+{
+    if constexpr (RECT)
+    {
+        M3<T> st = cp * staple(U, g, par, i, c, mu);
+        acc(st, cr * staple_rect(U, g, par, c, mu));
+        return st;
+    }
+    else
+        return staple(U, g, par, i, c, mu);
+}
+
+// Iterator::Checkerboard4 (iterators/iterators.hpp:141-166): for direction mu the links whose
+// sites satisfy (t + x + y + z + x_mu) mod 4 = sub (every extent a multiple of 4).  Thread k
+// of the V/4 in a sub-sweep gets the k-th such site, z fastest: for mu != z a stride-4 run of
+// z per (t, x, y) row, for mu = z a stride-2 run on the rows with t + x + y = sub (mod 2).
+LT_D int cb4_site(const Geom& g, int mu, int sub, int k, int c[4])
+{
+    if (mu != 3)
+    {
+        const int nz = g.n[3] >> 2, row = k / nz, j = k - row * nz;
+        c[2] = row % g.n[2];
+        const int r2 = row / g.n[2];
+        c[1] = r2 % g.n[1];
+        c[0] = r2 / g.n[1];
+        const int z0 = (sub - c[0] - c[1] - c[2] - c[mu]) & 3;
+        c[3] = z0 + 4 * j;
+    }
+    else
+    {
+        const int nz = g.n[3] >> 1, row = k / nz, j = k - row * nz;
+        const int ny = g.n[2] >> 1, m = row % ny, q = row / ny;
+        c[1] = q % g.n[1];
+        c[0] = q / g.n[1];
+        c[2] = 2 * m + ((sub - c[0] - c[1]) & 1);
+        const int z0 = ((sub - c[0] - c[1] - c[2]) & 3) >> 1;
+        c[3] = z0 + 2 * j;
+    }
+    return ((c[0] * g.n[1] + c[1]) * g.n[2] + c[2]) * g.n[3] + c[3];
+}
+
+// ---------------------------------------------------------------- staple output (tests)
+template <typename T, int NR, bool RECT>
+__global__ void k_staple_aos(Gauge<T, NR> U, Geom g, double* __restrict__ aos, T cp, T cr)
 {
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
-    M3<T> st = staple(U, g, par, i, c, mu);
+    M3<T> st = action_staple<RECT>(U, g, par, i, c, mu, cp, cr);
     double* a = aos + (size_t)18 * (4 * i + mu);
 #pragma unroll
     for (int k = 0; k < 9; ++k)
@@ -599,6 +692,23 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gau
     pdl_wait();
     if (s >= g.vh) return;
     or_update(U, g, mu, par, s);
+}
+
+// One (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the handle's action
+template <typename T, int NR, bool RECT>
+__global__ void __launch_bounds__(kThreads) k_overrelax4(Gauge<T, NR> U, Geom g, int mu, int sub, T cp, T cr)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    pdl_release();
+    pdl_wait();
+    if (k >= (g.V >> 2)) return;
+    int c[4];
+    const int i = cb4_site(g, mu, sub, k, c);
+    const int par = (c[0] + c[1] + c[2] + c[3]) & 1, s = i >> 1;
+    const M3<T> st = action_staple<RECT>(U, g, par, i, c, mu, cp, cr);
+    M3<T> u = U.ld(mu, par, s);
+    or_apply<T, NR>(u, st);
+    U.st(mu, par, s, u);
 }
 
 // ---------------------------------------------------------------- heatbath
@@ -713,12 +823,40 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_heatbath(Gaug
 }
 
 template <typename T, int NR>
+LT_D void hb_core(const Gauge<T, NR>& U, int mu, int par, int s, int i, const M3<T>& st, T prefactor,
+                  uint64_t counter, uint32_t k0, uint32_t k1, int max_iter, unsigned* status);
+
+template <typename T, int NR>
 LT_D void hb_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s, T prefactor, uint64_t counter,
                     uint32_t k0, uint32_t k1, int max_iter, unsigned* status)
 {
     int c[4];
     int i = site_coords(g, par, s, c);
-    M3<T> st = staple(U, g, par, i, c, mu);
+    hb_core(U, mu, par, s, i, staple(U, g, par, i, c, mu), prefactor, counter, k0, k1, max_iter, status);
+}
+
+// One (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the handle's action
+template <typename T, int NR, bool RECT>
+__global__ void __launch_bounds__(kThreads) k_heatbath4(Gauge<T, NR> U, Geom g, int mu, int sub, T prefactor,
+                                                        uint64_t counter, uint32_t k0, uint32_t k1, int max_iter,
+                                                        unsigned* status, T cp, T cr)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    pdl_release();
+    pdl_wait();
+    if (k >= (g.V >> 2)) return;
+    int c[4];
+    const int i = cb4_site(g, mu, sub, k, c);
+    const int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    hb_core(U, mu, par, i >> 1, i, action_staple<RECT>(U, g, par, i, c, mu, cp, cr), prefactor, counter, k0, k1,
+            max_iter, status);
+}
+
+// Cabibbo-Marinari update of U_mu at site i (checkerboard index s) against the staple st
+template <typename T, int NR>
+LT_D void hb_core(const Gauge<T, NR>& U, int mu, int par, int s, int i, const M3<T>& st, T prefactor,
+                  uint64_t counter, uint32_t k0, uint32_t k1, int max_iter, unsigned* status)
+{
     M3<T> u = U.ld(mu, par, s);
     M3<T> w = mul_nd(u, st);
     const uint32_t link = (uint32_t)(4 * i + mu);
@@ -801,9 +939,9 @@ template <int Unused = 0> __global__ void k_counter_add(uint64_t* c, uint64_t n)
 //   U'  <- exp(c_exp Z) U, Gram-Schmidt          (UpdateFields)
 // reading U from Uin and writing Uout (ping-pong), so all staples see the pre-stage field
 // exactly as the reference's separate Z and field sweeps do.
-template <typename T, int NR>
+template <typename T, int NR, bool RECT>
 __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
-                                                         T c_old, T c_new, T c_exp, int read_z, int write_z)
+                                                         T c_old, T c_new, T c_exp, int read_z, int write_z, T cp, T cr)
 {
     pdl_release();
     pdl_wait();
@@ -813,7 +951,7 @@ __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_flo
     int c[4];
     int i = site_coords(g, par, s, c);
     M3<T> u = Uin.ld(mu, par, s);
-    M3<T> st = staple(Uin, g, par, i, c, mu);
+    M3<T> st = action_staple<RECT>(Uin, g, par, i, c, mu, cp, cr);
     A8<T> a = algebra8(mul_nd(st, u));
     A8<T> z;
     if (read_z)
@@ -1174,15 +1312,15 @@ __global__ void __launch_bounds__(kRedThreads) k_polyakov(Gauge<T, NR> Ust, Geom
 // ---------------------------------------------------------------- HMC
 // HMC momentum kick P += eps * (beta/6 Algebra(st U^dag) + F)  (updates/hmc_gauge.hpp:450-464,
 // updates/hmc_metadynamics.hpp:441-459).  With P = null the force itself is written to F_out.
-template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_momenta(Gauge<T, NR> U, Alg<T> P, Alg<T> F, Geom g, T coef, T eps, int use_f)
+template <typename T, int NR, bool RECT>
+__global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_momenta(Gauge<T, NR> U, Alg<T> P, Alg<T> F, Geom g, T coef, T eps, int use_f, T cp, T cr)
 {
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
-    M3<T> st = staple(U, g, par, i, c, mu);
+    M3<T> st = action_staple<RECT>(U, g, par, i, c, mu, cp, cr);
     A8<T> a = algebra8(mul_nd(st, U.ld(mu, par, s)));
     A8<T> p = P.ld(mu, par, s);
     if (use_f)

@@ -273,13 +273,63 @@ static M3 staple(const Geo* g, const double* U, long s, int mu)
     return acc;
 }
 
+/* The gauge action of staples, sweeps, HMC forces and the flow: GaugeAction::Rectangular
+ * (rectangular_action.hpp:23-246) with stencil radius 1 (the plaquette staple) or 2. */
+static int g_act_radius = 1;
+static double g_act_cp = 1.0, g_act_cr = 0.0;
+
+void or_set_gauge_action(int stencil_radius, double c_plaq, double c_rect)
+{
+    g_act_radius = stencil_radius;
+    g_act_cp = c_plaq;
+    g_act_cr = c_rect;
+}
+
+/* Rectangular<2>::StapleRect (rectangular_action.hpp:187-233) */
+static M3 staple_rect(const Geo* g, const double* U, long s, int mu)
+{
+    M3 st = zero3();
+    for (int off = 1; off < 4; ++off)
+    {
+        int nu = (mu + off) % 4;
+        long nup = move(g, s, nu, 1), nupp = move(g, nup, nu, 1), mup_nup = move(g, nup, mu, 1);
+        long mup = move(g, s, mu, 1);
+        long nud = move(g, s, nu, -1), nudd = move(g, nud, nu, -1), mup_nudd = move(g, nudd, mu, 1);
+        long mup_nud = move(g, nud, mu, 1);
+        /* orthogonal to the link */
+        st = add(st, add(mul(mul(mul(mul(ld(U, s, nu), ld(U, nup, nu)), ld(U, nupp, mu)), dag(ld(U, mup_nup, nu))),
+                             dag(ld(U, mup, nu))),
+                         mul(mul(mul(mul(dag(ld(U, nud, nu)), dag(ld(U, nudd, nu))), ld(U, nudd, mu)),
+                                 ld(U, mup_nudd, nu)),
+                             ld(U, mup_nud, nu))));
+        /* along the link, from x */
+        long mupp = move(g, mup, mu, 1), mupp_nud = move(g, mup_nud, mu, 1);
+        st = add(st, mul(add(mul(mul(mul(ld(U, s, nu), ld(U, nup, mu)), ld(U, mup_nup, mu)), dag(ld(U, mupp, nu))),
+                             mul(mul(mul(dag(ld(U, nud, nu)), ld(U, nud, mu)), ld(U, mup_nud, mu)), ld(U, mupp_nud, nu))),
+                         dag(ld(U, mup, mu))));
+        /* along the link, from x - mu */
+        long mud = move(g, s, mu, -1), mud_nup = move(g, mud, nu, 1), mud_nud = move(g, mud, nu, -1);
+        st = add(st, mul(dag(ld(U, mud, mu)),
+                         add(mul(mul(mul(ld(U, mud, nu), ld(U, mud_nup, mu)), ld(U, nup, mu)), dag(ld(U, mup, nu))),
+                             mul(mul(mul(dag(ld(U, mud_nud, nu)), ld(U, mud_nud, mu)), ld(U, nud, mu)), ld(U, mup_nud, nu)))));
+    }
+    return st;
+}
+
+/* Rectangular<radius>::Staple (rectangular_action.hpp:236-246) */
+static M3 act_staple(const Geo* g, const double* U, long s, int mu)
+{
+    if (g_act_radius != 2) return staple(g, U, s, mu);
+    return add(scl(g_act_cp, staple(g, U, s, mu)), scl(g_act_cr, staple_rect(g, U, s, mu)));
+}
+
 void or_staples(const int ext[4], const double* U, double* out)
 {
     Geo g = geo(ext);
     for (long s = 0; s < g.V; ++s)
         for (int mu = 0; mu < 4; ++mu)
         {
-            M3 a = staple(&g, U, s, mu);
+            M3 a = act_staple(&g, U, s, mu);
             st(out, s, mu, &a);
         }
 }
@@ -359,7 +409,7 @@ static S2 or_su2(S2 A)
 /* OverrelaxationSubgroupKernel::operator() (overrelaxation.hpp:91-116) */
 static void or_link(const Geo* g, double* U, long s, int mu)
 {
-    M3 sa = dag(staple(g, U, s, mu));
+    M3 sa = dag(act_staple(g, U, s, mu));
     M3 u = ld(U, s, mu);
     for (int sg = 0; sg < 3; ++sg)
         u = embed_mul(or_su2(extract(mul(u, sa), sg)), sg, u);
@@ -455,7 +505,7 @@ static S2 hb_su2(S2 A, double prefactor, uint32_t link, int sg, uint64_t counter
 /* HeatbathKernel::operator() (heatbath.hpp:110-129), prefactor 3/beta (:40) */
 static void hb_link(const Geo* g, double* U, long s, int mu, double beta, uint64_t counter, uint64_t seed)
 {
-    M3 sa = dag(staple(g, U, s, mu));
+    M3 sa = dag(act_staple(g, U, s, mu));
     M3 u = ld(U, s, mu);
     uint32_t link = (uint32_t)(4 * s + mu);
     for (int sg = 0; sg < 3; ++sg)
@@ -479,6 +529,35 @@ void or_heatbath_sweeps(const int ext[4], double* U, double beta, int n_sweep, u
                 }
 }
 
+/* Iterator::Checkerboard4 (iterators.hpp:141-166): for mu, for sub = 0..3, the sites with
+ * (t + x + y + z + x_mu) mod 4 = sub; within one sub-sweep the updates are independent. */
+static int cb4_member(const Geo* g, long s, int mu, int sub)
+{
+    int c[4];
+    coords(g, s, c);
+    return (c[0] + c[1] + c[2] + c[3] + c[mu]) % 4 == sub;
+}
+
+void or_overrelax_sweeps4(const int ext[4], double* U, int n_sweep)
+{
+    Geo g = geo(ext);
+    for (int sw = 0; sw < n_sweep; ++sw)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int sub = 0; sub < 4; ++sub)
+                for (long s = 0; s < g.V; ++s)
+                    if (cb4_member(&g, s, mu, sub)) or_link(&g, U, s, mu);
+}
+
+void or_heatbath_sweeps4(const int ext[4], double* U, double beta, int n_sweep, uint64_t seed, uint64_t counter0)
+{
+    Geo g = geo(ext);
+    for (int sw = 0; sw < n_sweep; ++sw)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int sub = 0; sub < 4; ++sub)
+                for (long s = 0; s < g.V; ++s)
+                    if (cb4_member(&g, s, mu, sub)) hb_link(&g, U, s, mu, beta, counter0 + (uint64_t)sw, seed);
+}
+
 /* ---------------------------------------------------------------- gradient flow */
 /* Z = c_old * Z + c_new * Algebra(st U^dag) (gradient_flow.hpp:298-332) */
 static void flow_z(const Geo* g, const double* U, double* Z, double c_old, double c_new)
@@ -486,7 +565,7 @@ static void flow_z(const Geo* g, const double* U, double* Z, double c_old, doubl
     for (long s = 0; s < g->V; ++s)
         for (int mu = 0; mu < 4; ++mu)
         {
-            M3 a = algebra(mul(staple(g, U, s, mu), dag(ld(U, s, mu))));
+            M3 a = algebra(mul(act_staple(g, U, s, mu), dag(ld(U, s, mu))));
             M3 z = c_old == 0.0 ? scl(c_new, a) : add(scl(c_old, ld(Z, s, mu)), scl(c_new, a));
             st(Z, s, mu, &z);
         }
@@ -656,7 +735,7 @@ void or_gauge_force(const int ext[4], const double* U, double beta, double* out)
     for (long s = 0; s < g.V; ++s)
         for (int mu = 0; mu < 4; ++mu)
         {
-            M3 f = scl(beta / 6.0, algebra(mul(staple(&g, U, s, mu), dag(ld(U, s, mu)))));
+            M3 f = scl(beta / 6.0, algebra(mul(act_staple(&g, U, s, mu), dag(ld(U, s, mu)))));
             st(out, s, mu, &f);
         }
 }
@@ -715,7 +794,7 @@ static void hmc_update_momenta(const Geo* g, const double* U, double* P, double 
     for (long s = 0; s < g->V; ++s)
         for (int mu = 0; mu < 4; ++mu)
         {
-            M3 f = scl(beta / 6.0, algebra(mul(staple(g, U, s, mu), dag(ld(U, s, mu)))));
+            M3 f = scl(beta / 6.0, algebra(mul(act_staple(g, U, s, mu), dag(ld(U, s, mu)))));
             if (extra) f = add(f, ld(extra, s, mu));
             M3 p = add(ld(P, s, mu), scl(eps, f));
             st(P, s, mu, &p);
@@ -1017,7 +1096,7 @@ static void md_friction(MdState* s, double eps, double fric, int without_kick)
     for (long x = 0; x < s->g.V; ++x)
         for (int mu = 0; mu < 4; ++mu)
         {
-            M3 f = scl(eps * s->beta / 6.0, algebra(mul(staple(&s->g, s->U, x, mu), dag(ld(s->U, x, mu)))));
+            M3 f = scl(eps * s->beta / 6.0, algebra(mul(act_staple(&s->g, s->U, x, mu), dag(ld(s->U, x, mu)))));
             M3 p = without_kick ? add(scl(e, ld(s->P, x, mu)), f) : scl(e, add(ld(s->P, x, mu), f));
             st(s->P, x, mu, &p);
         }
@@ -1071,9 +1150,17 @@ static void md_friction_step(MdState* s, int omf4, double e, double* fric, int f
     md_friction(s, OMF4_A * e, *fric, 0);
 }
 
+/* Action(U) of the current gauge action (rectangular_action.hpp:61-94) */
+static double act_action(const int ext[4], const double* U, double beta)
+{
+    if (g_act_radius == 2) return or_rect_action(ext, U, beta, g_act_cp, g_act_cr);
+    Geo g = geo(ext);
+    return beta * g_act_cp * (6.0 * (double)g.V - or_plaquette_sum(ext, U) / 3.0);
+}
+
 static double md_energy(MdState* s)
 {
-    double h = or_wilson_action(s->ext, s->U, s->beta) + or_kinetic(s->ext, s->P);
+    double h = act_action(s->ext, s->U, s->beta) + or_kinetic(s->ext, s->P);
     if (s->metad) h += s->slope * or_metad_charge(s->ext, s->U, s->rho, s->n_stout);
     return h;
 }

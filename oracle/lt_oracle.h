@@ -42,6 +42,10 @@ void   or_random_momenta(const int ext[4], double* P, uint64_t seed, uint64_t co
 void   or_md_integrate(const int ext[4], double* U, double* P, double beta, double tau, int n_step, int integrator,
                        int metad, double rho, int n_stout, double slope, double* h_old, double* h_new);
 void   or_parity_update(const int ext[4], double* U);
+/* gauge action of staples, sweeps, HMC forces / energies and the flow (default 1, 1, 0) */
+void   or_set_gauge_action(int stencil_radius, double c_plaq, double c_rect);
+void   or_overrelax_sweeps4(const int ext[4], double* U, int n_sweep);
+void   or_heatbath_sweeps4(const int ext[4], double* U, double beta, int n_sweep, uint64_t seed, uint64_t counter0);
 double or_kinetic(const int ext[4], const double* P);
 
 /* MetaBiasPotential (metadynamics.hpp:29-187) */

@@ -170,6 +170,22 @@ bool run_integrator(int id, HMCFunctor& kernel, double tau, int n)
     default: return false;
     }
 }
+// Run f(action) with GaugeAction::Rectangular<radius>(beta, c_plaq, c_rect)
+template <typename F>
+void with_action(int radius, double b, double cp, double cr, F&& f)
+{
+    if (radius == 2)
+    {
+        GaugeAction::Rectangular<2> act(b, cp, cr);
+        f(act);
+    }
+    else
+    {
+        GaugeAction::Rectangular<1> act(b, cp, cr);
+        f(act);
+    }
+}
+
 } // namespace
 
 extern "C"
@@ -635,6 +651,87 @@ int ref_md_integrate(double* links, double* momenta, double b, double tau, int n
     store(*U, links);
     store(*P, momenta);
     return ok ? 1 : 0;
+}
+
+// Rectangular<radius>::Staple (rectangular_action.hpp:236-246) for every link
+void ref_action_staples(const double* links, double* out, int radius, double cp, double cr)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto S = std::make_unique<GaugeField>();
+    load(*U, links);
+    with_action(radius, 6.0, cp, cr, [&](auto& act) {
+        #pragma omp parallel for collapse(2)
+        for (int t = 0; t < Nt; ++t)
+        for (int x = 0; x < Nx; ++x)
+        for (int y = 0; y < Ny; ++y)
+        for (int z = 0; z < Nz; ++z)
+        for (int mu = 0; mu < 4; ++mu)
+        {
+            link_coord l {t, x, y, z, mu};
+            (*S)(l) = act.Staple(*U, l);
+        }
+    });
+    store(*S, out);
+}
+
+// n sweeps of OverrelaxationSubgroupKernel with the action over Iterator::Checkerboard4
+// (iterators.hpp:141-166); every extent must be a multiple of 4 (the reference exits otherwise)
+int ref_or_sweeps4(double* links, int n, int radius, double cp, double cr)
+{
+    if (Nt % 4 != 0 || Nx % 4 != 0 || Ny % 4 != 0 || Nz % 4 != 0) return 0;
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+    with_action(radius, 6.0, cp, cr, [&](auto& act) {
+        OverrelaxationSubgroupKernel OR(*U, act);
+        Iterator::Checkerboard4(OR, n);
+    });
+    store(*U, links);
+    return 1;
+}
+
+// Gauge-only MD with integrator `id` (0-7) under Rectangular<radius>(beta, cp, cr): H before and after
+int ref_md_action(double* links, double* momenta, double b, double tau, int n_step, int id, int radius, double cp,
+                  double cr, double* h_old, double* h_new)
+{
+    set_beta(b);
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    load(*P, momenta);
+    RunStatistics stats;
+    Integrators::HMC::OMF_2 omf2;
+    bool ok = true;
+    with_action(radius, b, cp, cr, [&](auto& act) {
+        GaugeUpdates::HMCKernel hmc(*U, *Uc, *P, omf2, act, prng(), stats, std::cout, tau);
+        *h_old = hmc.Hamiltonian();
+        if (id == 6) Integrators::HMC::Leapfrog_friction_slow{}(hmc, tau, n_step);
+        else if (id == 7) Integrators::HMC::OMF_4_friction_slow{}(hmc, tau, n_step);
+        else ok = run_integrator(id, hmc, tau, n_step);
+        *h_new = hmc.Hamiltonian();
+    });
+    store(*U, links);
+    store(*P, momenta);
+    return ok ? 1 : 0;
+}
+
+// GradientFlowKernel with integrator 0-3 (Euler, RK2, RK3, RK3W7) and Rectangular<radius>
+void ref_flow_action(const double* in, double* out, double eps, int n, int integrator, int radius, double cp, double cr)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto V = std::make_unique<GaugeField>();
+    auto F = std::make_unique<GaugeField>();
+    load(*U, in);
+    with_action(radius, 6.0, cp, cr, [&](auto& act) {
+        switch (integrator)
+        {
+            case 0: { Integrators::GradientFlow::Euler it(*F); GradientFlowKernel k(*U, *V, it, act, eps); k(n); break; }
+            case 1: { Integrators::GradientFlow::RK2 it(*F); GradientFlowKernel k(*U, *V, it, act, eps); k(n); break; }
+            case 2: { Integrators::GradientFlow::RK3 it(*F); GradientFlowKernel k(*U, *V, it, act, eps); k(n); break; }
+            default: { Integrators::GradientFlow::RK3W7 it(*F); GradientFlowKernel k(*U, *V, it, act, eps); k(n); break; }
+        }
+    });
+    store(*V, out);
 }
 
 // ParityUpdate (parity_update.hpp:22-47) in place

@@ -67,5 +67,17 @@ def golden_md(oracle):
 
 
 @pytest.fixture(scope="session")
+def golden_rect(oracle):
+    """Reference Rectangular<2> staples, Checkerboard4 overrelaxation, MD and flow on 8^4; "U"
+    and "P" are the regenerated inputs."""
+    from ltref import haar_links_numpy
+    d = dict(np.load(os.path.join(GOLDEN, "ref_rect.npz")))
+    ext = tuple(int(e) for e in d["ext"])
+    d["U"] = oracle.heatbath(ext, haar_links_numpy(ext, 4), 6.0, 3, 21, 0)
+    d["P"] = oracle.random_momenta(ext, 9, 0)
+    return d
+
+
+@pytest.fixture(scope="session")
 def golden_chain():
     return dict(np.load(os.path.join(GOLDEN, "ref_chain_8x8x8x8.npz")))

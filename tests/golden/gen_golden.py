@@ -228,11 +228,43 @@ def gen_md() -> dict:
     return out
 
 
+def gen_rect() -> dict:
+    """Rectangular<2> gauge actions (rectangular_action.hpp:23-276: Luescher-Weisz, Iwasaki,
+    DBW2) on the 8^4 input (Haar seed 4, 3 oracle heatbath sweeps at beta = 6): staples,
+    2 overrelaxation sweeps over Iterator::Checkerboard4 (also with the Wilson action), gauge MD
+    (OMF_4 for LW and Iwasaki, OMF_2 for DBW2; tau = 0.5, 3 steps, Philox momenta seed 9) and
+    10 RK3 flow steps of 0.02."""
+    from ltref import DBW2, IWASAKI, LUESCHER_WEISZ, WILSON, Oracle
+    ext = (8, 8, 8, 8)
+    o = Oracle()
+    U = o.heatbath(ext, haar_links_numpy(ext, 4), 6.0, 3, 21, 0)
+    P = o.random_momenta(ext, 9, 0)
+    ref = Reference(ext)
+    links = sample_links(int(np.prod(ext)), 8)[:32]
+    out = {"ext": np.array(ext), "U_ck": checksums(U), "P_ck": checksums(P), "links": links}
+    for name, act in (("lw", LUESCHER_WEISZ), ("iwasaki", IWASAKI), ("dbw2", DBW2), ("wilson", WILSON)):
+        out[name + "_act"] = np.array(act)
+        R = ref.overrelax4(U, 2, act)
+        out[name + "_or4"], out[name + "_or4_ck"] = take(R, links), checksums(R)
+        if name == "wilson":
+            continue
+        S = ref.action_staples(U, act)
+        out[name + "_staple"], out[name + "_staple_ck"] = take(S, links), checksums(S)
+        integ = 3 if name == "dbw2" else 5
+        U2, P2, ho, hn = ref.md_action(U, P, 6.0, 0.5, 3, integ, act)
+        out[name + "_md_integ"] = np.array(integ)
+        out[name + "_md_U"], out[name + "_md_P"] = take(U2, links), take(P2, links)
+        out[name + "_md_h"] = np.array([ho, hn])
+        F = ref.flow_action(U, 0.02, 10, 2, act)
+        out[name + "_flow"], out[name + "_flow_ck"] = take(F, links), checksums(F)
+    return out
+
+
 def main() -> int:
     import argparse
     import subprocess
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["chain", "bmw", "measure", "md"], default=None,
+    ap.add_argument("--only", choices=["chain", "bmw", "measure", "md", "rect"], default=None,
                     help="regenerate one fixture only")
     a = ap.parse_args()
     root = os.path.dirname(os.path.dirname(HERE))
@@ -243,6 +275,9 @@ def main() -> int:
         return 0
     if a.only == "measure":
         np.savez_compressed(os.path.join(HERE, "ref_measure.npz"), **gen_measure())
+        return 0
+    if a.only == "rect":
+        np.savez_compressed(os.path.join(HERE, "ref_rect.npz"), **gen_rect())
         return 0
     if a.only == "md":
         np.savez_compressed(os.path.join(HERE, "ref_md.npz"), **gen_md())
@@ -261,6 +296,7 @@ def main() -> int:
     np.savez_compressed(os.path.join(HERE, "ref_bmw.npz"), **gen_bmw())
     np.savez_compressed(os.path.join(HERE, "ref_measure.npz"), **gen_measure())
     np.savez_compressed(os.path.join(HERE, "ref_md.npz"), **gen_md())
+    np.savez_compressed(os.path.join(HERE, "ref_rect.npz"), **gen_rect())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

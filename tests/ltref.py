@@ -6,6 +6,7 @@ Fields are numpy float64 arrays in the reference AoS layout [V, 4, 3, 3, 2]
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -71,6 +72,9 @@ class Oracle:
             "or_bmw_decode": (u64, [_ip, C.c_void_p, i, _dp]),
             "or_md_integrate": (None, [_ip, _dp, _dp, d, d, i, i, i, d, i, d, C.POINTER(d), C.POINTER(d)]),
             "or_parity_update": (None, [_ip, _dp]),
+            "or_set_gauge_action": (None, [i, d, d]),
+            "or_overrelax_sweeps4": (None, [_ip, _dp, i]),
+            "or_heatbath_sweeps4": (None, [_ip, _dp, d, i, u64, u64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -81,6 +85,41 @@ class Oracle:
     @staticmethod
     def _e(ext):
         return np.ascontiguousarray(ext, dtype=np.int32)
+
+    @contextlib.contextmanager
+    def action(self, act):
+        """Run the block under GaugeAction::Rectangular act = (radius, c_plaq, c_rect) (None:
+        WilsonAction); the Wilson action is restored afterwards."""
+        if act is not None:
+            self.lib.or_set_gauge_action(int(act[0]), float(act[1]), float(act[2]))
+        try:
+            yield
+        finally:
+            self.lib.or_set_gauge_action(1, 1.0, 0.0)
+
+    def action_staples(self, ext, U, act):
+        with self.action(act):
+            return self.staples(ext, np.ascontiguousarray(U))
+
+    def overrelax4(self, ext, U, n, act=None):
+        V = np.ascontiguousarray(U).copy()
+        with self.action(act):
+            self.lib.or_overrelax_sweeps4(self._e(ext), V, n)
+        return V
+
+    def heatbath4(self, ext, U, beta, n, seed, counter, act=None):
+        V = np.ascontiguousarray(U).copy()
+        with self.action(act):
+            self.lib.or_heatbath_sweeps4(self._e(ext), V, beta, n, seed, counter)
+        return V
+
+    def md_integrate_action(self, ext, U, P, beta, tau, n, integrator, act):
+        with self.action(act):
+            return self.md_integrate(ext, U, P, beta, tau, n, integrator)
+
+    def flow_action(self, ext, U, eps, n, integrator, act):
+        with self.action(act):
+            return self.flow(ext, U, eps, n, integrator)
 
     def plaquette_sum(self, ext, U):
         return self.lib.or_plaquette_sum(self._e(ext), U)
@@ -251,6 +290,10 @@ class Reference:
                 "ref_load_bmw": (i, [C.c_char_p, i, _dp]),
                 "ref_md_integrate": (i, [_dp, _dp, d, d, i, i, i, d, d, C.POINTER(d), C.POINTER(d)]),
                 "ref_parity_update": (None, [_dp]),
+                "ref_action_staples": (None, [_dp, _dp, i, d, d]),
+                "ref_or_sweeps4": (i, [_dp, i, i, d, d]),
+                "ref_md_action": (i, [_dp, _dp, d, d, i, i, i, d, d, C.POINTER(d), C.POINTER(d)]),
+                "ref_flow_action": (None, [_dp, _dp, d, i, i, i, d, d]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(lib, name)
@@ -349,6 +392,31 @@ class Reference:
         self.lib.ref_parity_update(V)
         return V
 
+    def action_staples(self, U, act):
+        out = np.empty_like(U)
+        self.lib.ref_action_staples(np.ascontiguousarray(U), out, int(act[0]), float(act[1]), float(act[2]))
+        return out
+
+    def overrelax4(self, U, n, act):
+        V = np.ascontiguousarray(U).copy()
+        if not self.lib.ref_or_sweeps4(V, n, int(act[0]), float(act[1]), float(act[2])):
+            raise ValueError("Checkerboard4 needs every extent a multiple of 4")
+        return V
+
+    def md_action(self, U, P, beta, tau, n, integrator, act):
+        U2, P2 = np.ascontiguousarray(U).copy(), np.ascontiguousarray(P).copy()
+        ho, hn = C.c_double(), C.c_double()
+        if not self.lib.ref_md_action(U2, P2, beta, tau, n, integrator, int(act[0]), float(act[1]), float(act[2]),
+                                      C.byref(ho), C.byref(hn)):
+            raise ValueError("no such gauge integrator")
+        return U2, P2, ho.value, hn.value
+
+    def flow_action(self, U, eps, n, integrator, act):
+        out = np.empty_like(U)
+        self.lib.ref_flow_action(np.ascontiguousarray(U), out, eps, n, integrator, int(act[0]), float(act[1]),
+                                 float(act[2]))
+        return out
+
     def su3_exp(self, Q):
         Q = np.ascontiguousarray(Q, dtype=np.float64)
         out = np.empty_like(Q)
@@ -384,6 +452,13 @@ def bmw_header(ext, checksum: int, full: bool) -> bytes:
     h[:len(line)] = line
     h[len(line):len(line) + len(tail)] = tail
     return bytes(h)
+
+
+# GaugeAction named actions (rectangular_action.hpp:273-276) as (stencil radius, c_plaq, c_rect)
+WILSON = (1, 1.0, 0.0)
+LUESCHER_WEISZ = (2, 1.0 + 8.0 / 12.0, -1.0 / 12.0)
+IWASAKI = (2, 1.0 + 8.0 * 0.331, -0.331)
+DBW2 = (2, 1.0 + 8.0 * 1.4088, -1.4088)
 
 
 def haar_links_numpy(ext, seed):

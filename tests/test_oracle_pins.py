@@ -8,7 +8,7 @@ entry (FP64 on both sides; the only differences are summation order and libm rou
 import numpy as np
 import pytest
 
-from ltref import Reference, haar_links_numpy, ref_available, rel_err
+from ltref import DBW2, IWASAKI, LUESCHER_WEISZ, WILSON, Reference, haar_links_numpy, ref_available, rel_err
 
 TOL = 1e-12
 
@@ -292,3 +292,86 @@ class TestMDIntegrators:
             assert rel_err(a[0], b[0]) < 1e-12 and rel_err(a[1], b[1]) < 1e-12
             assert a[3] == pytest.approx(b[3], rel=1e-13)
         assert np.array_equal(oracle.parity_update(ext, U), ref.parity_update(U))
+
+
+RECT = (("lw", LUESCHER_WEISZ), ("iwasaki", IWASAKI), ("dbw2", DBW2))
+
+
+class TestRectangularActions:
+    """GaugeAction::Rectangular<2> (rectangular_action.hpp:23-276) staples, sweeps over
+    Iterator::Checkerboard4 (iterators.hpp:141-166), gauge MD and flow, against the reference."""
+
+    @pytest.mark.parametrize("name,act", RECT)
+    def test_against_fixture(self, oracle, golden_rect, name, act):
+        g = golden_rect
+        ext = tuple(int(e) for e in g["ext"])
+        assert close_ck(checksums(g["U"]), g["U_ck"], 1e-12) and close_ck(checksums(g["P"]), g["P_ck"], 1e-12)
+        assert tuple(g[name + "_act"]) == pytest.approx(act, rel=1e-15)
+        S = oracle.action_staples(ext, g["U"], act)
+        assert rel_err(links_of(S, g["links"]), g[name + "_staple"]) < 1e-13
+        assert close_ck(checksums(S), g[name + "_staple_ck"], 1e-11)
+        R = oracle.overrelax4(ext, g["U"], 2, act)
+        assert rel_err(links_of(R, g["links"]), g[name + "_or4"]) < 1e-11
+        U2, P2, ho, hn = oracle.md_integrate_action(ext, g["U"], g["P"], 6.0, 0.5, 3, int(g[name + "_md_integ"]), act)
+        assert rel_err(links_of(U2, g["links"]), g[name + "_md_U"]) < 1e-12
+        assert rel_err(links_of(P2, g["links"]), g[name + "_md_P"]) < 1e-12
+        assert ho == pytest.approx(g[name + "_md_h"][0], rel=1e-13) and hn == pytest.approx(g[name + "_md_h"][1], rel=1e-13)
+        F = oracle.flow_action(ext, g["U"], 0.02, 10, 2, act)
+        assert rel_err(links_of(F, g["links"]), g[name + "_flow"]) < 1e-12
+
+    def test_wilson_checkerboard4_fixture(self, oracle, golden_rect):
+        g = golden_rect
+        ext = tuple(int(e) for e in g["ext"])
+        R = oracle.overrelax4(ext, g["U"], 2, WILSON)
+        assert rel_err(links_of(R, g["links"]), g["wilson_or4"]) < 1e-11
+        # a different visiting order than Checkerboard: the fields differ
+        assert rel_err(R, oracle.overrelax(ext, g["U"], 2)) > 1e-6
+
+    def test_action_state_resets(self, oracle, golden_rect):
+        g = golden_rect
+        ext = tuple(int(e) for e in g["ext"])
+        oracle.action_staples(ext, g["U"], DBW2)
+        assert rel_err(oracle.staples(ext, g["U"]), oracle.action_staples(ext, g["U"], WILSON)) == 0.0
+
+    def test_rect_staple_is_action_derivative(self, oracle):
+        """d/dt S(exp(t X) U) at t = 0 equals -beta/3 Re tr(X U Staple^dag) summed over one link:
+        the rectangle staple is the derivative of the rectangle action."""
+        ext = (4, 4, 4, 4)
+        U = oracle.heatbath(ext, haar_links_numpy(ext, 6), 6.0, 2, 1, 0)
+        act = IWASAKI
+        S = oracle.action_staples(ext, U, act)
+        rng = np.random.default_rng(3)
+        site, mu = 37, 2
+        H = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+        X = 0.5j * (H + H.conj().T)
+        X -= np.trace(X) / 3 * np.eye(3)
+        Uc = U.reshape(-1, 4, 3, 3, 2)
+        u = Uc[site, mu, ..., 0] + 1j * Uc[site, mu, ..., 1]
+        st = S.reshape(-1, 4, 3, 3, 2)[site, mu]
+        st = st[..., 0] + 1j * st[..., 1]
+        want = -6.0 / 3.0 * np.real(np.trace(X @ u @ st.conj().T))
+
+        def action_at(t):
+            from scipy.linalg import expm
+            V = Uc.copy()
+            w = expm(t * X) @ u
+            V[site, mu, ..., 0], V[site, mu, ..., 1] = w.real, w.imag
+            return oracle.lib.or_rect_action(oracle._e(ext), np.ascontiguousarray(V.reshape(U.shape)), 6.0,
+                                             act[1], act[2])
+
+        h = 1e-5
+        assert (action_at(h) - action_at(-h)) / (2 * h) == pytest.approx(want, rel=1e-6)
+
+    @pytest.mark.skipif(not ref_available((4, 4, 4, 4)), reason="reference harness not built")
+    def test_live_reference(self, oracle):
+        ext = (4, 4, 4, 4)
+        U = oracle.heatbath(ext, haar_links_numpy(ext, 9), 5.9, 3, 4, 0)
+        P = oracle.random_momenta(ext, 3, 1)
+        ref = Reference(ext)
+        for act in (LUESCHER_WEISZ, DBW2, (2, 0.7, 0.2)):
+            assert rel_err(oracle.action_staples(ext, U, act), ref.action_staples(U, act)) < 1e-13
+            assert rel_err(oracle.overrelax4(ext, U, 1, act), ref.overrelax4(U, 1, act)) < 1e-11
+            a = oracle.md_integrate_action(ext, U, P, 5.9, 0.3, 2, 7, act)
+            b = ref.md_action(U, P, 5.9, 0.3, 2, 7, act)
+            assert rel_err(a[0], b[0]) < 1e-12 and a[3] == pytest.approx(b[3], rel=1e-13)
+            assert rel_err(oracle.flow_action(ext, U, 0.03, 3, 3, act), ref.flow_action(U, 0.03, 3, 3, act)) < 1e-12
