@@ -111,6 +111,52 @@ template <typename T, int NR> struct Gauge
     }
 };
 
+#ifndef LT_F32C_SCALAR
+// Two-row FP32 storage: the 12 floats of a link as three float4 chunks, chunk c of plane
+// (mu, par) at ((mu * 2 + par) * 3 + c) * vh, holding two consecutive complex entries of rows
+// 0-1 (e00 e01 | e02 e10 | e11 e12).  A link is three 16-byte loads; a warp reads 512
+// contiguous bytes per chunk.
+template <> struct Gauge<float, 2>
+{
+    cx<float>* __restrict__ p;
+    int vh;
+
+    LT_D const float4* chunk(int mu, int par, int c) const
+    {
+        return reinterpret_cast<const float4*>(p) + (size_t)((mu * 2 + par) * 3 + c) * (size_t)vh;
+    }
+
+    LT_D M3<float> ld_rows(int mu, int par, int s) const
+    {
+        const float4* q = chunk(mu, par, 0) + s;
+        const float4 a = q[0], b = q[vh], c = q[2 * (size_t)vh];
+        M3<float> m;
+        m.e[0][0] = mkc<float>(a.x, a.y);
+        m.e[0][1] = mkc<float>(a.z, a.w);
+        m.e[0][2] = mkc<float>(b.x, b.y);
+        m.e[1][0] = mkc<float>(b.z, b.w);
+        m.e[1][1] = mkc<float>(c.x, c.y);
+        m.e[1][2] = mkc<float>(c.z, c.w);
+        return m;
+    }
+
+    LT_D M3<float> ld(int mu, int par, int s) const
+    {
+        M3<float> m = ld_rows(mu, par, s);
+        restore_last_row(m);
+        return m;
+    }
+
+    LT_D void st(int mu, int par, int s, const M3<float>& m) const
+    {
+        float4* q = const_cast<float4*>(chunk(mu, par, 0)) + s;
+        q[0] = make_float4(m.e[0][0].r, m.e[0][0].i, m.e[0][1].r, m.e[0][1].i);
+        q[vh] = make_float4(m.e[0][2].r, m.e[0][2].i, m.e[1][0].r, m.e[1][0].i);
+        q[2 * (size_t)vh] = make_float4(m.e[1][1].r, m.e[1][1].i, m.e[1][2].r, m.e[1][2].i);
+    }
+};
+#endif
+
 template <typename T> struct Alg
 {
     T* __restrict__ p;

@@ -14,6 +14,9 @@ constexpr int kThreads = 128;
 #ifndef LT_MINB_SWEEP_F32
 #define LT_MINB_SWEEP_F32 5
 #endif
+#ifndef LT_MINB_OR_F32C
+#define LT_MINB_OR_F32C 7
+#endif
 #ifndef LT_MINB_SWEEP_F64
 #define LT_MINB_SWEEP_F64 3
 #endif
@@ -29,6 +32,11 @@ constexpr int kThreads = 128;
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int sweep = LT_MINB_SWEEP_F32, link = LT_MINB_LINK_F32; };
 template <> struct MinBlocks<double> { static constexpr int sweep = LT_MINB_SWEEP_F64, link = LT_MINB_LINK_F64; };
+// overrelaxation on two-row FP32 storage fits a tighter register budget than the heatbath
+template <typename T, int NR> struct OrMinBlocks
+{
+    static constexpr int value = (sizeof(T) == 4 && NR == 2) ? LT_MINB_OR_F32C : MinBlocks<T>::sweep;
+};
 // link-parallel kernels: two-row FP32 storage has its own setting
 template <typename T, int NR> struct LinkMinBlocks
 {
@@ -685,7 +693,7 @@ LT_D void or_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s
 }
 
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
+__global__ void __launch_bounds__(kThreads, (OrMinBlocks<T, NR>::value)) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_release();
