@@ -22,6 +22,7 @@ struct Ctx
     // or Rectangular<1> (rect = 0: the plaquette staple)
     int rect = 0;
     double cp = 1.0, cr = 0.0;
+    unsigned* order = nullptr;    // the handle's launch counter for alternating site orders
 };
 
 constexpr int kNumSlots = 8;

@@ -53,6 +53,7 @@ struct lt_lattice
     // stencil radius 1 (Wilson, the default) or 2 (plaquettes and 1x2 rectangles)
     int act_radius = 1;
     double act_cp = 1.0, act_cr = 0.0;
+    mutable unsigned order = 0;  // launches of the order-alternating sweep and flow kernels
 
     lt::Ctx ctx() const
     {
@@ -65,6 +66,7 @@ struct lt_lattice
         c.rect = act_radius == 2;
         c.cp = act_cp;
         c.cr = act_cr;
+        c.order = &order;
         return c;
     }
 };

@@ -9,6 +9,17 @@ namespace lt {
 
 inline int nblocks(long long n, int threads) { return (int)((n + threads - 1) / threads); }
 
+// Site order of the next launch on a handle: ascending and descending in turn (the handle
+// counts its launches), so a launch starts where the previous one ended
+inline int next_order(const Ctx& c)
+{
+#ifdef LT_NO_ORDER_FLIP
+    return 0;
+#else
+    return c.order ? ((*c.order)++ & 1) : 0;
+#endif
+}
+
 #ifndef LT_PDL
 #define LT_PDL 1
 #endif
@@ -111,13 +122,14 @@ public:
 
     void overrelax(const Ctx& c, void* U, int mu, int par) const override
     {
-        launch_chained(k_overrelax<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu, par);
+        launch_chained(k_overrelax<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu, par,
+                       next_order(c));
     }
     void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter, uint64_t seed,
                   int max_iter) const override
     {
         launch_chained(k_heatbath<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu, par,
-                       (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter, c.status);
+                       (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter, c.status, next_order(c));
     }
     void check_links(const Ctx& c, const void* U, double tol, unsigned* maxbits) const override
     {
@@ -176,7 +188,7 @@ public:
     {
         launch_chained(c.rect ? k_flow_stage<T, NR, true> : k_flow_stage<T, NR, false>, nblocks(c.g.V, kSitesPerBlock),
                        4 * kSitesPerBlock, c.stream, gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old,
-                       (T)c_new, (T)c_exp, read_z, write_z, (T)c.cp, (T)c.cr);
+                       (T)c_new, (T)c_exp, read_z, write_z, (T)c.cp, (T)c.cr, next_order(c));
     }
     void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
     {

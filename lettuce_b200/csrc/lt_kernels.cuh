@@ -106,6 +106,25 @@ LT_D bool link_of_thread(const Geom& g, int& mu, int& x)
     return x < g.V;
 }
 
+// The same with the site order reversed when rev != 0.  Consecutive launches over the same
+// fields alternate the order, so each launch starts on the sites the previous one touched
+// last, which are still in L2.
+LT_D bool link_of_thread(const Geom& g, int& mu, int& x, int rev)
+{
+    const bool ok = link_of_thread(g, mu, x);
+    if (rev) x = g.V - 1 - x;
+    return ok;
+}
+
+// Thread -> checkerboard index of a half-lattice kernel, reversed when rev != 0 (as above)
+LT_D bool half_site_of_thread(const Geom& g, int& s, int rev)
+{
+    s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = s < g.vh;
+    if (rev) s = g.vh - 1 - s;
+    return ok;
+}
+
 // ---------------------------------------------------------------- staple
 // Rectangular<1>::StaplePlaq (actions/gauge/rectangular_action.hpp:104-184):
 //   sum_{nu != mu} U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag + U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu)
@@ -693,12 +712,13 @@ LT_D void or_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s
 }
 
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, (OrMinBlocks<T, NR>::value)) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par)
+__global__ void __launch_bounds__(kThreads, (OrMinBlocks<T, NR>::value)) k_overrelax(Gauge<T, NR> U, Geom g, int mu, int par, int rev)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    int s;
+    const bool ok = half_site_of_thread(g, s, rev);
     pdl_release();
     pdl_wait();
-    if (s >= g.vh) return;
+    if (!ok) return;
     or_update(U, g, mu, par, s);
 }
 
@@ -821,12 +841,13 @@ template <> struct HB<float>
 template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_heatbath(Gauge<T, NR> U, Geom g, int mu, int par, T prefactor,
                                                        uint64_t counter, uint32_t k0, uint32_t k1, int max_iter,
-                                                       unsigned* status)
+                                                       unsigned* status, int rev)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    int s;
+    const bool ok = half_site_of_thread(g, s, rev);
     pdl_release();
     pdl_wait();
-    if (s >= g.vh) return;
+    if (!ok) return;
     hb_update(U, g, mu, par, s, prefactor, counter, k0, k1, max_iter, status);
 }
 
@@ -949,12 +970,13 @@ template <int Unused = 0> __global__ void k_counter_add(uint64_t* c, uint64_t n)
 // exactly as the reference's separate Z and field sweeps do.
 template <typename T, int NR, bool RECT>
 __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_flow_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Geom g,
-                                                         T c_old, T c_new, T c_exp, int read_z, int write_z, T cp, T cr)
+                                                         T c_old, T c_new, T c_exp, int read_z, int write_z, T cp, T cr,
+                                                         int rev)
 {
     pdl_release();
     pdl_wait();
     int mu, x;
-    if (!link_of_thread(g, mu, x)) return;
+    if (!link_of_thread(g, mu, x, rev)) return;
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
