@@ -65,6 +65,22 @@ LT_D int site_coords(const Geom& g, int par, int s, int c[4])
     return i0 - z0 + c[3];
 }
 
+// a[k] for a run-time k without indexing the array (keeps small arrays in registers)
+LT_D int pick4(const int a[4], int k) { return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : a[3]; }
+
+// Full-index offset of a +1 / -1 step along a run-time direction d from a site with
+// coordinates c
+LT_D int step_up_rt(const Geom& g, int d, const int c[4])
+{
+    const int n = pick4(g.n, d), st = pick4(g.stride, d);
+    return pick4(c, d) + 1 < n ? st : -(n - 1) * st;
+}
+LT_D int step_dn_rt(const Geom& g, int d, const int c[4])
+{
+    const int n = pick4(g.n, d), st = pick4(g.stride, d);
+    return pick4(c, d) > 0 ? -st : (n - 1) * st;
+}
+
 // Full-index offset of a +1 / -1 step along d from a site with coordinate cd along d
 LT_D int step_up(const Geom& g, int d, int cd) { return cd + 1 < g.n[d] ? g.stride[d] : -(g.n[d] - 1) * g.stride[d]; }
 LT_D int step_dn(const Geom& g, int d, int cd) { return cd > 0 ? -g.stride[d] : (g.n[d] - 1) * g.stride[d]; }

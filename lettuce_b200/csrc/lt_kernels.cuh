@@ -133,7 +133,7 @@ template <typename T, int NR>
 LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const int c[4], int mu)
 {
     const int op = par ^ 1;
-    const int dmu = step_up(g, mu, c[mu]);
+    const int dmu = step_up_rt(g, mu, c);
     const int imu = i + dmu;
     M3<T> acc = zero3<T>();
 #pragma unroll
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kRedThreads) k_plaquette(Gauge<T, NR> U, Geom 
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu)
         {
-            const int imu = i + step_up(g, mu, c[mu]);
+            const int imu = i + step_up_rt(g, mu, c);
             // products in FP64 whatever the storage: the action enters HMC's dH and the
             // plaquette the FP32-vs-FP64 error budget, so only storage rounding remains
             const M3<double> umu = cvt<double>(U.ld(mu, par, s));
@@ -1032,7 +1032,7 @@ LT_D auto clover_leaves(const F& U, const Geom& g, int par, int i, const int c[4
 {
     using M = decltype(U.ld(0, 0, 0));
     const int op = par ^ 1;
-    const int dmu_p = step_up(g, mu, c[mu]), dmu_m = step_dn(g, mu, c[mu]);
+    const int dmu_p = step_up_rt(g, mu, c), dmu_m = step_dn_rt(g, mu, c);
     const int dnu_p = step_up(g, nu, c[nu]), dnu_m = step_dn(g, nu, c[nu]);
     const int s = i >> 1;
     const M umu = U.ld(mu, par, s), unu = U.ld(nu, par, s);
@@ -1490,7 +1490,7 @@ LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const
                                   const int c[4], int mu, int nu, int rho, int sigma)
 {
     const int op = par ^ 1;
-    const int dmu = step_up(g, mu, c[mu]);
+    const int dmu = step_up_rt(g, mu, c);
     const int imu = i + dmu, inu = i + step_up(g, nu, c[nu]), ind = i + step_dn(g, nu, c[nu]);
     // x+mu+nu and x+mu-nu share the nu offsets of x (coordinate c[nu] unchanged by the mu step)
     const int imunu = inu + dmu, imund = ind + dmu;
@@ -1608,7 +1608,7 @@ __global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Al
     int c[4];
     int i = site_coords(g, par, s, c);
     const int op = par ^ 1;
-    const int dmu = step_up(g, mu, c[mu]);
+    const int dmu = step_up_rt(g, mu, c);
     const int imu = i + dmu;
     M3<T> fs = zero3<T>();
 #pragma unroll 1
