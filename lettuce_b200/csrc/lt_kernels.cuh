@@ -17,6 +17,9 @@ constexpr int kThreads = 128;
 #ifndef LT_MINB_OR_F32C
 #define LT_MINB_OR_F32C 7
 #endif
+#ifndef LT_MINB_HB_F32C
+#define LT_MINB_HB_F32C 6
+#endif
 #ifndef LT_MINB_SWEEP_F64
 #define LT_MINB_SWEEP_F64 3
 #endif
@@ -32,10 +35,15 @@ constexpr int kThreads = 128;
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int sweep = LT_MINB_SWEEP_F32, link = LT_MINB_LINK_F32; };
 template <> struct MinBlocks<double> { static constexpr int sweep = LT_MINB_SWEEP_F64, link = LT_MINB_LINK_F64; };
-// overrelaxation on two-row FP32 storage fits a tighter register budget than the heatbath
+// the sweeps on two-row FP32 storage fit tighter register budgets (no spills at 7 and 6
+// blocks of 128 per SM; measured fastest on B200)
 template <typename T, int NR> struct OrMinBlocks
 {
     static constexpr int value = (sizeof(T) == 4 && NR == 2) ? LT_MINB_OR_F32C : MinBlocks<T>::sweep;
+};
+template <typename T, int NR> struct HbMinBlocks
+{
+    static constexpr int value = (sizeof(T) == 4 && NR == 2) ? LT_MINB_HB_F32C : MinBlocks<T>::sweep;
 };
 // link-parallel kernels: two-row FP32 storage has its own setting
 template <typename T, int NR> struct LinkMinBlocks
@@ -839,7 +847,7 @@ template <> struct HB<float>
 
 // HeatbathKernel::operator() (updates/heatbath.hpp:110-129) for one (mu, parity) sub-sweep
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T>::sweep) k_heatbath(Gauge<T, NR> U, Geom g, int mu, int par, T prefactor,
+__global__ void __launch_bounds__(kThreads, (HbMinBlocks<T, NR>::value)) k_heatbath(Gauge<T, NR> U, Geom g, int mu, int par, T prefactor,
                                                        uint64_t counter, uint32_t k0, uint32_t k1, int max_iter,
                                                        unsigned* status, int rev)
 {
