@@ -234,7 +234,13 @@ def secondary_rates(lt, torch, timed, prec):
         for _ in range(3):
             k.CalculateTopologicalForce(dvdq=1.0, download=False)
         ms = timed(G, lambda: k.CalculateTopologicalForce(dvdq=1.0, download=False), 10)
-        out["metad_force_evals_per_s_16^4_fp32"] = 10 / (ms / 1000.0)
+        rate = 10 / (ms / 1000.0)
+        out["metad_force_evals_per_s_16^4_fp32"] = rate
+        links = 4 * G.Volume()
+        gbs = bm.metad_force_bytes_per_link("fp32", 4) * links * rate / 1e9
+        tfl = bm.FLOPS["metad_force_n4"] * links * rate / 1e12
+        out["metad_force_roofline"] = {"hbm_gbs": gbs, "hbm_frac": gbs / peaks()[0], "tflops": tfl,
+                                       "note": "algorithmic bytes (6.9 n + 3.5) b per link and ~70k flops per link"}
         del k, G
     except Exception as e:   # report, never hide
         out["metad_force_error"] = repr(e)
@@ -285,6 +291,20 @@ def secondary_rates(lt, torch, timed, prec):
         del G
     except Exception as e:
         out["bmw_error"] = repr(e)
+    try:
+        # Iterator::Checkerboard4 rounds (1 HB + 4 OR) at 32^4 with the Wilson and the
+        # Luescher-Weisz (rectangle) actions, the reference driver's iterator
+        ext = (32,) * 4
+        G = lt.GaugeField(ext, prec)
+        G.SetToHaarRandom(17)
+        for name, act in (("wilson", None), ("luescher_weisz", lt.LuescherWeiszAction(BETA))):
+            lt.UpdateSweeps4(G, BETA, 2, 1, 4, SEED, 0, act)
+            n = 3
+            ms = timed(G, lambda: lt.UpdateSweeps4(G, BETA, n, 1, 4, SEED, 0, act), 1)
+            out[f"checkerboard4_{name}_link_updates_per_s_32^4"] = n * 5 * 4 * G.Volume() / (ms / 1000.0)
+        del G
+    except Exception as e:
+        out["checkerboard4_error"] = repr(e)
     try:
         # the driver's measurement step at 32^4 (clover Q and E per timeslice, plaquette, plaquette
         # charge, Symanzik action, Wilson loops L = 2, 4, 8, Polyakov loop) from the given storage,

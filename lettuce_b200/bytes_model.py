@@ -12,7 +12,8 @@ job), so DRAM traffic measured by ncu above these figures means wasted re-reads.
   3 (read U + write U) + 2 Z writes + 2 Z reads = 6 b + 4 b_alg per link.
 * clover Q / E, plaquette: every link read once: 4 b per site.
 * metadynamics force through n stout levels (forward 2 n b, clover + derivative about 3.5 b,
-  backward about 4.9 b per level): (6.9 n + 3.5) b per link.
+  backward about 4.9 b per level): (6.9 n + 3.5) b per link, about 70k flops per link for
+  n = 4.
 
 Flops use 198 real flops per 3x3 complex product (27 complex multiplies at 6 flops plus 18
 complex additions at 2): staple about 2.5k, heatbath about 4.0k and overrelaxation about
@@ -23,7 +24,8 @@ from __future__ import annotations
 LINK_BYTES = {"fp64": 144, "fp32": 72, "fp32_12": 48}
 ALG_BYTES = {"fp64": 64, "fp32": 32, "fp32_12": 32}
 
-FLOPS = {"overrelax": 3.9e3, "heatbath": 4.0e3, "flow_step": 10.0e3, "clover_site": 15.0e3}
+FLOPS = {"overrelax": 3.9e3, "heatbath": 4.0e3, "flow_step": 10.0e3, "clover_site": 15.0e3,
+         "metad_force_n4": 70.0e3}
 
 
 def sweep_bytes_per_update(prec: str) -> int:

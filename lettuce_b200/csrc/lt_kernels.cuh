@@ -45,6 +45,11 @@ template <typename T, int NR> struct HbMinBlocks
 {
     static constexpr int value = (sizeof(T) == 4 && NR == 2) ? LT_MINB_HB_F32C : MinBlocks<T>::sweep;
 };
+// Checkerboard4 sub-sweeps (Wilson action) carry the sublattice enumeration on top
+template <typename T, int NR> struct Cb4MinBlocks
+{
+    static constexpr int value = (sizeof(T) == 4 && NR == 2) ? 5 : MinBlocks<T>::sweep;
+};
 // link-parallel kernels: two-row FP32 storage has its own setting
 template <typename T, int NR> struct LinkMinBlocks
 {
@@ -570,26 +575,29 @@ __global__ void __launch_bounds__(kRedThreads) k_check_links(Gauge<T, NR> U, Geo
 }
 
 // ---------------------------------------------------------------- rectangular actions
-// Full index of x + dm mu + dn nu (periodic) for the site x with coordinates c
-LT_D int site_at(const Geom& g, const int c[4], int mu, int dm, int nu, int dn)
+// Full-index offset of a shift by d (|d| <= 2) along direction a of the site with coordinates c
+LT_D int shift_offset(const Geom& g, const int c[4], int a, int d)
 {
-    int cc[4] = { c[0], c[1], c[2], c[3] };
-    cc[mu] += dm;
-    cc[mu] += cc[mu] < 0 ? g.n[mu] : cc[mu] >= g.n[mu] ? -g.n[mu] : 0;
-    cc[nu] += dn;
-    cc[nu] += cc[nu] < 0 ? g.n[nu] : cc[nu] >= g.n[nu] ? -g.n[nu] : 0;
-    return ((cc[0] * g.n[1] + cc[1]) * g.n[2] + cc[2]) * g.n[3] + cc[3];
+    const int n = pick4(g.n, a), x = pick4(c, a) + d;
+    const int w = x < 0 ? n : x >= n ? -n : 0;
+    return (d + w) * pick4(g.stride, a);
+}
+
+// Full index of x + dm mu + dn nu (periodic) for the site x = i with coordinates c
+LT_D int site_at(const Geom& g, int i, const int c[4], int mu, int dm, int nu, int dn)
+{
+    return i + shift_offset(g, c, mu, dm) + shift_offset(g, c, nu, dn);
 }
 
 // Rectangular<2>::StapleRect (actions/gauge/rectangular_action.hpp:187-233): for each
 // nu = mu+1, mu+2, mu+3 (mod 4), the 1x2 loops orthogonal to the link (up and down) and the
 // 2x1 loops along it that start at x and at x - mu, each with U_mu(x) removed.
 template <typename T, int NR>
-LT_D M3<T> staple_rect(const Gauge<T, NR>& U, const Geom& g, int par, const int c[4], int mu)
+LT_D M3<T> staple_rect(const Gauge<T, NR>& U, const Geom& g, int par, int i, const int c[4], int mu)
 {
     // link U_d at x + dm mu + dn nu
     auto L = [&](int d, int nu, int dm, int dn) -> M3<T> {
-        const int j = site_at(g, c, mu, dm, nu, dn);
+        const int j = site_at(g, i, c, mu, dm, nu, dn);
         return U.ld(d, par ^ ((dm + dn) & 1), j >> 1);
     };
     M3<T> st = zero3<T>();
@@ -626,7 +634,7 @@ LT_D M3<T> action_staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, c
     if constexpr (RECT)
     {
         M3<T> st = cp * staple(U, g, par, i, c, mu);
-        acc(st, cr * staple_rect(U, g, par, c, mu));
+        acc(st, cr * staple_rect(U, g, par, i, c, mu));
         return st;
     }
     else
@@ -732,7 +740,7 @@ __global__ void __launch_bounds__(kThreads, (OrMinBlocks<T, NR>::value)) k_overr
 
 // One (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the handle's action
 template <typename T, int NR, bool RECT>
-__global__ void __launch_bounds__(kThreads) k_overrelax4(Gauge<T, NR> U, Geom g, int mu, int sub, T cp, T cr)
+__global__ void __launch_bounds__(kThreads, (RECT ? 1 : Cb4MinBlocks<T, NR>::value)) k_overrelax4(Gauge<T, NR> U, Geom g, int mu, int sub, T cp, T cr)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_release();
@@ -874,7 +882,7 @@ LT_D void hb_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s
 
 // One (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the handle's action
 template <typename T, int NR, bool RECT>
-__global__ void __launch_bounds__(kThreads) k_heatbath4(Gauge<T, NR> U, Geom g, int mu, int sub, T prefactor,
+__global__ void __launch_bounds__(kThreads, (RECT ? 1 : Cb4MinBlocks<T, NR>::value)) k_heatbath4(Gauge<T, NR> U, Geom g, int mu, int sub, T prefactor,
                                                         uint64_t counter, uint32_t k0, uint32_t k1, int max_iter,
                                                         unsigned* status, T cp, T cr)
 {
