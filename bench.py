@@ -221,7 +221,10 @@ def secondary_rates(lt, torch, timed, prec):
     * metadynamics force evaluations/s at 16^4 (4 stout steps rho = 0.12, FP32 links);
     * tempering ensemble link updates/s: 8 streams of 12^4 plus 40 chains with extents drawn
       from {8,...,16}^4, beta in [5.8, 6.2], one batched round (1 HB + 4 OR) per step;
-    * one 48^4 HMC trajectory (OMF4, tau = 1, 20 steps, FP32 links, FP64 dH)."""
+    * BMW configuration files at 32^4 (device checksum pass, save and load);
+    * Iterator::Checkerboard4 rounds at 32^4 with the Wilson and the Luescher-Weisz actions;
+    * the driver's measurement step at 32^4;
+    * one 48^4 HMC trajectory (OMF4, tau = 1, 20 steps, FP32 links, FP64 dH) and the flow to t0."""
     import numpy as np
     out = {}
     try:
