@@ -31,16 +31,29 @@ constexpr unsigned kStatusHbCap = 4u;       // a heatbath subgroup update hit it
 
 struct Geom
 {
-    int n[4];       // Nt, Nx, Ny, Nz
-    int stride[4];  // full-index stride of each direction
-    int V;          // sites
-    int vh;         // sites per parity
+    int n[4];            // Nt, Nx, Ny, Nz
+    int stride[4];       // full-index stride of each direction
+    int V;               // sites
+    int vh;              // sites per parity
+    unsigned div_m[4];   // x / n[d] = umulhi(x, div_m[d]) >> div_s[d] for 0 <= x < 2^31
+    int div_s[4];
 };
 
 inline Geom make_geom(const int ext[4])
 {
     Geom g;
-    for (int d = 0; d < 4; ++d) g.n[d] = ext[d];
+    for (int d = 0; d < 4; ++d)
+    {
+        g.n[d] = ext[d];
+        // division by a run-time constant (Granlund-Montgomery): extents are >= 2, so with
+        // l = ceil(log2 n) >= 1, m = ceil(2^(31 + l) / n) < 2^32 and the error of
+        // x m / 2^(31 + l) stays below 1/n for x < 2^31
+        const unsigned n = (unsigned)(ext[d] > 2 ? ext[d] : 2);
+        int l = 1;
+        while ((1ull << l) < n) ++l;
+        g.div_m[d] = (unsigned)(((1ull << (31 + l)) + n - 1) / n);
+        g.div_s[d] = l - 1;
+    }
     g.stride[3] = 1;
     g.stride[2] = ext[3];
     g.stride[1] = ext[2] * ext[3];
@@ -50,15 +63,18 @@ inline Geom make_geom(const int ext[4])
     return g;
 }
 
+// x / n[d] for 0 <= x < 2^31 without a hardware division
+LT_D int div_by(const Geom& g, int x, int d) { return (int)(__umulhi((unsigned)x, g.div_m[d]) >> g.div_s[d]); }
+
 // Coordinates and full index of checkerboard site s of parity par
 LT_D int site_coords(const Geom& g, int par, int s, int c[4])
 {
     int i0 = 2 * s;
-    int r = i0 / g.n[3];
+    int r = div_by(g, i0, 3);
     int z0 = i0 - r * g.n[3];
-    int r2 = r / g.n[2];
+    int r2 = div_by(g, r, 2);
     c[2] = r - r2 * g.n[2];
-    int r3 = r2 / g.n[1];
+    int r3 = div_by(g, r2, 1);
     c[1] = r2 - r3 * g.n[1];
     c[0] = r3;
     c[3] = z0 + ((c[0] + c[1] + c[2] + par) & 1);

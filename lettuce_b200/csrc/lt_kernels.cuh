@@ -1141,13 +1141,12 @@ __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> Ust, Ge
 // Coordinates and parity of the site with full index i
 LT_D int coords_of(const Geom& g, int i, int c[4])
 {
-    int r = i;
-    c[3] = r % g.n[3];
-    r /= g.n[3];
-    c[2] = r % g.n[2];
-    r /= g.n[2];
-    c[1] = r % g.n[1];
-    c[0] = r / g.n[1];
+    const int r = div_by(g, i, 3);
+    c[3] = i - r * g.n[3];
+    const int r2 = div_by(g, r, 2);
+    c[2] = r - r2 * g.n[2];
+    c[0] = div_by(g, r2, 1);
+    c[1] = r2 - c[0] * g.n[1];
     return (c[0] + c[1] + c[2] + c[3]) & 1;
 }
 
