@@ -647,22 +647,23 @@ LT_D M3<T> action_staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, c
 // z per (t, x, y) row, for mu = z a stride-2 run on the rows with t + x + y = sub (mod 2).
 LT_D int cb4_site(const Geom& g, int mu, int sub, int k, int c[4])
 {
+    // divisions by n/4 and n/2 as floor(4x / n) and floor(2x / n) (4 V < 2^31)
     if (mu != 3)
     {
-        const int nz = g.n[3] >> 2, row = k / nz, j = k - row * nz;
-        c[2] = row % g.n[2];
-        const int r2 = row / g.n[2];
-        c[1] = r2 % g.n[1];
-        c[0] = r2 / g.n[1];
-        const int z0 = (sub - c[0] - c[1] - c[2] - c[mu]) & 3;
+        const int nz = g.n[3] >> 2, row = div_by(g, 4 * k, 3), j = k - row * nz;
+        const int r2 = div_by(g, row, 2);
+        c[2] = row - r2 * g.n[2];
+        c[0] = div_by(g, r2, 1);
+        c[1] = r2 - c[0] * g.n[1];
+        const int z0 = (sub - c[0] - c[1] - c[2] - pick4(c, mu)) & 3;
         c[3] = z0 + 4 * j;
     }
     else
     {
-        const int nz = g.n[3] >> 1, row = k / nz, j = k - row * nz;
-        const int ny = g.n[2] >> 1, m = row % ny, q = row / ny;
-        c[1] = q % g.n[1];
-        c[0] = q / g.n[1];
+        const int nz = g.n[3] >> 1, row = div_by(g, 2 * k, 3), j = k - row * nz;
+        const int ny = g.n[2] >> 1, q = div_by(g, 2 * row, 2), m = row - q * ny;
+        c[0] = div_by(g, q, 1);
+        c[1] = q - c[0] * g.n[1];
         c[2] = 2 * m + ((sub - c[0] - c[1]) & 1);
         const int z0 = ((sub - c[0] - c[1] - c[2]) & 3) >> 1;
         c[3] = z0 + 2 * j;
