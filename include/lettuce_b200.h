@@ -11,10 +11,11 @@
  * double[V][4][3][3][2]: site index ((t*Nx + x)*Ny + y)*Nz + z, direction mu fastest,
  * row-major 3x3, real/imaginary interleaved (LettuceGauge/lattice.hpp:366-382).
  *
- * Threading: every lattice handle owns one CUDA stream; calls on one handle are
- * serialised by the caller; distinct handles may be driven from distinct host threads.
- * Calls that return a host value synchronise the handle's stream.  No device wait in this
- * library spins without a bound.
+ * Threading: every lattice handle owns one CUDA stream on the device that was current when
+ * it was created; each call runs on that device and restores the caller's current device.
+ * Calls on one handle are serialised by the caller; distinct handles may be driven from
+ * distinct host threads.  Calls that return a host value synchronise the handle's stream.
+ * No device wait in this library spins without a bound.
  */
 #ifndef LETTUCE_B200_H
 #define LETTUCE_B200_H

@@ -90,6 +90,7 @@ extern "C" {
 int lt_bmw_checksum(lt_lattice* h, int full, uint64_t* checksum)
 {
     LT_TRY(check_h(h, "lt_bmw_checksum"));
+    const lt::DeviceScope device_scope(h->device);
     if (!checksum) return lt::set_error(LT_ERR_ARG, "lt_bmw_checksum: null pointer");
     return pack(h, full ? 1 : 0, false, checksum);
 }
@@ -97,6 +98,7 @@ int lt_bmw_checksum(lt_lattice* h, int full, uint64_t* checksum)
 int lt_save_bmw(lt_lattice* h, const char* path, int full, int overwrite, char* checksum_hex)
 {
     LT_TRY(check_h(h, "lt_save_bmw"));
+    const lt::DeviceScope device_scope(h->device);
     if (!path) return lt::set_error(LT_ERR_ARG, "lt_save_bmw: null path");
     full = full ? 1 : 0;
     if (!overwrite)
@@ -139,6 +141,7 @@ int lt_save_bmw(lt_lattice* h, const char* path, int full, int overwrite, char* 
 int lt_load_bmw(lt_lattice* h, const char* path, int full, int* checksum_ok, int* in_group)
 {
     LT_TRY(check_h(h, "lt_load_bmw"));
+    const lt::DeviceScope device_scope(h->device);
     if (!path) return lt::set_error(LT_ERR_ARG, "lt_load_bmw: null path");
     full = full ? 1 : 0;
     File file;

@@ -40,7 +40,6 @@ int check_h(const lt_lattice* h, const char* fn)
 int ensure(lt_lattice* h, void** p, size_t bytes)
 {
     if (*p) return LT_OK;
-    LT_CK(cudaSetDevice(h->device));
     LT_CK(cudaMalloc(p, bytes));
     return LT_OK;
 }
@@ -503,7 +502,7 @@ int lt_create(const int ext[4], int prec, lt_lattice** out)
 int lt_destroy(lt_lattice* h)
 {
     if (!h) return LT_OK;
-    cudaSetDevice(h->device);
+    const lt::DeviceScope device_scope(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,  h->R,      h->chainA,
                      h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB };
@@ -519,6 +518,7 @@ int lt_destroy(lt_lattice* h)
 int lt_get_extents(const lt_lattice* h, int ext[4], int* prec)
 {
     LT_TRY(check_h(h, "lt_get_extents"));
+    const lt::DeviceScope device_scope(h->device);
     if (ext) std::memcpy(ext, h->ext, sizeof(h->ext));
     if (prec) *prec = h->prec;
     return LT_OK;
@@ -527,6 +527,7 @@ int lt_get_extents(const lt_lattice* h, int ext[4], int* prec)
 int lt_upload_links(lt_lattice* h, const double* links)
 {
     LT_TRY(check_h(h, "lt_upload_links"));
+    const lt::DeviceScope device_scope(h->device);
     if (!links) return lt::set_error(LT_ERR_ARG, "lt_upload_links: null pointer");
     LT_TRY(ensure_aos(h));
     LT_CK(cudaMemcpyAsync(h->d_aos, links, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyHostToDevice,
@@ -540,6 +541,7 @@ int lt_upload_links(lt_lattice* h, const double* links)
 int lt_download_links(lt_lattice* h, double* links)
 {
     LT_TRY(check_h(h, "lt_download_links"));
+    const lt::DeviceScope device_scope(h->device);
     if (!links) return lt::set_error(LT_ERR_ARG, "lt_download_links: null pointer");
     LT_TRY(ensure_aos(h));
     h->be->to_aos(h->ctx(), h->U, h->d_aos);
@@ -566,12 +568,14 @@ static int link_access(lt_lattice* h, int64_t site, int mu, double* m, int write
 int lt_set_link(lt_lattice* h, int64_t site, int mu, const double* m)
 {
     LT_TRY(check_h(h, "lt_set_link"));
+    const lt::DeviceScope device_scope(h->device);
     return link_access(h, site, mu, const_cast<double*>(m), 1);
 }
 
 int lt_get_link(lt_lattice* h, int64_t site, int mu, double* m_out)
 {
     LT_TRY(check_h(h, "lt_get_link"));
+    const lt::DeviceScope device_scope(h->device);
     return link_access(h, site, mu, m_out, 0);
 }
 
@@ -579,6 +583,7 @@ int lt_copy(lt_lattice* dst, const lt_lattice* src)
 {
     LT_TRY(check_h(dst, "lt_copy"));
     LT_TRY(check_h(src, "lt_copy"));
+    const lt::DeviceScope device_scope(dst->device);
     if (dst == src) return LT_OK;
     if (std::memcmp(dst->ext, src->ext, sizeof(dst->ext)))
         return lt::set_error(LT_ERR_ARG, "lt_copy: extents differ");
@@ -603,6 +608,7 @@ int lt_swap(lt_lattice* a, lt_lattice* b)
 {
     LT_TRY(check_h(a, "lt_swap"));
     LT_TRY(check_h(b, "lt_swap"));
+    const lt::DeviceScope device_scope(a->device);
     if (std::memcmp(a->ext, b->ext, sizeof(a->ext)) || a->prec != b->prec)
         return lt::set_error(LT_ERR_ARG, "lt_swap: extents or formats differ");
     LT_CK(cudaStreamSynchronize(a->stream));
@@ -614,6 +620,7 @@ int lt_swap(lt_lattice* a, lt_lattice* b)
 int lt_set_identity(lt_lattice* h)
 {
     LT_TRY(check_h(h, "lt_set_identity"));
+    const lt::DeviceScope device_scope(h->device);
     h->be->set_unit(h->ctx(), h->U);
     return launched("lt_set_identity");
 }
@@ -621,6 +628,7 @@ int lt_set_identity(lt_lattice* h)
 int lt_set_haar_random(lt_lattice* h, uint64_t seed)
 {
     LT_TRY(check_h(h, "lt_set_haar_random"));
+    const lt::DeviceScope device_scope(h->device);
     std::vector<double> buf;
     try
     {
@@ -637,6 +645,7 @@ int lt_set_haar_random(lt_lattice* h, uint64_t seed)
 int lt_synchronize(lt_lattice* h)
 {
     LT_TRY(check_h(h, "lt_synchronize"));
+    const lt::DeviceScope device_scope(h->device);
     LT_CK(cudaStreamSynchronize(h->stream));
     return LT_OK;
 }
@@ -644,6 +653,7 @@ int lt_synchronize(lt_lattice* h)
 int lt_get_stream(const lt_lattice* h, void** stream_out)
 {
     LT_TRY(check_h(h, "lt_get_stream"));
+    const lt::DeviceScope device_scope(h->device);
     if (!stream_out) return lt::set_error(LT_ERR_ARG, "lt_get_stream: null pointer");
     *stream_out = (void*)h->stream;
     return LT_OK;
@@ -656,6 +666,7 @@ static_assert(LT_STATUS_NONFINITE == lt::kStatusNonFinite && LT_STATUS_UNITARITY
 int lt_status_word(lt_lattice* h, uint32_t* word, int clear)
 {
     LT_TRY(check_h(h, "lt_status_word"));
+    const lt::DeviceScope device_scope(h->device);
     if (!word) return lt::set_error(LT_ERR_ARG, "lt_status_word: null pointer");
     LT_CK(cudaMemcpyAsync(h->h_results, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
     if (clear) LT_CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream));
@@ -669,6 +680,7 @@ int lt_status_word(lt_lattice* h, uint32_t* word, int clear)
 int lt_check_links(lt_lattice* h, double* max_dev)
 {
     LT_TRY(check_h(h, "lt_check_links"));
+    const lt::DeviceScope device_scope(h->device);
     unsigned* maxbits = h->status + 1;
     LT_CK(cudaMemsetAsync(maxbits, 0, sizeof(unsigned), h->stream));
     const double tol = h->be->real_bytes() == 8 ? 1e-10 : 1e-4;
@@ -686,6 +698,7 @@ int lt_check_links(lt_lattice* h, double* max_dev)
 int lt_plaquette_sum(lt_lattice* h, double* out)
 {
     LT_TRY(check_h(h, "lt_plaquette_sum"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_plaquette_sum: null pointer");
     return plaq_of(h, h->U, out);
 }
@@ -693,6 +706,7 @@ int lt_plaquette_sum(lt_lattice* h, double* out)
 int lt_wilson_action(lt_lattice* h, double beta, double* out)
 {
     LT_TRY(check_h(h, "lt_wilson_action"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_wilson_action: null pointer");
     double p;
     LT_TRY(plaq_of(h, h->U, &p));
@@ -703,6 +717,7 @@ int lt_wilson_action(lt_lattice* h, double beta, double* out)
 int lt_topcharge_clover(lt_lattice* h, double* out)
 {
     LT_TRY(check_h(h, "lt_topcharge_clover"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_topcharge_clover: null pointer");
     return clover_q_e(h, h->U, out, nullptr);
 }
@@ -710,6 +725,7 @@ int lt_topcharge_clover(lt_lattice* h, double* out)
 int lt_energy_clover(lt_lattice* h, double* out)
 {
     LT_TRY(check_h(h, "lt_energy_clover"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_energy_clover: null pointer");
     return clover_q_e(h, h->U, nullptr, out);
 }
@@ -717,6 +733,7 @@ int lt_energy_clover(lt_lattice* h, double* out)
 int lt_clover_timeslices(lt_lattice* h, double* q_t, double* e_t)
 {
     LT_TRY(check_h(h, "lt_clover_timeslices"));
+    const lt::DeviceScope device_scope(h->device);
     if (!q_t && !e_t) return lt::set_error(LT_ERR_ARG, "lt_clover_timeslices: null pointers");
     const int nt = h->g.n[0];
     const int nbx = std::max(1, std::min(lt::kRedBlocks / nt, (h->g.V / nt + lt::kRedThreads - 1) / lt::kRedThreads));
@@ -749,6 +766,7 @@ int lt_clover_timeslices(lt_lattice* h, double* q_t, double* e_t)
 int lt_topcharge_plaquette(lt_lattice* h, double* out)
 {
     LT_TRY(check_h(h, "lt_topcharge_plaquette"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_topcharge_plaquette: null pointer");
     h->be->loops(h->ctx(), h->U, 4);
     double r[3];
@@ -760,6 +778,7 @@ int lt_topcharge_plaquette(lt_lattice* h, double* out)
 int lt_rect_action(lt_lattice* h, double beta, double c_plaq, double c_rect, double* out)
 {
     LT_TRY(check_h(h, "lt_rect_action"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_rect_action: null pointer");
     h->be->loops(h->ctx(), h->U, 4);
     double r[3];
@@ -772,6 +791,7 @@ int lt_rect_action(lt_lattice* h, double beta, double c_plaq, double c_rect, dou
 int lt_wilson_loop(lt_lattice* h, int L, double* out)
 {
     LT_TRY(check_h(h, "lt_wilson_loop"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out || L < 1) return lt::set_error(LT_ERR_ARG, "lt_wilson_loop: null pointer or L < 1");
     const size_t bytes = (size_t)4 * h->g.V * 9 * 2 * sizeof(double);
     LT_TRY(ensure(h, &h->chainA, bytes));
@@ -801,6 +821,7 @@ int lt_wilson_loop(lt_lattice* h, int L, double* out)
 int lt_polyakov_loop(lt_lattice* h, double* re, double* im)
 {
     LT_TRY(check_h(h, "lt_polyakov_loop"));
+    const lt::DeviceScope device_scope(h->device);
     if (!re || !im) return lt::set_error(LT_ERR_ARG, "lt_polyakov_loop: null pointer");
     h->be->polyakov(h->ctx(), h->U, 0);
     double r[2];
@@ -814,12 +835,14 @@ int lt_polyakov_loop(lt_lattice* h, double* re, double* im)
 int lt_clover_observables(lt_lattice* h, double* q_out, double* e_out)
 {
     LT_TRY(check_h(h, "lt_clover_observables"));
+    const lt::DeviceScope device_scope(h->device);
     return clover_q_e(h, h->U, q_out, e_out);
 }
 
 int lt_staples(lt_lattice* h, double* staples_out)
 {
     LT_TRY(check_h(h, "lt_staples"));
+    const lt::DeviceScope device_scope(h->device);
     if (!staples_out) return lt::set_error(LT_ERR_ARG, "lt_staples: null pointer");
     LT_TRY(ensure_aos(h));
     h->be->staples_aos(h->ctx(), h->U, h->d_aos);
@@ -834,6 +857,7 @@ int lt_staples(lt_lattice* h, double* staples_out)
 int lt_set_gauge_action(lt_lattice* h, int stencil_radius, double c_plaq, double c_rect)
 {
     LT_TRY(check_h(h, "lt_set_gauge_action"));
+    const lt::DeviceScope device_scope(h->device);
     if ((stencil_radius != 1 && stencil_radius != 2) || !std::isfinite(c_plaq) || !std::isfinite(c_rect))
         return lt::set_error(LT_ERR_ARG, "lt_set_gauge_action: stencil radius 1 or 2 and finite coefficients");
     h->act_radius = stencil_radius;
@@ -845,6 +869,7 @@ int lt_set_gauge_action(lt_lattice* h, int stencil_radius, double c_plaq, double
 int lt_get_gauge_action(lt_lattice* h, int* stencil_radius, double* c_plaq, double* c_rect)
 {
     LT_TRY(check_h(h, "lt_get_gauge_action"));
+    const lt::DeviceScope device_scope(h->device);
     if (stencil_radius) *stencil_radius = h->act_radius;
     if (c_plaq) *c_plaq = h->act_cp;
     if (c_rect) *c_rect = h->act_cr;
@@ -854,6 +879,7 @@ int lt_get_gauge_action(lt_lattice* h, int* stencil_radius, double* c_plaq, doub
 int lt_overrelax_sweeps(lt_lattice* h, int n_sweep)
 {
     LT_TRY(check_h(h, "lt_overrelax_sweeps"));
+    const lt::DeviceScope device_scope(h->device);
     if (n_sweep < 0) return lt::set_error(LT_ERR_ARG, "lt_overrelax_sweeps: n_sweep < 0");
     if (h->act_radius == 2)
         return lt::set_error(LT_ERR_ARG, "lt_overrelax_sweeps: a rectangular action needs Checkerboard4 (lt_overrelax_sweeps4)");
@@ -867,6 +893,7 @@ int lt_overrelax_sweeps(lt_lattice* h, int n_sweep)
 int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, uint64_t* counter)
 {
     LT_TRY(check_h(h, "lt_heatbath_sweeps"));
+    const lt::DeviceScope device_scope(h->device);
     if (n_sweep < 0 || !counter || !(beta > 0.0))
         return lt::set_error(LT_ERR_ARG, "lt_heatbath_sweeps: bad arguments");
     if (h->act_radius == 2)
@@ -884,6 +911,7 @@ int lt_heatbath_sweeps(lt_lattice* h, double beta, int n_sweep, uint64_t seed, u
 int lt_update_sweeps(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed, uint64_t* counter)
 {
     LT_TRY(check_h(h, "lt_update_sweeps"));
+    const lt::DeviceScope device_scope(h->device);
     if (n_sweep < 0 || n_hb < 0 || n_or < 0 || !counter || !(beta > 0.0))
         return lt::set_error(LT_ERR_ARG, "lt_update_sweeps: bad arguments");
     for (int s = 0; s < n_sweep; ++s)
@@ -905,6 +933,7 @@ static int check_cb4(const lt_lattice* h, const char* fn)
 int lt_overrelax_sweeps4(lt_lattice* h, int n_sweep)
 {
     LT_TRY(check_h(h, "lt_overrelax_sweeps4"));
+    const lt::DeviceScope device_scope(h->device);
     if (n_sweep < 0) return lt::set_error(LT_ERR_ARG, "lt_overrelax_sweeps4: n_sweep < 0");
     LT_TRY(check_cb4(h, "lt_overrelax_sweeps4"));
     const lt::Ctx c = h->ctx();
@@ -917,6 +946,7 @@ int lt_overrelax_sweeps4(lt_lattice* h, int n_sweep)
 int lt_heatbath_sweeps4(lt_lattice* h, double beta, int n_sweep, uint64_t seed, uint64_t* counter)
 {
     LT_TRY(check_h(h, "lt_heatbath_sweeps4"));
+    const lt::DeviceScope device_scope(h->device);
     if (n_sweep < 0 || !counter || !(beta > 0.0))
         return lt::set_error(LT_ERR_ARG, "lt_heatbath_sweeps4: bad arguments");
     LT_TRY(check_cb4(h, "lt_heatbath_sweeps4"));
@@ -933,6 +963,7 @@ int lt_heatbath_sweeps4(lt_lattice* h, double beta, int n_sweep, uint64_t seed, 
 int lt_update_sweeps4(lt_lattice* h, double beta, int n_sweep, int n_hb, int n_or, uint64_t seed, uint64_t* counter)
 {
     LT_TRY(check_h(h, "lt_update_sweeps4"));
+    const lt::DeviceScope device_scope(h->device);
     if (n_sweep < 0 || n_hb < 0 || n_or < 0 || !counter || !(beta > 0.0))
         return lt::set_error(LT_ERR_ARG, "lt_update_sweeps4: bad arguments");
     for (int s = 0; s < n_sweep; ++s)
@@ -948,6 +979,7 @@ int lt_flow_rk3(lt_lattice* in, lt_lattice* out, double eps, int n_step)
 {
     LT_TRY(check_h(in, "lt_flow_rk3"));
     LT_TRY(check_h(out, "lt_flow_rk3"));
+    const lt::DeviceScope device_scope(in->device);
     if (n_step < 0) return lt::set_error(LT_ERR_ARG, "lt_flow_rk3: n_step < 0");
     LT_TRY(lt_copy(out, in));
     return flow_steps(out, eps, n_step);
@@ -957,6 +989,7 @@ int lt_flow(lt_lattice* in, lt_lattice* out, int integrator, double eps, int n_s
 {
     LT_TRY(check_h(in, "lt_flow"));
     LT_TRY(check_h(out, "lt_flow"));
+    const lt::DeviceScope device_scope(in->device);
     if (n_step < 0 || integrator < LT_FLOW_EULER || integrator > LT_FLOW_RK3W7)
         return lt::set_error(LT_ERR_ARG, "lt_flow: n_step < 0 or unknown integrator");
     LT_TRY(lt_copy(out, in));
@@ -968,6 +1001,7 @@ int lt_flow_rk3_measure(lt_lattice* in, lt_lattice* out, double eps, int n_meas,
 {
     LT_TRY(check_h(in, "lt_flow_rk3_measure"));
     LT_TRY(check_h(out, "lt_flow_rk3_measure"));
+    const lt::DeviceScope device_scope(in->device);
     if (n_meas < 0 || every < 0) return lt::set_error(LT_ERR_ARG, "lt_flow_rk3_measure: negative count");
     LT_TRY(lt_copy(out, in));
     for (int m = 0; m < n_meas; ++m)
@@ -985,6 +1019,7 @@ int lt_flow_t0(lt_lattice* in, lt_lattice* out, double eps, double target, int m
 {
     LT_TRY(check_h(in, "lt_flow_t0"));
     LT_TRY(check_h(out, "lt_flow_t0"));
+    const lt::DeviceScope device_scope(in->device);
     if (!t0_out || !(eps > 0.0) || max_steps < 1) return lt::set_error(LT_ERR_ARG, "lt_flow_t0: bad arguments");
     LT_TRY(lt_copy(out, in));
     double t_prev = 0.0, y_prev = 0.0, q = 0.0, e = 0.0;
@@ -1010,6 +1045,7 @@ int lt_stout(lt_lattice* in, lt_lattice* out, double rho, int n)
 {
     LT_TRY(check_h(in, "lt_stout"));
     LT_TRY(check_h(out, "lt_stout"));
+    const lt::DeviceScope device_scope(in->device);
     if (n < 0) return lt::set_error(LT_ERR_ARG, "lt_stout: n < 0");
     LT_TRY(lt_copy(out, in));
     return stout_steps(out, rho, n);
@@ -1019,6 +1055,7 @@ int lt_stout(lt_lattice* in, lt_lattice* out, double rho, int n)
 int lt_gauge_force(lt_lattice* h, double beta, double* force_out)
 {
     LT_TRY(check_h(h, "lt_gauge_force"));
+    const lt::DeviceScope device_scope(h->device);
     if (!force_out) return lt::set_error(LT_ERR_ARG, "lt_gauge_force: null pointer");
     LT_TRY(ensure(h, &h->F, h->be->alg_bytes(h->g)));
     LT_CK(cudaMemsetAsync(h->F, 0, h->be->alg_bytes(h->g), h->stream));
@@ -1035,6 +1072,7 @@ int lt_gauge_force(lt_lattice* h, double beta, double* force_out)
 int lt_set_momenta(lt_lattice* h, const double* p)
 {
     LT_TRY(check_h(h, "lt_set_momenta"));
+    const lt::DeviceScope device_scope(h->device);
     if (!p) return lt::set_error(LT_ERR_ARG, "lt_set_momenta: null pointer");
     LT_TRY(ensure(h, &h->P, h->be->alg_bytes(h->g)));
     LT_TRY(ensure_aos(h));
@@ -1048,6 +1086,7 @@ int lt_set_momenta(lt_lattice* h, const double* p)
 int lt_get_momenta(lt_lattice* h, double* p_out)
 {
     LT_TRY(check_h(h, "lt_get_momenta"));
+    const lt::DeviceScope device_scope(h->device);
     if (!p_out) return lt::set_error(LT_ERR_ARG, "lt_get_momenta: null pointer");
     if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_get_momenta: no momenta set");
     LT_TRY(ensure_aos(h));
@@ -1062,6 +1101,7 @@ int lt_get_momenta(lt_lattice* h, double* p_out)
 int lt_random_momenta(lt_lattice* h, uint64_t seed, uint64_t counter)
 {
     LT_TRY(check_h(h, "lt_random_momenta"));
+    const lt::DeviceScope device_scope(h->device);
     LT_TRY(ensure(h, &h->P, h->be->alg_bytes(h->g)));
     h->be->random_momenta(h->ctx(), h->P, counter, seed);
     return launched("lt_random_momenta");
@@ -1070,6 +1110,7 @@ int lt_random_momenta(lt_lattice* h, uint64_t seed, uint64_t counter)
 int lt_hamiltonian(lt_lattice* h, double beta, double* out)
 {
     LT_TRY(check_h(h, "lt_hamiltonian"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_hamiltonian: null pointer");
     if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_hamiltonian: no momenta set");
     return hamiltonian(h, beta, out);
@@ -1078,6 +1119,7 @@ int lt_hamiltonian(lt_lattice* h, double beta, double* out)
 int lt_omf2(lt_lattice* h, double beta, double tau, int n_step, double* h_old, double* h_new)
 {
     LT_TRY(check_h(h, "lt_omf2"));
+    const lt::DeviceScope device_scope(h->device);
     if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_omf2: no momenta set");
     if (h_old) LT_TRY(hamiltonian(h, beta, h_old));
     LT_TRY(omf2(h, beta, tau, n_step, nullptr));
@@ -1095,6 +1137,7 @@ int lt_hmc_trajectory(lt_lattice* h, double beta, double tau, int n_step, uint64
 int lt_reverse_momenta(lt_lattice* h)
 {
     LT_TRY(check_h(h, "lt_reverse_momenta"));
+    const lt::DeviceScope device_scope(h->device);
     if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_reverse_momenta: no momenta set");
     h->be->alg_axpby(h->ctx(), h->P, nullptr, -1.0, 0.0);
     return launched("lt_reverse_momenta");
@@ -1103,6 +1146,7 @@ int lt_reverse_momenta(lt_lattice* h)
 int lt_parity_update(lt_lattice* h)
 {
     LT_TRY(check_h(h, "lt_parity_update"));
+    const lt::DeviceScope device_scope(h->device);
     LT_TRY(ensure(h, &h->U2, h->be->gauge_bytes(h->g)));
     h->be->parity(h->ctx(), h->U, h->U2);
     std::swap(h->U, h->U2);
@@ -1113,6 +1157,7 @@ int lt_parity_update(lt_lattice* h)
 int lt_clover_derivative(lt_lattice* h, double* out)
 {
     LT_TRY(check_h(h, "lt_clover_derivative"));
+    const lt::DeviceScope device_scope(h->device);
     if (!out) return lt::set_error(LT_ERR_ARG, "lt_clover_derivative: null pointer");
     LT_TRY(metad_backward(h, 0.0, 0, 1.0));
     LT_TRY(ensure_aos(h));
@@ -1126,6 +1171,7 @@ int lt_clover_derivative(lt_lattice* h, double* out)
 int lt_metad_charge(lt_lattice* h, double rho, int n_stout, double* q_out)
 {
     LT_TRY(check_h(h, "lt_metad_charge"));
+    const lt::DeviceScope device_scope(h->device);
     if (!q_out || n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_metad_charge: bad arguments");
     return metad_charge(h, rho, n_stout, q_out);
 }
@@ -1133,6 +1179,7 @@ int lt_metad_charge(lt_lattice* h, double rho, int n_stout, double* q_out)
 int lt_metad_force(lt_lattice* h, double rho, int n_stout, double dvdq, double* force_out, double* q_out)
 {
     LT_TRY(check_h(h, "lt_metad_force"));
+    const lt::DeviceScope device_scope(h->device);
     if (n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_metad_force: n_stout < 0");
     LT_TRY(metad_forward(h, rho, n_stout));
     if (q_out) LT_TRY(clover_q_e(h, level(h, n_stout), q_out, nullptr));
@@ -1153,6 +1200,7 @@ int lt_metad_omf2(lt_lattice* h, lt_bias* bias, double beta, double tau, int n_s
                   double* h_old, double* h_new)
 {
     LT_TRY(check_h(h, "lt_metad_omf2"));
+    const lt::DeviceScope device_scope(h->device);
     if (!bias) return lt::set_error(LT_ERR_ARG, "lt_metad_omf2: null bias");
     return lt_md_integrate(h, bias, LT_MD_OMF2, beta, tau, n_step, rho, n_stout, h_old, h_new);
 }
@@ -1162,6 +1210,7 @@ int lt_metad_hmc_trajectory(lt_lattice* h, lt_bias* bias, double beta, double ta
                             double* cv_out)
 {
     LT_TRY(check_h(h, "lt_metad_hmc_trajectory"));
+    const lt::DeviceScope device_scope(h->device);
     if (!bias) return lt::set_error(LT_ERR_ARG, "lt_metad_hmc_trajectory: null bias");
     return lt_md_trajectory(h, bias, LT_MD_OMF2, beta, tau, n_step, rho, n_stout, seed, counter, metropolis, dH,
                             accepted, cv_out);
@@ -1187,6 +1236,7 @@ int lt_md_integrate(lt_lattice* h, lt_bias* bias, int integrator, double beta, d
                     int n_stout, double* h_old, double* h_new)
 {
     LT_TRY(check_h(h, "lt_md_integrate"));
+    const lt::DeviceScope device_scope(h->device);
     if (!h->P) return lt::set_error(LT_ERR_STATE, "lt_md_integrate: no momenta set");
     if (bias && n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_md_integrate: n_stout < 0");
     LT_TRY(md_check(integrator, bias != nullptr, "lt_md_integrate"));
@@ -1206,6 +1256,7 @@ int lt_md_trajectory(lt_lattice* h, lt_bias* bias, int integrator, double beta, 
                      double* cv_out)
 {
     LT_TRY(check_h(h, "lt_md_trajectory"));
+    const lt::DeviceScope device_scope(h->device);
     if (!counter) return lt::set_error(LT_ERR_ARG, "lt_md_trajectory: null counter");
     if (bias && n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_md_trajectory: n_stout < 0");
     LT_TRY(md_check(integrator, bias != nullptr, "lt_md_trajectory"));

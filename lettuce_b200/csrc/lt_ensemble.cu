@@ -179,6 +179,10 @@ int lt_ensemble_create(lt_lattice* const* lattices, const double* betas, int n, 
         for (int j = 0; j < k; ++j)
             if (lattices[j] == lattices[k]) return lt::set_error(LT_ERR_ARG, "lt_ensemble_create: lattice listed twice");
     }
+    for (int k = 1; k < n; ++k)
+        if (lattices[k]->device != lattices[0]->device)
+            return lt::set_error(LT_ERR_ARG, "lt_ensemble_create: all lattices must live on one device");
+    const lt::DeviceScope device_scope(lattices[0]->device);
     auto* e = new (std::nothrow) lt_ensemble();
     if (!e) return lt::set_error(LT_ERR_NOMEM, "lt_ensemble_create: out of host memory");
     e->lats.assign(lattices, lattices + n);
@@ -209,6 +213,7 @@ int lt_ensemble_create(lt_lattice* const* lattices, const double* betas, int n, 
 int lt_ensemble_destroy(lt_ensemble* e)
 {
     if (!e) return LT_OK;
+    const lt::DeviceScope device_scope(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
     drop_graphs(e);
     if (e->d_desc) cudaFree(e->d_desc);
@@ -223,6 +228,7 @@ int lt_ensemble_sweeps(lt_ensemble* e, int n_sweep, int n_hb, int n_or, int reve
     if (!e || !counter || n_sweep < 0 || n_hb < 0 || n_or < 0)
         return lt::set_error(LT_ERR_ARG, "lt_ensemble_sweeps: bad arguments");
     if (n_sweep == 0 || n_hb + n_or == 0) return LT_OK;
+    const lt::DeviceScope device_scope(e->device);
     LT_TRY(join_in(e));
     LT_TRY(refresh(e));
     cudaGraphExec_t g;
@@ -239,6 +245,7 @@ int lt_ensemble_sweeps(lt_ensemble* e, int n_sweep, int n_hb, int n_or, int reve
 int lt_ensemble_autotune(lt_ensemble* e, int* threads_hb, int* threads_or)
 {
     if (!e) return lt::set_error(LT_ERR_ARG, "lt_ensemble_autotune: null ensemble");
+    const lt::DeviceScope device_scope(e->device);
     LT_TRY(join_in(e));
     LT_TRY(refresh(e));
     LT_CK(cudaStreamSynchronize(e->stream));

@@ -10,6 +10,23 @@
 namespace lt {
 // Records a CUDA error as this thread's last error; returns LT_ERR_NOMEM or LT_ERR_CUDA.
 int cuda_error(cudaError_t e, const char* what);
+
+// Makes a handle's device current for one C-ABI call and restores the caller's device after
+struct DeviceScope
+{
+    int prev = -1;
+    explicit DeviceScope(int dev)
+    {
+        int cur;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+};
 } // namespace lt
 
 #define LT_CK(call)                                                  \
