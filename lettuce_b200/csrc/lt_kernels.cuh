@@ -153,8 +153,8 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
     for (int nu = 0; nu < 4; ++nu)
     {
         if (nu == mu) continue;
-        const int inu = i + step_up(g, nu, c[nu]);
-        const int ind = i + step_dn(g, nu, c[nu]);
+        const int inu = i + step_up_rt(g, nu, c);
+        const int ind = i + step_dn_rt(g, nu, c);
         M3<T> up, dn;
 #ifdef LT_STAPLE_FULL_PRODUCTS
         if (false)
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(kRedThreads) k_plaquette(Gauge<T, NR> U, Geom 
 #pragma unroll
             for (int nu = mu + 1; nu < 4; ++nu)
             {
-                const int inu = i + step_up(g, nu, c[nu]);
+                const int inu = i + step_up_rt(g, nu, c);
                 // ReTr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag) = ReTr[(U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag]
                 M3<double> a = mul(umu, cvt<double>(U.ld(nu, op, imu >> 1)));
                 M3<double> b = mul(cvt<double>(U.ld(nu, par, s)), cvt<double>(U.ld(mu, op, inu >> 1)));
@@ -1050,7 +1050,7 @@ LT_D auto clover_leaves(const F& U, const Geom& g, int par, int i, const int c[4
     using M = decltype(U.ld(0, 0, 0));
     const int op = par ^ 1;
     const int dmu_p = step_up_rt(g, mu, c), dmu_m = step_dn_rt(g, mu, c);
-    const int dnu_p = step_up(g, nu, c[nu]), dnu_m = step_dn(g, nu, c[nu]);
+    const int dnu_p = step_up_rt(g, nu, c), dnu_m = step_dn_rt(g, nu, c);
     const int s = i >> 1;
     const M umu = U.ld(mu, par, s), unu = U.ld(nu, par, s);
     const int imd = i + dmu_m, ind = i + dnu_m;
@@ -1154,9 +1154,9 @@ LT_D int coords_of(const Geom& g, int i, int c[4])
 // Full index of the site c moved by L steps along d (periodic)
 LT_D int shifted(const Geom& g, const int c[4], int d, int L)
 {
-    int cc[4] = { c[0], c[1], c[2], c[3] };
-    cc[d] = (cc[d] + L) % g.n[d];
-    return ((cc[0] * g.n[1] + cc[1]) * g.n[2] + cc[2]) * g.n[3] + cc[3];
+    const int i = ((c[0] * g.n[1] + c[1]) * g.n[2] + c[2]) * g.n[3] + c[3];
+    const int n = pick4(g.n, d), x = pick4(c, d);
+    return i + ((x + L) % n - x) * pick4(g.stride, d);
 }
 
 // TopChargeCloverTimeslice / EnergyDensity::CloverTimeslice (topological_charge.hpp:338-364,
@@ -1507,7 +1507,7 @@ LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const
 {
     const int op = par ^ 1;
     const int dmu = step_up_rt(g, mu, c);
-    const int imu = i + dmu, inu = i + step_up(g, nu, c[nu]), ind = i + step_dn(g, nu, c[nu]);
+    const int imu = i + dmu, inu = i + step_up_rt(g, nu, c), ind = i + step_dn_rt(g, nu, c);
     // x+mu+nu and x+mu-nu share the nu offsets of x (coordinate c[nu] unchanged by the mu step)
     const int imunu = inu + dmu, imund = ind + dmu;
     const M3<T> u_s_nu = U.ld(nu, par, i >> 1);
@@ -1631,7 +1631,7 @@ __global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Al
     for (int nu = 0; nu < 4; ++nu)
     {
         if (nu == mu) continue;
-        const int inu = i + step_up(g, nu, c[nu]), ind = i + step_dn(g, nu, c[nu]);
+        const int inu = i + step_up_rt(g, nu, c), ind = i + step_dn_rt(g, nu, c);
         const int imund = ind + dmu;
         const M3<T> u_s_nu = U.ld(nu, par, i >> 1);
         const M3<T> u_nud_mu = U.ld(mu, op, ind >> 1);
