@@ -1417,10 +1417,12 @@ __global__ void __launch_bounds__(kThreads) k_parity(Gauge<T, NR> Uin, Gauge<T, 
     const int pl = l / g.vh, s = l - pl * g.vh, mu = pl >> 1, par = pl & 1;
     int c[4];
     site_coords(g, par, s, c);
-    int r[4] = { c[0], g.n[1] - c[1] - 1, g.n[2] - c[2] - 1, g.n[3] - c[3] - 1 };
-    if (mu > 0) r[mu] = (r[mu] - 1 + g.n[mu]) % g.n[mu];
-    const int j = ((r[0] * g.n[1] + r[1]) * g.n[2] + r[2]) * g.n[3] + r[3];
-    const int pj = (r[0] + r[1] + r[2] + r[3]) & 1;
+    int r1 = g.n[1] - c[1] - 1, r2 = g.n[2] - c[2] - 1, r3 = g.n[3] - c[3] - 1;
+    if (mu == 1) r1 = r1 > 0 ? r1 - 1 : g.n[1] - 1;
+    if (mu == 2) r2 = r2 > 0 ? r2 - 1 : g.n[2] - 1;
+    if (mu == 3) r3 = r3 > 0 ? r3 - 1 : g.n[3] - 1;
+    const int j = ((c[0] * g.n[1] + r1) * g.n[2] + r2) * g.n[3] + r3;
+    const int pj = (c[0] + r1 + r2 + r3) & 1;
     const M3<T> m = Uin.ld(mu, pj, j >> 1);
     Uout.st(mu, par, s, mu == 0 ? m : adj(m));
 }
@@ -1495,8 +1497,9 @@ __global__ void __launch_bounds__(kThreads) k_clover_R(Gauge<T, NR> U, Clov<T> R
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
-    const int pm[6] = { 0, 0, 0, 1, 1, 2 }, pn[6] = { 1, 2, 3, 2, 3, 3 };
-    M3<T> cl = clover_leaves(U, g, par, i, c, pm[pl], pn[pl]);
+    // planes 01 02 03 12 13 23
+    const int pm = pl < 3 ? 0 : pl < 5 ? 1 : 2, pn = pl < 3 ? pl + 1 : pl < 5 ? pl - 1 : 3;
+    M3<T> cl = clover_leaves(U, g, par, i, c, pm, pn);
     R.st(pl, par, s, cl - adj(cl));
 }
 
@@ -1539,18 +1542,17 @@ __global__ void __launch_bounds__(kThreads) k_clover_deriv(Gauge<T, NR> U, Clov<
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
-    // the three epsilon-tensor terms (sign, nu, rho, sigma) of each direction
-    const int tab[4][3][4] = {
-        { { +1, 1, 2, 3 }, { -1, 2, 1, 3 }, { +1, 3, 1, 2 } },
-        { { -1, 0, 2, 3 }, { +1, 2, 0, 3 }, { -1, 3, 0, 2 } },
-        { { +1, 0, 1, 3 }, { -1, 1, 0, 3 }, { +1, 3, 0, 1 } },
-        { { -1, 0, 1, 2 }, { +1, 1, 0, 2 }, { -1, 2, 0, 1 } } };
+    // the three epsilon-tensor terms of direction mu: nu = the k-th other direction, (rho,
+    // sigma) the remaining two in ascending order, sign = parity of (mu, nu, rho, sigma)
+    const int o0 = mu == 0 ? 1 : 0, o1 = mu <= 1 ? 2 : 1, o2 = mu <= 2 ? 3 : 2;
     M3<T> d = zero3<T>();
 #pragma unroll 1
     for (int k = 0; k < 3; ++k)
     {
-        M3<T> comp = clover_deriv_component(U, R, g, par, i, c, mu, tab[mu][k][1], tab[mu][k][2], tab[mu][k][3]);
-        d = tab[mu][k][0] > 0 ? d + comp : d - comp;
+        const int nu = k == 0 ? o0 : k == 1 ? o1 : o2, rho = k == 0 ? o1 : o0, sigma = k == 2 ? o1 : o2;
+        const int inv = (mu > nu) + (mu > rho) + (mu > sigma) + (nu > rho) + (nu > sigma) + (rho > sigma);
+        M3<T> comp = clover_deriv_component(U, R, g, par, i, c, mu, nu, rho, sigma);
+        d = (inv & 1) ? d - comp : d + comp;
     }
     d = mul(U.ld(mu, par, s), d);
     A8<T> a = algebra8(d);
