@@ -99,6 +99,8 @@ public:
                              int par, const uint64_t* counter, int max_iter) const = 0;
 
     virtual void clover_R(const Ctx& c, const void* U, void* R) const = 0;
+    // sum over sites of ReTr(R01 R23 - R02 R13 + R03 R12) into results[slot]
+    virtual void topcharge_R(const Ctx& c, const void* R, int slot) const = 0;
     virtual void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const = 0;
     virtual void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam,
                               void* Tloc, double rho) const = 0;

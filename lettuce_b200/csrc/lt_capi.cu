@@ -164,15 +164,33 @@ const void* level(const lt_lattice* h, int k) { return k == 0 ? h->U : h->levels
 
 // dvdq * dQ/dU into h->F, given the forward chain (CalculateTopologicalForce,
 // updates/hmc_metadynamics.hpp:374-436)
-int metad_backward(lt_lattice* h, double rho, int n_stout, double dvdq)
+// The clover planes R of the most smeared level (CalculateClover, hmc_metadynamics.hpp:397-399)
+int metad_clover(lt_lattice* h, int n_stout)
+{
+    LT_TRY(ensure(h, &h->R, h->be->clov_bytes(h->g)));
+    h->be->clover_R(h->ctx(), level(h, n_stout), h->R);
+    return launched("metad_clover");
+}
+
+// Q of the most smeared level from its clover planes (TopChargeClover(Clover),
+// topological_charge.hpp:202-231)
+int charge_from_R(lt_lattice* h, double* q)
+{
+    h->be->topcharge_R(h->ctx(), h->R, 7);
+    double r;
+    LT_TRY(fetch(h, 7, 1, &r));
+    *q = -1.0 / (64.0 * 4.0 * kPi * kPi) * r;
+    return LT_OK;
+}
+
+int metad_backward(lt_lattice* h, double rho, int n_stout, double dvdq, bool have_R = false)
 {
     LT_TRY(ensure(h, &h->F, h->be->alg_bytes(h->g)));
-    LT_TRY(ensure(h, &h->R, h->be->clov_bytes(h->g)));
     LT_TRY(ensure(h, &h->Lam, h->be->alg_bytes(h->g)));
     LT_TRY(ensure(h, &h->Tloc, h->be->full_bytes(h->g)));
+    if (!have_R) LT_TRY(metad_clover(h, n_stout));
     const lt::Ctx c = h->ctx();
     const void* top = level(h, n_stout);
-    h->be->clover_R(c, top, h->R);
     h->be->clover_deriv(c, top, h->R, h->F, dvdq);
     for (int k = n_stout; k > 0; --k)
     {
@@ -221,10 +239,11 @@ struct MetaDParams
 int metad_force_now(lt_lattice* h, const MetaDParams* md, bool submeasure)
 {
     LT_TRY(metad_forward(h, md->rho, md->n_stout));
+    LT_TRY(metad_clover(h, md->n_stout));
     double q;
-    LT_TRY(clover_q_e(h, level(h, md->n_stout), &q, nullptr));
+    LT_TRY(charge_from_R(h, &q));
     if (submeasure && md->samples) md->samples->push_back(q);
-    return metad_backward(h, md->rho, md->n_stout, md->bias->derivative(q));
+    return metad_backward(h, md->rho, md->n_stout, md->bias->derivative(q), true);
 }
 
 int kick(lt_lattice* h, double beta, double eps, const MetaDParams* md, bool submeasure)
@@ -1182,8 +1201,9 @@ int lt_metad_force(lt_lattice* h, double rho, int n_stout, double dvdq, double* 
     const lt::DeviceScope device_scope(h->device);
     if (n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_metad_force: n_stout < 0");
     LT_TRY(metad_forward(h, rho, n_stout));
-    if (q_out) LT_TRY(clover_q_e(h, level(h, n_stout), q_out, nullptr));
-    LT_TRY(metad_backward(h, rho, n_stout, dvdq));
+    LT_TRY(metad_clover(h, n_stout));
+    if (q_out) LT_TRY(charge_from_R(h, q_out));
+    LT_TRY(metad_backward(h, rho, n_stout, dvdq, true));
     if (force_out)
     {
         LT_TRY(ensure_aos(h));

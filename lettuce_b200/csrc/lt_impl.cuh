@@ -258,6 +258,11 @@ public:
     {
         k_clover_R<T, NR><<<nblocks(6LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), clov(R, c.g), c.g);
     }
+    void topcharge_R(const Ctx& c, const void* R, int slot) const override
+    {
+        k_topcharge_R<T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(clov(R, c.g), c.g, c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 1);
+    }
     void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const override
     {
         k_clover_deriv<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(

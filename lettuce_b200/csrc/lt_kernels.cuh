@@ -1503,6 +1503,27 @@ __global__ void __launch_bounds__(kThreads) k_clover_R(Gauge<T, NR> U, Clov<T> R
     R.st(pl, par, s, cl - adj(cl));
 }
 
+// TopChargeClover(const FullTensor&) (observables/topological_charge.hpp:202-231) from the
+// stored clover planes R = C - C^dag: per site ReTr(R01 R23 - R02 R13 + R03 R12), products
+// in FP64; the force of the metadynamics chain builds R anyway (CalculateClover,
+// hmc_metadynamics.hpp:397-399), so its charge costs one pass over R
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_topcharge_R(Clov<T> R, Geom g, double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    Kahan k;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.V; x += gridDim.x * blockDim.x)
+    {
+        const int par = x >= g.vh, s = x - par * g.vh;
+        double q = retr_mul(cvt<double>(R.ld(0, 1, par, s)), cvt<double>(R.ld(2, 3, par, s)));
+        q -= retr_mul(cvt<double>(R.ld(0, 2, par, s)), cvt<double>(R.ld(1, 3, par, s)));
+        q += retr_mul(cvt<double>(R.ld(0, 3, par, s)), cvt<double>(R.ld(1, 2, par, s)));
+        k.add(q);
+    }
+    double r = block_sum(k.s - k.c, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
 // CloverDerivativeComponent (observables/clover.hpp:238-276)
 template <typename T, int NR>
 LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const Geom& g, int par, int i,
