@@ -1608,15 +1608,44 @@ __global__ void __launch_bounds__(kThreads) k_stout_lambda(Gauge<T, NR> U, Gauge
 #pragma unroll
         for (int b = 0; b < 3; ++b) Q.e[a][b] = mkc<T>(rho * C.e[a][b].i, -rho * C.e[a][b].r);
     M3<T> Q2 = mul(Q, Q);
-    ExpScalars e = exp_scalars(Q, Q2);
-    ExpDerivScalars d = exp_deriv_scalars(e);
     M3<T> tmp = mul(u, sp);
     M3<T> Qt = mul(Q, tmp), tQ = mul(tmp, Q);
     // tr(B_j tmp) = b_j0 tr(tmp) + b_j1 tr(Q tmp) + b_j2 tr(Q^2 tmp)
-    cx<double> tr0 = cvt<double>(trace(tmp)), tr1 = cvt<double>(trace(Qt)), tr2 = cvt<double>(tr_mul(Q2, tmp));
-    cx<T> t1 = cvt<T>(d.b10 * tr0 + d.b11 * tr1 + d.b12 * tr2);
-    cx<T> t2 = cvt<T>(d.b20 * tr0 + d.b21 * tr1 + d.b22 * tr2);
-    cx<T> f1 = cvt<T>(d.f1), f2 = cvt<T>(d.f2);
+    const cx<T> r0 = trace(tmp), r1 = trace(Qt), r2 = tr_mul(Q2, tmp);
+    cx<T> t1, t2, f1, f2;
+    M3<T> ex;
+    const T c1 = (T)0.5 * (Q2.e[0][0].r + Q2.e[1][1].r + Q2.e[2][2].r);
+    if (sizeof(T) == 4 && c1 <= (T)0.5)
+    {
+        // FP32 links, small arguments (every stout step of the chain): the Cayley-Hamilton
+        // series and its derivatives in FP32 (17 terms), no transcendental scalar chain.  FP64
+        // keeps the closed form: its 23-term series costs more registers than it saves.
+        const T c0 = retr_mul(Q, Q2) * (T)(1.0 / 3.0);
+        cx<T> f[3], b2[3], b1[3];
+        exp_series_deriv<16>(c0, c1, f, b2, b1);
+        t1 = b1[0] * r0 + b1[1] * r1 + b1[2] * r2;
+        t2 = b2[0] * r0 + b2[1] * r1 + b2[2] * r2;
+        f1 = f[1];
+        f2 = f[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) ex.e[a][b] = lincomb2(f[1], Q.e[a][b], f[2], Q2.e[a][b]);
+        ex.e[0][0] = ex.e[0][0] + f[0];
+        ex.e[1][1] = ex.e[1][1] + f[0];
+        ex.e[2][2] = ex.e[2][2] + f[0];
+    }
+    else
+    {
+        ExpScalars e = exp_scalars(Q, Q2);
+        ExpDerivScalars d = exp_deriv_scalars(e);
+        const cx<double> tr0 = cvt<double>(r0), tr1 = cvt<double>(r1), tr2 = cvt<double>(r2);
+        t1 = cvt<T>(d.b10 * tr0 + d.b11 * tr1 + d.b12 * tr2);
+        t2 = cvt<T>(d.b20 * tr0 + d.b21 * tr1 + d.b22 * tr2);
+        f1 = cvt<T>(d.f1);
+        f2 = cvt<T>(d.f2);
+        ex = exp_from(e, Q, Q2);
+    }
     M3<T> lam;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -1625,7 +1654,6 @@ __global__ void __launch_bounds__(kThreads) k_stout_lambda(Gauge<T, NR> U, Gauge
             lam.e[a][b] = t1 * Q.e[a][b] + t2 * Q2.e[a][b] + f1 * tmp.e[a][b] + f2 * (Qt.e[a][b] + tQ.e[a][b]);
     A8<T> l8 = traceless_herm8(lam);
     Lam.st(mu, par, s, l8);
-    M3<T> ex = exp_from(e, Q, Q2);
     M3<T> loc = mul(sp, ex);
     M3<T> sl = mul_dn(st, unpack_h(l8));   // st^dag Lambda
 #pragma unroll

@@ -536,6 +536,53 @@ template <int N, typename S> LT_D void exp_series(S c0, S c1, cx<S>& f0, cx<S>& 
     f2 = mkc(f2r, f2i);
 }
 
+// The same series with its derivatives: f_j = sum_n i^n (a, b, c)_n / n! and d0_j = df_j/dc0,
+// d1_j = df_j/dc1 by differentiating the recursion term by term.  With dc0 = tr(Q^2 dQ) and
+// dc1 = tr(Q dQ), B_1 = sum_j d1_j Q^j and B_2 = sum_j d0_j Q^j are the matrices of
+// ExpDerivativeConstants (math/su3_exp.hpp:286-416; Morningstar-Peardon, hep-lat/0311018).
+template <int N, typename S>
+LT_D void exp_series_deriv(S c0, S c1, cx<S> f[3], cx<S> d0[3], cx<S> d1[3])
+{
+    S x[3] = { 1, 0, 0 }, y[3] = { 0, 0, 0 }, z[3] = { 0, 0, 0 };   // (a, b, c)_n / n! and d/dc0, d/dc1
+    S fr[3] = { 0, 0, 0 }, fi[3] = { 0, 0, 0 }, yr[3] = { 0, 0, 0 }, yi[3] = { 0, 0, 0 };
+    S zr[3] = { 0, 0, 0 }, zi[3] = { 0, 0, 0 };
+#pragma unroll
+    for (int n = 0; n <= N; ++n)
+    {
+        const S sg = (n & 2) ? (S)-1 : (S)1;   // i^n = sg (n even) or sg i (n odd)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+        {
+            if (n & 1)
+            {
+                fi[j] += sg * x[j];
+                yi[j] += sg * y[j];
+                zi[j] += sg * z[j];
+            }
+            else
+            {
+                fr[j] += sg * x[j];
+                yr[j] += sg * y[j];
+                zr[j] += sg * z[j];
+            }
+        }
+        const S inv = (S)(1.0 / (double)(n + 1));
+        const S na = x[2] * c0 * inv, nb = (x[0] + x[2] * c1) * inv, nc = x[1] * inv;
+        const S ya = (y[2] * c0 + x[2]) * inv, yb = (y[0] + y[2] * c1) * inv, yc = y[1] * inv;
+        const S za = z[2] * c0 * inv, zb = (z[0] + z[2] * c1 + x[2]) * inv, zc = z[1] * inv;
+        x[0] = na; x[1] = nb; x[2] = nc;
+        y[0] = ya; y[1] = yb; y[2] = yc;
+        z[0] = za; z[1] = zb; z[2] = zc;
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+    {
+        f[j] = mkc(fr[j], fi[j]);
+        d0[j] = mkc(yr[j], yi[j]);
+        d1[j] = mkc(zr[j], zi[j]);
+    }
+}
+
 // Q^2 of a Hermitian Q (upper triangle computed, lower mirrored)
 template <typename T> LT_D M3<T> herm_sq(const M3<T>& q)
 {

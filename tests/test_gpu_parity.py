@@ -273,6 +273,21 @@ class TestMetaD:
         assert q == pytest.approx(qo, rel=1e-11, abs=1e-13)
         assert rel_err(F, Fo) < 1e-11
 
+    @pytest.mark.parametrize("prec", ["fp32", "fp32_12"])
+    def test_metad_force_fp32(self, oracle, therm8, prec):
+        """FP32 links: the whole chain in FP32 (the stout adjoint's exponential derivative
+        from the series) against the FP64 oracle on the same rounded links: 1e-5 of the
+        largest force entry, Q to 1e-5."""
+        ext = (8, 8, 8, 8)
+        G = gpu(ext, therm8, prec)
+        W = G.download()
+        bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 10, 1000)
+        k = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(6.0), 1.0, 0.12, 4)
+        F, q = k.CalculateTopologicalForce(dvdq=0.7)
+        Fo, qo = oracle.metad_force(ext, W, 0.12, 4, 0.7)
+        assert q == pytest.approx(qo, abs=1e-5)
+        assert rel_err(F, Fo) < 1e-5
+
     @pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("fp32", 1e-4)])
     def test_metad_reversibility(self, therm8, prec, tol):
         """ReversibilityTest of the MetaD kernel (updates/hmc_metadynamics.hpp:657-674)."""
