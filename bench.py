@@ -218,18 +218,19 @@ def run_reference(a):
 # ---------------------------------------------------------------------------- secondary rates
 def secondary_rates(lt, torch, timed, prec):
     """Rates of the other workloads, reported beside the headline:
-    * metadynamics force evaluations/s at 16^4 (4 stout steps rho = 0.12, FP32 links);
+    * metadynamics force evaluations/s at 16^4 (4 stout steps rho = 0.12, bulk FP32 storage);
     * tempering ensemble link updates/s: 8 streams of 12^4 plus 40 chains with extents drawn
       from {8,...,16}^4, beta in [5.8, 6.2], one batched round (1 HB + 4 OR) per step;
     * BMW configuration files at 32^4 (device checksum pass, save and load);
     * Iterator::Checkerboard4 rounds at 32^4 with the Wilson and the Luescher-Weisz actions;
     * the driver's measurement step at 32^4;
-    * one 48^4 HMC trajectory (OMF4, tau = 1, 20 steps, FP32 links, FP64 dH) and the flow to t0."""
+    * one 48^4 HMC trajectory (OMF4, tau = 1, 20 steps, bulk FP32 storage, FP64 dH) and the
+      flow to t0."""
     import numpy as np
-    out = {}
+    out = {"storage": prec}
     try:
         ext = (16,) * 4
-        G = lt.GaugeField(ext, "fp32")
+        G = lt.GaugeField(ext, prec)
         G.SetToHaarRandom(3)
         lt.UpdateSweeps(G, BETA, 5, 1, 4, SEED)
         bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 10, 1000)
@@ -238,9 +239,9 @@ def secondary_rates(lt, torch, timed, prec):
             k.CalculateTopologicalForce(dvdq=1.0, download=False)
         ms = timed(G, lambda: k.CalculateTopologicalForce(dvdq=1.0, download=False), 10)
         rate = 10 / (ms / 1000.0)
-        out["metad_force_evals_per_s_16^4_fp32"] = rate
+        out["metad_force_evals_per_s_16^4"] = rate
         links = 4 * G.Volume()
-        gbs = bm.metad_force_bytes_per_link("fp32", 4) * links * rate / 1e9
+        gbs = bm.metad_force_bytes_per_link(prec, 4) * links * rate / 1e9
         tfl = bm.FLOPS["metad_force_n4"] * links * rate / 1e12
         out["metad_force_roofline"] = {"hbm_gbs": gbs, "hbm_frac": gbs / peaks()[0], "tflops": tfl,
                                        "note": "algorithmic bytes (6.9 n + 3.5) b per link and ~70k flops per link"}
@@ -331,7 +332,7 @@ def secondary_rates(lt, torch, timed, prec):
         # Wilson flow to t0
         # (t^2 E = 0.3) with clover Q and E at every step
         ext = (48,) * 4
-        G = lt.GaugeField(ext, "fp32")
+        G = lt.GaugeField(ext, prec)
         G.SetToHaarRandom(5)
         t0 = time.perf_counter()
         lt.UpdateSweeps(G, 6.3, 200, 1, 4, SEED)
@@ -341,11 +342,11 @@ def secondary_rates(lt, torch, timed, prec):
         hmc(20, True)
         t0 = time.perf_counter()
         acc = hmc(20, True)
-        out["hmc_48^4_fp32_s_per_trajectory"] = time.perf_counter() - t0
+        out["hmc_48^4_s_per_trajectory"] = time.perf_counter() - t0
         out["hmc_48^4_dH"] = [hmc.delta_H]
         out["hmc_48^4_accepted"] = bool(acc)
         del hmc
-        F = lt.GaugeField(ext, "fp32")
+        F = lt.GaugeField(ext, prec)
         flow = lt.GradientFlowKernel(G, F, lt.RK3, None, FLOW_EPS)
         t0 = time.perf_counter()
         tt0, q = flow.FlowToT0(0.3)
