@@ -144,6 +144,14 @@ int lt_rect_action(lt_lattice* h, double beta, double c_plaq, double c_rect, dou
 /* WilsonLoop (observables/wilson_loop.hpp:63-124): 1 - sum Re tr W_LxL / (18 V) over all sites
  * and the six planes, for square L x L loops (the driver measures L = 2, 4, 8). */
 int lt_wilson_loop(lt_lattice* h, int L, double* out);
+/* WilsonLoop<start, end, reset>(U, U_chain) (observables/wilson_loop.hpp:63-124) with the
+ * chain U_chain kept in the handle between calls: reset sets it to 1, then the links
+ * U(x + n mu) for n = start..end-1 are multiplied on, and the square loops of side `end` are
+ * evaluated from it.  The driver's sequence (0, 2, reset), (2, 4), (4, 8) builds each chain
+ * once (a straight run from the origin doubles with one product per link).  Without reset
+ * the previous call's chain is extended as it stands; LT_ERR_STATE if there is none
+ * (lt_wilson_loop reuses the chain's buffers and drops it). */
+int lt_wilson_loop_chain(lt_lattice* h, int start, int end, int reset, double* out);
 /* PolyakovLoop (observables/polyakov_loop.hpp:32-49): mean over the spatial sites of the trace
  * of the product of the links in direction t. */
 int lt_polyakov_loop(lt_lattice* h, double* re, double* im);

@@ -209,14 +209,15 @@ inline double TopChargePlaquette(const GaugeField& U)
 }
 
 // WilsonLoop<N_mu_start, N_mu_end, reset>(U, U_chain) (observables/wilson_loop.hpp:63-124):
-// 1 - sum Re tr W / (18 V) over the square N_mu_end x N_mu_end loops.  The device builds the
-// line products itself, so U_chain is accepted for the signature and left untouched.
+// 1 - sum Re tr W / (18 V) over the square N_mu_end x N_mu_end loops.  The chain of link
+// products lives in U's handle on the device (the same reset / extend semantics), so U_chain
+// is accepted for the signature and left untouched.
 template <int N_mu_start, int N_mu_end, bool reset>
 double WilsonLoop(const GaugeField& U, GaugeField& /*U_chain*/)
 {
     static_assert(N_mu_start >= 0 && N_mu_end >= 0, "The template parameters of WilsonLoop are not allowed to be negative!");
     double v;
-    check(lt_wilson_loop(U.handle(), N_mu_end, &v));
+    check(lt_wilson_loop_chain(U.handle(), N_mu_start, N_mu_end, reset ? 1 : 0, &v));
     return v;
 }
 

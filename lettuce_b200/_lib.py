@@ -74,6 +74,7 @@ SIGNATURES = {
     "lt_topcharge_plaquette": (_i, [_vp, _pd]),
     "lt_rect_action": (_i, [_vp, _d, _d, _d, _pd]),
     "lt_wilson_loop": (_i, [_vp, _i, _pd]),
+    "lt_wilson_loop_chain": (_i, [_vp, _i, _i, _i, _pd]),
     "lt_polyakov_loop": (_i, [_vp, _pd, _pd]),
     "lt_flow_rk3_measure": (_i, [_vp, _vp, _d, _i, _i, _vp, _vp, _vp]),
     "lt_flow_t0": (_i, [_vp, _vp, _d, _d, _i, _pd, _pd]),

@@ -717,6 +717,12 @@ def WilsonLoop(U: GaugeField, L: int) -> float:
     return _out1(lib().lt_wilson_loop, U.handle, int(L))
 
 
+def WilsonLoopChain(U: GaugeField, start: int, end: int, reset: bool) -> float:
+    """WilsonLoop<start, end, reset>(U, U_chain) with the chain kept in U's handle between
+    calls (observables/wilson_loop.hpp:63-124)."""
+    return _out1(lib().lt_wilson_loop_chain, U.handle, int(start), int(end), int(bool(reset)))
+
+
 def PolyakovLoop(U: GaugeField) -> complex:
     """observables/polyakov_loop.hpp:32-49."""
     re, im = C.c_double(), C.c_double()
@@ -733,8 +739,8 @@ def Measure(U: GaugeField, beta: float) -> dict:
     plaq = PlaquetteSum(U) / V
     return {"Wilson_Action": 1.0 - plaq / 18.0, "Improved_Action": SymanzikAction(beta).ActionNormalized(U),
             "Plaquette": plaq, "E_plaq": 36.0 - 2.0 * plaq, "E_clov": float(e_t.sum()), "E_clov_timeslice": e_t,
-            "Wilson_loop(L=2)": WilsonLoop(U, 2), "Wilson_loop(L=4)": WilsonLoop(U, 4),
-            "Wilson_loop(L=8)": WilsonLoop(U, 8), "Polyakov_loop": PolyakovLoop(U),
+            "Wilson_loop(L=2)": WilsonLoopChain(U, 0, 2, True), "Wilson_loop(L=4)": WilsonLoopChain(U, 2, 4, False),
+            "Wilson_loop(L=8)": WilsonLoopChain(U, 4, 8, False), "Polyakov_loop": PolyakovLoop(U),
             "TopChargeClov": float(q_t.sum()), "TopChargeClov_timeslice": q_t, "TopChargePlaq": TopChargePlaquette(U)}
 
 
@@ -769,7 +775,8 @@ __all__ = ["STATUS_NONFINITE", "STATUS_UNITARITY", "STATUS_HB_CAP", "GaugeField"
            "Iterator", "UpdateSweeps", "RK3", "GradientFlowKernel", "StoutSmearing4D", "StoutSmearingN",
            "MetaBiasPotential", "HMCKernel", "HMCMetaDKernel", "CloverDerivative", "LettuceError", "Ensemble",
            "TemperingSwap", "Euler", "RK2", "RK3W7", "TopChargeCloverTimeslice", "EnergyDensityCloverTimeslice",
-           "TopChargePlaquette", "RectangularAction", "SymanzikAction", "WilsonLoop", "PolyakovLoop", "Measure",
+           "TopChargePlaquette", "RectangularAction", "SymanzikAction", "WilsonLoop", "WilsonLoopChain", "PolyakovLoop",
+           "Measure",
            "Observables", "MDIntegrator", "Integrators", "Leapfrog_slow", "Leapfrog", "OMF_2_slow", "OMF_2",
            "OMF_4_slow", "OMF_4", "Leapfrog_friction_slow", "OMF_4_friction_slow", "Leapfrog_OMF_4",
            "OMF_2_OMF_4_slow", "OMF_2_OMF_4", "ParityUpdate", "LuescherWeiszAction", "IwasakiAction", "DBW2Action",

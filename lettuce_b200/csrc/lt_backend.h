@@ -63,6 +63,7 @@ public:
     virtual void loops(const Ctx& c, const void* U, int slot) const = 0;
     virtual void polyakov(const Ctx& c, const void* U, int slot) const = 0;
     virtual void chain_init(const Ctx& c, const void* U, void* C) const = 0;
+    virtual void chain_unit(const Ctx& c, void* C) const = 0;
     virtual void chain_extend(const Ctx& c, const void* Cin, const void* U, void* Cout, int L) const = 0;
     virtual void chain_double(const Ctx& c, const void* Cin, void* Cout, int L) const = 0;
     virtual void wilson_square(const Ctx& c, const void* C, int L, int slot) const = 0;

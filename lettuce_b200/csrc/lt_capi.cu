@@ -818,6 +818,9 @@ int lt_wilson_loop(lt_lattice* h, int L, double* out)
     const lt::Ctx c = h->ctx();
     h->be->chain_init(c, h->U, h->chainA);
     void *cur = h->chainA, *nxt = h->chainB;
+    // the buffers are the ones lt_wilson_loop_chain keeps its chain in
+    h->chain_len = -1;
+    h->chain_cur = nullptr;
     if ((L & (L - 1)) == 0)
         for (int len = 1; len < L; len *= 2)
         {
@@ -831,6 +834,69 @@ int lt_wilson_loop(lt_lattice* h, int L, double* out)
             std::swap(cur, nxt);
         }
     h->be->wilson_square(c, cur, L, 0);
+    double w;
+    LT_TRY(fetch(h, 0, 1, &w));
+    *out = 1.0 - w / (18.0 * (double)h->g.V);
+    return LT_OK;
+}
+
+int lt_wilson_loop_chain(lt_lattice* h, int start, int end, int reset, double* out)
+{
+    LT_TRY(check_h(h, "lt_wilson_loop_chain"));
+    const lt::DeviceScope device_scope(h->device);
+    if (!out || start < 0 || end < 1 || end < start)
+        return lt::set_error(LT_ERR_ARG, "lt_wilson_loop_chain: null pointer or not 0 <= start <= end, end >= 1");
+    if (!reset && h->chain_len < 0)
+        return lt::set_error(LT_ERR_STATE, "lt_wilson_loop_chain: no chain to extend (call with reset first)");
+    const size_t bytes = (size_t)4 * h->g.V * 9 * 2 * sizeof(double);
+    LT_TRY(ensure(h, &h->chainA, bytes));
+    LT_TRY(ensure(h, &h->chainB, bytes));
+    const lt::Ctx c = h->ctx();
+    void* cur = h->chain_cur ? h->chain_cur : h->chainA;
+    int n = start;   // the next factor is U(x + n mu)
+    if (reset)
+    {
+        // U_chain = 1, then the factors n = start..end-1 (wilson_loop.hpp:75-88); from the
+        // origin the first factor is a copy of the links
+        cur = h->chainA;
+        h->chain_origin = start;
+        h->chain_contig = true;
+        if (start == 0 && end > 0)
+        {
+            h->be->chain_init(c, h->U, cur);
+            h->chain_len = 1;
+            n = 1;
+        }
+        else
+        {
+            h->be->chain_unit(c, cur);
+            h->chain_len = 0;
+        }
+    }
+    else if (h->chain_origin + h->chain_len != start)
+        h->chain_contig = false;   // the chain no longer holds one straight run of links
+    while (n < end)
+    {
+        void* nxt = cur == h->chainA ? h->chainB : h->chainA;
+        if (h->chain_contig && h->chain_origin == 0 && h->chain_len == n && 2 * n <= end)
+        {
+            // C(x) C(x + n mu): the run of length n doubles with one product per link
+            h->be->chain_double(c, cur, nxt, n);
+            h->chain_len = 2 * n;
+            n *= 2;
+        }
+        else
+        {
+            h->be->chain_extend(c, cur, h->U, nxt, n);
+            if (h->chain_contig && h->chain_origin + h->chain_len == n) ++h->chain_len;
+            else h->chain_contig = false;
+            ++n;
+        }
+        cur = nxt;
+    }
+    h->chain_cur = cur;
+    LT_TRY(launched("lt_wilson_loop_chain"));
+    h->be->wilson_square(c, cur, end, 0);
     double w;
     LT_TRY(fetch(h, 0, 1, &w));
     *out = 1.0 - w / (18.0 * (double)h->g.V);

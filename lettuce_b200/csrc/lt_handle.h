@@ -66,6 +66,11 @@ struct lt_lattice
     unsigned* status = nullptr;  // device status word (lt_status_word) and scratch words
     void* chainA = nullptr;      // straight-line link products of lt_wilson_loop (FP64 full matrices)
     void* chainB = nullptr;
+    // the chain kept between lt_wilson_loop_chain calls (the reference's U_chain): the buffer
+    // holding it and the product U(x + o mu) ... U(x + (o + n - 1) mu) it holds (n = -1: none)
+    void* chain_cur = nullptr;
+    int chain_origin = 0, chain_len = -1;
+    bool chain_contig = true;
     // gauge action of staples, sweeps, HMC forces / Hamiltonian and flow (lt_set_gauge_action):
     // stencil radius 1 (Wilson, the default) or 2 (plaquettes and 1x2 rectangles)
     int act_radius = 1;

@@ -153,6 +153,10 @@ public:
     {
         k_chain_init<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(gauge(U, c.g), full64(C, c.g), c.g);
     }
+    void chain_unit(const Ctx& c, void* C) const override
+    {
+        k_chain_unit<<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(full64(C, c.g), c.g);
+    }
     void chain_extend(const Ctx& c, const void* Cin, const void* U, void* Cout, int L) const override
     {
         k_chain_extend<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(full64(Cin, c.g), gauge(U, c.g),

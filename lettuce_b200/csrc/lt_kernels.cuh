@@ -1260,6 +1260,15 @@ __global__ void k_chain_init(Gauge<T, NR> Ust, Full<double> C, Geom g)
     C.st(pl >> 1, pl & 1, s, cvt<double>(Ust.ld(pl >> 1, pl & 1, s)));
 }
 
+template <int Unused = 0>
+__global__ void k_chain_unit(Full<double> C, Geom g)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 4 * g.V) return;
+    const int pl = l / g.vh, s = l - pl * g.vh;
+    C.st(pl >> 1, pl & 1, s, unit3<double>());
+}
+
 template <typename T, int NR>
 __global__ void k_chain_extend(Full<double> Cin, Gauge<T, NR> Ust, Full<double> Cout, Geom g, int L)
 {

@@ -734,6 +734,21 @@ void ref_flow_action(const double* in, double* out, double eps, int n, int integ
     store(*V, out);
 }
 
+// WilsonLoop<start, end, reset>(U, U_chain) (wilson_loop.hpp:63-124) with start/end among
+// the instantiated pairs and U_chain kept in the library between calls
+double ref_wilson_loop_chain(const double* links, int start, int end, int reset)
+{
+    static std::unique_ptr<GaugeField> chain;
+    if (!chain) chain = std::make_unique<GaugeField>();
+    auto U = std::make_unique<GaugeField>();
+    load(*U, links);
+#define LT_WL(S, E)                                                                               \
+    if (start == S && end == E) return reset ? WilsonLoop<S, E, true>(*U, *chain) : WilsonLoop<S, E, false>(*U, *chain);
+    LT_WL(0, 1) LT_WL(0, 2) LT_WL(0, 3) LT_WL(2, 4) LT_WL(4, 8) LT_WL(3, 5) LT_WL(1, 3) LT_WL(2, 3) LT_WL(5, 6)
+#undef LT_WL
+    return std::nan("");
+}
+
 // ParityUpdate (parity_update.hpp:22-47) in place
 void ref_parity_update(double* links)
 {

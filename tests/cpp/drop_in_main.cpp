@@ -33,10 +33,12 @@ int main(int argc, char** argv)
     const std::complex<double> poly = PolyakovLoop(Gluon);
     double q_sum = 0.0;
     for (const double q : TopChargeCloverTimeslices(Gluon)) q_sum += q;
+    // the chain grows from call to call, so the loops are evaluated in order (SU3_main.cpp:141-143)
+    const double w2 = WilsonLoop<0, 2, true>(Gluon, Gluonchain);
+    const double w4 = WilsonLoop<2, 4, false>(Gluon, Gluonchain);
     std::printf("bundle S %.15f W2 %.15f W4 %.15f P %.15f %.15f Qplaq %.15f Qt %.15f E0 %.15f\n",
-                SymanzikAction.ActionNormalized(Gluon), WilsonLoop<0, 2, true>(Gluon, Gluonchain),
-                WilsonLoop<2, 4, false>(Gluon, Gluonchain), poly.real(), poly.imag(), TopChargePlaquette(Gluon), q_sum,
-                EnergyDensity::CloverTimeslice(Gluon, 0));
+                SymanzikAction.ActionNormalized(Gluon), w2, w4, poly.real(), poly.imag(), TopChargePlaquette(Gluon),
+                q_sum, EnergyDensity::CloverTimeslice(Gluon, 0));
     Integrators::GradientFlow::Euler euler;
     GradientFlowKernel EulerFlow(Gluon, Gluonchain, euler, SimulatedAction, 0.02);
     EulerFlow(5);

@@ -192,6 +192,13 @@ def gen_measure() -> dict:
     out = {"ext": np.array(ext), "U_ck": checksums(U)}
     for k, v in m.items():
         out[k] = np.array(v)
+    # WilsonLoop<start, end, reset> with its chain kept between calls: the driver's doubling
+    # sequence, a sequence with a non-power-of-two extension, and a reset away from the origin
+    # followed by a non-contiguous extension
+    Uc = np.ascontiguousarray(U)
+    seqs = [[(0, 2, 1), (2, 4, 0), (4, 8, 0)], [(0, 3, 1), (3, 5, 0)], [(2, 3, 1), (5, 6, 0)]]
+    out["wl_chain_seq"] = np.array([c for seq in seqs for c in seq])
+    out["wl_chain"] = np.array([ref.lib.ref_wilson_loop_chain(Uc, a, b, r) for seq in seqs for (a, b, r) in seq])
     links = sample_links(int(np.prod(ext)), 5)
     out["links"] = links
     for integ in range(4):

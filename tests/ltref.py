@@ -294,6 +294,7 @@ class Reference:
                 "ref_or_sweeps4": (i, [_dp, i, i, d, d]),
                 "ref_md_action": (i, [_dp, _dp, d, d, i, i, i, d, d, C.POINTER(d), C.POINTER(d)]),
                 "ref_flow_action": (None, [_dp, _dp, d, i, i, i, d, d]),
+                "ref_wilson_loop_chain": (d, [_dp, i, i, i]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(lib, name)

@@ -77,6 +77,21 @@ class TestBundle:
         want = oracle.lib.or_wilson_loop(oracle._e(ext), np.ascontiguousarray(U), L)
         assert lt.WilsonLoop(gpu(ext, U), L) == pytest.approx(want, rel=TOL)
 
+    def test_wilson_loop_chain(self, golden_measure):
+        """WilsonLoop<start, end, reset> with the chain kept between calls, against the
+        reference: the doubling sequence, an extension by single links, and a reset away from
+        the origin followed by a non-contiguous extension (the reference's literal semantics)."""
+        g = golden_measure
+        G = gpu(tuple(int(e) for e in g["ext"]), g["U"])
+        for (a, b, r), want in zip(g["wl_chain_seq"], g["wl_chain"]):
+            assert lt.WilsonLoopChain(G, int(a), int(b), bool(r)) == pytest.approx(float(want), rel=TOL), (a, b, r)
+        H = lt.GaugeField((4, 4, 4, 4))
+        with pytest.raises(lt.LettuceError):   # nothing to extend
+            lt.WilsonLoopChain(H, 2, 4, False)
+        lt.WilsonLoop(G, 2)                    # the plain form drops the kept chain
+        with pytest.raises(lt.LettuceError):
+            lt.WilsonLoopChain(G, 2, 4, False)
+
     def test_unit_field(self):
         ext = (4, 4, 6, 4)
         G = lt.GaugeField(ext)

@@ -210,6 +210,10 @@ class TestMeasurementBundle:
         np.testing.assert_allclose(m["q_t"], g["q_t"], rtol=1e-10, atol=1e-14)
         np.testing.assert_allclose(m["e_t"], g["e_t"], rtol=TOL)
         assert m["q_t"].sum() == pytest.approx(oracle.topcharge(ext, U), rel=1e-12, abs=1e-14)
+        # the reference's chained WilsonLoop along straight runs equals the loop of the end length
+        for (a, b, r), want in list(zip(g["wl_chain_seq"], g["wl_chain"]))[:5]:
+            assert oracle.lib.or_wilson_loop(oracle._e(ext), np.ascontiguousarray(U), int(b)) == pytest.approx(
+                float(want), rel=TOL)
         for integ in range(4):
             F = oracle.flow(ext, U, 0.02, 5, integ)
             assert rel_err(links_of(F, g["links"]), g[f"flow{integ}"]) < TOL, integ
