@@ -74,6 +74,39 @@ def test_null_handles_are_errors():
     assert lt.lib().lt_destroy(None) == _lib.LT_OK
 
 
+def test_create_rejects_oversized_lattice_without_device():
+    """4 V 9 complex entries must stay below 2^31 (96^4 does not)."""
+    h = C.c_void_p()
+    assert lt.lib().lt_create(np.array([96, 96, 96, 96], dtype=np.int32), 0, C.byref(h)) == _lib.LT_ERR_ARG
+    assert b"too large" in lt.lib().lt_last_error()
+    assert lt.lib().lt_create(np.array([2, 2, 2, 0], dtype=np.int32), 0, C.byref(h)) == _lib.LT_ERR_ARG
+
+
+def test_entry_points_check_handles_without_device():
+    """Every entry point refuses a null handle before touching a device."""
+    L = lt.lib()
+    v, w = C.c_double(), C.c_double()
+    u = C.c_uint64(0)
+    calls = {
+        "lt_md_integrate": lambda: L.lt_md_integrate(None, None, 3, 6.0, 1.0, 2, 0.1, 1, None, None),
+        "lt_md_trajectory": lambda: L.lt_md_trajectory(None, None, 3, 6.0, 1.0, 2, 0.1, 1, C.c_uint64(1), C.byref(u), 1,
+                                                       None, None, None),
+        "lt_reverse_momenta": lambda: L.lt_reverse_momenta(None),
+        "lt_parity_update": lambda: L.lt_parity_update(None),
+        "lt_set_gauge_action": lambda: L.lt_set_gauge_action(None, 2, 1.0, 0.0),
+        "lt_overrelax_sweeps4": lambda: L.lt_overrelax_sweeps4(None, 1),
+        "lt_heatbath_sweeps4": lambda: L.lt_heatbath_sweeps4(None, 6.0, 1, C.c_uint64(1), C.byref(u)),
+        "lt_wilson_loop_chain": lambda: L.lt_wilson_loop_chain(None, 0, 2, 1, C.byref(v)),
+        "lt_polyakov_loop": lambda: L.lt_polyakov_loop(None, C.byref(v), C.byref(w)),
+        "lt_flow": lambda: L.lt_flow(None, None, 0, 0.01, 1),
+        "lt_clover_timeslices": lambda: L.lt_clover_timeslices(None, None, None),
+        "lt_status_word": lambda: L.lt_status_word(None, C.byref(C.c_uint32()), 0),
+    }
+    for name, call in calls.items():
+        assert call() == _lib.LT_ERR_ARG, name
+        assert b"null handle" in L.lt_last_error(), name
+
+
 def test_bias_matches_reference_fixture(golden_bias):
     g = golden_bias
     for sym in (0, 1):
