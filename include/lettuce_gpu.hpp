@@ -65,6 +65,7 @@ public:
     void SetToIdentity() { check(lt_set_identity(h_)); }
     void SetToHaarRandom(std::uint64_t seed) { check(lt_set_haar_random(h_, seed)); }
     std::size_t Volume() const { return (std::size_t)ext_[0] * ext_[1] * ext_[2] * ext_[3]; }
+    std::size_t SpatialVolume() const { return (std::size_t)ext_[1] * ext_[2] * ext_[3]; }   // lattice.hpp:201-204
     int Length(int d) const { return ext_[d]; }
     std::array<int, 4> Shape() const { return ext_; }
 

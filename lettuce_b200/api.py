@@ -58,6 +58,9 @@ class GaugeField:
     def Volume(self) -> int:
         return int(np.prod(self.ext))
 
+    def SpatialVolume(self) -> int:
+        return int(np.prod(self.ext[1:]))
+
     def Length(self, d: int) -> int:
         return self.ext[d]
 
