@@ -158,10 +158,9 @@ template <> struct Gauge<float, 2>
         return reinterpret_cast<const float4*>(p) + (size_t)((mu * 2 + par) * 3 + c) * (size_t)vh;
     }
 
-    LT_D M3<float> ld_rows(int mu, int par, int s) const
+    // rows 0-1 of a link from its three chunks
+    static LT_D M3<float> rows_of(const float4& a, const float4& b, const float4& c)
     {
-        const float4* q = chunk(mu, par, 0) + s;
-        const float4 a = q[0], b = q[vh], c = q[2 * (size_t)vh];
         M3<float> m;
         m.e[0][0] = mkc<float>(a.x, a.y);
         m.e[0][1] = mkc<float>(a.z, a.w);
@@ -170,6 +169,12 @@ template <> struct Gauge<float, 2>
         m.e[1][1] = mkc<float>(c.x, c.y);
         m.e[1][2] = mkc<float>(c.z, c.w);
         return m;
+    }
+
+    LT_D M3<float> ld_rows(int mu, int par, int s) const
+    {
+        const float4* q = chunk(mu, par, 0) + s;
+        return rows_of(q[0], q[vh], q[2 * (size_t)vh]);
     }
 
     LT_D M3<float> ld(int mu, int par, int s) const

@@ -1,6 +1,8 @@
 // Backend implementation for one storage format: launches the kernels of lt_kernels.cuh.
 #pragma once
 #include <algorithm>
+#include <atomic>
+#include <type_traits>
 
 #include "lt_backend.h"
 #include "lt_kernels.cuh"
@@ -46,6 +48,19 @@ inline void launch_chained(void (*k)(KArgs...), int grid, int block, cudaStream_
 #else
     k<<<grid, block, 0, s>>>(static_cast<KArgs>(args)...);
 #endif
+}
+
+// Kernels with a shared-memory ring ask for the largest shared-memory carveout (set once per
+// device and kernel), so that their residency is bounded by registers and the ring alone
+template <auto K> inline void prefer_shared()
+{
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_relaxed) & bit) return;
+    cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    done.fetch_or(bit);
 }
 
 template <typename T, int NR> class BackendImpl final : public Backend
@@ -120,16 +135,34 @@ public:
         finish(c, slot, 1);
     }
 
+    static constexpr bool kStaged = LT_STAGED_STAPLE && std::is_same<T, float>::value && NR == 2;
+
     void overrelax(const Ctx& c, void* U, int mu, int par) const override
     {
-        launch_chained(k_overrelax<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu, par,
-                       next_order(c));
+        if constexpr (kStaged)
+        {
+            prefer_shared<k_overrelax_staged<0>>();
+            launch_chained(k_overrelax_staged<0>, nblocks(c.g.vh, kStagedThreads), kStagedThreads, c.stream, gauge(U, c.g), c.g, mu,
+                           par, next_order(c));
+        }
+        else
+            launch_chained(k_overrelax<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu,
+                           par, next_order(c));
     }
     void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter, uint64_t seed,
                   int max_iter) const override
     {
-        launch_chained(k_heatbath<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu, par,
-                       (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter, c.status, next_order(c));
+        if constexpr (kStaged)
+        {
+            prefer_shared<k_heatbath_staged<0>>();
+            launch_chained(k_heatbath_staged<0>, nblocks(c.g.vh, kStagedThreads), kStagedThreads, c.stream, gauge(U, c.g), c.g, mu,
+                           par, (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter, c.status,
+                           next_order(c));
+        }
+        else
+            launch_chained(k_heatbath<T, NR>, nblocks(c.g.vh, kThreads), kThreads, c.stream, gauge(U, c.g), c.g, mu,
+                           par, (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32), max_iter, c.status,
+                           next_order(c));
     }
     void check_links(const Ctx& c, const void* U, double tol, unsigned* maxbits) const override
     {

@@ -180,6 +180,132 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
     return acc;
 }
 
+// ---------------------------------------------------------------- staged staple
+// For two-row FP32 storage the sweep kernels stage the 18 staple links and the updated link
+// through shared memory: each thread copies the three links of a staple path with cp.async
+// (16-byte chunks, L2 only) two paths ahead of their use into its own slot of a two-path
+// ring, so the loads of path k+1 are in flight while path k is multiplied and hold no
+// registers meanwhile.  Same paths and products as staple() (summed path by path).
+#ifndef LT_STAGED_STAPLE
+#define LT_STAGED_STAPLE 1
+#endif
+#ifndef LT_STAGED_SLOTS
+#define LT_STAGED_SLOTS 2
+#endif
+#ifndef LT_MINB_STAGED
+#define LT_MINB_STAGED 6
+#endif
+#ifndef LT_STAGED_THREADS
+#define LT_STAGED_THREADS 128
+#endif
+constexpr int kStagedThreads = LT_STAGED_THREADS;
+
+LT_D void cp_async16(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+#ifdef LT_STAGED_CA
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+#else
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+#endif
+}
+LT_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> LT_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// LT_STAGED_SLOTS slots of three links (nine float4 chunks) per thread of a block of
+// kStagedThreads: 18,432 bytes per slot for 128 threads
+struct StapleRing
+{
+    float4 c[LT_STAGED_SLOTS][9][kStagedThreads];
+};
+
+LT_D void stage_link(StapleRing& r, int slot, int j, const float4* q, int vh)
+{
+    const int t = threadIdx.x;
+    cp_async16(&r.c[slot][3 * j][t], q);
+    cp_async16(&r.c[slot][3 * j + 1][t], q + vh);
+    cp_async16(&r.c[slot][3 * j + 2][t], q + 2 * (size_t)vh);
+}
+
+LT_D M3<float> staged_rows(const StapleRing& r, int slot, int j)
+{
+    const int t = threadIdx.x;
+    return Gauge<float, 2>::rows_of(r.c[slot][3 * j][t], r.c[slot][3 * j + 1][t], r.c[slot][3 * j + 2][t]);
+}
+
+LT_D M3<float> staged_link(const StapleRing& r, int slot, int j)
+{
+    M3<float> m = staged_rows(r, slot, j);
+    restore_last_row(m);
+    return m;
+}
+
+// Copies the links of stage K into `slot`.  Stages 0-5 are the staple paths: direction
+// nu = the (K/2)-th direction other than mu; the upper path U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag
+// for even K, the lower path U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu) for odd K.  Stage 6 is
+// the link (mu, x) itself; later stages copy nothing.  Every stage commits one group.
+template <int K>
+LT_D void stage_path(StapleRing& r, int slot, const Gauge<float, 2>& U, const Geom& g, int par, int i, int s,
+                     const int c[4], int mu, int dmu)
+{
+    const int op = par ^ 1;
+    const int nu = (K >> 1) + ((K >> 1) >= mu ? 1 : 0);
+    if (K < 6 && (K & 1) == 0)
+    {
+        const int inu = i + step_up_rt(g, nu, c);
+        stage_link(r, slot, 0, U.chunk(nu, par, 0) + (i >> 1), U.vh);
+        stage_link(r, slot, 1, U.chunk(mu, op, 0) + (inu >> 1), U.vh);
+        stage_link(r, slot, 2, U.chunk(nu, op, 0) + ((i + dmu) >> 1), U.vh);
+    }
+    else if (K < 6)
+    {
+        const int ind = i + step_dn_rt(g, nu, c);
+        stage_link(r, slot, 0, U.chunk(nu, op, 0) + (ind >> 1), U.vh);
+        stage_link(r, slot, 1, U.chunk(mu, op, 0) + (ind >> 1), U.vh);
+        stage_link(r, slot, 2, U.chunk(nu, par, 0) + ((ind + dmu) >> 1), U.vh);
+    }
+    else if (K == 6)
+        stage_link(r, slot, 0, U.chunk(mu, par, 0) + s, U.vh);
+    cp_async_commit();
+}
+
+// Staple of the link (mu, x) (site i, checkerboard index s) and, in `u`, the link itself.
+LT_D M3<float> staple_staged(StapleRing& r, const Gauge<float, 2>& U, const Geom& g, int par, int i, int s,
+                             const int c[4], int mu, M3<float>& u)
+{
+    constexpr int NS = LT_STAGED_SLOTS;
+    const int dmu = step_up_rt(g, mu, c);
+    stage_path<0>(r, 0, U, g, par, i, s, c, mu, dmu);
+    stage_path<1>(r, 1, U, g, par, i, s, c, mu, dmu);
+    if (NS > 2) stage_path<2>(r, 2 % NS, U, g, par, i, s, c, mu, dmu);
+    M3<float> acc = zero3<float>();
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+    {
+        const int slot = k % NS;
+        cp_async_wait<NS - 1>();
+        M3<float> p;
+        if ((k & 1) == 0)
+            p = mul_nd_rows(mul_rows(staged_rows(r, slot, 0), staged_link(r, slot, 1)), staged_link(r, slot, 2));
+        else
+            p = mul_rows(mul_dn_rows(staged_link(r, slot, 0), staged_link(r, slot, 1)), staged_link(r, slot, 2));
+        restore_last_row(p);
+        acc = acc + p;
+        switch (k + NS)
+        {
+        case 2: stage_path<2>(r, slot, U, g, par, i, s, c, mu, dmu); break;
+        case 3: stage_path<3>(r, slot, U, g, par, i, s, c, mu, dmu); break;
+        case 4: stage_path<4>(r, slot, U, g, par, i, s, c, mu, dmu); break;
+        case 5: stage_path<5>(r, slot, U, g, par, i, s, c, mu, dmu); break;
+        case 6: stage_path<6>(r, slot, U, g, par, i, s, c, mu, dmu); break;
+        default: cp_async_commit(); break;
+        }
+    }
+    cp_async_wait<0>();
+    u = staged_link(r, 6 % NS, 0);
+    return acc;
+}
+
 // exp(c X) U followed by GramSchmidt (gradient_flow.hpp:265-282, hmc_gauge.hpp:505-523,
 // stout_smearing.hpp:52-53).  With two-row storage only rows 0 and 1 are formed: the store
 // keeps only those and every load rebuilds the third.
@@ -739,6 +865,25 @@ __global__ void __launch_bounds__(kThreads, (OrMinBlocks<T, NR>::value)) k_overr
     or_update(U, g, mu, par, s);
 }
 
+// The same on two-row FP32 storage with the staged staple (6 blocks of 128 per SM: the
+// shared-memory ring of 36,864 bytes per block bounds residency)
+template <int Unused = 0>
+__global__ void __launch_bounds__(kStagedThreads, LT_MINB_STAGED) k_overrelax_staged(Gauge<float, 2> U, Geom g, int mu, int par, int rev)
+{
+    __shared__ StapleRing ring;
+    int s;
+    const bool ok = half_site_of_thread(g, s, rev);
+    pdl_release();
+    pdl_wait();
+    if (!ok) return;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    M3<float> u;
+    const M3<float> st = staple_staged(ring, U, g, par, i, s, c, mu, u);
+    or_apply<float, 2>(u, st);
+    U.st(mu, par, s, u);
+}
+
 // One (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the handle's action
 template <typename T, int NR, bool RECT>
 __global__ void __launch_bounds__(kThreads, (RECT ? 1 : Cb4MinBlocks<T, NR>::value)) k_overrelax4(Gauge<T, NR> U, Geom g, int mu, int sub, T cp, T cr)
@@ -881,6 +1026,29 @@ LT_D void hb_update(const Gauge<T, NR>& U, const Geom& g, int mu, int par, int s
     hb_core(U, mu, par, s, i, staple(U, g, par, i, c, mu), prefactor, counter, k0, k1, max_iter, status);
 }
 
+template <typename T, int NR>
+LT_D void hb_core_u(const Gauge<T, NR>& U, int mu, int par, int s, int i, M3<T> u, const M3<T>& st, T prefactor,
+                    uint64_t counter, uint32_t k0, uint32_t k1, int max_iter, unsigned* status);
+
+// k_heatbath on two-row FP32 storage with the staged staple
+template <int Unused = 0>
+__global__ void __launch_bounds__(kStagedThreads, LT_MINB_STAGED) k_heatbath_staged(Gauge<float, 2> U, Geom g, int mu, int par,
+                                                                 float prefactor, uint64_t counter, uint32_t k0,
+                                                                 uint32_t k1, int max_iter, unsigned* status, int rev)
+{
+    __shared__ StapleRing ring;
+    int s;
+    const bool ok = half_site_of_thread(g, s, rev);
+    pdl_release();
+    pdl_wait();
+    if (!ok) return;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    M3<float> u;
+    const M3<float> st = staple_staged(ring, U, g, par, i, s, c, mu, u);
+    hb_core_u(U, mu, par, s, i, u, st, prefactor, counter, k0, k1, max_iter, status);
+}
+
 // One (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the handle's action
 template <typename T, int NR, bool RECT>
 __global__ void __launch_bounds__(kThreads, (RECT ? 1 : Cb4MinBlocks<T, NR>::value)) k_heatbath4(Gauge<T, NR> U, Geom g, int mu, int sub, T prefactor,
@@ -903,7 +1071,14 @@ template <typename T, int NR>
 LT_D void hb_core(const Gauge<T, NR>& U, int mu, int par, int s, int i, const M3<T>& st, T prefactor,
                   uint64_t counter, uint32_t k0, uint32_t k1, int max_iter, unsigned* status)
 {
-    M3<T> u = U.ld(mu, par, s);
+    hb_core_u(U, mu, par, s, i, U.ld(mu, par, s), st, prefactor, counter, k0, k1, max_iter, status);
+}
+
+// The same with the link u already loaded
+template <typename T, int NR>
+LT_D void hb_core_u(const Gauge<T, NR>& U, int mu, int par, int s, int i, M3<T> u, const M3<T>& st, T prefactor,
+                    uint64_t counter, uint32_t k0, uint32_t k1, int max_iter, unsigned* status)
+{
     M3<T> w = mul_nd(u, st);
     const uint32_t link = (uint32_t)(4 * i + mu);
     bool capped = false;

@@ -143,6 +143,21 @@ class TestLocalUpdates:
         assert hb.counter.value == 6
         assert rel_err(G.download(), oracle.heatbath(ext, therm8, 6.0, 1, 777, 5)) < 1e-11
 
+    def test_heatbath_sweep_fp32_storages_same_stream(self, therm8):
+        """The FP32 sampler on two-row links (staged staple, third row rebuilt) against the same
+        sampler on full FP32 links: same Philox stream, same proposals, so all links but those
+        whose accept/reject comparison falls within FP32 rounding of its threshold agree to
+        FP32 accuracy."""
+        ext = (8, 8, 8, 8)
+        out = []
+        for prec in ("fp32", "fp32_12"):
+            G = gpu(ext, therm8, prec)
+            lt.Iterator.Checkerboard(lt.HeatbathKernel(G, lt.WilsonAction(6.0), seed=777, counter=5), 2)
+            out.append(G.download())
+        d = np.abs(out[0] - out[1]).reshape(-1, 18).max(axis=1)
+        assert np.median(d) < 1e-5
+        assert np.mean(d > 1e-3) < 0.01
+
     def test_heatbath_keeps_group(self, therm8):
         G = gpu((8, 8, 8, 8), therm8, "fp32")
         lt.Iterator.Checkerboard(lt.HeatbathKernel(G, lt.WilsonAction(6.0), seed=3), 3)
