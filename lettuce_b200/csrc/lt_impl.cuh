@@ -223,18 +223,46 @@ public:
     void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new, double c_exp,
                     int read_z, int write_z) const override
     {
+        if constexpr (kStaged)
+        {
+            if (!c.rect)
+            {
+                prefer_shared<k_flow_stage_staged<0>>();
+                launch_chained(k_flow_stage_staged<0>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
+                               gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp,
+                               read_z, write_z, next_order(c));
+                return;
+            }
+        }
         launch_chained(c.rect ? k_flow_stage<T, NR, true> : k_flow_stage<T, NR, false>, nblocks(c.g.V, kSitesPerBlock),
                        4 * kSitesPerBlock, c.stream, gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old,
                        (T)c_new, (T)c_exp, read_z, write_z, (T)c.cp, (T)c.cr, next_order(c));
     }
     void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
     {
+        if constexpr (kStaged)
+        {
+            prefer_shared<k_stout_staged<0>>();
+            launch_chained(k_stout_staged<0>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
+                           gauge(Uin, c.g), gauge(Uout, c.g), c.g, (T)rho);
+            return;
+        }
         launch_chained(k_stout<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
                        gauge(Uout, c.g), c.g, (T)rho);
     }
 
     void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const override
     {
+        if constexpr (kStaged)
+        {
+            if (!c.rect)
+            {
+                prefer_shared<k_momenta_staged<0>>();
+                k_momenta_staged<0><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
+                    gauge(U, c.g), alg(P, c.g), alg(F, c.g), c.g, (T)coef, (T)eps, F != nullptr);
+                return;
+            }
+        }
         auto k = c.rect ? k_momenta<T, NR, true> : k_momenta<T, NR, false>;
         k<<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
             gauge(U, c.g), alg(P, c.g), alg(F, c.g), c.g, (T)coef, (T)eps, F != nullptr, (T)c.cp, (T)c.cr);

@@ -169,6 +169,10 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
             restore_last_row(up);
             dn = mul_rows(mul_dn_rows(U.ld(nu, op, ind >> 1), U.ld(mu, op, ind >> 1)), U.ld(nu, par, (ind + dmu) >> 1));
             restore_last_row(dn);
+            // path by path, in the order of the staged staple (identical rounding)
+            acc = acc + up;
+            acc = acc + dn;
+            continue;
         }
         else
         {
@@ -189,9 +193,6 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
 #ifndef LT_STAGED_STAPLE
 #define LT_STAGED_STAPLE 1
 #endif
-#ifndef LT_STAGED_SLOTS
-#define LT_STAGED_SLOTS 2
-#endif
 #ifndef LT_MINB_STAGED
 #define LT_MINB_STAGED 6
 #endif
@@ -203,20 +204,16 @@ constexpr int kStagedThreads = LT_STAGED_THREADS;
 LT_D void cp_async16(void* dst, const void* src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-#ifdef LT_STAGED_CA
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-#else
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-#endif
 }
 LT_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> LT_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// LT_STAGED_SLOTS slots of three links (nine float4 chunks) per thread of a block of
-// kStagedThreads: 18,432 bytes per slot for 128 threads
+// Two slots of three links (nine float4 chunks) per thread of a block of kStagedThreads:
+// 36,864 bytes for 128 threads
 struct StapleRing
 {
-    float4 c[LT_STAGED_SLOTS][9][kStagedThreads];
+    float4 c[2][9][kStagedThreads];
 };
 
 LT_D void stage_link(StapleRing& r, int slot, int j, const float4* q, int vh)
@@ -240,69 +237,69 @@ LT_D M3<float> staged_link(const StapleRing& r, int slot, int j)
     return m;
 }
 
-// Copies the links of stage K into `slot`.  Stages 0-5 are the staple paths: direction
-// nu = the (K/2)-th direction other than mu; the upper path U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag
-// for even K, the lower path U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu) for odd K.  Stage 6 is
-// the link (mu, x) itself; later stages copy nothing.  Every stage commits one group.
-template <int K>
-LT_D void stage_path(StapleRing& r, int slot, const Gauge<float, 2>& U, const Geom& g, int par, int i, int s,
-                     const int c[4], int mu, int dmu)
+// Copies the three links of a staple path of (mu, x) along nu into `slot`: the upper path
+// U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag, or the lower path U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu).
+template <bool UP>
+LT_D void stage_path(StapleRing& r, int slot, const Gauge<float, 2>& U, const Geom& g, int par, int i,
+                     const int c[4], int mu, int nu, int dmu)
 {
     const int op = par ^ 1;
-    const int nu = (K >> 1) + ((K >> 1) >= mu ? 1 : 0);
-    if (K < 6 && (K & 1) == 0)
+    if (UP)
     {
         const int inu = i + step_up_rt(g, nu, c);
         stage_link(r, slot, 0, U.chunk(nu, par, 0) + (i >> 1), U.vh);
         stage_link(r, slot, 1, U.chunk(mu, op, 0) + (inu >> 1), U.vh);
         stage_link(r, slot, 2, U.chunk(nu, op, 0) + ((i + dmu) >> 1), U.vh);
     }
-    else if (K < 6)
+    else
     {
         const int ind = i + step_dn_rt(g, nu, c);
         stage_link(r, slot, 0, U.chunk(nu, op, 0) + (ind >> 1), U.vh);
         stage_link(r, slot, 1, U.chunk(mu, op, 0) + (ind >> 1), U.vh);
         stage_link(r, slot, 2, U.chunk(nu, par, 0) + ((ind + dmu) >> 1), U.vh);
     }
-    else if (K == 6)
-        stage_link(r, slot, 0, U.chunk(mu, par, 0) + s, U.vh);
-    cp_async_commit();
 }
 
 // Staple of the link (mu, x) (site i, checkerboard index s) and, in `u`, the link itself.
+// Slot 0 carries the upper paths, slot 1 the lower ones; the next direction's path is copied
+// into a slot as soon as its current path is multiplied out, and the link itself follows the
+// last upper path.  Each half-iteration commits one copy group (possibly empty), so waiting
+// for all but the latest group always completes the path about to be used.  The direction
+// loop is unrolled or not (ROLLED): the rolled loop keeps the larger heatbath and flow kernels
+// within the instruction caches (measured faster there, the unrolled one for overrelaxation).
+template <bool ROLLED>
 LT_D M3<float> staple_staged(StapleRing& r, const Gauge<float, 2>& U, const Geom& g, int par, int i, int s,
                              const int c[4], int mu, M3<float>& u)
 {
-    constexpr int NS = LT_STAGED_SLOTS;
     const int dmu = step_up_rt(g, mu, c);
-    stage_path<0>(r, 0, U, g, par, i, s, c, mu, dmu);
-    stage_path<1>(r, 1, U, g, par, i, s, c, mu, dmu);
-    if (NS > 2) stage_path<2>(r, 2 % NS, U, g, par, i, s, c, mu, dmu);
+    const int nu0 = mu == 0 ? 1 : 0;
+    stage_path<true>(r, 0, U, g, par, i, c, mu, nu0, dmu);
+    cp_async_commit();
+    stage_path<false>(r, 1, U, g, par, i, c, mu, nu0, dmu);
+    cp_async_commit();
     M3<float> acc = zero3<float>();
-#pragma unroll
-    for (int k = 0; k < 6; ++k)
+#pragma unroll(ROLLED ? 1 : 3)
+    for (int n = 0; n < 3; ++n)
     {
-        const int slot = k % NS;
-        cp_async_wait<NS - 1>();
-        M3<float> p;
-        if ((k & 1) == 0)
-            p = mul_nd_rows(mul_rows(staged_rows(r, slot, 0), staged_link(r, slot, 1)), staged_link(r, slot, 2));
-        else
-            p = mul_rows(mul_dn_rows(staged_link(r, slot, 0), staged_link(r, slot, 1)), staged_link(r, slot, 2));
+        const int nn = (n + 1) + (n + 1 >= mu ? 1 : 0);   // the direction after this one
+        cp_async_wait<1>();
+        M3<float> p = mul_nd_rows(mul_rows(staged_rows(r, 0, 0), staged_link(r, 0, 1)), staged_link(r, 0, 2));
         restore_last_row(p);
         acc = acc + p;
-        switch (k + NS)
-        {
-        case 2: stage_path<2>(r, slot, U, g, par, i, s, c, mu, dmu); break;
-        case 3: stage_path<3>(r, slot, U, g, par, i, s, c, mu, dmu); break;
-        case 4: stage_path<4>(r, slot, U, g, par, i, s, c, mu, dmu); break;
-        case 5: stage_path<5>(r, slot, U, g, par, i, s, c, mu, dmu); break;
-        case 6: stage_path<6>(r, slot, U, g, par, i, s, c, mu, dmu); break;
-        default: cp_async_commit(); break;
-        }
+        if (n < 2)
+            stage_path<true>(r, 0, U, g, par, i, c, mu, nn, dmu);
+        else
+            stage_link(r, 0, 0, U.chunk(mu, par, 0) + s, U.vh);
+        cp_async_commit();
+        cp_async_wait<1>();
+        p = mul_rows(mul_dn_rows(staged_link(r, 1, 0), staged_link(r, 1, 1)), staged_link(r, 1, 2));
+        restore_last_row(p);
+        acc = acc + p;
+        if (n < 2) stage_path<false>(r, 1, U, g, par, i, c, mu, nn, dmu);
+        cp_async_commit();
     }
     cp_async_wait<0>();
-    u = staged_link(r, 6 % NS, 0);
+    u = staged_link(r, 0, 0);
     return acc;
 }
 
@@ -879,7 +876,7 @@ __global__ void __launch_bounds__(kStagedThreads, LT_MINB_STAGED) k_overrelax_st
     int c[4];
     const int i = site_coords(g, par, s, c);
     M3<float> u;
-    const M3<float> st = staple_staged(ring, U, g, par, i, s, c, mu, u);
+    const M3<float> st = staple_staged<false>(ring, U, g, par, i, s, c, mu, u);
     or_apply<float, 2>(u, st);
     U.st(mu, par, s, u);
 }
@@ -1045,7 +1042,7 @@ __global__ void __launch_bounds__(kStagedThreads, LT_MINB_STAGED) k_heatbath_sta
     int c[4];
     const int i = site_coords(g, par, s, c);
     M3<float> u;
-    const M3<float> st = staple_staged(ring, U, g, par, i, s, c, mu, u);
+    const M3<float> st = staple_staged<true>(ring, U, g, par, i, s, c, mu, u);
     hb_core_u(U, mu, par, s, i, u, st, prefactor, counter, k0, k1, max_iter, status);
 }
 
@@ -1191,6 +1188,37 @@ __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_flo
     Uout.st(mu, par, s, exp_update<T, NR>(unpack_ah(z), c_exp, u));
 }
 
+// k_flow_stage (Wilson action) on two-row FP32 storage with the staged staple; Z of the link
+// is read before the staple so that its loads are in flight meanwhile
+#ifndef LT_MINB_FLOW_STAGED
+#define LT_MINB_FLOW_STAGED 5
+#endif
+template <int Unused = 0>
+__global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
+    k_flow_stage_staged(Gauge<float, 2> Uin, Gauge<float, 2> Uout, Alg<float> Z, Geom g, float c_old, float c_new,
+                        float c_exp, int read_z, int write_z, int rev)
+{
+    static_assert(4 * kSitesPerBlock == kStagedThreads, "one ring slot per thread");
+    __shared__ StapleRing ring;
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x, rev)) return;
+    const int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    A8<float> z;
+    if (read_z)
+        z = Z.ld(mu, par, s);
+    M3<float> u;
+    const M3<float> st = staple_staged<true>(ring, Uin, g, par, i, s, c, mu, u);
+    const A8<float> a = algebra8(mul_nd(st, u));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) z.a[k] = read_z ? c_old * z.a[k] + c_new * a.a[k] : c_new * a.a[k];
+    if (write_z) Z.st(mu, par, s, z);
+    Uout.st(mu, par, s, exp_update<float, 2>(unpack_ah(z), c_exp, u));
+}
+
 // ---------------------------------------------------------------- stout smearing
 // StoutSmearing4D (smearing/stout_smearing.hpp:29-57): U' = exp(rho Algebra(st U^dag)) U, Gram-Schmidt
 template <typename T, int NR>
@@ -1206,6 +1234,24 @@ __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_sto
     M3<T> u = Uin.ld(mu, par, s);
     M3<T> st = staple(Uin, g, par, i, c, mu);
     Uout.st(mu, par, s, exp_update<T, NR>(unpack_ah(algebra8(mul_nd(st, u))), rho, u));
+}
+
+// k_stout on two-row FP32 storage with the staged staple
+template <int Unused = 0>
+__global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
+    k_stout_staged(Gauge<float, 2> Uin, Gauge<float, 2> Uout, Geom g, float rho)
+{
+    __shared__ StapleRing ring;
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
+    const int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    M3<float> u;
+    const M3<float> st = staple_staged<true>(ring, Uin, g, par, i, s, c, mu, u);
+    Uout.st(mu, par, s, exp_update<float, 2>(unpack_ah(algebra8(mul_nd(st, u))), rho, u));
 }
 
 // ---------------------------------------------------------------- clover observables
@@ -1564,6 +1610,29 @@ __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_mom
 #pragma unroll
         for (int k = 0; k < 8; ++k) p.a[k] += eps * coef * a.a[k];
     }
+    P.st(mu, par, s, p);
+}
+
+// k_momenta (Wilson action) on two-row FP32 storage with the staged staple; P (and F) of the
+// link are read before the staple so that their loads are in flight meanwhile
+template <int Unused = 0>
+__global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
+    k_momenta_staged(Gauge<float, 2> U, Alg<float> P, Alg<float> F, Geom g, float coef, float eps, int use_f)
+{
+    __shared__ StapleRing ring;
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
+    const int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    A8<float> p = P.ld(mu, par, s), f;
+    if (use_f)
+        f = F.ld(mu, par, s);
+    M3<float> u;
+    const M3<float> st = staple_staged<true>(ring, U, g, par, i, s, c, mu, u);
+    const A8<float> a = algebra8(mul_nd(st, u));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) p.a[k] += use_f ? eps * (coef * a.a[k] + f.a[k]) : eps * coef * a.a[k];
     P.st(mu, par, s, p);
 }
 
