@@ -306,9 +306,15 @@ public:
     {
         const LatDesc* d = static_cast<const LatDesc*>(desc);
         if (op == 0)
+        {
+            if constexpr (kStaged && kBatchBlocks[SEL] <= 128) prefer_shared<k_batch_sweep<T, NR, SEL, 0>>();
             k_batch_sweep<T, NR, SEL, 0><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter);
+        }
         else
+        {
+            if constexpr (kStaged && kBatchBlocks[SEL] <= 128) prefer_shared<k_batch_sweep<T, NR, SEL, 1>>();
             k_batch_sweep<T, NR, SEL, 1><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter);
+        }
     }
 
     void batch_sweep(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int sel, int op, int mu, int par,

@@ -4,6 +4,7 @@
 // planes described in lt_field.cuh.
 #pragma once
 #include "lt_field.cuh"
+#include <type_traits>
 
 namespace lt {
 
@@ -209,14 +210,15 @@ LT_D void cp_async16(void* dst, const void* src)
 LT_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> LT_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// Two slots of three links (nine float4 chunks) per thread of a block of kStagedThreads:
-// 36,864 bytes for 128 threads
-struct StapleRing
+// Two slots of three links (nine float4 chunks) per thread of a block of NT threads: 36,864
+// bytes for 128 threads
+template <int NT> struct StapleRingT
 {
-    float4 c[2][9][kStagedThreads];
+    float4 c[2][9][NT];
 };
+using StapleRing = StapleRingT<kStagedThreads>;
 
-LT_D void stage_link(StapleRing& r, int slot, int j, const float4* q, int vh)
+template <int NT> LT_D void stage_link(StapleRingT<NT>& r, int slot, int j, const float4* q, int vh)
 {
     const int t = threadIdx.x;
     cp_async16(&r.c[slot][3 * j][t], q);
@@ -224,13 +226,13 @@ LT_D void stage_link(StapleRing& r, int slot, int j, const float4* q, int vh)
     cp_async16(&r.c[slot][3 * j + 2][t], q + 2 * (size_t)vh);
 }
 
-LT_D M3<float> staged_rows(const StapleRing& r, int slot, int j)
+template <int NT> LT_D M3<float> staged_rows(const StapleRingT<NT>& r, int slot, int j)
 {
     const int t = threadIdx.x;
     return Gauge<float, 2>::rows_of(r.c[slot][3 * j][t], r.c[slot][3 * j + 1][t], r.c[slot][3 * j + 2][t]);
 }
 
-LT_D M3<float> staged_link(const StapleRing& r, int slot, int j)
+template <int NT> LT_D M3<float> staged_link(const StapleRingT<NT>& r, int slot, int j)
 {
     M3<float> m = staged_rows(r, slot, j);
     restore_last_row(m);
@@ -239,8 +241,8 @@ LT_D M3<float> staged_link(const StapleRing& r, int slot, int j)
 
 // Copies the three links of a staple path of (mu, x) along nu into `slot`: the upper path
 // U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag, or the lower path U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu).
-template <bool UP>
-LT_D void stage_path(StapleRing& r, int slot, const Gauge<float, 2>& U, const Geom& g, int par, int i,
+template <bool UP, int NT>
+LT_D void stage_path(StapleRingT<NT>& r, int slot, const Gauge<float, 2>& U, const Geom& g, int par, int i,
                      const int c[4], int mu, int nu, int dmu)
 {
     const int op = par ^ 1;
@@ -267,8 +269,8 @@ LT_D void stage_path(StapleRing& r, int slot, const Gauge<float, 2>& U, const Ge
 // for all but the latest group always completes the path about to be used.  The direction
 // loop is unrolled or not (ROLLED): the rolled loop keeps the larger heatbath and flow kernels
 // within the instruction caches (measured faster there, the unrolled one for overrelaxation).
-template <bool ROLLED>
-LT_D M3<float> staple_staged(StapleRing& r, const Gauge<float, 2>& U, const Geom& g, int par, int i, int s,
+template <bool ROLLED, int NT>
+LT_D M3<float> staple_staged(StapleRingT<NT>& r, const Gauge<float, 2>& U, const Geom& g, int par, int i, int s,
                              const int c[4], int mu, M3<float>& u)
 {
     const int dmu = step_up_rt(g, mu, c);
@@ -1141,8 +1143,26 @@ __global__ void __launch_bounds__(kBatchBlocks[SEL], (BatchMinBlocks<T, kBatchBl
     Gauge<T, NR> U;
     U.p = (cx<T>*)d[k].U;
     U.vh = g.vh;
-    if (OP == 0) hb_update(U, g, mu, par, s, (T)d[k].prefactor, *counter, d[k].k0, d[k].k1, max_iter, d[k].status);
-    else or_update(U, g, mu, par, s);
+    if constexpr (LT_STAGED_STAPLE && std::is_same<T, float>::value && NR == 2 && BLOCK <= 128)
+    {
+        // two-row FP32 links: the staged staple of the single-lattice sweeps
+        __shared__ StapleRingT<BLOCK> ring;
+        int c[4];
+        const int i = site_coords(g, par, s, c);
+        M3<float> u;
+        const M3<float> st = staple_staged<OP == 0>(ring, U, g, par, i, s, c, mu, u);
+        if (OP == 0)
+            hb_core_u(U, mu, par, s, i, u, st, (T)d[k].prefactor, *counter, d[k].k0, d[k].k1, max_iter, d[k].status);
+        else
+        {
+            or_apply<float, 2>(u, st);
+            U.st(mu, par, s, u);
+        }
+    }
+    else if (OP == 0)
+        hb_update(U, g, mu, par, s, (T)d[k].prefactor, *counter, d[k].k0, d[k].k1, max_iter, d[k].status);
+    else
+        or_update(U, g, mu, par, s);
 }
 
 // Advances the device-side sweep counter (read by the heatbath inside captured graphs)
