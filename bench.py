@@ -476,7 +476,8 @@ def main():
     alg_bytes = bm.sweep_launch_bytes(a.prec, V)   # 9 link reads/writes per update, V/2 updates
     achieved = alg_bytes / (or_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": ncu_traffic(f"k_overrelax<{a.prec}>"), "kernel": f"k_overrelax ({a.prec})",
+                "traffic": ncu_traffic(f"k_overrelax<{a.prec}>"),
+                "kernel": f"k_overrelax_staged ({a.prec})" if a.prec == "fp32_12" else f"k_overrelax ({a.prec})",
                 "ms_per_launch": or_ms, "algorithmic_bytes_per_launch": alg_bytes,
                 "peak_source": f"{peak_kind} hbm_gbs",
                 "heatbath_ms_per_launch": hb_ms,
