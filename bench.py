@@ -542,21 +542,42 @@ def main():
         pinned = torch.empty(therm.size, dtype=torch.float64, pin_memory=True)
         host = pinned.numpy().reshape(therm.shape)
         host[...] = therm
-        E = lt.GaugeField(ext, a.prec)
-        E.upload(host)
-        sweep_round(E)
-        lt.PlaquetteSum(E)
+        # Two handles, each driven by its own host thread (the C ABI serialises calls per handle
+        # only, and ctypes releases the GIL inside them), so that one handle's upload overlaps
+        # the other's sweeps; every step still uploads its whole field and reads its plaquette.
+        fields = [lt.GaugeField(ext, a.prec) for _ in range(2)]
+        for F in fields:
+            F.upload(host)
+            sweep_round(F)
+            lt.PlaquetteSum(F)
         n_e2e = max(3, min(a.steps, 10))
+        errors = []
+
+        def e2e_worker(F, n):
+            try:
+                c = 0
+                for _ in range(n):
+                    F.upload(host)
+                    c = lt.UpdateSweeps(F, BETA, 1, N_HB, N_OR, SEED + rank, c)
+                    lt.PlaquetteSum(F)
+            except Exception as e:   # reported below
+                errors.append(e)
+
+        workers = [threading.Thread(target=e2e_worker, args=(F, n_e2e)) for F in fields]
         barrier()
         t0 = time.perf_counter()
-        for _ in range(n_e2e):
-            E.upload(host)
-            sweep_round(E)
-            lt.PlaquetteSum(E)
+        for w in workers:
+            w.start()
+        for w in workers:
+            w.join()
         dt = max_over_ranks(time.perf_counter() - t0)
-        line["e2e"] = {"value": world * n_e2e * upd_per_step / dt, "unit": UNIT,
+        if errors:
+            raise errors[0]
+        line["e2e"] = {"value": world * 2 * n_e2e * upd_per_step / dt, "unit": UNIT,
                        "h2d_bytes_per_step": int(therm.nbytes), "d2h_bytes_per_step": 8,
-                       "path": "lt_upload_links + lt_update_sweeps + lt_plaquette_sum"}
+                       "path": "lt_upload_links + lt_update_sweeps + lt_plaquette_sum, two handles on two "
+                               "host threads"}
+        del fields
 
         # ---- the other configurations' rates (each bounded to a few seconds)
         line["secondary"] = secondary_rates(lt, torch, timed, a.prec)
