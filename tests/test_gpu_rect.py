@@ -125,6 +125,26 @@ class TestRectangularActions:
         S = lt.LuescherWeiszAction(6.0).Staple(gpu(ext, W, prec))
         assert rel_err(S, oracle.action_staples(ext, W, LUESCHER_WEISZ)) < 1e-6
 
+    @pytest.mark.parametrize("prec", ["fp32", "fp32_12"])
+    def test_fp32_storage_wilson_checkerboard4(self, oracle, golden_rect, prec):
+        """Checkerboard4 with the Wilson action on FP32 links (the two-row storage runs the
+        staged-staple kernels): overrelaxation against the oracle; the heatbath of both FP32
+        storages draws the same stream, so they agree but for accept/reject flips."""
+        g = golden_rect
+        ext = tuple(g["ext"])
+        G = gpu(ext, g["U"], prec)
+        W = G.download()
+        lt.Iterator.Checkerboard4(lt.OverrelaxationSubgroupKernel(G), 1)
+        assert rel_err(G.download(), oracle.overrelax4(ext, W, 1)) < 5e-5
+        out = []
+        for p in ("fp32", prec):
+            H = gpu(ext, W, p)
+            lt.Iterator.Checkerboard4(lt.HeatbathKernel(H, lt.WilsonAction(6.0), seed=9, counter=1), 1)
+            out.append(H.download())
+        d = np.abs(out[0] - out[1]).reshape(-1, 18).max(axis=1)
+        assert np.median(d) < 1e-5
+        assert np.mean(d > 1e-3) < 0.01
+
     def test_checkerboard4_thermalises_like_checkerboard(self):
         """Both iterators sample the same Wilson-action distribution: plaquettes after 30
         rounds from one start agree within the statistical spread of 8^4."""
