@@ -186,11 +186,15 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
 }
 
 // ---------------------------------------------------------------- staged staple
-// For two-row FP32 storage the sweep kernels stage the 18 staple links and the updated link
-// through shared memory: each thread copies the three links of a staple path with cp.async
-// (16-byte chunks, L2 only) two paths ahead of their use into its own slot of a two-path
-// ring, so the loads of path k+1 are in flight while path k is multiplied and hold no
-// registers meanwhile.  Same paths and products as staple() (summed path by path).
+// For two-row FP32 storage the sweep, flow, stout and momentum kernels stage the 18 staple
+// links and the updated link through shared memory: each thread copies the three links of a
+// staple path with cp.async (16-byte chunks, L2 only) into its own slot of a two-path ring,
+// one path ahead of its use, so the loads of the next path are in flight while the current
+// one is multiplied and hold no registers meanwhile.  A slot is refilled only after the
+// products that read it, in program order (the copies are asm volatile with a memory
+// clobber); the thread that reads a slot is the one that filled it, so wait_group alone
+// orders the copies before the reads.  Same paths and products as staple(), summed path by
+// path.
 #ifndef LT_STAGED_STAPLE
 #define LT_STAGED_STAPLE 1
 #endif
