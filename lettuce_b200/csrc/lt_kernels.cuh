@@ -1866,13 +1866,18 @@ __global__ void __launch_bounds__(kThreads) k_clover_deriv(Gauge<T, NR> U, Clov<
 // with Q = -i rho Algebra(st U^dag); the exponential constants are recomputed from U here
 // rather than stored during the forward smearing.  Also writes the link-local part of the
 // recursion, Tloc = Sigma' exp(iQ) + i rho st^dag Lambda.
-// Lambda kernel: 3 blocks of 128 per SM (168 registers, a few spilled) measured 1.5 % faster
-// for the whole force than 2 blocks without spills
-#ifndef LT_MINB_LAMBDA
-#define LT_MINB_LAMBDA 3
+// Lambda kernel on FP32 links: 3 blocks of 128 per SM (168 registers, a few spilled) measured
+// 1.5 % faster for the whole force than 2 blocks without spills; FP64 keeps no cap (a cap of
+// 3 spills 2 KB per thread)
+#ifndef LT_MINB_LAMBDA_F32
+#define LT_MINB_LAMBDA_F32 3
 #endif
+template <typename T> struct LambdaMinBlocks
+{
+    static constexpr int value = sizeof(T) == 4 ? LT_MINB_LAMBDA_F32 : 1;
+};
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, LT_MINB_LAMBDA) k_stout_lambda(Gauge<T, NR> U, Gauge<T, NR> Up, Alg<T> Sigma, Alg<T> Lam,
+__global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_lambda(Gauge<T, NR> U, Gauge<T, NR> Up, Alg<T> Sigma, Alg<T> Lam,
                                                            Full<T> Tloc, Geom g, T rho)
 {
     int mu, x;
