@@ -167,12 +167,11 @@ LT_D M3<T> staple(const Gauge<T, NR>& U, const Geom& g, int par, int i, const in
             // rows are multiplied out and the third is rebuilt (RestoreLastRow), which also
             // spares the reconstruction of the leading factor of the upper path.
             up = mul_nd_rows(mul_rows(U.ld_rows(nu, par, i >> 1), U.ld(mu, op, inu >> 1)), U.ld(nu, op, imu >> 1));
-            restore_last_row(up);
             dn = mul_rows(mul_dn_rows(U.ld(nu, op, ind >> 1), U.ld(mu, op, ind >> 1)), U.ld(nu, par, (ind + dmu) >> 1));
-            restore_last_row(dn);
-            // path by path, in the order of the staged staple (identical rounding)
-            acc = acc + up;
-            acc = acc + dn;
+            // path by path with the third rows formed inside the sum, as in the staged staple
+            // (identical rounding)
+            acc_restored(acc, up);
+            acc_restored(acc, dn);
             continue;
         }
         else
@@ -290,8 +289,7 @@ LT_D M3<float> staple_staged(StapleRingT<NT>& r, const Gauge<float, 2>& U, const
         const int nn = (n + 1) + (n + 1 >= mu ? 1 : 0);   // the direction after this one
         cp_async_wait<1>();
         M3<float> p = mul_nd_rows(mul_rows(staged_rows(r, 0, 0), staged_link(r, 0, 1)), staged_link(r, 0, 2));
-        restore_last_row(p);
-        acc = acc + p;
+        acc_restored(acc, p);
         if (n < 2)
             stage_path<true>(r, 0, U, g, par, i, c, mu, nn, dmu);
         else
@@ -299,8 +297,7 @@ LT_D M3<float> staple_staged(StapleRingT<NT>& r, const Gauge<float, 2>& U, const
         cp_async_commit();
         cp_async_wait<1>();
         p = mul_rows(mul_dn_rows(staged_link(r, 1, 0), staged_link(r, 1, 1)), staged_link(r, 1, 2));
-        restore_last_row(p);
-        acc = acc + p;
+        acc_restored(acc, p);
         if (n < 2) stage_path<false>(r, 1, U, g, par, i, c, mu, nn, dmu);
         cp_async_commit();
     }

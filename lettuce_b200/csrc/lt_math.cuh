@@ -303,6 +303,35 @@ template <typename T> LT_HD cx<T> conj_cross(cx<T> p, cx<T> q, cx<T> r, cx<T> s)
     return mkc<T>(re, -im);
 }
 
+// a + conj(p q - r s) as an FMA chain
+template <typename T> LT_HD cx<T> acc_conj_cross(cx<T> a, cx<T> p, cx<T> q, cx<T> r, cx<T> s)
+{
+    T re = a.r;
+    re += p.r * q.r;
+    re -= p.i * q.i;
+    re -= r.r * s.r;
+    re += r.i * s.i;
+    T im = a.i;
+    im -= p.r * q.i;
+    im -= p.i * q.r;
+    im += r.r * s.i;
+    im += r.i * s.r;
+    return mkc<T>(re, im);
+}
+
+// a += p for an SU(3) matrix p of which only rows 0 and 1 are set: its third row
+// (RestoreLastRow) is formed inside the sum
+template <typename T> LT_HD void acc_restored(M3<T>& a, const M3<T>& p)
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.e[i][j] = a.e[i][j] + p.e[i][j];
+    a.e[2][0] = acc_conj_cross(a.e[2][0], p.e[0][1], p.e[1][2], p.e[0][2], p.e[1][1]);
+    a.e[2][1] = acc_conj_cross(a.e[2][1], p.e[0][2], p.e[1][0], p.e[0][0], p.e[1][2]);
+    a.e[2][2] = acc_conj_cross(a.e[2][2], p.e[0][0], p.e[1][1], p.e[0][1], p.e[1][0]);
+}
+
 template <typename T> LT_HD void restore_last_row(M3<T>& a)
 {
     a.e[2][0] = conj_cross(a.e[0][1], a.e[1][2], a.e[0][2], a.e[1][1]);
