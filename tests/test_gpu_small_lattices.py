@@ -66,6 +66,22 @@ def test_flow_stout_force(oracle, lattice):
     assert q == pytest.approx(wq, rel=1e-10, abs=1e-13)
 
 
+def test_two_row_fp32_staged_kernels(oracle, lattice):
+    """The two-row FP32 kernels that stage their staple links through shared memory, on lattices
+    whose blocks are partly empty (2^4 has 8 links per checkerboard plane): overrelaxation, the
+    flow stage and stout smearing against the FP64 oracle at FP32 accuracy."""
+    ext, U = lattice
+    G = gpu(ext, U, "fp32_12")
+    W = G.download()
+    lt.Iterator.Checkerboard(lt.OverrelaxationSubgroupKernel(G), 1)
+    assert rel_err(G.download(), oracle.overrelax(ext, W, 1)) < 1e-5
+    A, B = gpu(ext, W, "fp32_12"), lt.GaugeField(ext, "fp32_12")
+    lt.GradientFlowKernel(A, B, lt.RK3, None, 0.02)(2)
+    assert rel_err(B.download(), oracle.flow_rk3(ext, W, 0.02, 2)) < 1e-5
+    lt.StoutSmearingN(A, B, 1, 0.1)
+    assert rel_err(B.download(), oracle.stout(ext, W, 0.1, 1)) < 1e-5
+
+
 def test_rectangle_staple(oracle, lattice):
     """x + 2 nu wraps onto x itself when the extent along nu is 2."""
     ext, U = lattice
