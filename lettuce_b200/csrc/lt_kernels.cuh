@@ -1134,15 +1134,23 @@ template <int SEL> LT_D int find_lattice(const LatDesc* __restrict__ d, int n, i
     return lo;
 }
 
-// Registers capped at the level tuned for the single-lattice sweeps (640 resident threads per
-// SM in FP32, 384 in FP64)
-template <typename T, int BLOCK> struct BatchMinBlocks
+// Registers capped at the level tuned for the single-lattice sweeps: 640 resident threads per
+// SM in FP32, 384 in FP64, and 768 for the staged two-row FP32 kernels of 64 and 128 threads,
+// whose ring allows 6 blocks of 128 per SM (+2 % over 640; the unstaged FP32 kernels spill at
+// 768)
+#ifndef LT_BATCH_THREADS_F32C
+#define LT_BATCH_THREADS_F32C 768
+#endif
+template <typename T, int NR, int BLOCK> struct BatchMinBlocks
 {
-    static constexpr int value = (sizeof(T) == 4 ? 640 : 384) / BLOCK > 0 ? (sizeof(T) == 4 ? 640 : 384) / BLOCK : 1;
+    static constexpr int per_sm = (sizeof(T) == 4 && NR == 2 && LT_STAGED_STAPLE && BLOCK <= 128)
+                                      ? LT_BATCH_THREADS_F32C
+                                      : (sizeof(T) == 4 ? 640 : 384);
+    static constexpr int value = per_sm / BLOCK > 0 ? per_sm / BLOCK : 1;
 };
 
 template <typename T, int NR, int SEL, int OP>   // OP: 0 heatbath, 1 overrelaxation
-__global__ void __launch_bounds__(kBatchBlocks[SEL], (BatchMinBlocks<T, kBatchBlocks[SEL]>::value))
+__global__ void __launch_bounds__(kBatchBlocks[SEL], (BatchMinBlocks<T, NR, kBatchBlocks[SEL]>::value))
     k_batch_sweep(const LatDesc* __restrict__ d, int n, int mu, int par, const uint64_t* __restrict__ counter,
                   int max_iter)
 {
