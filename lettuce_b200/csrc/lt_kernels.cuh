@@ -922,7 +922,7 @@ template <typename T> struct HB;
 template <> struct HB<double>
 {
     LT_D static S2<double> su2(const S2<double>& A, double prefactor, uint32_t link, uint64_t counter,
-                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped)
+                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, float (&)[2])
     {
         double an = 1.0 / sqrt(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
@@ -966,10 +966,13 @@ template <> struct HB<double>
 // FP32: the special functions use the SFU approximations (__logf, __cosf, __sincosf, absolute
 // error about 1e-6 on these arguments), below the FP32 rounding of the rest of the update;
 // FP32 chains are validated statistically against the reference's chains.
+// The FP32 sampler draws the direction numbers of subgroups 0 and 1 from one Philox call (words
+// x, y for subgroup 0; z, w, kept in `spare`, for subgroup 1) and those of subgroup 2 from its
+// own
 template <> struct HB<float>
 {
     LT_D static S2<float> su2(const S2<float>& A, float prefactor, uint32_t link, uint64_t counter,
-                               uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped)
+                               uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, float (&spare)[2])
     {
         float an = 1.0f / sqrtf(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
@@ -985,6 +988,12 @@ template <> struct HB<float>
             if (k > max_iter)
             {
                 capped = true;
+                if (sg == 0)   // subgroup 1 still takes its direction numbers from this draw
+                {
+                    const U4 d = philox4x32(link, c1, c2, tw | 0xFFFFu, k0, k1);
+                    spare[0] = f01_from(d.z);
+                    spare[1] = 1.0f - 2.0f * f01_from(d.w);
+                }
                 S2<float> one;
                 one.e11 = mkc(1.0f, 0.0f);
                 one.e12 = mkc(0.0f, 0.0f);
@@ -994,9 +1003,20 @@ template <> struct HB<float>
         }
         float x0 = 1.0f - 2.0f * lsq;
         float ax = sqrtf(fmaxf(1.0f - x0 * x0, 0.0f));
-        U4 d = philox4x32(link, c1, c2, tw | 0xFFFFu, k0, k1);
-        float phi = f01_from(d.x);
-        float ct = 1.0f - 2.0f * f01_from(d.y);
+        float phi, ct;
+        if (sg == 1)
+        {
+            phi = spare[0];
+            ct = spare[1];
+        }
+        else
+        {
+            const U4 d = philox4x32(link, c1, c2, tw | 0xFFFFu, k0, k1);
+            phi = f01_from(d.x);
+            ct = 1.0f - 2.0f * f01_from(d.y);
+            spare[0] = f01_from(d.z);
+            spare[1] = 1.0f - 2.0f * f01_from(d.w);
+        }
         float vn = ax * sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
         float sp, cp;
         __sincosf(kTwoPiF * phi, &sp, &cp);
@@ -1092,11 +1112,12 @@ LT_D void hb_core_u(const Gauge<T, NR>& U, int mu, int par, int s, int i, M3<T> 
     M3<T> w = mul_nd(u, st);
     const uint32_t link = (uint32_t)(4 * i + mu);
     bool capped = false;
+    float spare[2] = { 0.0f, 0.0f };
     // unrolled so that the subgroup rows are compile-time indices (keeps u and w in registers)
 #pragma unroll
     for (int sg = 0; sg < 3; ++sg)
     {
-        S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter, capped);
+        S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter, capped, spare);
         embed_lmul(h, sg, u);
         if (sg < 2) embed_lmul(h, sg, w);
     }
