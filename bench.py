@@ -147,70 +147,143 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------- reference arm
-def cpu_reference_rate(size: int, steps: int, warmup: int, links):
-    """Link updates/s of the reference's own OpenMP CPU code (oracle/_ref) on this host, or of
-    the single-threaded C oracle when the reference harness was not built.  One sample =
-    1 heatbath + 1 overrelaxation sweep."""
-    import ctypes as C
+def headline_config(size: int, prec: str, world: int) -> dict:
+    """The workload both arms run: one step = N_HB heatbath + N_OR overrelaxation sweeps."""
+    return {"workload": f"{size}^4 SU(3) Wilson beta={BETA}: {N_HB} heatbath + {N_OR} overrelaxation "
+                        f"sweeps per step, {prec} links",
+            "lattice": [size] * 4, "beta": BETA, "storage": prec,
+            "l2": f"inputs larger than L2 ({size ** 4 * 4 * bm.LINK_BYTES[prec] / 1e6:.0f} MB of links per sweep)",
+            "parallelism": f"replicas x{world}"}
+
+
+def host_isa() -> str:
+    """x86-64 level of this host for the timing builds of the reference: v4 (AVX-512) or v3."""
+    try:
+        flags = set()
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                flags = set(line.split(":", 1)[1].split())
+                break
+        if {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags:
+            return "v4"
+    except OSError:
+        pass
+    return "v3"
+
+
+class CpuReference:
+    """The reference's own OpenMP code for the path (oracle/_ref, built from the reference
+    sources): the timing build (reference Makefile optimisation, contraction on, this host's
+    ISA level) when present, else the parity build.  Never the product library."""
+
+    def __init__(self, size: int):
+        import ctypes as C
+        self.ext = "x".join([str(size)] * 4)
+        ref_dir = os.path.join(ROOT, "oracle", "_ref")
+        cands = [(os.path.join(ref_dir, f"liblt_ref_fast_{self.ext}_{host_isa()}.so"),
+                  f"-O3 -march=x86-64-{host_isa()} -fopenmp, contraction on"),
+                 (os.path.join(ref_dir, f"liblt_ref_{self.ext}.so"), "-O3 -march=x86-64-v3 -fopenmp, no contraction")]
+        self.path, self.build = next(((p, b) for p, b in cands if os.path.exists(p)), (None, None))
+        if self.path is None:
+            raise FileNotFoundError(f"no reference harness for {self.ext} under oracle/_ref")
+        L = C.CDLL(self.path)
+        dp = C.c_void_p
+        L.ref_field_load.argtypes = [dp]
+        L.ref_field_rounds.argtypes = [C.c_double, C.c_int, C.c_int, C.c_int]
+        L.ref_field_flow_steps.argtypes = [C.c_double, C.c_int]
+        L.ref_threads.restype = C.c_int
+        self.lib = L
+
+    def load(self, links):
+        import numpy as np
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        self.lib.ref_field_load(a.ctypes.data)
+
+    def rounds(self, n: int):
+        self.lib.ref_field_rounds(BETA, n, N_HB, N_OR)
+
+    def flow(self, n: int):
+        self.lib.ref_field_flow_steps(FLOW_EPS, n)
+
+    def threads(self) -> int:
+        return int(self.lib.ref_threads())
+
+
+def cpu_reference_sample(size: int, links, n_round: int, n_flow: int):
+    """A bounded sample of the reference CPU path: n_round steps (1 HB + 4 OR sweeps) and
+    n_flow RK3 flow steps, timed with nothing else inside the timed regions."""
     import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from ltref import Oracle, ref_available, Reference
-    ext = (size,) * 4
     V = size ** 4
-    if ref_available(ext):
-        ref = Reference(ext)
-        L = ref.lib
-        L.ref_field_load.argtypes = [np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")]
-        L.ref_field_sweeps.restype = C.c_double
-        L.ref_field_sweeps.argtypes = [C.c_double, C.c_int, C.c_int]
-        L.ref_field_flow.restype = C.c_double
-        L.ref_field_flow.argtypes = [C.c_double, C.c_int]
-        L.ref_field_load(np.ascontiguousarray(links))
-        for _ in range(warmup):
-            L.ref_field_sweeps(BETA, 1, 1)
+    upd = (N_HB + N_OR) * 4 * V
+    try:
+        ref = CpuReference(size)
+    except (FileNotFoundError, OSError):
+        ref = None
+    if ref is not None:
+        ref.load(links)
+        ref.rounds(1)
         t0 = time.perf_counter()
-        for _ in range(steps):
-            L.ref_field_sweeps(BETA, 1, 1)
+        ref.rounds(n_round)
         dt = time.perf_counter() - t0
-        rate = steps * 2 * 4 * V / dt
         t0 = time.perf_counter()
-        L.ref_field_flow(FLOW_EPS, 1)
-        flow_rate = 1.0 / (time.perf_counter() - t0)
-        return {"value": rate, "unit": UNIT, "cores": int(L.ref_threads()), "kind": "reference",
-                "sample": f"{steps} x (1 heatbath + 1 overrelaxation sweep) at {size}^4, FP64, "
-                          f"reference OpenMP code (oracle/_ref), plaquette after each sample",
-                "flow_steps_per_s": flow_rate}
+        ref.flow(n_flow)
+        df = time.perf_counter() - t0
+        return {"value": n_round * upd / dt, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
+                "sample": f"{n_round} x (1 heatbath + 4 overrelaxation sweeps) and {n_flow} RK3 flow steps at "
+                          f"{size}^4, FP64, the reference's OpenMP code ({os.path.basename(ref.path)}: {ref.build})",
+                "flow_steps_per_s": n_flow / df}
+    # no reference harness here: the C oracle (a single-threaded restatement), one heatbath sweep
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ltref import Oracle
     o = Oracle()
-    e = np.array(ext, dtype=np.int32)
+    e = np.array([size] * 4, dtype=np.int32)
     U = np.ascontiguousarray(links)
     t0 = time.perf_counter()
-    o.lib.or_heatbath_sweeps(e, U, BETA, 1, 1, 0)
+    o.lib.or_heatbath_sweeps(e, U, BETA, 1, 0, 0)
     dt = time.perf_counter() - t0
     return {"value": 4 * V / dt, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"1 heatbath sweep at {size}^4, FP64, single-threaded C oracle"}
 
 
 def run_reference(a):
+    """--impl reference: the reference's CPU implementation of the headline workload on this
+    host's cores, the same config, steps and warm-up as our arm; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    import numpy as np
-    import lettuce_b200 as lt
-    ext = (a.size,) * 4
-    links = lt.haar_links(ext, SEED)
-    steps = max(1, min(a.steps, 10))
-    cb = cpu_reference_rate(a.size, steps, max(1, min(a.warmup, 3)), links)
-    ms = 1000.0 * 2 * 4 * a.size ** 4 / cb["value"]
-    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus, "steps": steps,
-            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ltref import haar_links_numpy
+    size = a.size
+    V = size ** 4
+    upd = (N_HB + N_OR) * 4 * V
+    links = haar_links_numpy((size,) * 4, SEED)
+    config = headline_config(size, a.prec, world)
+    try:
+        ref = CpuReference(size)
+    except (FileNotFoundError, OSError) as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference harness not built: {e}"}))
+        return 0
+    ref.load(links)
+    ref.rounds(a.warmup)
+    t0 = time.perf_counter()
+    ref.rounds(a.steps)
+    dt = time.perf_counter() - t0
+    n_flow = 10
+    t1 = time.perf_counter()
+    ref.flow(n_flow)
+    df = time.perf_counter() - t1
+    value = a.steps * upd / dt
+    sample = (f"{a.steps} x (1 heatbath + 4 overrelaxation sweeps) at {size}^4 after {a.warmup} warm-up steps, FP64, "
+              f"the reference's OpenMP code ({os.path.basename(ref.path)}: {ref.build}), seeded Haar start")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1000.0 * dt / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded Haar-random SU(3) start",
-            "impl": "reference",
-            "config": {"workload": f"{a.size}^4 SU(3) Wilson beta={BETA}: heatbath + overrelaxation sweeps",
-                       "lattice": list(ext), "beta": BETA},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if "flow_steps_per_s" in cb:
-        line["flow_steps_per_s"] = cb["flow_steps_per_s"]
+            "impl": "reference", "config": config,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "flow_steps_per_s": n_flow / df}
     print(json.dumps(line))
     return 0
 
@@ -219,6 +292,7 @@ def run_reference(a):
 def secondary_rates(lt, torch, timed, prec):
     """Rates of the other workloads, reported beside the headline:
     * metadynamics force evaluations/s at 16^4 (4 stout steps rho = 0.12, bulk FP32 storage);
+    * MetaD-HMC trajectories/s at 16^4 with the Gaussian-free binned bias deposits;
     * tempering ensemble link updates/s: 8 streams of 12^4 plus 40 chains with extents drawn
       from {8,...,16}^4, beta in [5.8, 6.2], one batched round (1 HB + 4 OR) per step;
     * BMW configuration files at 32^4 (device checksum pass, save and load);
@@ -248,6 +322,31 @@ def secondary_rates(lt, torch, timed, prec):
         del k, G
     except Exception as e:   # report, never hide
         out["metad_force_error"] = repr(e)
+    try:
+        # the metadynamics configuration: MetaD-HMC at 16^4 (OMF2, tau = 1, 10 steps; CV = clover
+        # Q after 4 stout steps of rho = 0.12; bias over [-8, 8] with 800 bins, Gaussian-free
+        # binned deposits after every trajectory), bulk FP32 links, FP64 bias and dH
+        ext = (16,) * 4
+        G = lt.GaugeField(ext, prec)
+        G.SetToHaarRandom(21)
+        lt.UpdateSweeps(G, BETA, 20, 1, 4, SEED)
+        bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 4 * 16.0 / 800, 10, 1000)
+        bias.SetUpdateMode("binned")
+        hmc = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(BETA), 1.0, 0.12, 4, seed=SEED)
+        for _ in range(2):
+            hmc(10, True)
+        n_traj, acc, dH = 8, 0, []
+        t0 = time.perf_counter()
+        for _ in range(n_traj):
+            acc += int(hmc(10, True))
+            dH.append(hmc.delta_H)
+        dt = time.perf_counter() - t0
+        out["metad_hmc_binned_16^4"] = {"trajectories_per_s": n_traj / dt, "acceptance": acc / n_traj,
+                                        "dH": dH, "deposited_grid_points": int(np.count_nonzero(bias.grid())),
+                                        "integrator": "OMF2, tau = 1, 10 steps", "storage": prec}
+        del hmc, G
+    except Exception as e:
+        out["metad_hmc_binned_error"] = repr(e)
     try:
         rng = np.random.default_rng(4)
         lats = [lt.GaugeField((12,) * 4, prec) for _ in range(8)]
@@ -487,12 +586,7 @@ def main():
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if a.prec != "fp64" else "f64",
             "data": "synthetic: seeded Haar-random SU(3) start (per rank)",
-            "config": {"workload": f"{a.size}^4 SU(3) Wilson beta={BETA}: {N_HB} heatbath + {N_OR} overrelaxation "
-                                   f"sweeps per step, {a.prec} links",
-                       "lattice": list(ext), "beta": BETA, "storage": a.prec,
-                       "l2": f"inputs larger than L2 ({G.Volume() * 4 * bm.LINK_BYTES[a.prec] / 1e6:.0f} MB "
-                             "of links per sweep)",
-                       "parallelism": f"replicas x{world}"},
+            "config": headline_config(a.size, a.prec, world),
             "roofline": roofline, "clocks": clocks.summary(), "gpu_launches": launches}
 
     if not a.no_extras:
@@ -584,10 +678,16 @@ def main():
 
         # ---- CPU baseline on this host, rank 0, bounded sample
         if rank == 0:
-            cb = cpu_reference_rate(a.size, 2, 1, therm)
+            cb = cpu_reference_sample(a.size, therm, 2, 10)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
             if "flow_steps_per_s" in cb:
                 line["cpu_baseline"]["flow_steps_per_s"] = cb["flow_steps_per_s"]
+                # each GPU arm over the reference's CPU code, sweeps and flow
+                line["gpu_over_cpu"] = {
+                    "bulk_link_updates": value / world / cb["value"],
+                    "fp64_link_updates": line["fp64"]["link_updates_per_s"] / cb["value"],
+                    "bulk_flow_steps": line["flow_steps_per_s"] / cb["flow_steps_per_s"],
+                    "fp64_flow_steps": line["fp64"]["flow_steps_per_s"] / cb["flow_steps_per_s"]}
 
     if rank == 0:
         print(json.dumps(line))

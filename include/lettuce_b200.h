@@ -160,8 +160,9 @@ int lt_staples(lt_lattice* h, double* staples_out);
 /* Plaquette sum of a field that the caller already holds in device memory, in the reference
  * layout double[V][4][3][3][2], written as one double to the caller's device pointer
  * out_dev, on the caller's stream (NULL = default stream).  No counterpart in the reference:
- * this entry point exists for callers that cannot allocate device memory at the call (code
- * under stream capture, framework-managed memory pools, allocation-free timing loops).  It
+ * this entry point exists for callers that may not allocate device memory -- frameworks whose
+ * memory pool owns all device memory (a raw cudaMalloc escapes its accounting), and timing or
+ * monitoring loops that cudaMalloc/cudaFree would stall by synchronising the device.  It
  * allocates nothing: its scratch is a fixed 128 KiB static device array (present on every
  * GPU that loads the library), so volumes above 16,777,216 sites (64^4) are rejected with
  * LT_ERR_ARG.  The first call on a device looks up that array's address (make it before
@@ -239,6 +240,19 @@ int lt_tempering_swap(lt_lattice* a, lt_lattice* b, const lt_bias* bias, double 
 /* GradientFlowKernel (:252-367) with any of the integrators: out = in flowed by n_step steps
  * of size eps (in == out continues a flow, as GradientFlowKernel::Resume). */
 int lt_flow(lt_lattice* in, lt_lattice* out, int integrator, double eps, int n_step);
+/* The force of the flows run into a handle (lt_flow, lt_flow_rk3, lt_flow_rk3_measure,
+ * lt_flow_t0 with that handle as `out`):
+ *   LT_FLOW_ACTION_GAUGE   Z = Algebra(st U^dag) of the handle's gauge action, the reference's
+ *                          GradientFlowKernel<IntegratorT, ActionT> (:298-332); the default;
+ *   LT_FLOW_ACTION_ZEUTHEN the Zeuthen flow (Ramos and Sint, arXiv:1508.05552): the
+ *                          Luescher-Weisz force X acted on by 1 + 1/12 nabla*_mu nabla_mu,
+ *                          F_mu(x) = X_mu(x) + [U_mu(x) X_mu(x+mu) U_mu(x)^dag
+ *                          + U_mu(x-mu)^dag X_mu(x-mu) U_mu(x-mu) - 2 X_mu(x)] / 12.
+ * No counterpart in the reference (it has no Zeuthen flow). */
+#define LT_FLOW_ACTION_GAUGE   0
+#define LT_FLOW_ACTION_ZEUTHEN 1
+int lt_set_flow_action(lt_lattice* h, int flow_action);
+int lt_get_flow_action(lt_lattice* h, int* flow_action);
 /* GradientFlowKernel<RK3>::operator() (smearing/gradient_flow.hpp:120-168, :339-345):
  * out = in flowed by n_step RK3 steps of size eps.  in == out continues in place
  * (GradientFlowKernel::Resume, :347-351). */
@@ -330,13 +344,38 @@ int lt_reverse_momenta(lt_lattice* h);
  * the action unchanged, in place. */
 int lt_parity_update(lt_lattice* h);
 
+/* ---- diagnostics for tests (no counterpart in the reference) ---------------------------- */
+#define LT_EXP_DISPATCH     0  /* the branch choice of the flow / stout / HMC kernels            */
+#define LT_EXP_CLOSED       1  /* the closed form of ExpConstants (FP64 scalar chain)            */
+#define LT_EXP_SERIES_SHORT 2  /* Cayley-Hamilton series, short term count (valid for c1 <= 1/32) */
+#define LT_EXP_SERIES_LONG  3  /* Cayley-Hamilton series, long term count (valid for c1 <= 1/2)  */
+/* SU3::exp (math/su3_exp.hpp:419-432) on the device: out[k] = exp(i Q_k) for n traceless
+ * Hermitian 3x3 matrices q_in[k] (18 doubles each, row-major, re/im interleaved; host
+ * memory), computed in the arithmetic of storage format prec by the branch `path`
+ * (LT_EXP_*).  Allocates and synchronises: a test entry point, not a hot path. */
+int lt_su3_exp_test(const double* q_in, double* out, int n, int prec, int path);
+/* binaryVersion and ptxVersion (cudaFuncGetAttributes) of the library's kernels on the
+ * current device: 100 for code built for sm_100a. */
+int lt_device_arch(int* binary_version, int* ptx_version);
+
 /* ---- bias potential: MetaBiasPotential (actions/bias_potential/metadynamics.hpp:29-507) -- */
 /* Constructor (:60-91); fails with LT_ERR_ARG where the reference throws (:70-77). */
 int lt_bias_create(double cv_min, double cv_max, int bin_number, double weight, double width,
                    double well_tempered_parameter, double threshold_weight, lt_bias** out);
 int lt_bias_destroy(lt_bias* b);
-/* UpdatePotential (:103-131) or UpdatePotentialSymmetric (:134-147) for n CV samples. */
+/* UpdatePotential (:103-131) or UpdatePotentialSymmetric (:134-147) for n CV samples, with
+ * the bias's deposit mode (lt_bias_set_update_mode).  The MetaD trajectories deposit through
+ * the same mode. */
 int lt_bias_update(lt_bias* b, const double* cv, int n, int symmetric);
+#define LT_BIAS_GAUSSIAN 0  /* the reference's well-tempered Gaussian deposit (the default) */
+#define LT_BIAS_BINNED   1  /* Gaussian-free binned deposit: the weight is split linearly between
+                             * the two grid points bracketing the CV, each share well-tempered by
+                             * exp(-V_point / well_tempered_parameter); CVs outside [cv_min,
+                             * cv_max) deposit nothing and are counted as exceeded */
+/* Selects the deposit of lt_bias_update and of the MetaD trajectories.  No counterpart in the
+ * reference (its deposits are Gaussians, metadynamics.hpp:103-147). */
+int lt_bias_set_update_mode(lt_bias* b, int mode);
+int lt_bias_get_update_mode(const lt_bias* b, int* mode);
 /* ReturnPotential (:151-179). */
 int lt_bias_potential(const lt_bias* b, double cv, double* out);
 /* ReturnDerivative (:181-187). */

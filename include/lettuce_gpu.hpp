@@ -161,6 +161,16 @@ inline Rectangular<2> LüscherWeiszAction(6.0, 1.0 + 8.0 * 1.0 / 12.0, -1.0 / 12
 inline Rectangular<2>& LuescherWeiszAction = LüscherWeiszAction;
 inline Rectangular<2> IwasakiAction(6.0, 1.0 + 8.0 * 0.331, -0.331);
 inline Rectangular<2> DBW2Action(6.0, 1.0 + 8.0 * 1.4088, -1.4088);
+
+// The Zeuthen flow (Ramos and Sint, arXiv:1508.05552) as the ActionT of a GradientFlowKernel:
+// the Luescher-Weisz force acted on by 1 + 1/12 nabla*_mu nabla_mu (lt_set_flow_action).  Not
+// in the reference, which flows with its gauge actions only.
+struct ZeuthenFlow
+{
+    double beta = 6.0;
+    double GetBeta() const { return beta; }
+};
+inline ZeuthenFlow ZeuthenFlowAction;
 } // namespace GaugeAction
 
 // The action a kernel runs with: its device form and a view of its coupling, which the kernels
@@ -170,11 +180,21 @@ struct ActionRef
     int radius;
     double c_plaq, c_rect;
     const double* beta;
+    int flow = LT_FLOW_ACTION_GAUGE;
     template <int R>
     ActionRef(const GaugeAction::Rectangular<R>& a) : radius(R), c_plaq(a.c_plaq), c_rect(a.c_rect), beta(&a.beta)
     {
     }
-    void Apply(const GaugeField& U) const { check(lt_set_gauge_action(U.handle(), radius, c_plaq, c_rect)); }
+    // as the action of a flow: the Zeuthen force (the gauge action of the field is left alone)
+    ActionRef(const GaugeAction::ZeuthenFlow& a)
+        : radius(0), c_plaq(0.0), c_rect(0.0), beta(&a.beta), flow(LT_FLOW_ACTION_ZEUTHEN)
+    {
+    }
+    void Apply(const GaugeField& U) const
+    {
+        check(lt_set_flow_action(U.handle(), flow));
+        if (flow == LT_FLOW_ACTION_GAUGE) check(lt_set_gauge_action(U.handle(), radius, c_plaq, c_rect));
+    }
     double GetBeta() const { return *beta; }
 };
 
@@ -488,6 +508,9 @@ public:
     MetaBiasPotential(const MetaBiasPotential&) = delete;
     MetaBiasPotential& operator=(const MetaBiasPotential&) = delete;
     ~MetaBiasPotential() { lt_bias_destroy(b_); }
+    // the deposit of the updates and of MetaD trajectories: LT_BIAS_GAUSSIAN (the reference's)
+    // or LT_BIAS_BINNED (Gaussian-free binned weights; no counterpart in the reference)
+    void SetUpdateMode(int mode) { check(lt_bias_set_update_mode(b_, mode)); }
     void UpdatePotential(double cv) { check(lt_bias_update(b_, &cv, 1, 0)); }
     void UpdatePotentialSymmetric(double cv) { check(lt_bias_update(b_, &cv, 1, 1)); }
     void UpdatePotentialSymmetric(const std::vector<double>& cv)

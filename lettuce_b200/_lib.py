@@ -54,6 +54,8 @@ SIGNATURES = {
     "lt_clover_observables": (_i, [_vp, _pd, _pd]),
     "lt_staples": (_i, [_vp, _dp]),
     "lt_plaquette_sum_noalloc": (_i, [_vp, _ip, _vp, _vp]),
+    "lt_su3_exp_test": (_i, [_dp, _dp, _i, _i, _i]),
+    "lt_device_arch": (_i, [_pi, _pi]),
     "lt_overrelax_sweeps": (_i, [_vp, _i]),
     "lt_heatbath_sweeps": (_i, [_vp, _d, _i, _u64, _pu64]),
     "lt_update_sweeps": (_i, [_vp, _d, _i, _i, _i, _u64, _pu64]),
@@ -70,6 +72,8 @@ SIGNATURES = {
     "lt_tempering_swap": (_i, [_vp, _vp, _vp, _d, _d, _d, _d, _d, _pi, _pd]),
     "lt_flow_rk3": (_i, [_vp, _vp, _d, _i]),
     "lt_flow": (_i, [_vp, _vp, _i, _d, _i]),
+    "lt_set_flow_action": (_i, [_vp, _i]),
+    "lt_get_flow_action": (_i, [_vp, _pi]),
     "lt_clover_timeslices": (_i, [_vp, _vp, _vp]),
     "lt_topcharge_plaquette": (_i, [_vp, _pd]),
     "lt_rect_action": (_i, [_vp, _d, _d, _d, _pd]),
@@ -98,6 +102,8 @@ SIGNATURES = {
     "lt_bias_create": (_i, [_d, _d, _i, _d, _d, _d, _d, C.POINTER(_vp)]),
     "lt_bias_destroy": (_i, [_vp]),
     "lt_bias_update": (_i, [_vp, _vp, _i, _i]),
+    "lt_bias_set_update_mode": (_i, [_vp, _i]),
+    "lt_bias_get_update_mode": (_i, [_vp, _pi]),
     "lt_bias_potential": (_i, [_vp, _d, _pd]),
     "lt_bias_derivative": (_i, [_vp, _d, _pd]),
     "lt_bias_get_grid": (_i, [_vp, _dp, _i]),

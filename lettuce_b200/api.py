@@ -188,6 +188,23 @@ def _set_action(U: GaugeField, action) -> None:
                                         float(action.c_rect)))
 
 
+class ZeuthenFlow:
+    """The Zeuthen flow (Ramos and Sint, arXiv:1508.05552) as the `action` of a
+    GradientFlowKernel: the Luescher-Weisz force acted on by 1 + 1/12 nabla*_mu nabla_mu
+    (lt_set_flow_action).  Not in the reference, which flows with its gauge actions only."""
+
+    c_plaq, c_rect = 1.0 + 8.0 / 12.0, -1.0 / 12.0
+
+
+def _set_flow(U: GaugeField, action) -> None:
+    """The force of flows run into U: the Zeuthen flow, or `action`'s (None: Wilson)."""
+    if isinstance(action, ZeuthenFlow) or action is ZeuthenFlow:
+        check(lib().lt_set_flow_action(U.handle, 1))
+        return
+    check(lib().lt_set_flow_action(U.handle, 0))
+    _set_action(U, action)
+
+
 class WilsonAction:
     """GaugeAction::Rectangular<1> with (c_plaq, c_rect) = (1, 0)
     (actions/gauge/rectangular_action.hpp:23-294)."""
@@ -338,7 +355,7 @@ class GradientFlowKernel:
         self.U_unflowed, self.U_flowed, self.epsilon = U_unflowed, U_flowed, float(epsilon)
 
     def _run(self, src: GaugeField, n_step: int) -> None:
-        _set_action(self.U_flowed, self.action)
+        _set_flow(self.U_flowed, self.action)
         if self.integrator is RK3:
             check(lib().lt_flow_rk3(src.handle, self.U_flowed.handle, self.epsilon, int(n_step)))
         else:
@@ -356,7 +373,7 @@ class GradientFlowKernel:
     def Measure(self, n_meas: int, every: int):
         """Flow from U_unflowed with (plaquette sum, Q, E) after every `every` steps."""
         p, q, e = np.empty(n_meas), np.empty(n_meas), np.empty(n_meas)
-        _set_action(self.U_flowed, self.action)
+        _set_flow(self.U_flowed, self.action)
         check(lib().lt_flow_rk3_measure(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, int(n_meas),
                                         int(every), p.ctypes.data, q.ctypes.data, e.ctypes.data))
         return p, q, e
@@ -364,7 +381,7 @@ class GradientFlowKernel:
     def FlowToT0(self, target: float = 0.3, max_steps: int = 100000) -> tuple[float, float]:
         """Flow U_unflowed into U_flowed until t^2 E = target; returns (t0, Q at the last step)."""
         t0, q = C.c_double(), C.c_double()
-        _set_action(self.U_flowed, self.action)
+        _set_flow(self.U_flowed, self.action)
         check(lib().lt_flow_t0(self.U_unflowed.handle, self.U_flowed.handle, self.epsilon, float(target),
                                int(max_steps), C.byref(t0), C.byref(q)))
         return t0.value, q.value
@@ -410,6 +427,21 @@ class MetaBiasPotential:
                 lib().lt_bias_destroy(self._h)
         except Exception:
             pass
+
+    GAUSSIAN, BINNED = 0, 1
+
+    def SetUpdateMode(self, mode) -> None:
+        """The deposit of UpdatePotential* and of MetaD trajectories: "gaussian" (the
+        reference's well-tempered Gaussian, the default) or "binned" (Gaussian-free: the
+        weight split linearly between the two grid points bracketing the CV, each share
+        well-tempered by its point's value)."""
+        m = {"gaussian": 0, "binned": 1}.get(mode, mode)
+        check(lib().lt_bias_set_update_mode(self._h, int(m)))
+
+    def GetUpdateMode(self) -> str:
+        m = C.c_int()
+        check(lib().lt_bias_get_update_mode(self._h, C.byref(m)))
+        return ("gaussian", "binned")[m.value]
 
     def UpdatePotential(self, cv) -> None:
         a = np.atleast_1d(np.asarray(cv, dtype=np.float64))
@@ -783,4 +815,4 @@ __all__ = ["STATUS_NONFINITE", "STATUS_UNITARITY", "STATUS_HB_CAP", "GaugeField"
            "Observables", "MDIntegrator", "Integrators", "Leapfrog_slow", "Leapfrog", "OMF_2_slow", "OMF_2",
            "OMF_4_slow", "OMF_4", "Leapfrog_friction_slow", "OMF_4_friction_slow", "Leapfrog_OMF_4",
            "OMF_2_OMF_4_slow", "OMF_2_OMF_4", "ParityUpdate", "LuescherWeiszAction", "IwasakiAction", "DBW2Action",
-           "UpdateSweeps4"]
+           "UpdateSweeps4", "ZeuthenFlow"]

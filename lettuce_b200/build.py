@@ -25,7 +25,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "-I", CSRC, "-I", INCLUDE]
 
 SOURCES = ["lt_impl_fp64.cu", "lt_impl_fp32.cu", "lt_impl_fp32_12.cu", "lt_capi.cu", "lt_ensemble.cu", "lt_host.cpp",
-           "lt_noalloc.cu", "lt_bmw.cu"]
+           "lt_noalloc.cu", "lt_bmw.cu", "lt_selftest.cu"]
 HEADERS = ["lt_math.cuh", "lt_field.cuh", "lt_kernels.cuh", "lt_impl.cuh", "lt_backend.h", "lt_host.h", "lt_handle.h"]
 
 

@@ -85,6 +85,11 @@ public:
     virtual void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new,
                             double c_exp, int read_z, int write_z) const = 0;
     virtual void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const = 0;
+    // Zeuthen flow stage: X <- the Luescher-Weisz force (c_plaq cp, c_rect cr) of Uin, then the
+    // Zeuthen force from X and the stage's Z and link update Uin -> Uout
+    virtual void flow_zeuthen_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, void* X, double c_old,
+                                    double c_new, double c_exp, int read_z, int write_z, double cp,
+                                    double cr) const = 0;
 
     virtual void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const = 0;
     virtual void fields(const Ctx& c, void* U, const void* P, double eps) const = 0;

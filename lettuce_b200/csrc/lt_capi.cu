@@ -101,12 +101,20 @@ int flow_steps(lt_lattice* h, double eps, int n_step, int integrator = LT_FLOW_R
     const int ns = integrator == LT_FLOW_EULER ? 1 : integrator == LT_FLOW_RK2 ? 2 : 3;
     LT_TRY(ensure(h, &h->U2, h->be->gauge_bytes(h->g)));
     if (ns > 1) LT_TRY(ensure(h, &h->Z, h->be->alg_bytes(h->g)));
+    const bool zeuthen = h->flow_action == LT_FLOW_ACTION_ZEUTHEN;
+    if (zeuthen) LT_TRY(ensure(h, &h->Xz, h->be->alg_bytes(h->g)));
     const lt::Ctx c = h->ctx();
     for (int k = 0; k < n_step; ++k)
         for (int j = 0; j < ns; ++j)
         {
-            h->be->flow_stage(c, h->U, h->U2, h->Z, st[j].c_old, st[j].c_new * eps, st[j].c_exp, st[j].read_z,
-                              st[j].write_z);
+            if (zeuthen)
+                // the Zeuthen flow's force is that of the Luescher-Weisz action whatever the
+                // handle's gauge action (c_plaq = 5/3, c_rect = -1/12)
+                h->be->flow_zeuthen_stage(c, h->U, h->U2, h->Z, h->Xz, st[j].c_old, st[j].c_new * eps, st[j].c_exp,
+                                          st[j].read_z, st[j].write_z, 5.0 / 3.0, -1.0 / 12.0);
+            else
+                h->be->flow_stage(c, h->U, h->U2, h->Z, st[j].c_old, st[j].c_new * eps, st[j].c_exp, st[j].read_z,
+                                  st[j].write_z);
             std::swap(h->U, h->U2);
         }
     return launched("flow");
@@ -478,10 +486,15 @@ int lt_create(const int ext[4], int prec, lt_lattice** out)
 {
     if (!out || !ext) return lt::set_error(LT_ERR_ARG, "lt_create: null pointer");
     *out = nullptr;
+    // 4 V 9 complex entries index the field in 32-bit arithmetic: the running product is checked
+    // after every factor, so huge extents are refused before any multiplication can wrap
+    long long V = 1;
     for (int d = 0; d < 4; ++d)
+    {
         if (ext[d] < 2 || ext[d] % 2) return lt::set_error(LT_ERR_ARG, "lt_create: extents must be even and >= 2");
-    long long V = (long long)ext[0] * ext[1] * ext[2] * ext[3];
-    if (V * 4 * 9 >= (1LL << 31)) return lt::set_error(LT_ERR_ARG, "lt_create: lattice too large");
+        V *= ext[d];
+        if (V * 4 * 9 >= (1LL << 31)) return lt::set_error(LT_ERR_ARG, "lt_create: lattice too large");
+    }
     const lt::Backend* be = prec == LT_PREC_FP64 ? lt::backend_fp64()
                           : prec == LT_PREC_FP32 ? lt::backend_fp32()
                           : prec == LT_PREC_FP32_12 ? lt::backend_fp32_12() : nullptr;
@@ -523,8 +536,8 @@ int lt_destroy(lt_lattice* h)
     if (!h) return LT_OK;
     const lt::DeviceScope device_scope(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,  h->R,      h->chainA,
-                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB };
+    void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,   h->R,      h->chainA,
+                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB, h->Xz };
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (void* p : h->levels) cudaFree(p);
@@ -630,6 +643,9 @@ int lt_swap(lt_lattice* a, lt_lattice* b)
     const lt::DeviceScope device_scope(a->device);
     if (std::memcmp(a->ext, b->ext, sizeof(a->ext)) || a->prec != b->prec)
         return lt::set_error(LT_ERR_ARG, "lt_swap: extents or formats differ");
+    // the link buffers change owners: a buffer on another GPU would be read by this handle's
+    // kernels through a pointer its device cannot dereference
+    if (a->device != b->device) return lt::set_error(LT_ERR_ARG, "lt_swap: handles live on different devices");
     LT_CK(cudaStreamSynchronize(a->stream));
     LT_CK(cudaStreamSynchronize(b->stream));
     std::swap(a->U, b->U);
@@ -1079,6 +1095,23 @@ int lt_flow(lt_lattice* in, lt_lattice* out, int integrator, double eps, int n_s
         return lt::set_error(LT_ERR_ARG, "lt_flow: n_step < 0 or unknown integrator");
     LT_TRY(lt_copy(out, in));
     return flow_steps(out, eps, n_step, integrator);
+}
+
+int lt_set_flow_action(lt_lattice* h, int flow_action)
+{
+    LT_TRY(check_h(h, "lt_set_flow_action"));
+    if (flow_action != LT_FLOW_ACTION_GAUGE && flow_action != LT_FLOW_ACTION_ZEUTHEN)
+        return lt::set_error(LT_ERR_ARG, "lt_set_flow_action: unknown flow action");
+    h->flow_action = flow_action;
+    return LT_OK;
+}
+
+int lt_get_flow_action(lt_lattice* h, int* flow_action)
+{
+    LT_TRY(check_h(h, "lt_get_flow_action"));
+    if (!flow_action) return lt::set_error(LT_ERR_ARG, "lt_get_flow_action: null pointer");
+    *flow_action = h->flow_action;
+    return LT_OK;
 }
 
 int lt_flow_rk3_measure(lt_lattice* in, lt_lattice* out, double eps, int n_meas, int every, double* plaq_out,

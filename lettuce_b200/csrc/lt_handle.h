@@ -75,6 +75,10 @@ struct lt_lattice
     // stencil radius 1 (Wilson, the default) or 2 (plaquettes and 1x2 rectangles)
     int act_radius = 1;
     double act_cp = 1.0, act_cr = 0.0;
+    // force of the gradient flow run into this handle (lt_set_flow_action): the gauge action's
+    // (LT_FLOW_ACTION_GAUGE, the reference's GradientFlowKernel) or the Zeuthen flow's
+    int flow_action = LT_FLOW_ACTION_GAUGE;
+    void* Xz = nullptr;          // Luescher-Weisz force of a Zeuthen flow stage (algebra)
     mutable unsigned order = 0;  // launches of the order-alternating sweep and flow kernels
 
     lt::Ctx ctx() const

@@ -1,5 +1,6 @@
 // Host-side parts of the C ABI that need no device: the seeded Haar-random start and the
 // metadynamics bias potential (one 801-point grid; negligible next to the lattice work).
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -82,8 +83,38 @@ Bias::Bias(double cv_min_, double cv_max_, int bins_, double weight_, double wid
 {
 }
 
-// UpdatePotential, well-tempered branch (metadynamics.hpp:103-124)
 void Bias::update(double cv)
+{
+    if (mode == 1) update_binned(cv);
+    else update_gaussian(cv);
+}
+
+// Gaussian-free binned deposit (not in the reference, whose deposits are Gaussians): the weight
+// goes to the two grid points that bracket the CV, split linearly (cloud in cell), so the
+// linearly interpolated potential (ReturnPotential) gains exactly `weight` of area per deposit
+// and its value at a grid point rises by `weight`.  Each point's share is well-tempered by its
+// own current value, exp(-V_i / wt), as the reference tempers each grid point
+// (metadynamics.hpp:116-118).  A CV outside [cv_min, cv_max) deposits nothing -- there is no
+// grid point to carry it -- and is counted in `exceeded` like the reference's out-of-range CVs.
+void Bias::update_binned(double cv)
+{
+    if (!(cv >= cv_min && cv < cv_max))
+    {
+        ++exceeded;
+        return;
+    }
+    // the bracketing points i, i + 1 (clamped against rounding at the upper edge) and the
+    // linear share a of point i + 1
+    const int i = std::min(std::max((int)std::floor((cv - cv_min) * bin_width_inv), 0), bins - 1);
+    const double a = std::min(std::max((cv - (cv_min + i * bin_width)) * bin_width_inv, 0.0), 1.0);
+    const double w0 = weight * (1.0 - a) * std::exp(-grid[i] / wt);
+    const double w1 = weight * a * std::exp(-grid[i + 1] / wt);
+    grid[i] += w0;
+    grid[i + 1] += w1;
+}
+
+// UpdatePotential, well-tempered branch (metadynamics.hpp:103-124)
+void Bias::update_gaussian(double cv)
 {
     if (cv < cv_min || cv >= cv_max) ++exceeded;
     const double wis = 1.0 / (width * width);
@@ -161,6 +192,22 @@ int lt_bias_update(lt_bias* b, const double* cv, int n, int symmetric)
         p->update(cv[k]);
         if (symmetric) p->update(-cv[k]);
     }
+    return LT_OK;
+}
+
+int lt_bias_set_update_mode(lt_bias* b, int mode)
+{
+    if (!b) return lt::set_error(LT_ERR_ARG, "lt_bias_set_update_mode: null bias");
+    if (mode != LT_BIAS_GAUSSIAN && mode != LT_BIAS_BINNED)
+        return lt::set_error(LT_ERR_ARG, "lt_bias_set_update_mode: unknown mode");
+    reinterpret_cast<lt::Bias*>(b)->mode = mode;
+    return LT_OK;
+}
+
+int lt_bias_get_update_mode(const lt_bias* b, int* mode)
+{
+    if (!b || !mode) return lt::set_error(LT_ERR_ARG, "lt_bias_get_update_mode: null pointer");
+    *mode = reinterpret_cast<const lt::Bias*>(b)->mode;
     return LT_OK;
 }
 

@@ -238,6 +238,16 @@ public:
                        4 * kSitesPerBlock, c.stream, gauge(Uin, c.g), gauge(Uout, c.g), alg(Z, c.g), c.g, (T)c_old,
                        (T)c_new, (T)c_exp, read_z, write_z, (T)c.cp, (T)c.cr, next_order(c));
     }
+    void flow_zeuthen_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, void* X, double c_old, double c_new,
+                            double c_exp, int read_z, int write_z, double cp, double cr) const override
+    {
+        const int nb = nblocks(c.g.V, kSitesPerBlock);
+        launch_chained(k_flow_force<T, NR>, nb, 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g), alg(X, c.g), c.g,
+                       (T)cp, (T)cr, next_order(c));
+        launch_chained(k_flow_zeuthen_stage<T, NR>, nb, 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
+                       gauge(Uout, c.g), alg(Z, c.g), alg(X, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z,
+                       write_z, next_order(c));
+    }
     void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
     {
         if constexpr (kStaged)

@@ -1279,6 +1279,76 @@ __global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
     Uout.st(mu, par, s, exp_update<float, 2>(unpack_ah(z), c_exp, u));
 }
 
+// ---------------------------------------------------------------- Zeuthen flow
+// The Zeuthen flow (Ramos and Sint, Eur. Phys. J. C 76 (2016) 15, arXiv:1508.05552; not in the
+// reference, which flows with the simulated action's force only, gradient_flow.hpp:298-332):
+// the force of the Luescher-Weisz action, X_mu(x) = Algebra(st_LW U_mu(x)^dag), acted on by
+// (1 + 1/12 nabla*_mu nabla_mu), the adjoint covariant second difference along the link:
+//   F_mu(x) = X_mu(x) + 1/12 [U_mu(x) X_mu(x+mu) U_mu(x)^dag
+//                             + U_mu(x-mu)^dag X_mu(x-mu) U_mu(x-mu) - 2 X_mu(x)],
+// integrated with the stages of the flow integrators exactly as the plain force.
+// Pass 1 of a stage: X for every link.
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_flow_force(Gauge<T, NR> U, Alg<T> X, Geom g, T cp, T cr, int rev)
+{
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x, rev)) return;
+    const int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    const M3<T> u = U.ld(mu, par, s);
+    X.st(mu, par, s, algebra8(mul_nd(action_staple<true>(U, g, par, i, c, mu, cp, cr), u)));
+}
+
+// Pass 2: the Zeuthen force from X at x and x +- mu, then the stage's Z update and exponential
+// update (as k_flow_stage), Uin -> Uout
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_flow_zeuthen_stage(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z,
+                                                                 Alg<T> X, Geom g, T c_old, T c_new, T c_exp,
+                                                                 int read_z, int write_z, int rev)
+{
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x, rev)) return;
+    const int par = x >= g.vh, s = x - par * g.vh, op = par ^ 1;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    const int ip = (i + step_up_rt(g, mu, c)) >> 1, im = (i + step_dn_rt(g, mu, c)) >> 1;
+    const M3<T> u = Uin.ld(mu, par, s);
+    const M3<T> um = Uin.ld(mu, op, im);
+    const M3<T> xc = unpack_ah(X.ld(mu, par, s));
+    const M3<T> fwd = mul_nd(mul(u, unpack_ah(X.ld(mu, op, ip))), u);
+    const M3<T> bwd = mul(mul_dn(um, unpack_ah(X.ld(mu, op, im))), um);
+    M3<T> f = xc;
+    const T k12 = (T)(1.0 / 12.0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+        {
+            f.e[a][b].r += k12 * (fwd.e[a][b].r + bwd.e[a][b].r - (T)2 * xc.e[a][b].r);
+            f.e[a][b].i += k12 * (fwd.e[a][b].i + bwd.e[a][b].i - (T)2 * xc.e[a][b].i);
+        }
+    const A8<T> a = algebra8(f);
+    A8<T> z;
+    if (read_z)
+    {
+        const A8<T> zo = Z.ld(mu, par, s);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z.a[k] = c_old * zo.a[k] + c_new * a.a[k];
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z.a[k] = c_new * a.a[k];
+    }
+    if (write_z) Z.st(mu, par, s, z);
+    Uout.st(mu, par, s, exp_update<T, NR>(unpack_ah(z), c_exp, u));
+}
+
 // ---------------------------------------------------------------- stout smearing
 // StoutSmearing4D (smearing/stout_smearing.hpp:29-57): U' = exp(rho Algebra(st U^dag)) U, Gram-Schmidt
 template <typename T, int NR>

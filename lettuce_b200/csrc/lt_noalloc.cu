@@ -1,12 +1,13 @@
 // lt_plaquette_sum_noalloc: the plaquette sum of a caller-owned device field, computed
 // without any device allocation.
 //
-// Who needs this: callers that must not allocate device memory at the point of the call,
-// e.g. code running while a CUDA stream is being captured into a graph (cudaMalloc is not
-// capturable), code inside a framework that owns all device memory through its own pool
-// and forbids raw cudaMalloc/cudaFree (allocator-managed tensors), and tight measurement
-// loops where an allocation would synchronise the device.  Everything else in this
-// library allocates its scratch lazily per lattice handle.
+// Who needs this: callers that may not call cudaMalloc/cudaFree themselves or have the
+// library do it for them.  A framework that hands out all device memory from its own pool
+// (allocator-managed tensors) forbids raw allocations, because memory taken behind the pool's
+// back is invisible to its accounting and can make its own allocations fail; and a timing or
+// monitoring loop cannot afford one, because cudaMalloc/cudaFree synchronise the device and
+// would stall the work it measures.  Every other entry point of this library allocates its
+// scratch lazily per lattice handle.
 //
 // The block partial sums live in the file-scope array g_partials below: kMaxBlocks
 // doubles (128 KiB), resident on every GPU that loads the library until the process exits.
@@ -16,6 +17,11 @@
 // before the final pass reads them), so nothing has to be cleared between calls; calls
 // that overlap on the GPU (different streams, or different host threads on one device)
 // race on the shared array and must be serialised by the caller.
+//
+// Set-up: host code cannot pass g_partials itself to a kernel (its name on the host is a
+// stand-in, not a device address).  The first call on each device looks up the array's
+// device address with cudaGetSymbolAddress, with that device current, and caches it; that
+// first call should therefore come before any stream capture on the device.
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -110,13 +116,17 @@ int scratch_for_current_device(double** out)
 extern "C" int lt_plaquette_sum_noalloc(const double* links_dev, const int ext[4], double* out_dev, void* stream)
 {
     if (!links_dev || !ext || !out_dev) return lt::set_error(LT_ERR_ARG, "lt_plaquette_sum_noalloc: null pointer");
+    // the volume is checked after every factor, so no product of huge extents can wrap past the limit
+    long long V = 1;
     for (int d = 0; d < 4; ++d)
+    {
         if (ext[d] < 2 || ext[d] % 2)
             return lt::set_error(LT_ERR_ARG, "lt_plaquette_sum_noalloc: extents must be even and >= 2");
-    const long long V = (long long)ext[0] * ext[1] * ext[2] * ext[3];
-    if (V > (long long)kMaxBlocks * kSitesPerBlock)
-        return lt::set_error(LT_ERR_ARG, "lt_plaquette_sum_noalloc: lattice volume exceeds the 16,777,216-site "
-                                         "(64^4) limit of the static scratch");
+        V *= ext[d];
+        if (V > (long long)kMaxBlocks * kSitesPerBlock)
+            return lt::set_error(LT_ERR_ARG, "lt_plaquette_sum_noalloc: lattice volume exceeds the 16,777,216-site "
+                                             "(64^4) limit of the static scratch");
+    }
     double* scratch = nullptr;
     int r = scratch_for_current_device(&scratch);
     if (r != LT_OK) return r;

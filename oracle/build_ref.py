@@ -7,7 +7,17 @@ Copies the reference's ``LettuceGauge/`` headers from the read-only reference ch
 The reference's own build system (Makefile) is not used.  Eigen and PCG are taken from
 where they lie in the reference checkout.
 
-Usage: python oracle/build_ref.py [--ref /root/reference] [--extents 4x4x4x4 8x8x8x8 ...]
+Besides these parity builds (``-ffp-contract=off``, a fixed x86-64-v3 target), the CPU
+baseline is timed on ``oracle/_ref/liblt_ref_fast_<ext>_<isa>.so``: the same harness compiled
+with the optimisation of the reference Makefile (``Makefile:89``: ``-O3 -DNDEBUG
+-fno-math-errno -fopenmp``, ``-march=native``) with floating-point contraction on.  The GPU
+hosts are not this machine, so ``-march=native`` is built for both x86-64-v4 (AVX-512) and
+x86-64-v3 (AVX2) and the bench loads the best one the running host supports.
+
+The reference checkout is found at ``$LETTUCE_REFERENCE`` (default: the read-only checkout
+of this build environment).
+
+Usage: python oracle/build_ref.py [--ref DIR] [--extents 4x4x4x4 8x8x8x8 ...] [--fast]
 """
 from __future__ import annotations
 
@@ -32,6 +42,16 @@ DEFAULT_EXTENTS = ["4x4x4x4", "4x6x8x10", "8x8x8x8", "12x12x12x12", "16x16x16x16
 # the GPU hosts, and -ffp-contract=off so results do not depend on FMA contraction.
 CXXFLAGS = ["-std=c++20", "-O3", "-DNDEBUG", "-fno-math-errno", "-march=x86-64-v3",
             "-ffp-contract=off", "-fopenmp", "-DFIXED_SEED", "-fPIC", "-shared", "-w"]
+
+# The timing builds: the reference Makefile's optimisation with contraction on, per ISA level
+FAST_EXTENTS = ["32x32x32x32", "16x16x16x16"]
+FAST_ISAS = {"v4": "-march=x86-64-v4", "v3": "-march=x86-64-v3"}
+FAST_CXXFLAGS = ["-std=c++20", "-O3", "-DNDEBUG", "-fno-math-errno", "-ffp-contract=fast", "-fopenmp",
+                 "-DFIXED_SEED", "-fPIC", "-shared", "-w"]
+
+
+def default_reference() -> str:
+    return os.environ.get("LETTUCE_REFERENCE", "/root/reference")
 
 
 def lib_name(ext: str) -> str:
@@ -60,37 +80,54 @@ def stage_sources(ref: str) -> None:
     open(defines, "w").write(text)
 
 
-def build_one(ext: str) -> str:
+def fast_lib_name(ext: str, isa: str) -> str:
+    return os.path.join(OUT, f"liblt_ref_fast_{ext}_{isa}.so")
+
+
+def build_one(job) -> str:
+    ext, isa = job
     t, x, y, z = (int(v) for v in ext.split("x"))
-    cmd = ["g++", *CXXFLAGS, f"-DLT_NT={t}", f"-DLT_NX={x}", f"-DLT_NY={y}", f"-DLT_NZ={z}",
+    flags = CXXFLAGS if isa is None else [*FAST_CXXFLAGS, FAST_ISAS[isa]]
+    out = lib_name(ext) if isa is None else fast_lib_name(ext, isa)
+    cmd = ["g++", *flags, f"-DLT_NT={t}", f"-DLT_NX={x}", f"-DLT_NY={y}", f"-DLT_NZ={z}",
            "-I", SRC, "-I", os.path.join(SRC, "Eigen_3.4"),
-           os.path.join(HERE, "ref_harness.cpp"), "-o", lib_name(ext)]
+           os.path.join(HERE, "ref_harness.cpp"), "-o", out]
     subprocess.run(cmd, check=True)
-    return lib_name(ext)
+    return out
 
 
-def build(ref: str = "/root/reference", extents=None, force: bool = False) -> list[str]:
+def build(ref: str | None = None, extents=None, force: bool = False, fast: bool = True) -> list[str]:
+    ref = ref or default_reference()
     extents = list(extents or DEFAULT_EXTENTS)
     if not os.path.isdir(os.path.join(ref, "LettuceGauge")):
         raise FileNotFoundError(f"reference checkout not found at {ref}")
     harness = os.path.join(HERE, "ref_harness.cpp")
-    todo = [e for e in extents if force or not os.path.exists(lib_name(e))
-            or os.path.getmtime(lib_name(e)) < os.path.getmtime(harness)]
+    jobs = [(e, None) for e in extents]
+    if fast:
+        jobs += [(e, isa) for e in FAST_EXTENTS if e in extents for isa in FAST_ISAS]
+    outs = [lib_name(e) if isa is None else fast_lib_name(e, isa) for e, isa in jobs]
+    todo = [j for j, o in zip(jobs, outs) if force or not os.path.exists(o)
+            or os.path.getmtime(o) < os.path.getmtime(harness)]
     if not todo:
-        return [lib_name(e) for e in extents]
+        return outs
     stage_sources(ref)
     with cf.ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 1)) as pool:
         list(pool.map(build_one, todo))
-    return [lib_name(e) for e in extents]
+    return outs
+
+
+def reference_present() -> bool:
+    return os.path.isdir(os.path.join(default_reference(), "LettuceGauge"))
 
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None)
     ap.add_argument("--extents", nargs="*", default=None)
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--no-fast", action="store_true", help="skip the timing builds")
     a = ap.parse_args()
-    for p in build(a.ref, a.extents, a.force):
+    for p in build(a.ref, a.extents, a.force, fast=not a.no_fast):
         print(p)
     return 0
 

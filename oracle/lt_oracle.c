@@ -643,6 +643,69 @@ void or_flow(const int ext[4], const double* in, double* out, double eps, int n_
     free(Z);
 }
 
+/* ---------------------------------------------------------------- Zeuthen flow */
+/* The Zeuthen flow (Ramos and Sint, Eur. Phys. J. C 76 (2016) 15, arXiv:1508.05552; not in the
+ * reference, parity unpinned): the force is the Luescher-Weisz action's, X = Algebra(st_LW U^dag)
+ * (c_plaq = 5/3, c_rect = -1/12), acted on by 1 + (1/12) nabla*_mu nabla_mu with the adjoint
+ * covariant differences along the link direction:
+ *   nabla_mu w(x)  = U_mu(x) w(x+mu) U_mu(x)^dag - w(x)
+ *   nabla*_mu w(x) = w(x) - U_mu(x-mu)^dag w(x-mu) U_mu(x-mu)
+ * Z = c_old Z + c_new Algebra(X + nabla*_mu nabla_mu X / 12), then the integrator's update. */
+static void flow_z_zeuthen(const Geo* g, const double* U, double* Z, double* X, double c_old, double c_new)
+{
+    const int r0 = g_act_radius;
+    const double cp0 = g_act_cp, cr0 = g_act_cr;
+    long s;
+    int mu;
+    or_set_gauge_action(2, 5.0 / 3.0, -1.0 / 12.0);
+    for (s = 0; s < g->V; ++s)
+        for (mu = 0; mu < 4; ++mu)
+        {
+            M3 x = algebra(mul(act_staple(g, U, s, mu), dag(ld(U, s, mu))));
+            st(X, s, mu, &x);
+        }
+    or_set_gauge_action(r0, cp0, cr0);
+    for (s = 0; s < g->V; ++s)
+        for (mu = 0; mu < 4; ++mu)
+        {
+            long sp = move(g, s, mu, 1), sm = move(g, s, mu, -1);
+            M3 u = ld(U, s, mu), um = ld(U, sm, mu), x = ld(X, s, mu);
+            /* nabla w at x and at x - mu, then the backward difference of the two */
+            M3 dx = add(mul(mul(u, ld(X, sp, mu)), dag(u)), scl(-1.0, x));
+            M3 dxm = add(mul(mul(um, x), dag(um)), scl(-1.0, ld(X, sm, mu)));
+            M3 lap = add(dx, scl(-1.0, mul(mul(dag(um), dxm), um)));
+            M3 a = algebra(add(x, scl(1.0 / 12.0, lap)));
+            M3 z = c_old == 0.0 ? scl(c_new, a) : add(scl(c_old, ld(Z, s, mu)), scl(c_new, a));
+            st(Z, s, mu, &z);
+        }
+}
+
+/* The Zeuthen flow integrated with the stages of Integrators::GradientFlow (0 Euler, 1 RK2,
+ * 2 RK3, 3 RK3W7; gradient_flow.hpp:31-168) */
+void or_flow_zeuthen(const int ext[4], const double* in, double* out, double eps, int n_step, int integrator)
+{
+    static const double stages[4][3][3] = {
+        { { 0.0, 1.0, 1.0 } },
+        { { 0.0, 1.0, 0.5 }, { -0.5, 1.0, 1.0 } },
+        { { 0.0, 1.0, 0.25 }, { -17.0 / 36.0, 8.0 / 9.0, 1.0 }, { -1.0, 3.0 / 4.0, 1.0 } },
+        { { 0.0, 1.0, 1.0 / 3.0 }, { -25.0 / 48.0, 15.0 / 16.0, 1.0 }, { -17.0 / 25.0, 8.0 / 15.0, 1.0 } } };
+    static const int n_stage[4] = { 1, 2, 3, 3 };
+    Geo g = geo(ext);
+    size_t n = (size_t)g.V * 4 * 18;
+    double* Z = (double*)calloc(n, sizeof(double));
+    double* X = (double*)calloc(n, sizeof(double));
+    int k, j;
+    if (out != in) memcpy(out, in, n * sizeof(double));
+    for (k = 0; k < n_step; ++k)
+        for (j = 0; j < n_stage[integrator]; ++j)
+        {
+            flow_z_zeuthen(&g, out, Z, X, stages[integrator][j][0], stages[integrator][j][1] * eps);
+            flow_update(&g, out, Z, stages[integrator][j][2]);
+        }
+    free(Z);
+    free(X);
+}
+
 /* ---------------------------------------------------------------- stout smearing */
 /* StoutSmearing4D (stout_smearing.hpp:29-57) */
 static void stout_step(const Geo* g, const double* in, double* out, double rho)
@@ -1316,6 +1379,29 @@ void or_bias_update(or_bias* b, double cv)
         double d = cv - (b->cv_min + i * b->bin_width);
         b->grid[i] += b->weight * exp(-0.5 * wis * d * d - b->grid[i] / b->wt);
     }
+}
+
+/* The Gaussian-free binned deposit (semantics not in the reference, which deposits Gaussians;
+ * parity unpinned): with x = (cv - cv_min) / bin_width the grid points floor(x) and
+ * floor(x) + 1 receive weight (1 - frac(x)) and weight frac(x), each times
+ * exp(-V_point / wt) (the reference's per-point well-tempering, metadynamics.hpp:116-118).
+ * Out-of-range CVs deposit nothing. */
+void or_bias_update_binned(or_bias* b, double cv)
+{
+    double x, a, v0, v1;
+    int i;
+    if (!(cv >= b->cv_min && cv < b->cv_max)) return;
+    x = (cv - b->cv_min) / b->bin_width;
+    i = (int)floor(x);
+    if (i < 0) i = 0;
+    if (i > b->bins - 1) i = b->bins - 1;
+    a = x - (double)i;
+    if (a < 0.0) a = 0.0;
+    if (a > 1.0) a = 1.0;
+    v0 = b->grid[i];
+    v1 = b->grid[i + 1];
+    b->grid[i] = v0 + b->weight * (1.0 - a) * exp(-v0 / b->wt);
+    b->grid[i + 1] = v1 + b->weight * a * exp(-v1 / b->wt);
 }
 
 void or_bias_update_symmetric(or_bias* b, double cv)

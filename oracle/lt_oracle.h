@@ -59,11 +59,14 @@ or_bias* or_bias_create(double cv_min, double cv_max, int bins, double weight, d
 void     or_bias_destroy(or_bias* b);
 void     or_bias_update(or_bias* b, double cv);
 void     or_bias_update_symmetric(or_bias* b, double cv);
+void     or_bias_update_binned(or_bias* b, double cv);
 double   or_bias_potential(const or_bias* b, double cv);
 double   or_bias_derivative(const or_bias* b, double cv);
 
 /* Flow with any of the reference's integrators: 0 Euler, 1 RK2, 2 RK3, 3 RK3W7 */
 void   or_flow(const int ext[4], const double* in, double* out, double eps, int n_step, int integrator);
+/* The Zeuthen flow (not in the reference) with the same integrators */
+void   or_flow_zeuthen(const int ext[4], const double* in, double* out, double eps, int n_step, int integrator);
 
 /* The measurement bundle of SU3_main.cpp:89-235 */
 void   or_clover_timeslices(const int ext[4], const double* U, double* q_t, double* e_t);

@@ -68,6 +68,7 @@
 #include "LettuceGauge/updates/overrelaxation.hpp"
 #include "LettuceGauge/IO/config_io/bmw_format.hpp"
 #include "LettuceGauge/updates/parity_update.hpp"
+#include "LettuceGauge/updates/tempering.hpp"
 // Only the two HMC headers are compiled with `private` mapped to `public` (they hold no
 // OpenMP `private(...)` clauses, which the mapping would break).
 #define private public
@@ -509,6 +510,43 @@ void ref_bias_probe(double cv_min, double cv_max, int bins, double weight, doubl
     }
 }
 
+// MetadynamicsTemperingKernel::operator() (updates/tempering.hpp:51-72) once, on the
+// unbiased stream's links `links_u` (Gluon) and the biased stream's `links_temper`
+// (Gluon_temper), with the bias of the reference driver (SU3_main.cpp:566-578) after
+// well-tempered deposits at `deposits`, and CV_current = cv_current.  The kernel draws its
+// uniform from a fresh FIXED_SEED generator; a second fresh generator gives the same first
+// draw, recorded here.  out = {CV_new (MetaCharge of links_u), CV_old, delta_V_tempering,
+// uniform, accepted, CV_current afterwards}; on acceptance the two fields come back swapped.
+void ref_tempering(double* links_u, double* links_temper, double rho, double cv_current, const double* deposits,
+                   int n_dep, double* out)
+{
+    auto U  = std::make_unique<GaugeField>();
+    auto Ut = std::make_unique<GaugeField>();
+    auto C1 = std::make_unique<GaugeField>();
+    auto C2 = std::make_unique<GaugeField>();
+    load(*U, links_u);
+    load(*Ut, links_temper);
+    MetaBiasPotential bias(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0);
+    std::vector<double> cvs(deposits, deposits + n_dep);
+    if (n_dep > 0) bias.UpdatePotential(cvs);
+    bias.SetCV_current(cv_current);
+    auto gen_probe = MakeRandomGenerator();
+    PRNG probe(gen_probe);
+    const double q = probe.UniformReal();
+    auto gen = MakeRandomGenerator();
+    auto p = std::make_unique<PRNG>(gen);
+    RunStatistics stats;
+    GaugeUpdates::MetadynamicsTemperingKernel<PRNG> kern(*U, *Ut, *C1, *C2, bias, *p, stats, rho);
+    out[0] = kern.MetaCharge(*U, *C1, *C2, n_smear_meta, rho);
+    out[1] = bias.ReturnCV_current();
+    out[4] = kern() ? 1.0 : 0.0;
+    out[2] = stats.delta_V_tempering;
+    out[3] = q;
+    out[5] = bias.ReturnCV_current();
+    store(*U, links_u);
+    store(*Ut, links_temper);
+}
+
 // A field kept resident in the library between calls, so timed CPU-baseline samples do
 // not include the layout conversion of ref_* entry points above.
 static std::unique_ptr<GaugeField> g_field, g_flowed, g_force;
@@ -534,6 +572,33 @@ double ref_field_sweeps(double b, int n_hb, int n_or)
     Iterator::Checkerboard(HB, n_hb);
     Iterator::Checkerboard(OR, n_or);
     return PlaquetteSum(*g_field);
+}
+
+// n_round rounds of (n_hb heatbath + n_or overrelaxation sweeps) on the resident field, as
+// the reference driver's update loop runs them (SU3_main.cpp: Iterator::Checkerboard of the
+// heatbath kernel, then of the overrelaxation kernel, per round); no observable in between.
+// This is the timed CPU baseline.
+void ref_field_rounds(double b, int n_round, int n_hb, int n_or)
+{
+    set_beta(b);
+    HeatbathKernel HB(*g_field, GaugeAction::WilsonAction, prng());
+    OverrelaxationSubgroupKernel OR(*g_field, GaugeAction::WilsonAction);
+    for (int r = 0; r < n_round; ++r)
+    {
+        Iterator::Checkerboard(HB, n_hb);
+        Iterator::Checkerboard(OR, n_or);
+    }
+}
+
+// n RK3 flow steps of the resident field into a second resident field, nothing measured
+// (the timed flow baseline)
+void ref_field_flow_steps(double eps, int n)
+{
+    if (!g_flowed) g_flowed = std::make_unique<GaugeField>();
+    if (!g_force) g_force = std::make_unique<GaugeField>();
+    Integrators::GradientFlow::RK3 rk3(*g_force);
+    GradientFlowKernel Flow(*g_field, *g_flowed, rk3, GaugeAction::WilsonAction, eps);
+    Flow(n);
 }
 
 // n RK3 flow steps of the resident field into a second resident field; returns its plaquette sum

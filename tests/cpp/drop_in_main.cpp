@@ -54,6 +54,11 @@ int main(int argc, char** argv)
                     EnergyDensityClover(Gluonsmeared1));
     }
 
+    // the Zeuthen flow as the flow's action (no counterpart in the reference)
+    GradientFlowKernel ZeuthenFlow(Gluon, Gluonchain, rk3, GaugeAction::ZeuthenFlowAction, 0.01);
+    ZeuthenFlow(10);
+    std::printf("zeuthen E %.15f\n", EnergyDensityClover(Gluonchain));
+
     // the reference driver's HMC integrator, OMF_4 (SU3_main.cpp:331), then a parity update (:527-531)
     Integrators::HMC::OMF_4 omf4;
     RunStatistics hmc_statistics;
@@ -64,6 +69,7 @@ int main(int argc, char** argv)
     std::printf("parity dH %.10f Q %.12f %.12f\n", hmc_statistics.delta_H_hmc, q_before, TopChargeClover(Gluon));
 
     MetaBiasPotential TopBiasPotential(-8.0, 8.0, 800, 0.05, 4 * 16.0 / 800, 10.0, 1000.0);
+    TopBiasPotential.SetUpdateMode(LT_BIAS_BINNED);
     RunStatistics statistics;
     Integrators::HMC::OMF_2_OMF_4 omf2_omf4;
     GaugeUpdates::HMCMetaDKernel HMC_MetaD(Gluon, TopBiasPotential, omf2_omf4, SimulatedAction, statistics, 1.0, 0.12, 4, 99);

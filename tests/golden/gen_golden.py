@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-from ltref import Reference, haar_links_numpy  # noqa: E402
+from ltref import Reference, checksums, haar_links_numpy, large_input  # noqa: E402
 
 BETA = 6.0
 N_SAMPLE = 64
@@ -29,11 +29,6 @@ def sample_links(V: int, seed: int) -> np.ndarray:
     return np.sort(rng.choice(4 * V, size=N_SAMPLE, replace=False))
 
 
-def checksums(field: np.ndarray) -> np.ndarray:
-    """Size-independent summary of a full field: sum, sum of squares, index-weighted sum."""
-    f = field.reshape(-1)
-    w = np.arange(f.size, dtype=np.float64) % 97.0
-    return np.array([f.sum(), (f * f).sum(), (w * f).sum()])
 
 
 def take(field: np.ndarray, links: np.ndarray) -> np.ndarray:
@@ -267,16 +262,164 @@ def gen_rect() -> dict:
     return out
 
 
+N_SAMPLE_LARGE = 256
+
+
+def gen_large() -> dict:
+    """The benchmarked 32^4 configuration: one overrelaxation sweep and 10 RK3 flow steps of
+    the reference, one heatbath sweep of the C oracle (the GPU's Philox stream), and P, Q, E
+    of the input, as 256 sampled links plus full-field checksums."""
+    from ltref import Oracle
+    o = Oracle()
+    ext = (32, 32, 32, 32)
+    V = int(np.prod(ext))
+    ref = Reference(ext)
+    U = large_input(ext, 32, 77, o)
+    rng = np.random.default_rng(3232)
+    links = np.sort(rng.choice(4 * V, size=N_SAMPLE_LARGE, replace=False))
+    d = {"ext": np.array(ext, dtype=np.int32), "seed": np.array(32), "hb_seed": np.array(77), "links": links,
+         "U_ck": checksums(U), "plaq": np.array(ref.plaquette_sum(U)), "Q": np.array(ref.topcharge(U)),
+         "E": np.array(ref.energy(U))}
+    O = ref.overrelax(U, 1)
+    d["or1"], d["or1_ck"], d["or1_plaq"] = take(O, links), checksums(O), np.array(ref.plaquette_sum(O))
+    del O
+    F = ref.flow_rk3(U, 0.01, 10)
+    d["flow10"], d["flow10_ck"] = take(F, links), checksums(F)
+    d["flow10_plaq"], d["flow10_q"] = np.array(ref.plaquette_sum(F)), np.array(ref.topcharge(F))
+    del F
+    H = o.heatbath(ext, U, BETA, 1, 555, 3)
+    d["hb1_oracle"], d["hb1_oracle_ck"] = take(H, links), checksums(H)
+    return d
+
+
+def gen_flow_large() -> dict:
+    """The reference's FP64 RK3 flow (eps = 0.01) of the 32^4 parity input to t = 4, with
+    the plaquette sum, clover Q and clover E at t = 0.5, 1, 1.5, ..., 4 (every 50 steps)."""
+    ext = (32, 32, 32, 32)
+    ref = Reference(ext)
+    U = large_input(ext, 32, 77)
+    p, q, e = ref.flow_rk3_measure(U, 0.01, 8, 50)
+    return {"ext": np.array(ext, dtype=np.int32), "eps": np.array(0.01), "every": np.array(50),
+            "t": 0.01 * 50 * np.arange(1, 9), "plaq": p, "Q": q, "E": e}
+
+
+def gen_metad16() -> dict:
+    """The reference's metadynamics force (4 stout steps of rho = 0.12, dV/dQ = 1) at 16^4."""
+    ext = (16, 16, 16, 16)
+    V = int(np.prod(ext))
+    ref = Reference(ext)
+    U = large_input(ext, 16, 7)
+    links = sample_links(V, 1616)
+    M, q = ref.metad_force(U, 0.12, 1.0)
+    return {"ext": np.array(ext, dtype=np.int32), "seed": np.array(16), "hb_seed": np.array(7), "links": links,
+            "U_ck": checksums(U), "metad": take(M, links), "metad_ck": checksums(M), "metad_q": np.array(q),
+            "metad_nstout": np.array(ref.lib.ref_n_smear_meta()), "Q": np.array(ref.topcharge(U))}
+
+
+def gen_tempering() -> dict:
+    """MetadynamicsTemperingKernel::operator() of the reference (updates/tempering.hpp:51-72)
+    on two thermalised 8^4 fields for five biases: flat, deposits at the candidate's charge
+    (rejection), at the biased stream's charge (acceptance), CV_current beyond the grid (the
+    wall), and a bias tuned so that exp(-dV) lies near the kernel's uniform."""
+    from ltref import Oracle
+    o = Oracle()
+    ext = (8, 8, 8, 8)
+    ref = Reference(ext)
+    Ua = o.heatbath(ext, haar_links_numpy(ext, 81), BETA, 30, 5, 0)
+    Ub = o.heatbath(ext, haar_links_numpy(ext, 82), BETA, 30, 6, 0)
+    rho = 0.12
+    probe = np.empty(6)
+    ref.lib.ref_tempering(Ua.copy(), Ub.copy(), rho, 0.0, np.zeros(1), 0, probe)
+    cv_new, q = probe[0], probe[3]
+    cv_old = cv_new + 1.3
+    cases = [(cv_old, np.zeros(0)), (cv_old, np.full(400, cv_new)), (cv_old, np.full(25, cv_old)),
+             (9.5, np.full(5, cv_new)), (cv_new - 0.2, np.concatenate([np.full(3, cv_new), np.full(2, cv_new - 0.2)]))]
+    res, dep_all, dep_n = [], [], []
+    for cvo, dep in cases:
+        out = np.empty(6)
+        ref.lib.ref_tempering(Ua.copy(), Ub.copy(), rho, cvo, np.ascontiguousarray(dep) if dep.size else np.zeros(1),
+                              int(dep.size), out)
+        res.append(out)
+        dep_all.append(dep)
+        dep_n.append(dep.size)
+    return {"ext": np.array(ext, dtype=np.int32), "rho": np.array(rho), "seeds": np.array([81, 82, 5, 6, 30]),
+            "Ua_ck": checksums(Ua), "Ub_ck": checksums(Ub), "out": np.array(res),
+            "deposits": np.concatenate(dep_all), "n_dep": np.array(dep_n), "cv_old": np.array([c for c, _ in cases]),
+            "uniform": np.array(q)}
+
+
+def exp_inputs(seed: int) -> np.ndarray:
+    """Traceless Hermitian matrices for every branch of the device exponential and of the
+    reference's SU3::exp: generic (c1 > 1/2), the long (1/32 < c1 <= 1/2) and short series
+    ranges, tiny arguments, negative determinants (sign flip), exactly degenerate spectra
+    (theta = 0, w = 0: the Taylor branches of xi_0, xi_1), nearly degenerate ones, diagonal
+    and zero matrices."""
+    rng = np.random.default_rng(seed)
+    out = []
+
+    def herm(scale):
+        M = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+        H = 0.5 * (M + M.conj().T)
+        H -= np.trace(H) / 3.0 * np.eye(3)
+        return H / np.sqrt(0.5 * np.trace(H @ H).real) * scale   # scale = sqrt(c1)
+
+    def rotate(D):
+        M = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+        Q, _ = np.linalg.qr(M)
+        return Q @ D @ Q.conj().T
+
+    for s in (3.0, 1.5, 0.9, 0.7, 0.6, 0.5, 0.35, 0.2, 0.17, 0.12, 0.05, 1e-2, 1e-4, 1e-8):
+        for _ in range(4):
+            H = herm(s)
+            out += [H, -H]
+    for a in (0.4, 0.05, 1e-3, 1.2):
+        D = np.diag([a, a, -2 * a]).astype(np.complex128)
+        out += [D, -D, rotate(D), -rotate(D)]
+        for eps in (1e-3, 1e-6, 1e-9):
+            D2 = np.diag([a, a + eps * a, -2 * a - eps * a]).astype(np.complex128)
+            out += [rotate(D2), -rotate(D2)]
+    out.append(np.zeros((3, 3), dtype=np.complex128))
+    A = np.array(out)
+    r = np.empty(A.shape + (2,))
+    r[..., 0], r[..., 1] = A.real, A.imag
+    return r
+
+
+def gen_exp() -> dict:
+    ref = Reference((4, 4, 4, 4))
+    Hm = exp_inputs(4242)
+    return {"exp_in": Hm, "exp_out": ref.su3_exp(np.ascontiguousarray(Hm).reshape(-1)).reshape(Hm.shape)}
+
+
 def main() -> int:
     import argparse
     import subprocess
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["chain", "bmw", "measure", "md", "rect"], default=None,
+    ap.add_argument("--only", choices=["chain", "bmw", "measure", "md", "rect", "large", "flow_large", "metad16",
+                                       "exp", "tempering"], default=None,
                     help="regenerate one fixture only")
     a = ap.parse_args()
     root = os.path.dirname(os.path.dirname(HERE))
     subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "4x4x4x4",
                     "4x6x8x10", "8x8x8x8", "2x4x6x8"], check=True)
+    if a.only in ("large", "flow_large"):
+        subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "32x32x32x32"],
+                       check=True)
+        out = gen_large() if a.only == "large" else gen_flow_large()
+        name = "ref_32x32x32x32.npz" if a.only == "large" else "ref_flow_32x32x32x32.npz"
+        np.savez_compressed(os.path.join(HERE, name), **out)
+        return 0
+    if a.only == "metad16":
+        subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "16x16x16x16"],
+                       check=True)
+        np.savez_compressed(os.path.join(HERE, "ref_metad_16x16x16x16.npz"), **gen_metad16())
+        return 0
+    if a.only == "tempering":
+        np.savez_compressed(os.path.join(HERE, "ref_tempering.npz"), **gen_tempering())
+        return 0
+    if a.only == "exp":
+        np.savez_compressed(os.path.join(HERE, "ref_exp.npz"), **gen_exp())
+        return 0
     if a.only == "chain":
         np.savez_compressed(os.path.join(HERE, "ref_chain_8x8x8x8.npz"), **gen_chain())
         return 0

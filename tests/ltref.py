@@ -60,10 +60,12 @@ class Oracle:
             "or_bias_destroy": (None, [C.c_void_p]),
             "or_bias_update": (None, [C.c_void_p, d]),
             "or_bias_update_symmetric": (None, [C.c_void_p, d]),
+            "or_bias_update_binned": (None, [C.c_void_p, d]),
             "or_bias_potential": (d, [C.c_void_p, d]),
             "or_bias_derivative": (d, [C.c_void_p, d]),
             "or_bmw_encode": (u64, [_ip, _dp, i, C.c_void_p]),
             "or_flow": (None, [_ip, _dp, _dp, d, i, i]),
+            "or_flow_zeuthen": (None, [_ip, _dp, _dp, d, i, i]),
             "or_clover_timeslices": (None, [_ip, _dp, _dp, _dp]),
             "or_topcharge_plaquette": (d, [_ip, _dp]),
             "or_rect_action": (d, [_ip, _dp, d, d, d]),
@@ -213,6 +215,11 @@ class Oracle:
         self.lib.or_flow(self._e(ext), np.ascontiguousarray(U), out, eps, n, integrator)
         return out
 
+    def flow_zeuthen(self, ext, U, eps, n, integrator=2):
+        out = np.empty_like(U)
+        self.lib.or_flow_zeuthen(self._e(ext), np.ascontiguousarray(U), out, eps, n, integrator)
+        return out
+
     def measure(self, ext, U, beta=6.0):
         """The bundle of SU3_main.cpp:89-235 on one field: dict of the observables."""
         U = np.ascontiguousarray(U)
@@ -295,6 +302,7 @@ class Reference:
                 "ref_md_action": (i, [_dp, _dp, d, d, i, i, i, d, d, C.POINTER(d), C.POINTER(d)]),
                 "ref_flow_action": (None, [_dp, _dp, d, i, i, i, d, d]),
                 "ref_wilson_loop_chain": (d, [_dp, i, i, i]),
+                "ref_tempering": (None, [_dp, _dp, d, d, _dp, i, _dp]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(lib, name)
@@ -478,6 +486,22 @@ def haar_links_numpy(ext, seed):
     out[..., 0] = Qr.real
     out[..., 1] = Qr.imag
     return out
+
+
+def checksums(field: np.ndarray) -> np.ndarray:
+    """Size-independent summary of a full field: sum, sum of squares, index-weighted sum."""
+    f = np.asarray(field, dtype=np.float64).reshape(-1)
+    w = np.arange(f.size, dtype=np.float64) % 97.0
+    return np.array([f.sum(), (f * f).sum(), (w * f).sum()])
+
+
+def large_input(ext, seed: int, hb_seed: int, oracle=None) -> np.ndarray:
+    """Input of the full-size parity fixtures: numpy Haar start, then one heatbath sweep of
+    the C oracle (Philox stream hb_seed, beta = 6), so that no SU(2) projection of the first
+    overrelaxation sweep is near-singular.  Regenerated bit for bit on any host by the same
+    two calls."""
+    o = oracle or Oracle()
+    return o.heatbath(ext, haar_links_numpy(ext, seed), 6.0, 1, hb_seed, 0)
 
 
 def rel_err(a, b):

@@ -30,9 +30,12 @@ def test_exports_every_declared_symbol():
     assert set(declared) <= set(_lib.SIGNATURES), set(declared) - set(_lib.SIGNATURES)
 
 
-def test_kernels_are_sm100a():
-    out = subprocess.run(["cuobjdump", "--list-elf", _lib.LIB_PATH], capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+def test_build_targets_sm100a_only():
+    """The recipe compiles every translation unit for sm_100a and nothing else (the device
+    side is checked on a B200 by lt_device_arch, tests/test_gpu_exp.py)."""
+    from lettuce_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert "lt_selftest.cu" in build.SOURCES
 
 
 def test_version():
@@ -80,6 +83,21 @@ def test_create_rejects_oversized_lattice_without_device():
     assert lt.lib().lt_create(np.array([96, 96, 96, 96], dtype=np.int32), 0, C.byref(h)) == _lib.LT_ERR_ARG
     assert b"too large" in lt.lib().lt_last_error()
     assert lt.lib().lt_create(np.array([2, 2, 2, 0], dtype=np.int32), 0, C.byref(h)) == _lib.LT_ERR_ARG
+    # extents whose product wraps 64-bit arithmetic are refused before the product is formed
+    big = 1 << 30
+    assert lt.lib().lt_create(np.array([big, big, 16, 2], dtype=np.int32), 0, C.byref(h)) == _lib.LT_ERR_ARG
+    assert b"too large" in lt.lib().lt_last_error()
+    assert not h.value
+
+
+def test_exp_test_entry_checks_arguments_without_device():
+    q = np.zeros(18)
+    out = np.zeros(18)
+    L = lt.lib()
+    assert L.lt_su3_exp_test(q, out, 1, 7, 0) == _lib.LT_ERR_ARG
+    assert L.lt_su3_exp_test(q, out, 1, 0, 9) == _lib.LT_ERR_ARG
+    assert L.lt_su3_exp_test(q, out, -1, 0, 0) == _lib.LT_ERR_ARG
+    assert L.lt_su3_exp_test(q, out, 0, 0, 0) == _lib.LT_OK
 
 
 def test_entry_points_check_handles_without_device():

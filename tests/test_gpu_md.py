@@ -160,3 +160,28 @@ class TestParity:
         tol = 1e-12 if prec == "fp64" else 1e-5
         assert lt.TopChargeClover(G) == pytest.approx(-q, rel=tol, abs=tol)
         assert lt.WilsonAction(6.0).Action(G) == pytest.approx(s, rel=tol)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32_12"])
+def test_metad_trajectories_with_binned_bias(oracle, prec):
+    """MetaD-HMC with the Gaussian-free binned deposits (the metadynamics configuration):
+    every trajectory deposits symmetrically at its path samples, so without tempering the grid
+    sum grows by 2 weight per sample and the deposits form mirror pairs."""
+    import lettuce_b200 as lt
+    from ltref import haar_links_numpy
+    ext = (8, 8, 8, 8)
+    U = oracle.heatbath(ext, haar_links_numpy(ext, 12), 6.0, 10, 3, 0)
+    G = lt.GaugeField(ext, prec)
+    G.upload(U)
+    bias = lt.MetaBiasPotential(-8, 8, 800, 0.05, 0.08, 1e300, 1000)
+    bias.SetUpdateMode("binned")
+    hmc = lt.HMCMetaDKernel(G, bias, lt.WilsonAction(6.0), 1.0, 0.12, 4, seed=9)
+    sums = [0.0]
+    for _ in range(3):
+        hmc(10, True)
+        g = bias.grid()
+        sums.append(g.sum())
+        assert np.allclose(g, g[::-1], rtol=1e-12, atol=1e-14)
+    steps = np.diff(sums) / (2 * 0.05)
+    assert np.all(steps >= 1) and np.allclose(steps, np.round(steps), atol=1e-9)
+    assert np.count_nonzero(bias.grid()) <= 4 * int(round(sum(steps)))

@@ -5,10 +5,14 @@ own code (tests/golden/gen_golden.py) and, where the reference harness is built 
 the reference run live on fresh inputs.  Tolerance: 1e-12 relative to the field's largest
 entry (FP64 on both sides; the only differences are summation order and libm rounding).
 """
+import os
+
 import numpy as np
 import pytest
 
 from ltref import DBW2, IWASAKI, LUESCHER_WEISZ, WILSON, Reference, haar_links_numpy, ref_available, rel_err
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 TOL = 1e-12
 
@@ -91,6 +95,19 @@ class TestGolden4:
         g = golden4
         out = oracle.su3_exp(g["exp_in"].reshape(-1)).reshape(g["exp_out"].shape)
         assert np.max(np.abs(out - g["exp_out"])) < 1e-13
+
+    def test_su3_exp_branch_cases(self, oracle):
+        """Every branch range of the exponential (tests/golden/ref_exp.npz): the oracle and
+        the reference agree, and both agree with an independent Pade evaluation of expm."""
+        import scipy.linalg as sl
+        g = dict(np.load(os.path.join(GOLDEN, "ref_exp.npz")))
+        out = oracle.su3_exp(g["exp_in"].reshape(-1)).reshape(g["exp_out"].shape)
+        assert np.max(np.abs(out - g["exp_out"])) < 1e-13
+        q = g["exp_in"].reshape(-1, 9, 2)
+        Q = (q[..., 0] + 1j * q[..., 1]).reshape(-1, 3, 3)
+        E = np.array([sl.expm(1j * M) for M in Q])
+        R = g["exp_out"].reshape(-1, 9, 2)
+        assert np.max(np.abs(E.reshape(-1, 9) - (R[..., 0] + 1j * R[..., 1]))) < 1e-13
 
 
 class TestGoldenOdd:
@@ -379,3 +396,29 @@ class TestRectangularActions:
             b = ref.md_action(U, P, 5.9, 0.3, 2, 7, act)
             assert rel_err(a[0], b[0]) < 1e-12 and a[3] == pytest.approx(b[3], rel=1e-13)
             assert rel_err(oracle.flow_action(ext, U, 0.03, 3, 3, act), ref.flow_action(U, 0.03, 3, 3, act)) < 1e-12
+
+
+class TestLargeFixtures:
+    """The full-size fixtures used by the GPU parity tests at the benchmarked sizes: their
+    inputs regenerate bit for bit here, and the oracle reproduces the reference's
+    overrelaxation sweep at 32^4."""
+
+    def test_32x4_input_and_overrelaxation(self, oracle):
+        from ltref import checksums, large_input
+        g = dict(np.load(os.path.join(GOLDEN, "ref_32x32x32x32.npz")))
+        ext = tuple(int(e) for e in g["ext"])
+        U = large_input(ext, int(g["seed"]), int(g["hb_seed"]), oracle)
+        np.testing.assert_allclose(checksums(U), g["U_ck"], rtol=1e-13)
+        O = oracle.overrelax(ext, U, 1)
+        assert rel_err(O.reshape(-1, 18)[g["links"]], g["or1"]) < TOL
+        assert oracle.plaquette_sum(ext, O) == pytest.approx(float(g["or1_plaq"]), rel=TOL)
+
+    def test_16x4_metad_input(self, oracle):
+        from ltref import checksums, large_input
+        g = dict(np.load(os.path.join(GOLDEN, "ref_metad_16x16x16x16.npz")))
+        ext = tuple(int(e) for e in g["ext"])
+        U = large_input(ext, int(g["seed"]), int(g["hb_seed"]), oracle)
+        np.testing.assert_allclose(checksums(U), g["U_ck"], rtol=1e-13)
+        F, q = oracle.metad_force(ext, U, 0.12, int(g["metad_nstout"]), 1.0)
+        assert q == pytest.approx(float(g["metad_q"]), rel=1e-11, abs=1e-12)
+        assert rel_err(F.reshape(-1, 18)[g["links"]], g["metad"]) < 1e-11
