@@ -155,6 +155,16 @@ int lt_wilson_loop_chain(lt_lattice* h, int start, int end, int reset, double* o
 /* PolyakovLoop (observables/polyakov_loop.hpp:32-49): mean over the spatial sites of the trace
  * of the product of the links in direction t. */
 int lt_polyakov_loop(lt_lattice* h, double* re, double* im);
+/* CalculateClover<1, 1> (observables/clover.hpp:94-152): the clover field of the handle's
+ * links as a FullTensor4D (lattice.hpp:447-590) in its layout double[V][4][4][3][3][2]
+ * (index ((site * 4 + mu) * 4 + nu)), FP64 products whatever the storage.  The tensor is kept
+ * in device memory with the handle (16 V 3x3 complex: 2304 bytes per site) and copied to
+ * tensor_out unless that is NULL. */
+int lt_clover_tensor(lt_lattice* h, double* tensor_out);
+/* TopChargeClover(const FullTensor&) (observables/topological_charge.hpp:202-231): Q of the
+ * tensor `tensor` (host memory, the layout above, the handle's extents), or of the tensor the
+ * handle keeps from lt_clover_tensor when tensor is NULL. */
+int lt_topcharge_clover_tensor(lt_lattice* h, const double* tensor, double* q_out);
 /* WilsonAction::Staple for every link (rectangular_action.hpp:104-184), reference layout. */
 int lt_staples(lt_lattice* h, double* staples_out);
 /* Plaquette sum of a field that the caller already holds in device memory, in the reference

@@ -110,6 +110,45 @@ inline double TopChargeClover(const GaugeField& U)
     return v;
 }
 
+// FullTensor4D (lattice.hpp:447-590): 16 3x3 complex matrices per site in host memory, layout
+// double[V][4][4][3][3][2]; CalculateClover<1, 1> (observables/clover.hpp:94-152) fills it on
+// the device, TopChargeClover(const FullTensor&) (topological_charge.hpp:202-231) reads it
+class FullTensor
+{
+public:
+    explicit FullTensor(std::array<int, 4> ext)
+        : ext_(ext), data_((std::size_t)ext[0] * ext[1] * ext[2] * ext[3] * 16 * 18, 0.0)
+    {
+    }
+    std::array<int, 4> Shape() const { return ext_; }
+    std::size_t Volume() const { return data_.size() / (16 * 18); }
+    // the 18 doubles of C_{mu nu} at site (reference site index)
+    const double* operator()(std::size_t site, int mu, int nu) const { return data_.data() + 18 * ((site * 4 + mu) * 4 + nu); }
+    double* operator()(std::size_t site, int mu, int nu) { return data_.data() + 18 * ((site * 4 + mu) * 4 + nu); }
+    const std::vector<double>& Data() const { return data_; }
+    std::vector<double>& Data() { return data_; }
+
+private:
+    std::array<int, 4> ext_;
+    std::vector<double> data_;
+};
+
+template <int N = 1>
+inline void CalculateClover(const GaugeField& U, FullTensor& Clov)
+{
+    static_assert(N == 1, "only the plaquette clover CalculateClover<1, 1> is provided");
+    if (Clov.Shape() != U.Shape()) throw Error(LT_ERR_ARG, "CalculateClover: tensor and field extents differ");
+    check(lt_clover_tensor(U.handle(), Clov.Data().data()));
+}
+
+inline double TopChargeClover(const FullTensor& Clov)
+{
+    GaugeField scratch(Clov.Shape());   // supplies the extents, stream and reduction scratch
+    double v;
+    check(lt_topcharge_clover_tensor(scratch.handle(), Clov.Data().data(), &v));
+    return v;
+}
+
 // EnergyDensity::Clover of the traceless clover field strength (field_strength_tensor.hpp:154-175)
 inline double EnergyDensityClover(const GaugeField& U)
 {

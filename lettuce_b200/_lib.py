@@ -53,6 +53,8 @@ SIGNATURES = {
     "lt_energy_clover": (_i, [_vp, _pd]),
     "lt_clover_observables": (_i, [_vp, _pd, _pd]),
     "lt_staples": (_i, [_vp, _dp]),
+    "lt_clover_tensor": (_i, [_vp, _vp]),
+    "lt_topcharge_clover_tensor": (_i, [_vp, _vp, _pd]),
     "lt_plaquette_sum_noalloc": (_i, [_vp, _ip, _vp, _vp]),
     "lt_su3_exp_test": (_i, [_dp, _dp, _i, _i, _i]),
     "lt_device_arch": (_i, [_pi, _pi]),

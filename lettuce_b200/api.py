@@ -156,8 +156,42 @@ def PlaquetteSum(U: GaugeField) -> float:
     return _out1(lib().lt_plaquette_sum, U.handle)
 
 
-def TopChargeClover(U: GaugeField) -> float:
-    """observables/topological_charge.hpp:97-200."""
+class FullTensor:
+    """FullTensor4D (lattice.hpp:447-590): 16 3x3 complex matrices per site in the reference
+    layout [V, 4, 4, 3, 3, 2] (host memory).  CalculateClover fills it; TopChargeClover accepts
+    it as the reference's TopChargeClover(const FullTensor&) does."""
+
+    def __init__(self, ext):
+        self.ext = tuple(int(e) for e in ext)
+        self.data = np.zeros((int(np.prod(self.ext)), 4, 4, 3, 3, 2))
+        self._field = None
+
+    def __call__(self, site: int, mu: int, nu: int) -> np.ndarray:
+        m = self.data[site, mu, nu]
+        return m[..., 0] + 1j * m[..., 1]
+
+
+def CalculateClover(U: GaugeField, Clov: "FullTensor | None" = None) -> FullTensor:
+    """CalculateClover<1, 1> (observables/clover.hpp:94-152): the four-leaf clover C_{mu nu}
+    of every site (C_{nu mu} = C_{mu nu}^dag, zero diagonal), FP64 products."""
+    if Clov is None:
+        Clov = FullTensor(U.ext)
+    if Clov.ext != tuple(U.ext):
+        raise ValueError("tensor and field extents differ")
+    check(lib().lt_clover_tensor(U.handle, Clov.data.ctypes.data))
+    Clov._field = U
+    return Clov
+
+
+def TopChargeClover(U) -> float:
+    """observables/topological_charge.hpp:97-200 for a GaugeField; for a FullTensor,
+    TopChargeClover(const FullTensor&) (:202-231) of the tensor as given."""
+    if isinstance(U, FullTensor):
+        h = U._field if U._field is not None else GaugeField(U.ext)
+        q = C.c_double()
+        data = np.ascontiguousarray(U.data)
+        check(lib().lt_topcharge_clover_tensor(h.handle, data.ctypes.data, C.byref(q)))
+        return q.value
     return _out1(lib().lt_topcharge_clover, U.handle)
 
 
@@ -815,4 +849,4 @@ __all__ = ["STATUS_NONFINITE", "STATUS_UNITARITY", "STATUS_HB_CAP", "GaugeField"
            "Observables", "MDIntegrator", "Integrators", "Leapfrog_slow", "Leapfrog", "OMF_2_slow", "OMF_2",
            "OMF_4_slow", "OMF_4", "Leapfrog_friction_slow", "OMF_4_friction_slow", "Leapfrog_OMF_4",
            "OMF_2_OMF_4_slow", "OMF_2_OMF_4", "ParityUpdate", "LuescherWeiszAction", "IwasakiAction", "DBW2Action",
-           "UpdateSweeps4", "ZeuthenFlow"]
+           "UpdateSweeps4", "ZeuthenFlow", "FullTensor", "CalculateClover"]

@@ -104,6 +104,10 @@ public:
     virtual void batch_sweep(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int sel, int op, int mu,
                              int par, const uint64_t* counter, int max_iter) const = 0;
 
+    // FullTensor4D of CalculateClover<1, 1> in the reference layout (FP64, device memory,
+    // zeroed by the caller); Q sum of a tensor into results[slot] (unnormalised)
+    virtual void clover_tensor(const Ctx& c, const void* U, double* tensor) const = 0;
+    virtual void topcharge_tensor(const Ctx& c, const double* tensor, int slot) const = 0;
     virtual void clover_R(const Ctx& c, const void* U, void* R) const = 0;
     // sum over sites of ReTr(R01 R23 - R02 R13 + R03 R12) into results[slot]
     virtual void topcharge_R(const Ctx& c, const void* R, int slot) const = 0;

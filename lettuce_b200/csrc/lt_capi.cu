@@ -537,7 +537,8 @@ int lt_destroy(lt_lattice* h)
     const lt::DeviceScope device_scope(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,   h->R,      h->chainA,
-                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB, h->Xz };
+                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB, h->Xz,
+                     h->tensor };
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (void* p : h->levels) cudaFree(p);
@@ -1095,6 +1096,44 @@ int lt_flow(lt_lattice* in, lt_lattice* out, int integrator, double eps, int n_s
         return lt::set_error(LT_ERR_ARG, "lt_flow: n_step < 0 or unknown integrator");
     LT_TRY(lt_copy(out, in));
     return flow_steps(out, eps, n_step, integrator);
+}
+
+// ---------------------------------------------------------------- clover tensor
+int lt_clover_tensor(lt_lattice* h, double* tensor_out)
+{
+    LT_TRY(check_h(h, "lt_clover_tensor"));
+    const lt::DeviceScope device_scope(h->device);
+    const size_t bytes = (size_t)h->g.V * 16 * 18 * sizeof(double);
+    LT_TRY(ensure(h, (void**)&h->tensor, bytes));
+    LT_CK(cudaMemsetAsync(h->tensor, 0, bytes, h->stream));
+    h->be->clover_tensor(h->ctx(), h->U, h->tensor);
+    LT_TRY(launched("lt_clover_tensor"));
+    if (tensor_out)
+    {
+        LT_CK(cudaMemcpyAsync(tensor_out, h->tensor, bytes, cudaMemcpyDeviceToHost, h->stream));
+        LT_CK(cudaStreamSynchronize(h->stream));
+    }
+    return LT_OK;
+}
+
+int lt_topcharge_clover_tensor(lt_lattice* h, const double* tensor, double* q_out)
+{
+    LT_TRY(check_h(h, "lt_topcharge_clover_tensor"));
+    if (!q_out) return lt::set_error(LT_ERR_ARG, "lt_topcharge_clover_tensor: null output");
+    const lt::DeviceScope device_scope(h->device);
+    const size_t bytes = (size_t)h->g.V * 16 * 18 * sizeof(double);
+    if (tensor)
+    {
+        LT_TRY(ensure(h, (void**)&h->tensor, bytes));
+        LT_CK(cudaMemcpyAsync(h->tensor, tensor, bytes, cudaMemcpyHostToDevice, h->stream));
+    }
+    else if (!h->tensor)
+        return lt::set_error(LT_ERR_STATE, "lt_topcharge_clover_tensor: no tensor given and none computed");
+    h->be->topcharge_tensor(h->ctx(), h->tensor, 0);
+    double r;
+    LT_TRY(fetch(h, 0, 1, &r));
+    *q_out = -1.0 / (64.0 * 4.0 * kPi * kPi) * r;
+    return LT_OK;
 }
 
 int lt_set_flow_action(lt_lattice* h, int flow_action)

@@ -79,6 +79,7 @@ struct lt_lattice
     // (LT_FLOW_ACTION_GAUGE, the reference's GradientFlowKernel) or the Zeuthen flow's
     int flow_action = LT_FLOW_ACTION_GAUGE;
     void* Xz = nullptr;          // Luescher-Weisz force of a Zeuthen flow stage (algebra)
+    double* tensor = nullptr;    // FullTensor4D of lt_clover_tensor (FP64, reference layout)
     mutable unsigned order = 0;  // launches of the order-alternating sweep and flow kernels
 
     lt::Ctx ctx() const

@@ -335,6 +335,16 @@ public:
         else batch_launch<2>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
     }
 
+    void clover_tensor(const Ctx& c, const void* U, double* tensor) const override
+    {
+        k_clover_tensor<T, NR><<<nblocks(6LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), c.g, tensor);
+    }
+    void topcharge_tensor(const Ctx& c, const double* tensor, int slot) const override
+    {
+        k_topcharge_tensor<0><<<kRedBlocks, kRedThreads, 0, c.stream>>>(tensor, c.g.V,
+                                                                        c.partials + (size_t)slot * kRedBlocks);
+        finish(c, slot, 1);
+    }
     void clover_R(const Ctx& c, const void* U, void* R) const override
     {
         k_clover_R<T, NR><<<nblocks(6LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), clov(R, c.g), c.g);

@@ -1486,6 +1486,73 @@ __global__ void __launch_bounds__(kRedThreads) k_clover_obs(Gauge<T, NR> Ust, Ge
     }
 }
 
+// CalculateClover<1, 1> (observables/clover.hpp:94-152) into a FullTensor4D in the reference
+// layout double[V][4][4][3][3][2] (lattice.hpp:447-590, index ((site 4 + mu) 4 + nu)):
+// C_{mu nu} for mu < nu from FP64 products, C_{nu mu} = C_{mu nu}^dag; the diagonal is left to
+// the caller's zeroed buffer.  One thread per (site, plane mu < nu).
+template <typename T, int NR>
+__global__ void k_clover_tensor(Gauge<T, NR> Ust, Geom g, double* __restrict__ out)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6LL * g.V) return;
+    const int plane = (int)(t % 6), x = (int)(t / 6);
+    const int mu = plane < 3 ? 0 : plane < 5 ? 1 : 2;
+    const int nu = plane < 3 ? plane + 1 : plane < 5 ? plane - 1 : 3;
+    const Widened<T, NR> U{ Ust };
+    const int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    const M3<double> C = clover_leaves(U, g, par, i, c, mu, nu);
+    double* a = out + (size_t)18 * (16 * (size_t)i + 4 * mu + nu);
+    double* b = out + (size_t)18 * (16 * (size_t)i + 4 * nu + mu);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+        {
+            a[6 * r + 2 * q] = C.e[r][q].r;
+            a[6 * r + 2 * q + 1] = C.e[r][q].i;
+            b[6 * q + 2 * r] = C.e[r][q].r;
+            b[6 * q + 2 * r + 1] = -C.e[r][q].i;
+        }
+}
+
+// TopChargeClover(const FullTensor&) (observables/topological_charge.hpp:202-231): per site
+// F_{mu nu} = C_{mu nu} - C_{nu mu} from the tensor as given, ReTr(F01 F23 - F02 F13 + F03 F12),
+// Kahan-summed per thread, block partials to partials[blockIdx.x]
+LT_D M3<double> tensor_entry(const double* __restrict__ C, int i, int mu, int nu)
+{
+    const double* p = C + (size_t)18 * (16 * (size_t)i + 4 * mu + nu);
+    M3<double> m;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m.e[k / 3][k % 3] = mkc(p[2 * k], p[2 * k + 1]);
+    return m;
+}
+
+template <int Unused = 0>
+__global__ void __launch_bounds__(kRedThreads) k_topcharge_tensor(const double* __restrict__ C, int V,
+                                                                  double* __restrict__ partials)
+{
+    __shared__ double sh[32];
+    Kahan k;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x)
+    {
+        const int pairs[3][4] = { { 0, 1, 2, 3 }, { 0, 2, 1, 3 }, { 0, 3, 1, 2 } };
+        double q = 0.0;
+#pragma unroll 1
+        for (int p = 0; p < 3; ++p)
+        {
+            const M3<double> fa = tensor_entry(C, i, pairs[p][0], pairs[p][1]) - tensor_entry(C, i, pairs[p][1], pairs[p][0]);
+            const M3<double> fb = tensor_entry(C, i, pairs[p][2], pairs[p][3]) - tensor_entry(C, i, pairs[p][3], pairs[p][2]);
+            const double t = retr_mul(fa, fb);
+            q += p == 1 ? -t : t;
+        }
+        k.add(q);
+    }
+    const double r = block_sum(k.s - k.c, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
 // ---------------------------------------------------------------- measurement bundle
 // The observables of the reference driver's measurement step (SU3_main.cpp:89-235), all with
 // products in FP64 whatever the storage.

@@ -405,6 +405,25 @@ void ref_clover_derivative(const double* links, double* out)
     store(*D, out);
 }
 
+// CalculateClover<1, 1> (observables/clover.hpp:94-152) into the FullTensor layout
+// double[V][4][4][3][3][2] (lattice.hpp:447-590), and TopChargeClover(const FullTensor&)
+// (topological_charge.hpp:202-231) of that tensor
+double ref_clover_tensor(const double* links, double* tensor_out)
+{
+    auto U = std::make_unique<GaugeField>();
+    auto C = std::make_unique<FullTensor>();
+    load(*U, links);
+    CalculateClover<1>(*U, *C);
+    for (std::size_t k = 0; k < kV * 16; ++k)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+            {
+                tensor_out[18 * k + 6 * i + 2 * j]     = std::real((*C)(k)(i, j));
+                tensor_out[18 * k + 6 * i + 2 * j + 1] = std::imag((*C)(k)(i, j));
+            }
+    return TopChargeClover(*C);
+}
+
 // The MetaD force chain of HMCMetaDKernel::CalculateTopologicalForce (hmc_metadynamics.hpp:374-436)
 // with n_smear_meta (= 4, defines.hpp:74) stout levels of parameter rho, under a bias with
 // dV/dQ = slope.  Writes ForceFatLink (the force on the thin links) and returns the CV.

@@ -54,6 +54,11 @@ int main(int argc, char** argv)
                     EnergyDensityClover(Gluonsmeared1));
     }
 
+    // the clover field as a FullTensor (CalculateClover<1, 1>) and Q from it
+    FullTensor Clover(Gluon.Shape());
+    CalculateClover(Gluon, Clover);
+    std::printf("tensor Q %.15f %.15f\n", TopChargeClover(Clover), TopChargeClover(Gluon));
+
     // the Zeuthen flow as the flow's action (no counterpart in the reference)
     GradientFlowKernel ZeuthenFlow(Gluon, Gluonchain, rk3, GaugeAction::ZeuthenFlowAction, 0.01);
     ZeuthenFlow(10);

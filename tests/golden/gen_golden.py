@@ -348,6 +348,22 @@ def gen_tempering() -> dict:
             "uniform": np.array(q)}
 
 
+def gen_tensor() -> dict:
+    """CalculateClover<1, 1> as a FullTensor4D and TopChargeClover(const FullTensor&) of the
+    reference on a partly thermalised 4x6x8x10 field: 48 sampled sites (all 16 matrices each)
+    and full-tensor checksums."""
+    from ltref import Oracle
+    ext = (4, 6, 8, 10)
+    V = int(np.prod(ext))
+    ref = Reference(ext)
+    U = Oracle().heatbath(ext, haar_links_numpy(ext, 46), BETA, 3, 8, 0)
+    T = np.empty((V, 4, 4, 3, 3, 2))
+    q = ref.lib.ref_clover_tensor(U, T.reshape(-1))
+    sites = np.sort(np.random.default_rng(4681).choice(V, size=48, replace=False))
+    return {"ext": np.array(ext, dtype=np.int32), "seeds": np.array([46, 8, 3]), "U_ck": checksums(U),
+            "sites": sites, "tensor": T[sites], "tensor_ck": checksums(T), "Q": np.array(q)}
+
+
 def exp_inputs(seed: int) -> np.ndarray:
     """Traceless Hermitian matrices for every branch of the device exponential and of the
     reference's SU3::exp: generic (c1 > 1/2), the long (1/32 < c1 <= 1/2) and short series
@@ -396,7 +412,7 @@ def main() -> int:
     import subprocess
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", choices=["chain", "bmw", "measure", "md", "rect", "large", "flow_large", "metad16",
-                                       "exp", "tempering"], default=None,
+                                       "exp", "tempering", "tensor"], default=None,
                     help="regenerate one fixture only")
     a = ap.parse_args()
     root = os.path.dirname(os.path.dirname(HERE))
@@ -413,6 +429,9 @@ def main() -> int:
         subprocess.run([sys.executable, os.path.join(root, "oracle", "build_ref.py"), "--extents", "16x16x16x16"],
                        check=True)
         np.savez_compressed(os.path.join(HERE, "ref_metad_16x16x16x16.npz"), **gen_metad16())
+        return 0
+    if a.only == "tensor":
+        np.savez_compressed(os.path.join(HERE, "ref_tensor_4x6x8x10.npz"), **gen_tensor())
         return 0
     if a.only == "tempering":
         np.savez_compressed(os.path.join(HERE, "ref_tempering.npz"), **gen_tempering())

@@ -303,6 +303,7 @@ class Reference:
                 "ref_flow_action": (None, [_dp, _dp, d, i, i, i, d, d]),
                 "ref_wilson_loop_chain": (d, [_dp, i, i, i]),
                 "ref_tempering": (None, [_dp, _dp, d, d, _dp, i, _dp]),
+                "ref_clover_tensor": (d, [_dp, _dp]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(lib, name)

@@ -57,6 +57,8 @@ def test_dropin_runs_like_python_mirror(tmp_path):
     F = lt.GaugeField((8, 8, 8, 8))
     lt.GradientFlowKernel(G, F, lt.Euler, None, 0.02)(5)
     assert float(lines["euler"].split()[2]) == pytest.approx(lt.EnergyDensityClover(F), rel=1e-13)
+    tq = lines["tensor"].split()
+    assert float(tq[2]) == pytest.approx(float(tq[3]), rel=1e-11, abs=1e-13)
     Fz = lt.GaugeField((8, 8, 8, 8))
     lt.GradientFlowKernel(G, Fz, lt.RK3, lt.ZeuthenFlow(), 0.01)(10)
     assert float(lines["zeuthen"].split()[2]) == pytest.approx(lt.EnergyDensityClover(Fz), rel=1e-13)
