@@ -359,12 +359,22 @@ def secondary_rates(lt, torch, timed, prec):
             g.SetToHaarRandom(100 + j)
         ens = lt.Ensemble(lats, betas, SEED)
         out["ensemble_autotuned_threads"] = ens.autotune()
+        out["ensemble_autotuned_mode"] = ens.get_mode()
         ens.sweeps(3, 1, 4)
         n = 10
         ms = timed(lats[0], lambda: ens.sweeps(n, 1, 4), 1)
         upd = 5 * 4 * sum(g.Volume() for g in lats)
         out["ensemble_link_updates_per_s"] = n * upd / (ms / 1000.0)
         out["ensemble_lattices"] = len(lats)
+        # both ways of running a round: a graph of 40 batched launches, or one persistent
+        # cooperative launch with 39 grid barriers (at each residency)
+        modes = {}
+        for mode, bps in (("graph", 0), ("persistent", 0), ("persistent", 4), ("persistent", 2)):
+            ens.set_mode(mode, bps)
+            ens.sweeps(2, 1, 4)
+            ms = timed(lats[0], lambda: ens.sweeps(n, 1, 4), 1)
+            modes[f"{mode}_{ens.get_mode()[1]}"] = n * upd / (ms / 1000.0)
+        out["ensemble_link_updates_per_s_by_mode"] = modes
         del ens, lats
     except Exception as e:
         out["ensemble_error"] = repr(e)

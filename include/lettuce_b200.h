@@ -34,6 +34,7 @@ extern "C" {
 #define LT_ERR_STATE   4   /* operation not valid in the handle's current state              */
 #define LT_ERR_NUMERIC 5   /* non-finite value detected in a result                          */
 #define LT_ERR_IO      6   /* file cannot be opened, read or written, or has a malformed header */
+#define LT_ERR_TIMEOUT 7   /* a bounded device-side wait gave up (the result is not valid)     */
 
 /* Storage format of the link field. */
 #define LT_PREC_FP64    0  /* 18 doubles per link (the reference's Matrix_SU3, defines.hpp:122)   */
@@ -89,6 +90,7 @@ int lt_get_stream(const lt_lattice* h, void** stream_out);
 #define LT_STATUS_NONFINITE 1u /* a link holds NaN or Inf (set by lt_check_links) */
 #define LT_STATUS_UNITARITY 2u /* a link has an entry of |U U^dag - 1| above 1e-4 (FP32) or 1e-10 (FP64) */
 #define LT_STATUS_HB_CAP 4u    /* a heatbath subgroup update hit the 10-retry cap and took the unit matrix */
+#define LT_STATUS_BARRIER_TIMEOUT 8u /* a grid barrier of a persistent ensemble round gave up waiting */
 /* Reads the status word (synchronising the handle's stream); clear = 1 resets it to 0. */
 int lt_status_word(lt_lattice* h, uint32_t* word, int clear);
 /* Scans every link, sets LT_STATUS_NONFINITE / LT_STATUS_UNITARITY, and returns the largest
@@ -234,6 +236,23 @@ int lt_ensemble_sweeps(lt_ensemble* e, int n_sweep, int n_hb, int n_or, int reve
 int lt_ensemble_autotune(lt_ensemble* e, int* threads_hb, int* threads_or);
 /* Fix the block sizes (64, 128 or 256 threads). */
 int lt_ensemble_set_block(lt_ensemble* e, int threads_hb, int threads_or);
+/* How a round runs (lt_ensemble_autotune picks the faster, with its residency):
+ *   LT_ENSEMBLE_GRAPH       one batched launch per (mu, parity) sub-sweep, the round captured
+ *                           as a CUDA graph and replayed (the default);
+ *   LT_ENSEMBLE_PERSISTENT  one cooperative launch per round: every block resident, the
+ *                           sub-sweeps separated by grid barriers whose waits are bounded (a
+ *                           barrier that gives up makes lt_ensemble_sweeps return
+ *                           LT_ERR_TIMEOUT), blocks_per_sm blocks per SM (0: the occupancy
+ *                           limit).
+ * The reference runs each sub-sweep as an OpenMP loop with its implicit barrier
+ * (iterators.hpp:65-87); the rounds advance every lattice identically in both modes. */
+#define LT_ENSEMBLE_GRAPH      0
+#define LT_ENSEMBLE_PERSISTENT 1
+int lt_ensemble_set_mode(lt_ensemble* e, int mode, int blocks_per_sm);
+int lt_ensemble_get_mode(lt_ensemble* e, int* mode, int* blocks_per_sm);
+/* The wait bound of the persistent round's grid barriers, in polls of about 100 ns (default
+ * 10,000,000: about a second). */
+int lt_ensemble_set_barrier_polls(lt_ensemble* e, long long polls);
 /* Tempering exchange between streams a and b sampling exp(-S - scale V(Q)) with CVs q_a, q_b
  * (generalises MetadynamicsTemperingKernel::operator(), updates/tempering.hpp:51-72):
  * accepted when u <= exp(-dE), dE = (scale_a - scale_b)(V(q_b) - V(q_a)); on acceptance the

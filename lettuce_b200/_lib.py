@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("LETTUCE_B200_LIB", os.path.join(HERE, "liblettuce_b200.so"))
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "lettuce_b200.h")
 
-LT_OK, LT_ERR_ARG, LT_ERR_CUDA, LT_ERR_NOMEM, LT_ERR_STATE, LT_ERR_NUMERIC, LT_ERR_IO = range(7)
+LT_OK, LT_ERR_ARG, LT_ERR_CUDA, LT_ERR_NOMEM, LT_ERR_STATE, LT_ERR_NUMERIC, LT_ERR_IO, LT_ERR_TIMEOUT = range(8)
 PREC = {"fp64": 0, "fp32": 1, "fp32_12": 2}
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -71,6 +71,9 @@ SIGNATURES = {
     "lt_ensemble_sweeps": (_i, [_vp, _i, _i, _i, _i, _pu64]),
     "lt_ensemble_autotune": (_i, [_vp, _pi, _pi]),
     "lt_ensemble_set_block": (_i, [_vp, _i, _i]),
+    "lt_ensemble_set_mode": (_i, [_vp, _i, _i]),
+    "lt_ensemble_get_mode": (_i, [_vp, _pi, _pi]),
+    "lt_ensemble_set_barrier_polls": (_i, [_vp, C.c_longlong]),
     "lt_tempering_swap": (_i, [_vp, _vp, _vp, _d, _d, _d, _d, _d, _pi, _pd]),
     "lt_flow_rk3": (_i, [_vp, _vp, _d, _i]),
     "lt_flow": (_i, [_vp, _vp, _i, _d, _i]),

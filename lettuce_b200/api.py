@@ -664,7 +664,8 @@ def ParityUpdate(U: GaugeField) -> None:
 
 class Ensemble:
     """Lattices of any even extents (one storage format) advanced together: one launch per
-    (mu, parity) sub-sweep over all of them, rounds replayed as CUDA graphs."""
+    (mu, parity) sub-sweep over all of them, rounds replayed as CUDA graphs, or one persistent
+    launch per round (set_mode; autotune picks the faster)."""
 
     def __init__(self, lattices, betas, seed: int = 1):
         self.lattices = list(lattices)
@@ -693,6 +694,22 @@ class Ensemble:
 
     def set_block(self, threads_hb: int, threads_or: int) -> None:
         check(lib().lt_ensemble_set_block(self._h, int(threads_hb), int(threads_or)))
+
+    GRAPH, PERSISTENT = 0, 1
+
+    def set_mode(self, mode, blocks_per_sm: int = 0) -> None:
+        """"graph": one batched launch per sub-sweep, replayed as a CUDA graph; "persistent":
+        one cooperative launch per round with bounded grid barriers between sub-sweeps."""
+        m = {"graph": 0, "persistent": 1}.get(mode, mode)
+        check(lib().lt_ensemble_set_mode(self._h, int(m), int(blocks_per_sm)))
+
+    def get_mode(self) -> tuple[str, int]:
+        m, b = C.c_int(), C.c_int()
+        check(lib().lt_ensemble_get_mode(self._h, C.byref(m), C.byref(b)))
+        return ("graph", "persistent")[m.value], b.value
+
+    def set_barrier_polls(self, polls: int) -> None:
+        check(lib().lt_ensemble_set_barrier_polls(self._h, int(polls)))
 
 
 def TemperingSwap(a: GaugeField, b: GaugeField, bias: MetaBiasPotential, scale_a: float, scale_b: float,

@@ -108,6 +108,15 @@ public:
     // zeroed by the caller); Q sum of a tensor into results[slot] (unnormalised)
     virtual void clover_tensor(const Ctx& c, const void* U, double* tensor) const = 0;
     virtual void topcharge_tensor(const Ctx& c, const double* tensor, int slot) const = 0;
+    // One persistent cooperative launch of a whole round (n_hb heatbath + n_or overrelaxation
+    // sweeps) over a batch of lattices (blocks of 128 threads: n_units = the batch's block
+    // count), blocks_per_sm blocks resident per SM; bar = {count, gen, status} words for the
+    // bounded grid barrier (count zero at launch), polls = its wait bound.  Returns the launch
+    // status.  max_blocks_per_sm: the occupancy limit of that kernel.
+    virtual cudaError_t batch_round(cudaStream_t s, const void* desc, int n_lat, int n_units, int blocks_per_sm,
+                                    int n_hb, int n_or, int reverse, uint64_t* counter, int max_iter, unsigned* bar,
+                                    long long polls) const = 0;
+    virtual int batch_round_max_blocks_per_sm() const = 0;
     virtual void clover_R(const Ctx& c, const void* U, void* R) const = 0;
     // sum over sites of ReTr(R01 R23 - R02 R13 + R03 R12) into results[slot]
     virtual void topcharge_R(const Ctx& c, const void* R, int slot) const = 0;

@@ -32,6 +32,12 @@ struct lt_ensemble
     int n_blocks[3] = { 0, 0, 0 };
     int sel_hb = 1, sel_or = 1;   // 64 / 128 / 256 threads per block: index 0 / 1 / 2
     std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;
+    // LT_ENSEMBLE_GRAPH: a captured graph of one batched launch per sub-sweep;
+    // LT_ENSEMBLE_PERSISTENT: one cooperative launch per round with grid barriers
+    int mode = LT_ENSEMBLE_GRAPH;
+    int blocks_per_sm = 0;        // persistent mode: resident blocks per SM (0: the occupancy limit)
+    unsigned* d_bar = nullptr;    // persistent mode: barrier count, generation, status
+    long long polls = LT_PERSIST_POLLS;
 };
 
 namespace {
@@ -160,6 +166,42 @@ void drop_graphs(lt_ensemble* e)
     e->graphs.clear();
 }
 
+int persistent_blocks(const lt_ensemble* e)
+{
+    const int mx = e->be->batch_round_max_blocks_per_sm();
+    if (mx < 1) return 0;
+    return e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, mx) : mx;
+}
+
+// n_sweep rounds as persistent launches on stream s with the given counter; the barrier words
+// start at zero and are left at zero by a completed launch.  A barrier that gave up leaves
+// kStatusBarrierTimeout in d_bar[2]: reported as LT_ERR_TIMEOUT after the stream drains, with
+// the words reset for the next call.
+int persistent_rounds(lt_ensemble* e, cudaStream_t s, int n_sweep, int n_hb, int n_or, int reverse,
+                      uint64_t* counter)
+{
+    const int bps = persistent_blocks(e);
+    if (bps < 1) return lt::set_error(LT_ERR_CUDA, "lt_ensemble: the persistent kernel cannot be resident");
+    const int n_units = e->n_blocks[1];
+    for (int k = 0; k < n_sweep; ++k)
+    {
+        cudaError_t ce = e->be->batch_round(s, e->d_desc, (int)e->lats.size(), n_units, bps, n_hb, n_or, reverse,
+                                            counter, 10, e->d_bar, e->polls);
+        if (ce != cudaSuccess) return lt::cuda_error(ce, "lt_ensemble: persistent launch");
+    }
+    unsigned words[3];
+    LT_CK(cudaMemcpyAsync(words, e->d_bar, sizeof(words), cudaMemcpyDeviceToHost, s));
+    LT_CK(cudaStreamSynchronize(s));
+    if (words[2] & lt::kStatusBarrierTimeout)
+    {
+        LT_CK(cudaMemsetAsync(e->d_bar, 0, 3 * sizeof(unsigned), s));
+        LT_CK(cudaStreamSynchronize(s));
+        return lt::set_error(LT_ERR_TIMEOUT, "lt_ensemble_sweeps: a grid barrier of the persistent round gave up "
+                                             "waiting; the lattices are inconsistent");
+    }
+    return LT_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -194,6 +236,8 @@ int lt_ensemble_create(lt_lattice* const* lattices, const double* betas, int n, 
     cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_desc, sizeof(lt::LatDesc) * n);
     if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_counter, sizeof(uint64_t));
+    if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_bar, 3 * sizeof(unsigned));
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(e->d_bar, 0, 3 * sizeof(unsigned), e->stream);
     if (ce != cudaSuccess)
     {
         int r = lt::cuda_error(ce, "lt_ensemble_create");
@@ -218,6 +262,7 @@ int lt_ensemble_destroy(lt_ensemble* e)
     drop_graphs(e);
     if (e->d_desc) cudaFree(e->d_desc);
     if (e->d_counter) cudaFree(e->d_counter);
+    if (e->d_bar) cudaFree(e->d_bar);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
     return LT_OK;
@@ -231,10 +276,22 @@ int lt_ensemble_sweeps(lt_ensemble* e, int n_sweep, int n_hb, int n_or, int reve
     const lt::DeviceScope device_scope(e->device);
     LT_TRY(join_in(e));
     LT_TRY(refresh(e));
-    cudaGraphExec_t g;
-    LT_TRY(graph_for(e, n_hb, n_or, reverse ? 1 : 0, &g));
     LT_CK(cudaMemcpyAsync(e->d_counter, counter, sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
-    for (int k = 0; k < n_sweep; ++k) LT_CK(cudaGraphLaunch(g, e->stream));
+    if (e->mode == LT_ENSEMBLE_PERSISTENT)
+    {
+        const int r = persistent_rounds(e, e->stream, n_sweep, n_hb, n_or, reverse ? 1 : 0, e->d_counter);
+        if (r != LT_OK)
+        {
+            join_out(e);
+            return r;
+        }
+    }
+    else
+    {
+        cudaGraphExec_t g;
+        LT_TRY(graph_for(e, n_hb, n_or, reverse ? 1 : 0, &g));
+        for (int k = 0; k < n_sweep; ++k) LT_CK(cudaGraphLaunch(g, e->stream));
+    }
     LT_TRY(launched("lt_ensemble_sweeps"));
     LT_TRY(join_out(e));
     LT_CK(cudaStreamSynchronize(e->stream));
@@ -296,6 +353,55 @@ int lt_ensemble_autotune(lt_ensemble* e, int* threads_hb, int* threads_or)
                 pick[op] = sel;
             }
         }
+    // the round as a whole: the graph of batched launches (blocks just chosen) against the
+    // persistent cooperative round at each residency from the occupancy limit down to 1 block
+    // per SM; one untimed and two timed rounds of 1 heatbath + 1 overrelaxation sweep each
+    float best_round = 1e30f;
+    int pick_mode = LT_ENSEMBLE_GRAPH, pick_bps = 0;
+    if (rc == LT_OK)
+    {
+        auto time_round = [&](auto&& launch_round, float* ms_out) -> int {
+            launch_round();
+            cudaEventRecord(t0, e->stream);
+            launch_round();
+            launch_round();
+            cudaEventRecord(t1, e->stream);
+            cudaError_t ce = cudaEventSynchronize(t1);
+            if (ce != cudaSuccess) return lt::cuda_error(ce, "lt_ensemble_autotune: round timing");
+            ce = cudaGetLastError();
+            if (ce != cudaSuccess) return lt::cuda_error(ce, "lt_ensemble_autotune: round launch");
+            cudaEventElapsedTime(ms_out, t0, t1);
+            return LT_OK;
+        };
+        float ms = 0.f;
+        rc = time_round([&] { enqueue_round(e, e->stream, 1, 1, 0, pick[0], pick[1], d_scratch_counter); }, &ms);
+        if (rc == LT_OK) best_round = ms;
+        const int mx = e->be->batch_round_max_blocks_per_sm();
+        for (int bps = mx; bps >= 1 && bps >= mx - 3 && rc == LT_OK; --bps)
+        {
+            cudaError_t le = cudaSuccess;
+            rc = time_round([&] {
+                if (le == cudaSuccess)
+                    le = e->be->batch_round(e->stream, e->d_desc, (int)e->lats.size(), e->n_blocks[1], bps, 1, 1, 0,
+                                            d_scratch_counter, 10, e->d_bar, e->polls);
+            }, &ms);
+            if (rc == LT_OK && le != cudaSuccess) rc = lt::cuda_error(le, "lt_ensemble_autotune: persistent launch");
+            unsigned words[3] = { 0, 0, 0 };
+            if (rc == LT_OK && cudaMemcpy(words, e->d_bar, sizeof(words), cudaMemcpyDeviceToHost) != cudaSuccess)
+                rc = lt::set_error(LT_ERR_CUDA, "lt_ensemble_autotune: barrier words");
+            if (rc == LT_OK && (words[2] & lt::kStatusBarrierTimeout))
+            {
+                cudaMemset(e->d_bar, 0, sizeof(words));
+                rc = lt::set_error(LT_ERR_TIMEOUT, "lt_ensemble_autotune: a grid barrier gave up waiting");
+            }
+            if (rc == LT_OK && ms < best_round)
+            {
+                best_round = ms;
+                pick_mode = LT_ENSEMBLE_PERSISTENT;
+                pick_bps = bps;
+            }
+        }
+    }
     // restore the links whatever happened above
     for (size_t k = 0; k < e->lats.size(); ++k)
         if (saved[k])
@@ -313,9 +419,37 @@ int lt_ensemble_autotune(lt_ensemble* e, int* threads_hb, int* threads_or)
     if (pick[0] != e->sel_hb || pick[1] != e->sel_or) drop_graphs(e);
     e->sel_hb = pick[0];
     e->sel_or = pick[1];
+    e->mode = pick_mode;
+    e->blocks_per_sm = pick_bps;
     if (threads_hb) *threads_hb = lt::kBatchBlocks[pick[0]];
     if (threads_or) *threads_or = lt::kBatchBlocks[pick[1]];
     LT_TRY(join_out(e));
+    return LT_OK;
+}
+
+int lt_ensemble_set_mode(lt_ensemble* e, int mode, int blocks_per_sm)
+{
+    if (!e) return lt::set_error(LT_ERR_ARG, "lt_ensemble_set_mode: null ensemble");
+    if ((mode != LT_ENSEMBLE_GRAPH && mode != LT_ENSEMBLE_PERSISTENT) || blocks_per_sm < 0)
+        return lt::set_error(LT_ERR_ARG, "lt_ensemble_set_mode: unknown mode or negative block count");
+    e->mode = mode;
+    e->blocks_per_sm = blocks_per_sm;
+    return LT_OK;
+}
+
+int lt_ensemble_get_mode(lt_ensemble* e, int* mode, int* blocks_per_sm)
+{
+    if (!e || !mode || !blocks_per_sm) return lt::set_error(LT_ERR_ARG, "lt_ensemble_get_mode: null pointer");
+    const lt::DeviceScope device_scope(e->device);
+    *mode = e->mode;
+    *blocks_per_sm = e->mode == LT_ENSEMBLE_PERSISTENT ? persistent_blocks(e) : 0;
+    return LT_OK;
+}
+
+int lt_ensemble_set_barrier_polls(lt_ensemble* e, long long polls)
+{
+    if (!e || polls < 0) return lt::set_error(LT_ERR_ARG, "lt_ensemble_set_barrier_polls: bad arguments");
+    e->polls = polls;
     return LT_OK;
 }
 

@@ -28,6 +28,7 @@ constexpr int kRedThreads = 256;
 constexpr unsigned kStatusNonFinite = 1u;   // a link holds NaN or Inf
 constexpr unsigned kStatusUnitarity = 2u;   // max |U U^dag - 1| above the storage's tolerance
 constexpr unsigned kStatusHbCap = 4u;       // a heatbath subgroup update hit its iteration cap
+constexpr unsigned kStatusBarrierTimeout = 8u;   // a grid barrier of a persistent kernel gave up waiting
 
 struct Geom
 {

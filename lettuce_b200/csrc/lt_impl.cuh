@@ -335,6 +335,29 @@ public:
         else batch_launch<2>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
     }
 
+    cudaError_t batch_round(cudaStream_t s, const void* desc, int n_lat, int n_units, int blocks_per_sm, int n_hb,
+                            int n_or, int reverse, uint64_t* counter, int max_iter, unsigned* bar,
+                            long long polls) const override
+    {
+        if constexpr (kStaged) prefer_shared<k_batch_round<T, NR>>();
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const LatDesc* d = static_cast<const LatDesc*>(desc);
+        GridBarrier b{ bar, bar + 1, bar + 2, polls };
+        void* args[] = { (void*)&d, (void*)&n_lat, (void*)&n_units, (void*)&n_hb, (void*)&n_or, (void*)&reverse,
+                         (void*)&counter, (void*)&max_iter, (void*)&b };
+        return cudaLaunchCooperativeKernel((const void*)k_batch_round<T, NR>, dim3(blocks_per_sm * sms), dim3(128),
+                                           args, 0, s);
+    }
+    int batch_round_max_blocks_per_sm() const override
+    {
+        if constexpr (kStaged) prefer_shared<k_batch_round<T, NR>>();
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_round<T, NR>, 128, 0);
+        return n;
+    }
+
     void clover_tensor(const Ctx& c, const void* U, double* tensor) const override
     {
         k_clover_tensor<T, NR><<<nblocks(6LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), c.g, tensor);

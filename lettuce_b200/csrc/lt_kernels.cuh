@@ -1205,6 +1205,132 @@ __global__ void __launch_bounds__(kBatchBlocks[SEL], (BatchMinBlocks<T, NR, kBat
         or_update(U, g, mu, par, s);
 }
 
+// ---------------------------------------------------------------- persistent batched round
+// One launch for a whole round (n_hb heatbath + n_or overrelaxation sweeps, 8 (mu, parity)
+// sub-sweeps each) over all lattices of an ensemble: the grid is cooperative (every block
+// resident at once), each block walks the batch's work units (the blocks of k_batch_sweep)
+// of a sub-sweep with a grid stride, and a grid barrier separates consecutive sub-sweeps.
+//
+// The barrier waits a bounded time: a block that waits more than `limit` polls, or that sees
+// another block's timeout flag, sets kStatusBarrierTimeout in *status and the whole kernel
+// returns early (the links are then inconsistent and the host reports an error).  Nothing
+// here can hang: every wait either sees the last arrival or gives up.
+struct GridBarrier
+{
+    unsigned* count;     // arrivals at the current barrier (zeroed by the host before the launch)
+    unsigned* gen;       // generation, bumped by the last arrival
+    unsigned* status;    // kStatusBarrierTimeout on give-up
+    long long limit;     // polls before giving up (each poll sleeps about 100 ns)
+};
+
+LT_D bool grid_barrier(const GridBarrier& b)
+{
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int ok = 1;
+        volatile unsigned* vgen = b.gen;
+        volatile unsigned* vstatus = b.status;
+        const unsigned g = *vgen;
+        __threadfence();   // this block's link updates before its arrival
+        const unsigned arrived = atomicAdd(b.count, 1u);
+        if (arrived == gridDim.x - 1)
+        {
+            atomicExch(b.count, 0u);
+            __threadfence();
+            atomicAdd(b.gen, 1u);
+        }
+        else
+        {
+            long long polls = 0;
+            while (*vgen == g)
+            {
+                if (++polls > b.limit || (*vstatus & kStatusBarrierTimeout))
+                {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        if (!ok) atomicOr(b.status, kStatusBarrierTimeout);
+        __threadfence();   // the other blocks' updates before this block reads them
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// One work unit u of a batched sub-sweep (the body of k_batch_sweep for block u)
+template <typename T, int NR, int BLOCK, int RB>
+LT_D void batch_unit(StapleRingT<RB>& ring, const LatDesc* __restrict__ d, int n, int u, int op, int mu, int par,
+                     uint64_t counter, int max_iter)
+{
+    const int k = find_lattice<BLOCK == 64 ? 0 : BLOCK == 128 ? 1 : 2>(d, n, u);
+    const int sel = BLOCK == 64 ? 0 : BLOCK == 128 ? 1 : 2;
+    const Geom g = d[k].g;
+    const int s = (u - d[k].blk_begin[sel]) * BLOCK + threadIdx.x;
+    if (s >= g.vh) return;
+    Gauge<T, NR> U;
+    U.p = (cx<T>*)d[k].U;
+    U.vh = g.vh;
+    if constexpr (LT_STAGED_STAPLE && std::is_same<T, float>::value && NR == 2 && BLOCK <= 128 && RB == BLOCK)
+    {
+        int c[4];
+        const int i = site_coords(g, par, s, c);
+        M3<float> uu;
+        if (op == 0)
+        {
+            const M3<float> st = staple_staged<true>(ring, U, g, par, i, s, c, mu, uu);
+            hb_core_u(U, mu, par, s, i, uu, st, (T)d[k].prefactor, counter, d[k].k0, d[k].k1, max_iter, d[k].status);
+        }
+        else
+        {
+            const M3<float> st = staple_staged<false>(ring, U, g, par, i, s, c, mu, uu);
+            or_apply<float, 2>(uu, st);
+            U.st(mu, par, s, uu);
+        }
+    }
+    else if (op == 0)
+        hb_update(U, g, mu, par, s, (T)d[k].prefactor, counter, d[k].k0, d[k].k1, max_iter, d[k].status);
+    else
+        or_update(U, g, mu, par, s);
+}
+
+#ifndef LT_PERSIST_POLLS
+#define LT_PERSIST_POLLS 10000000   // about one second of polling at ~100 ns per poll
+#endif
+
+// Blocks of 128 threads (the staged kernels' tuned size); register cap as k_batch_sweep's
+template <typename T, int NR>
+__global__ void __launch_bounds__(128, (BatchMinBlocks<T, NR, 128>::value))
+    k_batch_round(const LatDesc* __restrict__ d, int n, int n_units, int n_hb, int n_or, int reverse,
+                  uint64_t* __restrict__ counter, int max_iter, GridBarrier bar)
+{
+    // the staged staple's ring for two-row FP32 links; a token one otherwise
+    constexpr bool kStagedRound = LT_STAGED_STAPLE && std::is_same<T, float>::value && NR == 2;
+    __shared__ StapleRingT<kStagedRound ? 128 : 1> ring;
+    const uint64_t c0 = *counter;
+    const int n_sub = 8 * (n_hb + n_or);
+    for (int q = 0; q < n_sub; ++q)
+    {
+        // the reference's order (iterators.hpp:65-87): n_hb heatbath sweeps then n_or
+        // overrelaxation sweeps, (mu, parity) lexicographic within each; reversed in full.
+        // Heatbath sweeps take consecutive counter values in the order they run.
+        const int qq = reverse ? n_sub - 1 - q : q;
+        const int sweep = qq >> 3, idx = qq & 7;
+        const int op = sweep < n_hb ? 0 : 1;
+        const int hb_rank = reverse ? n_hb - 1 - sweep : sweep;
+        const uint64_t cnt = c0 + (uint64_t)(op == 0 ? hb_rank : 0);
+        const int mu = idx >> 1, par = idx & 1;
+        for (int u = blockIdx.x; u < n_units; u += gridDim.x)
+            batch_unit<T, NR, 128>(ring, d, n, u, op, mu, par, cnt, max_iter);
+        if (q + 1 < n_sub && !grid_barrier(bar)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *counter = c0 + (uint64_t)n_hb;
+}
+
 // Advances the device-side sweep counter (read by the heatbath inside captured graphs)
 template <int Unused = 0> __global__ void k_counter_add(uint64_t* c, uint64_t n)
 {

@@ -108,3 +108,74 @@ def test_tempering_swap_rule():
     assert acc
     assert np.array_equal(b.download(), Ua)
     assert lt.PlaquetteSum(a) == pytest.approx(18 * 256, rel=1e-14)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32_12"])
+@pytest.mark.parametrize("reverse", [False, True])
+def test_persistent_round_matches_graph(prec, reverse):
+    """One cooperative launch per round (grid barriers between the sub-sweeps) advances every
+    lattice exactly as the graph of batched launches: same sub-sweeps in the same order, same
+    heatbath counters (two heatbath sweeps per round check their order)."""
+    starts = [lt.haar_links(e, 30 + k) for k, e in enumerate(EXTS)]
+    out = {}
+    for mode in ("graph", "persistent"):
+        lats = []
+        for e, U in zip(EXTS, starts):
+            G = lt.GaugeField(e, prec)
+            G.upload(U)
+            lats.append(G)
+        ens = lt.Ensemble(lats, BETAS, seed=99)
+        ens.set_mode(mode)
+        assert ens.get_mode()[0] == mode
+        ens.counter.value = 3
+        ens.sweeps(2, 2, 3, reverse=reverse)
+        assert ens.counter.value == 7
+        out[mode] = [G.download() for G in lats]
+    for a, b in zip(out["graph"], out["persistent"]):
+        assert rel_err(b, a) < (1e-12 if prec == "fp64" else 1e-5)
+
+
+def test_persistent_barrier_gives_up_and_recovers():
+    """A wait bound of zero polls makes the grid barriers give up at once: the call returns
+    LT_ERR_TIMEOUT instead of waiting, and with the default bound the same ensemble runs a
+    correct round afterwards."""
+    from lettuce_b200._lib import LT_ERR_TIMEOUT
+    starts = [lt.haar_links(e, 50 + k) for k, e in enumerate(EXTS)]
+    lats = [lt.GaugeField(e, "fp32_12") for e in EXTS]
+    for G, U in zip(lats, starts):
+        G.upload(U)
+    ens = lt.Ensemble(lats, BETAS, seed=5)
+    ens.set_mode("persistent")
+    ens.set_barrier_polls(0)
+    with pytest.raises(lt.LettuceError) as err:
+        ens.sweeps(1, 1, 1)
+    assert err.value.code == LT_ERR_TIMEOUT
+    assert b"gave up" in lt.lib().lt_last_error()
+    ens.set_barrier_polls(10_000_000)
+    for G, U in zip(lats, starts):
+        G.upload(U)
+    ens.counter.value = 0
+    ens.sweeps(1, 1, 1)
+    got = [G.download() for G in lats]
+    ref = []
+    for k, (e, U) in enumerate(zip(EXTS, starts)):
+        H = lt.GaugeField(e, "fp32_12")
+        H.upload(U)
+        lt.UpdateSweeps(H, BETAS[k], 1, 1, 1, seed=5 + k, counter=0)
+        ref.append(H.download())
+    for a, b in zip(got, ref):
+        assert rel_err(a, b) < 1e-5
+
+
+def test_autotune_chooses_a_mode():
+    lats = [lt.GaugeField(e, "fp32_12") for e in EXTS]
+    for k, G in enumerate(lats):
+        G.SetToHaarRandom(k)
+    before = [G.download() for G in lats]
+    ens = lt.Ensemble(lats, BETAS, seed=1)
+    ens.autotune()
+    mode, bps = ens.get_mode()
+    assert mode in ("graph", "persistent")
+    assert (bps >= 1) if mode == "persistent" else (bps == 0)
+    for G, b in zip(lats, before):
+        assert np.array_equal(G.download(), b)
