@@ -40,6 +40,13 @@ FLOW_EPS = 0.01
 N_THERM = 100
 
 
+def _jsonable(o):
+    """numpy scalars and arrays in the JSON line"""
+    if hasattr(o, "tolist"):
+        return o.tolist()
+    raise TypeError(f"{type(o).__name__} is not JSON serializable")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -284,7 +291,7 @@ def run_reference(a):
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "flow_steps_per_s": n_flow / df}
-    print(json.dumps(line))
+    print(json.dumps(line, default=_jsonable))
     return 0
 
 
@@ -499,7 +506,7 @@ def run_secondary(a, lt, torch, ext, links, timed, barrier, max_over_ranks, worl
             "config": {"workload": f"{a.workload} at {ext[0]}^4, {a.prec} links", "lattice": list(ext),
                        "storage": a.prec}, "gpu_launches": a.steps * launches_per_step}
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(line, default=_jsonable))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -653,7 +660,7 @@ def main():
         # above are the FP32 errors against the oracle to that accuracy
         line["dQ_vs_oracle_abs"] = max(dQ)
         line["dP_vs_oracle_abs"] = max(dP)
-        line["error_bound_1e-6"] = {"dP": max(dP) <= 1e-6, "dQ": max(dQ) <= 1e-6}
+        line["error_bound_1e-6"] = {"dP": bool(max(dP) <= 1e-6), "dQ": bool(max(dQ) <= 1e-6)}
         line["dP_flow_max_rel"] = max(d / abs(p) for d, p in zip(dP, res["fp64"]["plaq"]))
         line["dQ_flow_max_rel"] = max(d / max(abs(q), 1.0) for d, q in zip(dQ, res["fp64"]["Q"]))
         line["flow_roofline"] = flow_roofline(torch, a.prec, V, res[a.prec]["flow_ms"], res["fp64"]["flow_ms"], peak)
@@ -717,7 +724,7 @@ def main():
                     "fp64_flow_steps": line["fp64"]["flow_steps_per_s"] / cb["flow_steps_per_s"]}
 
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(line, default=_jsonable))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
