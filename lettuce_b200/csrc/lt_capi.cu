@@ -1340,8 +1340,16 @@ int lt_metad_force(lt_lattice* h, double rho, int n_stout, double dvdq, double* 
     if (n_stout < 0) return lt::set_error(LT_ERR_ARG, "lt_metad_force: n_stout < 0");
     LT_TRY(metad_forward(h, rho, n_stout));
     LT_TRY(metad_clover(h, n_stout));
-    if (q_out) LT_TRY(charge_from_R(h, q_out));
+    // the charge is summed before the backward chain but read after it, so the host does not
+    // wait between the two halves of the force
+    if (q_out) h->be->topcharge_R(h->ctx(), h->R, 7);
     LT_TRY(metad_backward(h, rho, n_stout, dvdq, true));
+    if (q_out)
+    {
+        double r;
+        LT_TRY(fetch(h, 7, 1, &r));
+        *q_out = -1.0 / (64.0 * 4.0 * kPi * kPi) * r;
+    }
     if (force_out)
     {
         LT_TRY(ensure_aos(h));

@@ -370,7 +370,8 @@ public:
     }
     void clover_R(const Ctx& c, const void* U, void* R) const override
     {
-        k_clover_R<T, NR><<<nblocks(6LL * c.g.V, kThreads), kThreads, 0, c.stream>>>(gauge(U, c.g), clov(R, c.g), c.g);
+        launch_chained(k_clover_R<T, NR>, nblocks(6LL * c.g.V, kThreads), kThreads, c.stream, gauge(U, c.g),
+                       clov(R, c.g), c.g);
     }
     void topcharge_R(const Ctx& c, const void* R, int slot) const override
     {
@@ -379,20 +380,28 @@ public:
     }
     void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const override
     {
-        k_clover_deriv<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
-            gauge(U, c.g), clov(R, c.g), alg(out, c.g), c.g, (T)scale);
+        launch_chained(k_clover_deriv<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
+                       gauge(U, c.g), clov(R, c.g), alg(out, c.g), c.g, (T)scale);
     }
     void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam, void* Tloc,
                       double rho) const override
     {
-        k_stout_lambda<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
-            gauge(U, c.g), gauge(Up, c.g), alg(Sigma, c.g), alg(Lam, c.g), full(Tloc, c.g), c.g, (T)rho);
+        if constexpr (kStaged)
+        {
+            prefer_shared<k_stout_lambda_staged<0>>();
+            launch_chained(k_stout_lambda_staged<0>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
+                           gauge(U, c.g), gauge(Up, c.g), alg(Sigma, c.g), alg(Lam, c.g), full(Tloc, c.g), c.g,
+                           (T)rho);
+            return;
+        }
+        launch_chained(k_stout_lambda<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
+                       gauge(U, c.g), gauge(Up, c.g), alg(Sigma, c.g), alg(Lam, c.g), full(Tloc, c.g), c.g, (T)rho);
     }
     void stout_recursion(const Ctx& c, const void* U, const void* Lam, const void* Tloc, void* Sigma,
                          double rho) const override
     {
-        k_stout_recursion<T, NR><<<nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, 0, c.stream>>>(
-            gauge(U, c.g), alg(Lam, c.g), full(Tloc, c.g), alg(Sigma, c.g), c.g, (T)rho);
+        launch_chained(k_stout_recursion<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
+                       gauge(U, c.g), alg(Lam, c.g), full(Tloc, c.g), alg(Sigma, c.g), c.g, (T)rho);
     }
 };
 

@@ -919,10 +919,19 @@ __global__ void __launch_bounds__(kThreads, (RECT ? RectMinBlocks<T, NR>::value 
 // Random numbers: Philox4x32-10, counter {link, counter lo, counter hi, tag|subgroup|call}.
 template <typename T> struct HB;
 
+// Random numbers carried between the three subgroup draws of one FP32 update: the direction
+// numbers of subgroup 1 (drawn with those of subgroup 0) and the low 8 bits of the four words
+// of subgroup 0's and subgroup 1's last proposals (the FP32 uniforms use the high 24 bits only)
+struct HbCarry
+{
+    float spare[2];
+    uint32_t low[2];
+};
+
 template <> struct HB<double>
 {
     LT_D static S2<double> su2(const S2<double>& A, double prefactor, uint32_t link, uint64_t counter,
-                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, float (&)[2])
+                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, HbCarry&)
     {
         double an = 1.0 / sqrt(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
@@ -966,13 +975,21 @@ template <> struct HB<double>
 // FP32: the special functions use the SFU approximations (__logf, __cosf, __sincosf, absolute
 // error about 1e-6 on these arguments), below the FP32 rounding of the rest of the update;
 // FP32 chains are validated statistically against the reference's chains.
-// The FP32 sampler draws the direction numbers of subgroups 0 and 1 from one Philox call (words
-// x, y for subgroup 0; z, w, kept in `spare`, for subgroup 1) and those of subgroup 2 from its
-// own
+// Philox calls per update: one per proposal and one more for all three directions.  The
+// direction numbers of subgroups 0 and 1 come from one call (words x, y for subgroup 0; z, w,
+// kept in carry.spare, for subgroup 1); those of subgroup 2 from the unused low bytes of the
+// last proposals of subgroups 0 and 1 (each proposal word feeds a 24-bit uniform from its high
+// bits; the low 8 bits of four words make one further 32-bit word, uniform and independent of
+// the accept/reject test, which saw only the high bits).
+LT_D uint32_t low_bytes(const U4& a)
+{
+    return (a.x & 0xffu) | ((a.y & 0xffu) << 8) | ((a.z & 0xffu) << 16) | ((a.w & 0xffu) << 24);
+}
+
 template <> struct HB<float>
 {
     LT_D static S2<float> su2(const S2<float>& A, float prefactor, uint32_t link, uint64_t counter,
-                               uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, float (&spare)[2])
+                               uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, HbCarry& carry)
     {
         float an = 1.0f / sqrtf(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
@@ -985,14 +1002,15 @@ template <> struct HB<float>
             float r3 = 1.0f - f01_from(a.z), r0 = f01_from(a.w);
             float x2 = __cosf(kTwoPiF * r2);
             lsq = -0.25f * prefactor * an * (__logf(r1) + x2 * x2 * __logf(r3));
+            if (sg < 2) carry.low[sg] = low_bytes(a);
             if (k > max_iter)
             {
                 capped = true;
                 if (sg == 0)   // subgroup 1 still takes its direction numbers from this draw
                 {
                     const U4 d = philox4x32(link, c1, c2, tw | 0xFFFFu, k0, k1);
-                    spare[0] = f01_from(d.z);
-                    spare[1] = 1.0f - 2.0f * f01_from(d.w);
+                    carry.spare[0] = f01_from(d.z);
+                    carry.spare[1] = 1.0f - 2.0f * f01_from(d.w);
                 }
                 S2<float> one;
                 one.e11 = mkc(1.0f, 0.0f);
@@ -1006,16 +1024,21 @@ template <> struct HB<float>
         float phi, ct;
         if (sg == 1)
         {
-            phi = spare[0];
-            ct = spare[1];
+            phi = carry.spare[0];
+            ct = carry.spare[1];
+        }
+        else if (sg == 2)
+        {
+            phi = f01_from(carry.low[0]);
+            ct = 1.0f - 2.0f * f01_from(carry.low[1]);
         }
         else
         {
             const U4 d = philox4x32(link, c1, c2, tw | 0xFFFFu, k0, k1);
             phi = f01_from(d.x);
             ct = 1.0f - 2.0f * f01_from(d.y);
-            spare[0] = f01_from(d.z);
-            spare[1] = 1.0f - 2.0f * f01_from(d.w);
+            carry.spare[0] = f01_from(d.z);
+            carry.spare[1] = 1.0f - 2.0f * f01_from(d.w);
         }
         float vn = ax * sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
         float sp, cp;
@@ -1112,12 +1135,12 @@ LT_D void hb_core_u(const Gauge<T, NR>& U, int mu, int par, int s, int i, M3<T> 
     M3<T> w = mul_nd(u, st);
     const uint32_t link = (uint32_t)(4 * i + mu);
     bool capped = false;
-    float spare[2] = { 0.0f, 0.0f };
+    HbCarry carry = { { 0.0f, 0.0f }, { 0u, 0u } };
     // unrolled so that the subgroup rows are compile-time indices (keeps u and w in registers)
 #pragma unroll
     for (int sg = 0; sg < 3; ++sg)
     {
-        S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter, capped, spare);
+        S2<T> h = HB<T>::su2(extract(w, sg), prefactor, link, counter, (uint32_t)sg, k0, k1, max_iter, capped, carry);
         embed_lmul(h, sg, u);
         if (sg < 2) embed_lmul(h, sg, w);
     }
@@ -2067,6 +2090,8 @@ __global__ void __launch_bounds__(kRedThreads) k_kinetic(Alg<T> P, int nlink, do
 template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads) k_clover_R(Gauge<T, NR> U, Clov<T> R, Geom g)
 {
+    pdl_release();
+    pdl_wait();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 6 * g.V) return;
     int pl = t / g.V, x = t - pl * g.V;
@@ -2134,6 +2159,8 @@ LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const
 template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads) k_clover_deriv(Gauge<T, NR> U, Clov<T> R, Alg<T> out, Geom g, T scale)
 {
+    pdl_release();
+    pdl_wait();
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
@@ -2175,18 +2202,13 @@ template <typename T> struct LambdaMinBlocks
 {
     static constexpr int value = sizeof(T) == 4 ? LT_MINB_LAMBDA_F32 : 1;
 };
+// First half of StoutForceRecursion for the link (mu, x) given its level-(k-1) link u and
+// staple st: Lambda (written) and the link-local term Tloc (written)
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_lambda(Gauge<T, NR> U, Gauge<T, NR> Up, Alg<T> Sigma, Alg<T> Lam,
-                                                           Full<T> Tloc, Geom g, T rho)
+LT_D void stout_lambda_core(const Gauge<T, NR>& Up, const Alg<T>& Sigma, const Alg<T>& Lam, const Full<T>& Tloc,
+                            T rho, int mu, int par, int s, const M3<T>& u, const M3<T>& st)
 {
-    int mu, x;
-    if (!link_of_thread(g, mu, x)) return;
-    int par = x >= g.vh, s = x - par * g.vh;
-    int c[4];
-    int i = site_coords(g, par, s, c);
-    M3<T> u = U.ld(mu, par, s);
     M3<T> sp = mul_dn(Up.ld(mu, par, s), unpack_ah(Sigma.ld(mu, par, s)));
-    M3<T> st = staple(U, g, par, i, c, mu);
     M3<T> C = unpack_ah(algebra8(mul_nd(st, u)));
     M3<T> Q;
 #pragma unroll
@@ -2254,12 +2276,47 @@ __global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_l
     Tloc.st(mu, par, s, loc);
 }
 
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_lambda(Gauge<T, NR> U, Gauge<T, NR> Up, Alg<T> Sigma, Alg<T> Lam,
+                                                           Full<T> Tloc, Geom g, T rho)
+{
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
+    stout_lambda_core(Up, Sigma, Lam, Tloc, rho, mu, par, s, U.ld(mu, par, s), staple(U, g, par, i, c, mu));
+}
+
+// k_stout_lambda on two-row FP32 storage with the staged staple
+template <int Unused = 0>
+__global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_LAMBDA_F32)
+    k_stout_lambda_staged(Gauge<float, 2> U, Gauge<float, 2> Up, Alg<float> Sigma, Alg<float> Lam, Full<float> Tloc,
+                          Geom g, float rho)
+{
+    __shared__ StapleRing ring;
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
+    const int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    const int i = site_coords(g, par, s, c);
+    M3<float> u;
+    const M3<float> st = staple_staged<true>(ring, U, g, par, i, s, c, mu, u);
+    stout_lambda_core(Up, Sigma, Lam, Tloc, rho, mu, par, s, u, st);
+}
+
 // Second half of StoutForceRecursion (smearing/stout_smearing.hpp:177-230):
 // Sigma_{k-1} = Algebra(U (Tloc - i rho sum_{nu != mu} [six-term neighbour sum of U and Lambda]))
 template <typename T, int NR>
 __global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Alg<T> Lam, Full<T> Tloc, Alg<T> Sigma,
                                                               Geom g, T rho)
 {
+    pdl_release();
+    pdl_wait();
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
     int par = x >= g.vh, s = x - par * g.vh;
