@@ -111,8 +111,9 @@ public:
     // One persistent cooperative launch of a whole round (n_hb heatbath + n_or overrelaxation
     // sweeps) over a batch of lattices (blocks of 128 threads: n_units = the batch's block
     // count), blocks_per_sm blocks resident per SM; bar = {count, gen, status} words for the
-    // bounded grid barrier (count zero at launch), polls = its wait bound.  Returns the launch
-    // status.  max_blocks_per_sm: the occupancy limit of that kernel.
+    // bounded grid barrier (count zero at launch) followed by one work-unit counter per
+    // sub-sweep from bar[4] on (8 (n_hb + n_or) words, zeroed here), polls = its wait bound.
+    // Returns the launch status.  max_blocks_per_sm: the occupancy limit of that kernel.
     virtual cudaError_t batch_round(cudaStream_t s, const void* desc, int n_lat, int n_units, int blocks_per_sm,
                                     int n_hb, int n_or, int reverse, uint64_t* counter, int max_iter, unsigned* bar,
                                     long long polls) const = 0;

@@ -36,7 +36,7 @@ struct lt_ensemble
     // LT_ENSEMBLE_PERSISTENT: one cooperative launch per round with grid barriers
     int mode = LT_ENSEMBLE_GRAPH;
     int blocks_per_sm = 0;        // persistent mode: resident blocks per SM (0: the occupancy limit)
-    unsigned* d_bar = nullptr;    // persistent mode: barrier count, generation, status
+    unsigned* d_bar = nullptr;    // persistent mode: barrier count, generation, status, (pad), unit counters
     long long polls = LT_PERSIST_POLLS;
 };
 
@@ -166,6 +166,9 @@ void drop_graphs(lt_ensemble* e)
     e->graphs.clear();
 }
 
+// persistent mode: at most this many sweeps (heatbath + overrelaxation) in one round
+constexpr int kMaxRoundSweeps = 256;
+
 int persistent_blocks(const lt_ensemble* e)
 {
     const int mx = e->be->batch_round_max_blocks_per_sm();
@@ -182,6 +185,8 @@ int persistent_rounds(lt_ensemble* e, cudaStream_t s, int n_sweep, int n_hb, int
 {
     const int bps = persistent_blocks(e);
     if (bps < 1) return lt::set_error(LT_ERR_CUDA, "lt_ensemble: the persistent kernel cannot be resident");
+    if (n_hb + n_or > kMaxRoundSweeps)
+        return lt::set_error(LT_ERR_ARG, "lt_ensemble_sweeps: a persistent round holds at most 256 sweeps");
     const int n_units = e->n_blocks[1];
     for (int k = 0; k < n_sweep; ++k)
     {
@@ -236,8 +241,8 @@ int lt_ensemble_create(lt_lattice* const* lattices, const double* betas, int n, 
     cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_desc, sizeof(lt::LatDesc) * n);
     if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_counter, sizeof(uint64_t));
-    if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_bar, 3 * sizeof(unsigned));
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(e->d_bar, 0, 3 * sizeof(unsigned), e->stream);
+    if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_bar, (4 + 8 * kMaxRoundSweeps) * sizeof(unsigned));
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(e->d_bar, 0, 4 * sizeof(unsigned), e->stream);
     if (ce != cudaSuccess)
     {
         int r = lt::cuda_error(ce, "lt_ensemble_create");

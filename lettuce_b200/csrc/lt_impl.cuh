@@ -345,8 +345,11 @@ public:
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const LatDesc* d = static_cast<const LatDesc*>(desc);
         GridBarrier b{ bar, bar + 1, bar + 2, polls };
+        unsigned* next = bar + 4;   // one unit counter per sub-sweep, zeroed before the launch
+        cudaError_t e = cudaMemsetAsync(next, 0, sizeof(unsigned) * 8 * (size_t)(n_hb + n_or), s);
+        if (e != cudaSuccess) return e;
         void* args[] = { (void*)&d, (void*)&n_lat, (void*)&n_units, (void*)&n_hb, (void*)&n_or, (void*)&reverse,
-                         (void*)&counter, (void*)&max_iter, (void*)&b };
+                         (void*)&counter, (void*)&max_iter, (void*)&b, (void*)&next };
         return cudaLaunchCooperativeKernel((const void*)k_batch_round<T, NR>, dim3(blocks_per_sm * sms), dim3(128),
                                            args, 0, s);
     }

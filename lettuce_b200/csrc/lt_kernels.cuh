@@ -1326,14 +1326,18 @@ LT_D void batch_unit(StapleRingT<RB>& ring, const LatDesc* __restrict__ d, int n
 #endif
 
 // Blocks of 128 threads (the staged kernels' tuned size); register cap as k_batch_sweep's
+// Work units are handed out dynamically: each block takes the next unit of the current
+// sub-sweep from the sub-sweep's own counter in next[] (zeroed by the host before the launch),
+// as the hardware scheduler hands out the blocks of a batched launch.
 template <typename T, int NR>
 __global__ void __launch_bounds__(128, (BatchMinBlocks<T, NR, 128>::value))
     k_batch_round(const LatDesc* __restrict__ d, int n, int n_units, int n_hb, int n_or, int reverse,
-                  uint64_t* __restrict__ counter, int max_iter, GridBarrier bar)
+                  uint64_t* __restrict__ counter, int max_iter, GridBarrier bar, unsigned* __restrict__ next)
 {
     // the staged staple's ring for two-row FP32 links; a token one otherwise
     constexpr bool kStagedRound = LT_STAGED_STAPLE && std::is_same<T, float>::value && NR == 2;
     __shared__ StapleRingT<kStagedRound ? 128 : 1> ring;
+    __shared__ int unit_s;
     const uint64_t c0 = *counter;
     const int n_sub = 8 * (n_hb + n_or);
     for (int q = 0; q < n_sub; ++q)
@@ -1347,8 +1351,15 @@ __global__ void __launch_bounds__(128, (BatchMinBlocks<T, NR, 128>::value))
         const int hb_rank = reverse ? n_hb - 1 - sweep : sweep;
         const uint64_t cnt = c0 + (uint64_t)(op == 0 ? hb_rank : 0);
         const int mu = idx >> 1, par = idx & 1;
-        for (int u = blockIdx.x; u < n_units; u += gridDim.x)
+        for (;;)
+        {
+            if (threadIdx.x == 0) unit_s = (int)atomicAdd(&next[q], 1u);
+            __syncthreads();
+            const int u = unit_s;
+            __syncthreads();   // every thread has read unit_s before thread 0 overwrites it
+            if (u >= n_units) break;
             batch_unit<T, NR, 128>(ring, d, n, u, op, mu, par, cnt, max_iter);
+        }
         if (q + 1 < n_sub && !grid_barrier(bar)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *counter = c0 + (uint64_t)n_hb;
