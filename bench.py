@@ -305,8 +305,8 @@ def secondary_rates(lt, torch, timed, prec):
     * BMW configuration files at 32^4 (device checksum pass, save and load);
     * Iterator::Checkerboard4 rounds at 32^4 with the Wilson and the Luescher-Weisz actions;
     * the driver's measurement step at 32^4;
-    * one 48^4 HMC trajectory (OMF4, tau = 1, 20 steps, bulk FP32 storage, FP64 dH) and the
-      flow to t0."""
+    * one 48^4 HMC trajectory (OMF4, tau = 1, 20 steps, bulk FP32 storage, FP64 dH), the
+      Wilson flow to t0 and the Zeuthen flow's rate."""
     import numpy as np
     out = {"storage": prec}
     try:
@@ -469,6 +469,12 @@ def secondary_rates(lt, torch, timed, prec):
         out["flow_to_t0_48^4_s"] = time.perf_counter() - t0
         out["t0_48^4_beta6.3"] = tt0
         out["Q_at_t0_48^4"] = q
+        # the Zeuthen flow of the same configuration: RK3 steps/s
+        zflow = lt.GradientFlowKernel(G, F, lt.RK3, lt.ZeuthenFlow(), FLOW_EPS)
+        zflow(2)
+        n_z = 10
+        ms = timed(F, lambda: zflow.Resume(n_z), 1)
+        out["zeuthen_flow_steps_per_s_48^4"] = n_z / (ms / 1000.0)
         del F, G
     except Exception as e:
         out["hmc_48_error"] = repr(e)
