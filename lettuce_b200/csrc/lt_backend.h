@@ -82,8 +82,11 @@ public:
                         uint64_t seed, int max_iter) const = 0;
     virtual void heatbath(const Ctx& c, void* U, int mu, int par, double prefactor, uint64_t counter,
                           uint64_t seed, int max_iter) const = 0;
+    // flow_split(): the format runs a flow stage as two kernels and wants an algebra scratch
+    // field X (flow_stage's last argument; null: the fused stage)
+    virtual bool flow_split() const = 0;
     virtual void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new,
-                            double c_exp, int read_z, int write_z) const = 0;
+                            double c_exp, int read_z, int write_z, void* X) const = 0;
     virtual void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const = 0;
     // Zeuthen flow stage: X <- the Luescher-Weisz force (c_plaq cp, c_rect cr) of Uin, then the
     // Zeuthen force from X and the stage's Z and link update Uin -> Uout

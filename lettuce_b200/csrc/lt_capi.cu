@@ -102,7 +102,7 @@ int flow_steps(lt_lattice* h, double eps, int n_step, int integrator = LT_FLOW_R
     LT_TRY(ensure(h, &h->U2, h->be->gauge_bytes(h->g)));
     if (ns > 1) LT_TRY(ensure(h, &h->Z, h->be->alg_bytes(h->g)));
     const bool zeuthen = h->flow_action == LT_FLOW_ACTION_ZEUTHEN;
-    if (zeuthen) LT_TRY(ensure(h, &h->Xz, h->be->alg_bytes(h->g)));
+    if (zeuthen || h->be->flow_split()) LT_TRY(ensure(h, &h->Xz, h->be->alg_bytes(h->g)));
     const lt::Ctx c = h->ctx();
     for (int k = 0; k < n_step; ++k)
         for (int j = 0; j < ns; ++j)
@@ -114,7 +114,7 @@ int flow_steps(lt_lattice* h, double eps, int n_step, int integrator = LT_FLOW_R
                                           st[j].read_z, st[j].write_z, 5.0 / 3.0, -1.0 / 12.0);
             else
                 h->be->flow_stage(c, h->U, h->U2, h->Z, st[j].c_old, st[j].c_new * eps, st[j].c_exp, st[j].read_z,
-                                  st[j].write_z);
+                                  st[j].write_z, h->be->flow_split() ? h->Xz : nullptr);
             std::swap(h->U, h->U2);
         }
     return launched("flow");

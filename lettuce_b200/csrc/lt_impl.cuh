@@ -220,9 +220,23 @@ public:
         else
             k_bmw_unpack<T, NR, 12><<<kRedBlocks, kRedThreads, 0, c.stream>>>(gauge(U, c.g), c.g, p, partials, flags);
     }
+    bool flow_split() const override { return std::is_same<T, double>::value; }
     void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new, double c_exp,
-                    int read_z, int write_z) const override
+                    int read_z, int write_z, void* X) const override
     {
+        if constexpr (std::is_same<T, double>::value)
+        {
+            if (X)
+            {
+                const int nb = nblocks(c.g.V, kSitesPerBlock);
+                launch_chained(c.rect ? k_flow_force<T, NR, true> : k_flow_force<T, NR, false>, nb, 4 * kSitesPerBlock,
+                               c.stream, gauge(Uin, c.g), alg(X, c.g), c.g, (T)c.cp, (T)c.cr, next_order(c));
+                launch_chained(k_flow_update<T, NR>, nb, 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
+                               gauge(Uout, c.g), alg(Z, c.g), alg(X, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z,
+                               write_z, next_order(c));
+                return;
+            }
+        }
         if constexpr (kStaged)
         {
             if (!c.rect)
@@ -242,8 +256,8 @@ public:
                             double c_exp, int read_z, int write_z, double cp, double cr) const override
     {
         const int nb = nblocks(c.g.V, kSitesPerBlock);
-        launch_chained(k_flow_force<T, NR>, nb, 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g), alg(X, c.g), c.g,
-                       (T)cp, (T)cr, next_order(c));
+        launch_chained(k_flow_force<T, NR, true>, nb, 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g), alg(X, c.g),
+                       c.g, (T)cp, (T)cr, next_order(c));
         launch_chained(k_flow_zeuthen_stage<T, NR>, nb, 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
                        gauge(Uout, c.g), alg(Z, c.g), alg(X, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z,
                        write_z, next_order(c));

@@ -1448,7 +1448,8 @@ __global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
 //                             + U_mu(x-mu)^dag X_mu(x-mu) U_mu(x-mu) - 2 X_mu(x)],
 // integrated with the stages of the flow integrators exactly as the plain force.
 // Pass 1 of a stage: X for every link.
-template <typename T, int NR>
+// (Also the first half of the split FP64 flow stage, below, with the handle's action.)
+template <typename T, int NR, bool RECT>
 __global__ void __launch_bounds__(kThreads) k_flow_force(Gauge<T, NR> U, Alg<T> X, Geom g, T cp, T cr, int rev)
 {
     pdl_release();
@@ -1459,7 +1460,37 @@ __global__ void __launch_bounds__(kThreads) k_flow_force(Gauge<T, NR> U, Alg<T> 
     int c[4];
     const int i = site_coords(g, par, s, c);
     const M3<T> u = U.ld(mu, par, s);
-    X.st(mu, par, s, algebra8(mul_nd(action_staple<true>(U, g, par, i, c, mu, cp, cr), u)));
+    X.st(mu, par, s, algebra8(mul_nd(action_staple<RECT>(U, g, par, i, c, mu, cp, cr), u)));
+}
+
+// The second half of a split flow stage: Z <- c_old Z + c_new X, U' = exp(c_exp Z) U, with
+// X = Algebra(st U^dag) from k_flow_force.  FP64 links run the stage as these two kernels:
+// the fused stage needs 254 registers (two blocks of 128 per SM), the halves far fewer each.
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads) k_flow_update(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Alg<T> Z, Alg<T> X,
+                                                          Geom g, T c_old, T c_new, T c_exp, int read_z, int write_z,
+                                                          int rev)
+{
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x, rev)) return;
+    const int par = x >= g.vh, s = x - par * g.vh;
+    const A8<T> a = X.ld(mu, par, s);
+    A8<T> z;
+    if (read_z)
+    {
+        const A8<T> zo = Z.ld(mu, par, s);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z.a[k] = c_old * zo.a[k] + c_new * a.a[k];
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z.a[k] = c_new * a.a[k];
+    }
+    if (write_z) Z.st(mu, par, s, z);
+    Uout.st(mu, par, s, exp_update<T, NR>(unpack_ah(z), c_exp, Uin.ld(mu, par, s)));
 }
 
 // Pass 2: the Zeuthen force from X at x and x +- mu, then the stage's Z update and exponential
