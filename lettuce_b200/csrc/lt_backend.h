@@ -87,7 +87,8 @@ public:
     virtual bool flow_split() const = 0;
     virtual void flow_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, double c_old, double c_new,
                             double c_exp, int read_z, int write_z, void* X) const = 0;
-    virtual void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const = 0;
+    // st_out (may be null): the staple of every link, one full 3x3 per link
+    virtual void stout(const Ctx& c, const void* Uin, void* Uout, double rho, void* st_out) const = 0;
     // Zeuthen flow stage: X <- the Luescher-Weisz force (c_plaq cp, c_rect cr) of Uin, then the
     // Zeuthen force from X and the stage's Z and link update Uin -> Uout
     virtual void flow_zeuthen_stage(const Ctx& c, const void* Uin, void* Uout, void* Z, void* X, double c_old,
@@ -126,7 +127,7 @@ public:
     virtual void topcharge_R(const Ctx& c, const void* R, int slot) const = 0;
     virtual void clover_deriv(const Ctx& c, const void* U, const void* R, void* out, double scale) const = 0;
     virtual void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam,
-                              void* Tloc, double rho) const = 0;
+                              void* Tloc, double rho, const void* st_in) const = 0;
     virtual void stout_recursion(const Ctx& c, const void* U, const void* Lam, const void* Tloc, void* Sigma,
                                  double rho) const = 0;
 };

@@ -126,7 +126,7 @@ int stout_steps(lt_lattice* h, double rho, int n)
     const lt::Ctx c = h->ctx();
     for (int k = 0; k < n; ++k)
     {
-        h->be->stout(c, h->U, h->U2, rho);
+        h->be->stout(c, h->U, h->U2, rho, nullptr);
         std::swap(h->U, h->U2);
     }
     return launched("stout");
@@ -149,7 +149,9 @@ int plaq_of(lt_lattice* h, const void* U, double* out)
 }
 
 // Forward stout chain U -> levels[1..n] (StoutSmearing4DWithConstants,
-// smearing/stout_smearing.hpp:92-119, without storing the exponential constants)
+// smearing/stout_smearing.hpp:92-119): the exponential constants are not stored (the adjoint
+// recomputes them), the staple of every level is (the adjoint's Lambda step reads it back
+// instead of computing it again)
 int metad_forward(lt_lattice* h, double rho, int n_stout)
 {
     while ((int)h->levels.size() < n_stout)
@@ -158,11 +160,17 @@ int metad_forward(lt_lattice* h, double rho, int n_stout)
         LT_CK(cudaMalloc(&p, h->be->gauge_bytes(h->g)));
         h->levels.push_back(p);
     }
+    while ((int)h->staples.size() < n_stout)
+    {
+        void* p = nullptr;
+        LT_CK(cudaMalloc(&p, h->be->full_bytes(h->g)));
+        h->staples.push_back(p);
+    }
     const lt::Ctx c = h->ctx();
     const void* prev = h->U;
     for (int k = 0; k < n_stout; ++k)
     {
-        h->be->stout(c, prev, h->levels[k], rho);
+        h->be->stout(c, prev, h->levels[k], rho, h->staples[k]);
         prev = h->levels[k];
     }
     return launched("metad_forward");
@@ -202,7 +210,7 @@ int metad_backward(lt_lattice* h, double rho, int n_stout, double dvdq, bool hav
     h->be->clover_deriv(c, top, h->R, h->F, dvdq);
     for (int k = n_stout; k > 0; --k)
     {
-        h->be->stout_lambda(c, level(h, k - 1), level(h, k), h->F, h->Lam, h->Tloc, rho);
+        h->be->stout_lambda(c, level(h, k - 1), level(h, k), h->F, h->Lam, h->Tloc, rho, h->staples[k - 1]);
         h->be->stout_recursion(c, level(h, k - 1), h->Lam, h->Tloc, h->F, rho);
     }
     return launched("metad_backward");
@@ -542,6 +550,7 @@ int lt_destroy(lt_lattice* h)
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (void* p : h->levels) cudaFree(p);
+    for (void* p : h->staples) cudaFree(p);
     if (h->h_results) cudaFreeHost(h->h_results);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

@@ -59,6 +59,7 @@ struct lt_lattice
     void* Lam = nullptr;     // Lambda (algebra)
     void* Tloc = nullptr;    // link-local recursion term (full matrix)
     std::vector<void*> levels;   // smeared levels 1..n of the MetaD chain
+    std::vector<void*> staples;  // the staples of levels 0..n-1 (full 3x3 per link), for the adjoint
     double* partials = nullptr;
     double* results = nullptr;
     double* h_results = nullptr; // pinned

@@ -262,17 +262,17 @@ public:
                        gauge(Uout, c.g), alg(Z, c.g), alg(X, c.g), c.g, (T)c_old, (T)c_new, (T)c_exp, read_z,
                        write_z, next_order(c));
     }
-    void stout(const Ctx& c, const void* Uin, void* Uout, double rho) const override
+    void stout(const Ctx& c, const void* Uin, void* Uout, double rho, void* st_out) const override
     {
         if constexpr (kStaged)
         {
             prefer_shared<k_stout_staged<0>>();
             launch_chained(k_stout_staged<0>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
-                           gauge(Uin, c.g), gauge(Uout, c.g), c.g, (T)rho);
+                           gauge(Uin, c.g), gauge(Uout, c.g), c.g, (T)rho, full(st_out, c.g));
             return;
         }
         launch_chained(k_stout<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream, gauge(Uin, c.g),
-                       gauge(Uout, c.g), c.g, (T)rho);
+                       gauge(Uout, c.g), c.g, (T)rho, full(st_out, c.g));
     }
 
     void momenta(const Ctx& c, const void* U, void* P, const void* F, double coef, double eps) const override
@@ -401,8 +401,15 @@ public:
                        gauge(U, c.g), clov(R, c.g), alg(out, c.g), c.g, (T)scale);
     }
     void stout_lambda(const Ctx& c, const void* U, const void* Up, const void* Sigma, void* Lam, void* Tloc,
-                      double rho) const override
+                      double rho, const void* st_in) const override
     {
+        if (st_in)
+        {
+            launch_chained(k_stout_lambda_st<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
+                           gauge(U, c.g), gauge(Up, c.g), alg(Sigma, c.g), alg(Lam, c.g), full(Tloc, c.g),
+                           full(st_in, c.g), c.g, (T)rho);
+            return;
+        }
         if constexpr (kStaged)
         {
             prefer_shared<k_stout_lambda_staged<0>>();

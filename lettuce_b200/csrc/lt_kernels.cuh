@@ -1542,8 +1542,11 @@ __global__ void __launch_bounds__(kThreads) k_flow_zeuthen_stage(Gauge<T, NR> Ui
 
 // ---------------------------------------------------------------- stout smearing
 // StoutSmearing4D (smearing/stout_smearing.hpp:29-57): U' = exp(rho Algebra(st U^dag)) U, Gram-Schmidt
+// With St.p set, the staple of every link is also stored (the metadynamics force's Lambda
+// kernel reads it back instead of recomputing it).
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho)
+__global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_stout(Gauge<T, NR> Uin, Gauge<T, NR> Uout, Geom g, T rho,
+                                                    Full<T> St)
 {
     pdl_release();
     pdl_wait();
@@ -1554,13 +1557,14 @@ __global__ void __launch_bounds__(kThreads, (LinkMinBlocks<T, NR>::value)) k_sto
     int i = site_coords(g, par, s, c);
     M3<T> u = Uin.ld(mu, par, s);
     M3<T> st = staple(Uin, g, par, i, c, mu);
+    if (St.p) St.st(mu, par, s, st);
     Uout.st(mu, par, s, exp_update<T, NR>(unpack_ah(algebra8(mul_nd(st, u))), rho, u));
 }
 
 // k_stout on two-row FP32 storage with the staged staple
 template <int Unused = 0>
 __global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
-    k_stout_staged(Gauge<float, 2> Uin, Gauge<float, 2> Uout, Geom g, float rho)
+    k_stout_staged(Gauge<float, 2> Uin, Gauge<float, 2> Uout, Geom g, float rho, Full<float> St)
 {
     __shared__ StapleRing ring;
     pdl_release();
@@ -1572,6 +1576,7 @@ __global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
     const int i = site_coords(g, par, s, c);
     M3<float> u;
     const M3<float> st = staple_staged<true>(ring, Uin, g, par, i, s, c, mu, u);
+    if (St.p) St.st(mu, par, s, st);
     Uout.st(mu, par, s, exp_update<float, 2>(unpack_ah(algebra8(mul_nd(st, u))), rho, u));
 }
 
@@ -2330,6 +2335,19 @@ __global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_l
     int c[4];
     int i = site_coords(g, par, s, c);
     stout_lambda_core(Up, Sigma, Lam, Tloc, rho, mu, par, s, U.ld(mu, par, s), staple(U, g, par, i, c, mu));
+}
+
+// k_stout_lambda with the staple stored by the forward stout step of the level (St)
+template <typename T, int NR>
+__global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_lambda_st(Gauge<T, NR> U, Gauge<T, NR> Up, Alg<T> Sigma, Alg<T> Lam,
+                                                              Full<T> Tloc, Full<T> St, Geom g, T rho)
+{
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
+    const int par = x >= g.vh, s = x - par * g.vh;
+    stout_lambda_core(Up, Sigma, Lam, Tloc, rho, mu, par, s, U.ld(mu, par, s), St.ld(mu, par, s));
 }
 
 // k_stout_lambda on two-row FP32 storage with the staged staple
