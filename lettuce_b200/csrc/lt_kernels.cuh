@@ -2182,29 +2182,43 @@ LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const
     const int imu = i + dmu, inu = i + step_up_rt(g, nu, c), ind = i + step_dn_rt(g, nu, c);
     // x+mu+nu and x+mu-nu share the nu offsets of x (coordinate c[nu] unchanged by the mu step)
     const int imunu = inu + dmu, imund = ind + dmu;
-    const M3<T> u_s_nu = U.ld(nu, par, i >> 1);
-    const M3<T> u_mup_nu = U.ld(nu, op, imu >> 1);
-    const M3<T> u_nup_mu = U.ld(mu, op, inu >> 1);
-    const M3<T> u_mupnud_nu = U.ld(nu, par, imund >> 1);
-    const M3<T> u_nud_mu = U.ld(mu, op, ind >> 1);
-    const M3<T> u_nud_nu = U.ld(nu, op, ind >> 1);
-    const M3<T> R_s = R.ld(rho, sigma, par, i >> 1);
-    const M3<T> R_mup = R.ld(rho, sigma, op, imu >> 1);
-    M3<T> tmp1 = mul_nd(u_mup_nu, u_nup_mu);          // U(x+mu,nu) U(x+nu,mu)^dag
-    M3<T> tmp2 = mul_dd(u_nup_mu, u_s_nu);            // U(x+nu,mu)^dag U(x,nu)^dag
-    M3<T> tmp3 = mul_dd(u_mupnud_nu, u_nud_mu);       // U(x+mu-nu,nu)^dag U(x-nu,mu)^dag
-    M3<T> tmp4 = mul_dn(u_nud_mu, u_nud_nu);          // U(x-nu,mu)^dag U(x-nu,nu)
-    M3<T> r = mul(tmp1, mul_dn(u_s_nu, R_s) + mul_nd(R.ld(rho, sigma, op, inu >> 1), u_s_nu));
-    acc(r, mul(mul(u_mup_nu, R.ld(rho, sigma, par, imunu >> 1)) + mul(R_mup, u_mup_nu), tmp2));
-    r = r - mul(tmp3, mul(u_nud_nu, R_s) + mul(R.ld(rho, sigma, op, ind >> 1), u_nud_nu));
-    r = r - mul(mul_dn(u_mupnud_nu, R.ld(rho, sigma, par, imund >> 1)) + mul_nd(R_mup, u_mupnud_nu), tmp4);
+    M3<T> r;
+    {
+        const M3<T> u_s_nu = U.ld(nu, par, i >> 1);
+        const M3<T> u_mup_nu = U.ld(nu, op, imu >> 1);
+        const M3<T> u_nup_mu = U.ld(mu, op, inu >> 1);
+        const M3<T> R_s = R.ld(rho, sigma, par, i >> 1);
+        M3<T> tmp1 = mul_nd(u_mup_nu, u_nup_mu);
+        r = mul(tmp1, mul_dn(u_s_nu, R_s) + mul_nd(R.ld(rho, sigma, op, inu >> 1), u_s_nu));
+        asm volatile("" ::: "memory");
+        M3<T> tmp2 = mul_dd(u_nup_mu, u_s_nu);
+        acc(r, mul(mul(u_mup_nu, R.ld(rho, sigma, par, imunu >> 1)) + mul(R.ld(rho, sigma, op, imu >> 1), u_mup_nu), tmp2));
+    }
+    asm volatile("" ::: "memory");
+    {
+        const M3<T> u_mupnud_nu = U.ld(nu, par, imund >> 1);
+        const M3<T> u_nud_mu = U.ld(mu, op, ind >> 1);
+        const M3<T> u_nud_nu = U.ld(nu, op, ind >> 1);
+        M3<T> tmp3 = mul_dd(u_mupnud_nu, u_nud_mu);
+        r = r - mul(tmp3, mul(u_nud_nu, R.ld(rho, sigma, par, i >> 1)) + mul(R.ld(rho, sigma, op, ind >> 1), u_nud_nu));
+        asm volatile("" ::: "memory");
+        M3<T> tmp4 = mul_dn(u_nud_mu, u_nud_nu);
+        r = r - mul(mul_dn(u_mupnud_nu, R.ld(rho, sigma, par, imund >> 1)) + mul_nd(R.ld(rho, sigma, op, imu >> 1), u_mupnud_nu), tmp4);
+    }
     return r;
 }
 
 // CloverDerivative (observables/clover.hpp:279-321) times `scale` (dV/dQ):
 // Sigma_n = scale * (-2/(512 pi^2)) Algebra(U_mu(x) sum_eps-terms)
+// The component is computed in two halves separated by compiler memory fences, so that the
+// loads of the second half are not hoisted into the first: FP32 links then fit 3 blocks of
+// 128 per SM (168 registers, no spills; 201 registers unfenced without a cap, 253 before)
+template <typename T> struct CloverDerivMinBlocks
+{
+    static constexpr int value = sizeof(T) == 4 ? 3 : 1;
+};
 template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads) k_clover_deriv(Gauge<T, NR> U, Clov<T> R, Alg<T> out, Geom g, T scale)
+__global__ void __launch_bounds__(kThreads, CloverDerivMinBlocks<T>::value) k_clover_deriv(Gauge<T, NR> U, Clov<T> R, Alg<T> out, Geom g, T scale)
 {
     pdl_release();
     pdl_wait();
