@@ -290,6 +290,29 @@ template <typename T> struct Clov
         m.e[2][1] = mkc<T>(-v[7], v[8]);
         return m;
     }
+
+    // -i R_{rho sigma}: the Hermitian matrix (real diagonal) whose i-multiple is the plane
+    LT_D M3<T> ld_h(int rho, int sigma, int par, int s) const
+    {
+        int a = rho < sigma ? rho : sigma, b = rho < sigma ? sigma : rho;
+        int pl = a == 0 ? b - 1 : (a == 1 ? b + 1 : 5);
+        T sg = rho < sigma ? (T)1 : (T)-1;
+        const T* q = p + plane(pl, par, 0) + s;
+        T v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = sg * q[(size_t)k * vh];
+        M3<T> m;
+        m.e[0][0] = mkc<T>(v[0], 0);
+        m.e[1][1] = mkc<T>(v[1], 0);
+        m.e[2][2] = mkc<T>(v[2], 0);
+        m.e[0][1] = mkc<T>(v[4], -v[3]);
+        m.e[0][2] = mkc<T>(v[6], -v[5]);
+        m.e[1][2] = mkc<T>(v[8], -v[7]);
+        m.e[1][0] = mkc<T>(v[4], v[3]);
+        m.e[2][0] = mkc<T>(v[6], v[5]);
+        m.e[2][1] = mkc<T>(v[8], v[7]);
+        return m;
+    }
 };
 
 } // namespace lt

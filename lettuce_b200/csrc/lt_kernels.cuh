@@ -2182,29 +2182,35 @@ LT_D M3<T> clover_deriv_component(const Gauge<T, NR>& U, const Clov<T>& R, const
     const int imu = i + dmu, inu = i + step_up_rt(g, nu, c), ind = i + step_dn_rt(g, nu, c);
     // x+mu+nu and x+mu-nu share the nu offsets of x (coordinate c[nu] unchanged by the mu step)
     const int imunu = inu + dmu, imund = ind + dmu;
+    // Every term is linear in the planes R: with R = i H (H = -i R Hermitian, real diagonal) the
+    // sum is computed with H through the Hermitian-aware products and multiplied by i at the end
     M3<T> r;
     {
         const M3<T> u_s_nu = U.ld(nu, par, i >> 1);
         const M3<T> u_mup_nu = U.ld(nu, op, imu >> 1);
         const M3<T> u_nup_mu = U.ld(mu, op, inu >> 1);
-        const M3<T> R_s = R.ld(rho, sigma, par, i >> 1);
-        M3<T> tmp1 = mul_nd(u_mup_nu, u_nup_mu);
-        r = mul(tmp1, mul_dn(u_s_nu, R_s) + mul_nd(R.ld(rho, sigma, op, inu >> 1), u_s_nu));
+        const M3<T> H_s = R.ld_h(rho, sigma, par, i >> 1);
+        M3<T> tmp1 = mul_nd(u_mup_nu, u_nup_mu);          // U(x+mu,nu) U(x+nu,mu)^dag
+        r = mul(tmp1, mul_dh(u_s_nu, H_s) + mul_hd(R.ld_h(rho, sigma, op, inu >> 1), u_s_nu));
         asm volatile("" ::: "memory");
-        M3<T> tmp2 = mul_dd(u_nup_mu, u_s_nu);
-        acc(r, mul(mul(u_mup_nu, R.ld(rho, sigma, par, imunu >> 1)) + mul(R.ld(rho, sigma, op, imu >> 1), u_mup_nu), tmp2));
+        M3<T> tmp2 = mul_dd(u_nup_mu, u_s_nu);            // U(x+nu,mu)^dag U(x,nu)^dag
+        acc(r, mul(mul_xh(u_mup_nu, R.ld_h(rho, sigma, par, imunu >> 1)) + mul_hx(R.ld_h(rho, sigma, op, imu >> 1), u_mup_nu), tmp2));
     }
     asm volatile("" ::: "memory");
     {
         const M3<T> u_mupnud_nu = U.ld(nu, par, imund >> 1);
         const M3<T> u_nud_mu = U.ld(mu, op, ind >> 1);
         const M3<T> u_nud_nu = U.ld(nu, op, ind >> 1);
-        M3<T> tmp3 = mul_dd(u_mupnud_nu, u_nud_mu);
-        r = r - mul(tmp3, mul(u_nud_nu, R.ld(rho, sigma, par, i >> 1)) + mul(R.ld(rho, sigma, op, ind >> 1), u_nud_nu));
+        M3<T> tmp3 = mul_dd(u_mupnud_nu, u_nud_mu);       // U(x+mu-nu,nu)^dag U(x-nu,mu)^dag
+        r = r - mul(tmp3, mul_xh(u_nud_nu, R.ld_h(rho, sigma, par, i >> 1)) + mul_hx(R.ld_h(rho, sigma, op, ind >> 1), u_nud_nu));
         asm volatile("" ::: "memory");
-        M3<T> tmp4 = mul_dn(u_nud_mu, u_nud_nu);
-        r = r - mul(mul_dn(u_mupnud_nu, R.ld(rho, sigma, par, imund >> 1)) + mul_nd(R.ld(rho, sigma, op, imu >> 1), u_mupnud_nu), tmp4);
+        M3<T> tmp4 = mul_dn(u_nud_mu, u_nud_nu);          // U(x-nu,mu)^dag U(x-nu,nu)
+        r = r - mul(mul_dh(u_mupnud_nu, R.ld_h(rho, sigma, par, imund >> 1)) + mul_hd(R.ld_h(rho, sigma, op, imu >> 1), u_mupnud_nu), tmp4);
     }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) r.e[a][b] = timesi(r.e[a][b]);
     return r;
 }
 
@@ -2270,15 +2276,22 @@ LT_D void stout_lambda_core(const Gauge<T, NR>& Up, const Alg<T>& Sigma, const A
                             T rho, int mu, int par, int s, const M3<T>& u, const M3<T>& st)
 {
     M3<T> sp = mul_dn(Up.ld(mu, par, s), unpack_ah(Sigma.ld(mu, par, s)));
-    M3<T> C = unpack_ah(algebra8(mul_nd(st, u)));
-    M3<T> Q;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) Q.e[a][b] = mkc<T>(rho * C.e[a][b].i, -rho * C.e[a][b].r);
-    M3<T> Q2 = mul(Q, Q);
+    // Q = -i rho C with C = Algebra(st U^dag), packed as a Hermitian matrix (real diagonal):
+    // for C = unpack_ah(c), Q = unpack_h(rho (c0, c1, c3, -c2, c5, -c4, c7, -c6))
+    const A8<T> c8 = algebra8(mul_nd(st, u));
+    A8<T> q8;
+    q8.a[0] = rho * c8.a[0];
+    q8.a[1] = rho * c8.a[1];
+    q8.a[2] = rho * c8.a[3];
+    q8.a[3] = -rho * c8.a[2];
+    q8.a[4] = rho * c8.a[5];
+    q8.a[5] = -rho * c8.a[4];
+    q8.a[6] = rho * c8.a[7];
+    q8.a[7] = -rho * c8.a[6];
+    const M3<T> Q = unpack_h(q8);
+    M3<T> Q2 = herm_sq(Q);
     M3<T> tmp = mul(u, sp);
-    M3<T> Qt = mul(Q, tmp), tQ = mul(tmp, Q);
+    M3<T> Qt = mul_hx(Q, tmp), tQ = mul_xh(tmp, Q);
     // tr(B_j tmp) = b_j0 tr(tmp) + b_j1 tr(Q tmp) + b_j2 tr(Q^2 tmp)
     const cx<T> r0 = trace(tmp), r1 = trace(Qt), r2 = tr_mul(Q2, tmp);
     cx<T> t1, t2, f1, f2;
@@ -2329,7 +2342,7 @@ LT_D void stout_lambda_core(const Gauge<T, NR>& Up, const Alg<T>& Sigma, const A
     A8<T> l8 = traceless_herm8(lam);
     Lam.st(mu, par, s, l8);
     M3<T> loc = mul(sp, ex);
-    M3<T> sl = mul_dn(st, unpack_h(l8));   // st^dag Lambda
+    M3<T> sl = mul_dh(st, unpack_h(l8));   // st^dag Lambda
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -2410,15 +2423,15 @@ __global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Al
         const M3<T> u_nud_mu = U.ld(mu, op, ind >> 1);
         const M3<T> u_mupnud_nu = U.ld(nu, par, imund >> 1);
         M3<T> tmp1 = mul_nd(U.ld(nu, op, imu >> 1), U.ld(mu, op, inu >> 1));
-        M3<T> tmp2 = mul_dn(u_nud_mu, unpack_h(Lam.ld(mu, op, ind >> 1)) - unpack_h(Lam.ld(nu, op, ind >> 1)));
+        M3<T> tmp2 = mul_dh(u_nud_mu, unpack_h(Lam.ld(mu, op, ind >> 1)) - unpack_h(Lam.ld(nu, op, ind >> 1)));
         // rows 1 and 6 of eq. C6 in arXiv:2307.04742
-        acc(fs, mul(tmp1, mul_dn(u_s_nu, unpack_h(Lam.ld(nu, par, i >> 1)))
-                          + mul_nd(unpack_h(Lam.ld(mu, op, inu >> 1)), u_s_nu)));
+        acc(fs, mul(tmp1, mul_dh(u_s_nu, unpack_h(Lam.ld(nu, par, i >> 1)))
+                          + mul_hd(unpack_h(Lam.ld(mu, op, inu >> 1)), u_s_nu)));
         // rows 2, 3 and 4
-        acc(fs, mul(mul_dn(u_mupnud_nu, tmp2 + mul_nd(unpack_h(Lam.ld(nu, par, imund >> 1)), u_nud_mu)),
+        acc(fs, mul(mul_dn(u_mupnud_nu, tmp2 + mul_hd(unpack_h(Lam.ld(nu, par, imund >> 1)), u_nud_mu)),
                     U.ld(nu, op, ind >> 1)));
         // row 5
-        fs = fs - mul_nd(mul(unpack_h(Lam.ld(nu, op, imu >> 1)), tmp1), u_s_nu);
+        fs = fs - mul_nd(mul_hx(unpack_h(Lam.ld(nu, op, imu >> 1)), tmp1), u_s_nu);
     }
     M3<T> loc = Tloc.ld(mu, par, s);
 #pragma unroll

@@ -59,7 +59,10 @@ template <typename T> LT_HD M3<T> unit3()
 // chains: each complex term adds two fused multiply-adds to each running sum.  (A single
 // expression like `re += a*b - c*d` would cost a multiply, an FMA and an add per term,
 // since the compiler may not reassociate it.)  ROWS < 3 computes only the leading rows.
-template <bool DA, bool DB, int ROWS = 3, typename T> LT_HD M3<T> prod(const M3<T>& a, const M3<T>& b)
+// RA / RB: the diagonal of a / b is known to be real (a Hermitian factor), so the products with
+// its zero imaginary parts are left out (the compiler may not drop a multiplication by 0.0).
+template <bool DA, bool DB, int ROWS = 3, bool RA = false, bool RB = false, typename T>
+LT_HD M3<T> prod(const M3<T>& a, const M3<T>& b)
 {
     M3<T> r;
 #pragma unroll
@@ -71,14 +74,15 @@ template <bool DA, bool DB, int ROWS = 3, typename T> LT_HD M3<T> prod(const M3<
 #pragma unroll
             for (int k = 0; k < 3; ++k)
             {
+                const bool xreal = RA && k == i, yreal = RB && k == j;
                 const T xr = DA ? a.e[k][i].r : a.e[i][k].r;
                 const T xi = DA ? -a.e[k][i].i : a.e[i][k].i;
                 const T yr = DB ? b.e[j][k].r : b.e[k][j].r;
                 const T yi = DB ? -b.e[j][k].i : b.e[k][j].i;
                 re += xr * yr;
-                re -= xi * yi;
-                im += xr * yi;
-                im += xi * yr;
+                if (!xreal && !yreal) re -= xi * yi;
+                if (!yreal) im += xr * yi;
+                if (!xreal) im += xi * yr;
             }
             r.e[i][j] = mkc<T>(re, im);
         }
@@ -87,6 +91,11 @@ template <bool DA, bool DB, int ROWS = 3, typename T> LT_HD M3<T> prod(const M3<
 
 // A * B
 template <typename T> LT_HD M3<T> mul(const M3<T>& a, const M3<T>& b) { return prod<false, false>(a, b); }
+// Products with a Hermitian factor H (real diagonal): H X, X H, U^dagger H, H U^dagger
+template <typename T> LT_HD M3<T> mul_hx(const M3<T>& h, const M3<T>& b) { return prod<false, false, 3, true, false>(h, b); }
+template <typename T> LT_HD M3<T> mul_xh(const M3<T>& a, const M3<T>& h) { return prod<false, false, 3, false, true>(a, h); }
+template <typename T> LT_HD M3<T> mul_dh(const M3<T>& a, const M3<T>& h) { return prod<true, false, 3, false, true>(a, h); }
+template <typename T> LT_HD M3<T> mul_hd(const M3<T>& h, const M3<T>& b) { return prod<false, true, 3, true, false>(h, b); }
 // A * B^dagger
 template <typename T> LT_HD M3<T> mul_nd(const M3<T>& a, const M3<T>& b) { return prod<false, true>(a, b); }
 // A^dagger * B
