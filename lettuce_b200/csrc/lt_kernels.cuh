@@ -991,7 +991,7 @@ template <> struct HB<float>
     LT_D static S2<float> su2(const S2<float>& A, float prefactor, uint32_t link, uint64_t counter,
                                uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, HbCarry& carry)
     {
-        float an = 1.0f / sqrtf(s2_det(A));
+        float an = rsqrtf(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
         const uint32_t tw = (TAG_HEATBATH << 24) | (sg << 16);
         float lsq = 0.0f;

@@ -350,7 +350,10 @@ template <typename T> LT_HD void restore_last_row(M3<T>& a)
 
 template <typename T> LT_D T rsqrt_t(T x);
 template <> LT_D double rsqrt_t<double>(double x) { return 1.0 / sqrt(x); }
-template <> LT_D float rsqrt_t<float>(float x) { return 1.0f / sqrtf(x); }
+// FP32: the hardware reciprocal square root (rsqrtf, 2 ulp) instead of an IEEE square root and
+// an IEEE division; every use normalises a vector or an SU(2) matrix whose FP32 rounding is of
+// the same order, and each update ends with a Gram-Schmidt projection
+template <> LT_D float rsqrt_t<float>(float x) { return rsqrtf(x); }
 
 // GramSchmidt (math/su3.hpp:370-394); RESTORE = false skips the third row (two-row storage)
 template <typename T, bool RESTORE = true> LT_D void gram_schmidt(M3<T>& a)
