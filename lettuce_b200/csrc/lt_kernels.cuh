@@ -1020,7 +1020,7 @@ template <> struct HB<float>
             if (r0 * r0 + lsq < 1.0f) break;
         }
         float x0 = 1.0f - 2.0f * lsq;
-        float ax = sqrtf(fmaxf(1.0f - x0 * x0, 0.0f));
+        float ax = sqrt_approx(fmaxf(1.0f - x0 * x0, 0.0f));
         float phi, ct;
         if (sg == 1)
         {
@@ -1040,7 +1040,7 @@ template <> struct HB<float>
             carry.spare[0] = f01_from(d.z);
             carry.spare[1] = 1.0f - 2.0f * f01_from(d.w);
         }
-        float vn = ax * sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
+        float vn = ax * sqrt_approx(fmaxf(1.0f - ct * ct, 0.0f));
         float sp, cp;
         __sincosf(kTwoPiF * phi, &sp, &cp);
         S2<float> x, V;

@@ -354,6 +354,14 @@ template <> LT_D double rsqrt_t<double>(double x) { return 1.0 / sqrt(x); }
 // an IEEE division; every use normalises a vector or an SU(2) matrix whose FP32 rounding is of
 // the same order, and each update ends with a Gram-Schmidt projection
 template <> LT_D float rsqrt_t<float>(float x) { return rsqrtf(x); }
+// FP32 square root by the hardware approximation (PTX sqrt.approx.f32, relative error within
+// 2^-23 per the PTX ISA), for the sampler's sqrt(1 - x^2) terms; sqrt_approx(0) = 0
+LT_D float sqrt_approx(float x)
+{
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 // GramSchmidt (math/su3.hpp:370-394); RESTORE = false skips the third row (two-row storage)
 template <typename T, bool RESTORE = true> LT_D void gram_schmidt(M3<T>& a)
