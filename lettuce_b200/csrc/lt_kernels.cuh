@@ -933,7 +933,7 @@ template <> struct HB<double>
     LT_D static S2<double> su2(const S2<double>& A, double prefactor, uint32_t link, uint64_t counter,
                                 uint32_t sg, uint32_t k0, uint32_t k1, int max_iter, bool& capped, HbCarry&)
     {
-        double an = 1.0 / sqrt(s2_det(A));
+        double an = rsqrt(s2_det(A));
         const uint32_t c1 = (uint32_t)counter, c2 = (uint32_t)(counter >> 32);
         const uint32_t tw = (TAG_HEATBATH << 24) | (sg << 16);
         double lsq = 0.0;

@@ -349,7 +349,9 @@ template <typename T> LT_HD void restore_last_row(M3<T>& a)
 }
 
 template <typename T> LT_D T rsqrt_t(T x);
-template <> LT_D double rsqrt_t<double>(double x) { return 1.0 / sqrt(x); }
+// FP64: CUDA's double-precision reciprocal square root (within 1 ulp), not a square root and a
+// division; the normalised results agree with 1 / sqrt to rounding
+template <> LT_D double rsqrt_t<double>(double x) { return rsqrt(x); }
 // FP32: the hardware reciprocal square root (rsqrtf, 2 ulp) instead of an IEEE square root and
 // an IEEE division; every use normalises a vector or an SU(2) matrix whose FP32 rounding is of
 // the same order, and each update ends with a Gram-Schmidt projection
