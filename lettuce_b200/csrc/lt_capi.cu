@@ -1,11 +1,13 @@
 // C ABI of the lattice handle: device memory, one stream per handle, and the sequencing
 // of kernels for sweeps, flow, stout smearing, HMC and the metadynamics force.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "lt_handle.h"
@@ -484,6 +486,106 @@ double accept_uniform(uint64_t seed, uint64_t counter)
 
 } // namespace
 
+// FP32 storages: the reference-layout FP64 links are rounded and packed into the device layout
+// on the host, by all host threads, chunk by chunk into a pinned staging buffer, and each
+// chunk is copied to the device while the threads pack the next: the PCIe link then carries
+// the stored 48 (two-row) or 72 bytes per link instead of the 144 of the FP64 input, and the
+// packing overlaps the copies.  The rounding (IEEE round to nearest, double to float) and the
+// layout are those of the device conversion k_from_aos.
+namespace {
+
+constexpr int kUploadChunks = 8;
+
+// Packs the sites [i0, i1) (reference site order) of the FP64 links into dst in the device
+// layout of the storage (nr = 2: three float4 chunks per link; nr = 3: nine complex planes)
+void pack_sites(const lt::Geom& g, int nr, const double* aos, float* dst, long long i0, long long i1)
+{
+    const size_t vh = (size_t)g.vh;
+    for (long long i = i0; i < i1; ++i)
+    {
+        long long r = i;
+        const int z = (int)(r % g.n[3]);
+        r /= g.n[3];
+        const int y = (int)(r % g.n[2]);
+        r /= g.n[2];
+        const int x = (int)(r % g.n[1]);
+        const int t = (int)(r / g.n[1]);
+        const int par = (t + x + y + z) & 1;
+        const size_t s = (size_t)(i >> 1);
+        for (int mu = 0; mu < 4; ++mu)
+        {
+            const double* a = aos + (size_t)18 * (4 * (size_t)i + mu);
+            if (nr == 2)
+            {
+                // chunk c of plane (mu, par) holds floats 4c .. 4c + 3 of rows 0-1
+                for (int c = 0; c < 3; ++c)
+                {
+                    float* q = dst + 4 * (((size_t)(mu * 2 + par) * 3 + c) * vh + s);
+                    for (int k = 0; k < 4; ++k) q[k] = (float)a[4 * c + k];
+                }
+            }
+            else
+            {
+                for (int e = 0; e < 9; ++e)
+                {
+                    float* q = dst + 2 * (((size_t)(mu * 2 + par) * 9 + e) * vh + s);
+                    q[0] = (float)a[2 * e];
+                    q[1] = (float)a[2 * e + 1];
+                }
+            }
+        }
+    }
+}
+
+int upload_packed_fp32(lt_lattice* h, const double* links)
+{
+    const int nr = h->prec == LT_PREC_FP32_12 ? 2 : 3;
+    const size_t elem = nr == 2 ? 16 : 8;           // bytes of one plane entry
+    const int planes = nr == 2 ? 24 : 72;           // (mu, par) x chunks or elements
+    const size_t bytes = h->be->gauge_bytes(h->g);
+    if (!h->h_stage) LT_CK(cudaMallocHost(&h->h_stage, bytes));
+    // the staging buffer may still feed a copy of an earlier call on this stream
+    LT_CK(cudaStreamSynchronize(h->stream));
+    const long long vh = h->g.vh;
+    long long bound[kUploadChunks + 1];
+    for (int k = 0; k <= kUploadChunks; ++k) bound[k] = vh * k / kUploadChunks;   // checkerboard indices
+    unsigned nt = std::thread::hardware_concurrency();
+    if (nt == 0) nt = 1;
+    if (h->g.V < 65536) nt = 1;
+    std::atomic<int> done[kUploadChunks];
+    for (auto& d : done) d.store(0);
+    float* dst = static_cast<float*>(h->h_stage);
+    std::vector<std::thread> pool;
+    const lt::Geom g = h->g;
+    // sites 2s and 2s + 1 share checkerboard index s (the z extent is even), so chunk k of
+    // checkerboard indices is the contiguous site range [2 bound[k], 2 bound[k+1])
+    for (unsigned t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (int k = 0; k < kUploadChunks; ++k)
+            {
+                const long long a = 2 * bound[k], b = 2 * bound[k + 1], n = b - a;
+                pack_sites(g, nr, links, dst, a + n * t / nt, a + n * (t + 1) / nt);
+                done[k].fetch_add(1, std::memory_order_release);
+            }
+        });
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < kUploadChunks; ++k)
+    {
+        while (done[k].load(std::memory_order_acquire) < (int)nt) std::this_thread::yield();
+        const size_t off = (size_t)bound[k] * elem, width = (size_t)(bound[k + 1] - bound[k]) * elem;
+        if (e == cudaSuccess && width)
+            e = cudaMemcpy2DAsync(static_cast<char*>(h->U) + off, (size_t)vh * elem,
+                                  reinterpret_cast<const char*>(dst) + off, (size_t)vh * elem, width, planes,
+                                  cudaMemcpyHostToDevice, h->stream);
+    }
+    for (auto& th : pool) th.join();
+    if (e != cudaSuccess) return lt::cuda_error(e, "lt_upload_links: copy");
+    LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+} // namespace
+
 extern "C" {
 
 const char* lt_last_error(void) { return lt::g_last_error.c_str(); }
@@ -552,6 +654,7 @@ int lt_destroy(lt_lattice* h)
     for (void* p : h->levels) cudaFree(p);
     for (void* p : h->staples) cudaFree(p);
     if (h->h_results) cudaFreeHost(h->h_results);
+    if (h->h_stage) cudaFreeHost(h->h_stage);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LT_OK;
@@ -571,6 +674,7 @@ int lt_upload_links(lt_lattice* h, const double* links)
     LT_TRY(check_h(h, "lt_upload_links"));
     const lt::DeviceScope device_scope(h->device);
     if (!links) return lt::set_error(LT_ERR_ARG, "lt_upload_links: null pointer");
+    if (h->prec != LT_PREC_FP64) return upload_packed_fp32(h, links);
     LT_TRY(ensure_aos(h));
     LT_CK(cudaMemcpyAsync(h->d_aos, links, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyHostToDevice,
                           h->stream));

@@ -63,6 +63,7 @@ struct lt_lattice
     double* partials = nullptr;
     double* results = nullptr;
     double* h_results = nullptr; // pinned
+    void* h_stage = nullptr;     // pinned: FP32 links packed in the device layout on the host (upload)
     double* d_aos = nullptr;     // staging buffer for host transfers (reference layout)
     unsigned* status = nullptr;  // device status word (lt_status_word) and scratch words
     void* chainA = nullptr;      // straight-line link products of lt_wilson_loop (FP64 full matrices)
