@@ -9,6 +9,9 @@
 #include <string>
 #include <thread>
 #include <vector>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include "lt_handle.h"
 
@@ -496,41 +499,70 @@ namespace {
 
 constexpr int kUploadChunks = 8;
 
-// Packs the sites [i0, i1) (reference site order) of the FP64 links into dst in the device
-// layout of the storage (nr = 2: three float4 chunks per link; nr = 3: nine complex planes)
+// Packs the sites [i0, i1) (reference site order; i0 and i1 even) of the FP64 links into dst
+// in the device layout of the storage (nr = 2: three float4 chunks per link; nr = 3: nine
+// complex planes).  Sites 2s and 2s + 1 share the checkerboard index s and have opposite
+// parities (the z extent is even), so the loop walks site pairs and steps the coordinates
+// with carries instead of dividing.
 void pack_sites(const lt::Geom& g, int nr, const double* aos, float* dst, long long i0, long long i1)
 {
     const size_t vh = (size_t)g.vh;
-    for (long long i = i0; i < i1; ++i)
+    if (i0 >= i1) return;
+    long long r = i0;
+    int z = (int)(r % g.n[3]);
+    r /= g.n[3];
+    int y = (int)(r % g.n[2]);
+    r /= g.n[2];
+    int x = (int)(r % g.n[1]);
+    int t = (int)(r / g.n[1]);
+    for (long long i = i0; i < i1; i += 2)
     {
-        long long r = i;
-        const int z = (int)(r % g.n[3]);
-        r /= g.n[3];
-        const int y = (int)(r % g.n[2]);
-        r /= g.n[2];
-        const int x = (int)(r % g.n[1]);
-        const int t = (int)(r / g.n[1]);
-        const int par = (t + x + y + z) & 1;
+        const int p0 = (t + x + y + z) & 1;   // parity of site i; site i + 1 has the other
         const size_t s = (size_t)(i >> 1);
-        for (int mu = 0; mu < 4; ++mu)
+        for (int h = 0; h < 2; ++h)
         {
-            const double* a = aos + (size_t)18 * (4 * (size_t)i + mu);
-            if (nr == 2)
+            const int par = p0 ^ h;
+            const double* site = aos + (size_t)72 * (size_t)(i + h);
+            for (int mu = 0; mu < 4; ++mu)
             {
-                // chunk c of plane (mu, par) holds floats 4c .. 4c + 3 of rows 0-1
-                for (int c = 0; c < 3; ++c)
+                const double* a = site + 18 * mu;
+                if (nr == 2)
                 {
-                    float* q = dst + 4 * (((size_t)(mu * 2 + par) * 3 + c) * vh + s);
-                    for (int k = 0; k < 4; ++k) q[k] = (float)a[4 * c + k];
+                    // chunk c of plane (mu, par) holds floats 4c .. 4c + 3 of rows 0-1
+                    float* q = dst + 4 * ((size_t)(mu * 2 + par) * 3 * vh + s);
+                    for (int c = 0; c < 3; ++c)
+                    {
+#if defined(__SSE2__)
+                        const __m128 lo = _mm_cvtpd_ps(_mm_loadu_pd(a + 4 * c));
+                        const __m128 hi = _mm_cvtpd_ps(_mm_loadu_pd(a + 4 * c + 2));
+                        _mm_store_ps(q + 4 * c * vh, _mm_movelh_ps(lo, hi));
+#else
+                        for (int k = 0; k < 4; ++k) q[4 * c * vh + k] = (float)a[4 * c + k];
+#endif
+                    }
+                }
+                else
+                {
+                    for (int e = 0; e < 9; ++e)
+                    {
+                        float* q = dst + 2 * (((size_t)(mu * 2 + par) * 9 + e) * vh + s);
+                        q[0] = (float)a[2 * e];
+                        q[1] = (float)a[2 * e + 1];
+                    }
                 }
             }
-            else
+        }
+        z += 2;
+        if (z == g.n[3])
+        {
+            z = 0;
+            if (++y == g.n[2])
             {
-                for (int e = 0; e < 9; ++e)
+                y = 0;
+                if (++x == g.n[1])
                 {
-                    float* q = dst + 2 * (((size_t)(mu * 2 + par) * 9 + e) * vh + s);
-                    q[0] = (float)a[2 * e];
-                    q[1] = (float)a[2 * e + 1];
+                    x = 0;
+                    ++t;
                 }
             }
         }
@@ -563,8 +595,10 @@ int upload_packed_fp32(lt_lattice* h, const double* links)
         pool.emplace_back([&, t] {
             for (int k = 0; k < kUploadChunks; ++k)
             {
-                const long long a = 2 * bound[k], b = 2 * bound[k + 1], n = b - a;
-                pack_sites(g, nr, links, dst, a + n * t / nt, a + n * (t + 1) / nt);
+                // whole site pairs per thread: pair range [bound[k], bound[k+1]) split evenly
+                const long long n = bound[k + 1] - bound[k];
+                const long long a = bound[k] + n * t / nt, b = bound[k] + n * (t + 1) / nt;
+                pack_sites(g, nr, links, dst, 2 * a, 2 * b);
                 done[k].fetch_add(1, std::memory_order_release);
             }
         });
