@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -489,11 +490,13 @@ double accept_uniform(uint64_t seed, uint64_t counter)
 
 } // namespace
 
-// FP32 storages: the reference-layout FP64 links are rounded and packed into the device layout
-// on the host, by all host threads, chunk by chunk into a pinned staging buffer, and each
-// chunk is copied to the device while the threads pack the next: the PCIe link then carries
-// the stored 48 (two-row) or 72 bytes per link instead of the 144 of the FP64 input, and the
-// packing overlaps the copies.  The rounding (IEEE round to nearest, double to float) and the
+// Two-row FP32 storage: the reference-layout FP64 links are rounded and packed into the device
+// layout on the host, by all host threads, chunk by chunk into a pinned staging buffer, and
+// each chunk is copied to the device while the threads pack the next: the PCIe link then
+// carries the stored 48 bytes per link instead of the 144 of the FP64 input, and the packing
+// overlaps the copies (32^4: 8.8 ms against 11.2 ms for the FP64 copy at 55 GB/s).  The
+// 18-real FP32 storage keeps the device conversion: its host packing (72 bytes per link) was
+// slower than the FP64 copy.  The rounding (IEEE round to nearest, double to float) and the
 // layout are those of the device conversion k_from_aos.
 namespace {
 
@@ -569,8 +572,15 @@ void pack_sites(const lt::Geom& g, int nr, const double* aos, float* dst, long l
     }
 }
 
+// One packing upload at a time per process: the packing is bound by host memory bandwidth and
+// uses every core, so two handles packing at once only contend (measured on the GPU hosts: 8.8
+// ms for one 32^4 upload alone, 25 ms each for two at once); serialised, one handle packs
+// while the other's copy and kernels run.
+std::mutex g_pack_mutex;
+
 int upload_packed_fp32(lt_lattice* h, const double* links)
 {
+    std::lock_guard<std::mutex> pack_lock(g_pack_mutex);
     const int nr = h->prec == LT_PREC_FP32_12 ? 2 : 3;
     const size_t elem = nr == 2 ? 16 : 8;           // bytes of one plane entry
     const int planes = nr == 2 ? 24 : 72;           // (mu, par) x chunks or elements
@@ -708,7 +718,7 @@ int lt_upload_links(lt_lattice* h, const double* links)
     LT_TRY(check_h(h, "lt_upload_links"));
     const lt::DeviceScope device_scope(h->device);
     if (!links) return lt::set_error(LT_ERR_ARG, "lt_upload_links: null pointer");
-    if (h->prec != LT_PREC_FP64) return upload_packed_fp32(h, links);
+    if (h->prec == LT_PREC_FP32_12) return upload_packed_fp32(h, links);
     LT_TRY(ensure_aos(h));
     LT_CK(cudaMemcpyAsync(h->d_aos, links, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyHostToDevice,
                           h->stream));
