@@ -494,7 +494,9 @@ double accept_uniform(uint64_t seed, uint64_t counter)
 // layout on the host, by all host threads, chunk by chunk into a pinned staging buffer, and
 // each chunk is copied to the device while the threads pack the next: the PCIe link then
 // carries the stored 48 bytes per link instead of the 144 of the FP64 input, and the packing
-// overlaps the copies (32^4: 8.8 ms against 11.2 ms for the FP64 copy at 55 GB/s).  The
+// overlaps the copies (32^4: 8.8 to 9.4 ms against 11.2 ms for the FP64 copy at 55 GB/s).  A
+// handle's first upload takes the device conversion: the pinned staging buffer (its
+// allocation costs more than one upload) is set up for handles that are uploaded again.  The
 // 18-real FP32 storage keeps the device conversion: its host packing (72 bytes per link) was
 // slower than the FP64 copy.  The rounding (IEEE round to nearest, double to float) and the
 // layout are those of the device conversion k_from_aos.
@@ -718,7 +720,9 @@ int lt_upload_links(lt_lattice* h, const double* links)
     LT_TRY(check_h(h, "lt_upload_links"));
     const lt::DeviceScope device_scope(h->device);
     if (!links) return lt::set_error(LT_ERR_ARG, "lt_upload_links: null pointer");
-    if (h->prec == LT_PREC_FP32_12) return upload_packed_fp32(h, links);
+    // a handle uploaded more than once (a field streamed in step after step) packs on the host;
+    // a single upload does not pay the pinned staging buffer's allocation
+    if (h->prec == LT_PREC_FP32_12 && h->uploads++ > 0) return upload_packed_fp32(h, links);
     LT_TRY(ensure_aos(h));
     LT_CK(cudaMemcpyAsync(h->d_aos, links, (size_t)4 * h->g.V * 18 * sizeof(double), cudaMemcpyHostToDevice,
                           h->stream));

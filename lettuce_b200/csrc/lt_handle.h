@@ -64,6 +64,7 @@ struct lt_lattice
     double* results = nullptr;
     double* h_results = nullptr; // pinned
     void* h_stage = nullptr;     // pinned: FP32 links packed in the device layout on the host (upload)
+    int uploads = 0;             // lt_upload_links calls so far (the staging is set up from the second)
     double* d_aos = nullptr;     // staging buffer for host transfers (reference layout)
     unsigned* status = nullptr;  // device status word (lt_status_word) and scratch words
     void* chainA = nullptr;      // straight-line link products of lt_wilson_loop (FP64 full matrices)
