@@ -47,6 +47,24 @@ class TestContainer:
         G = gpu(golden4["ext"], golden4["U"], "fp32_12")
         assert rel_err(G.download(), golden4["U"]) < 1e-6
 
+    @pytest.mark.parametrize("ext", [(4, 6, 8, 10), (2, 4, 2, 6), (16, 16, 16, 16), (16, 8, 18, 32)])
+    def test_repeated_upload_packs_on_host_identically(self, ext):
+        """From its second upload on, a two-row FP32 handle packs the links into the stored
+        format on the host threads (single- and multi-threaded by volume) and copies them in
+        chunks; the stored field must be bit for bit the one the device conversion of the first
+        upload makes."""
+        U1, U2 = lt.haar_links(ext, 71), lt.haar_links(ext, 72)
+        fresh = []
+        for U in (U1, U2):
+            F = lt.GaugeField(ext, "fp32_12")
+            F.upload(U)            # first upload: device conversion
+            fresh.append(F.download())
+        G = lt.GaugeField(ext, "fp32_12")
+        G.upload(U2)
+        for k, U in enumerate((U1, U2, U1)):
+            G.upload(U)            # packed on the host
+            assert np.array_equal(G.download(), fresh[k % 2]), k
+
     def test_identity_and_copy_swap(self, golden4):
         ext = golden4["ext"]
         A, B = gpu(ext, golden4["U"]), lt.GaugeField(ext)
