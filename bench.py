@@ -680,8 +680,11 @@ def main():
         # only, and ctypes releases the GIL inside them), so that one handle's upload overlaps
         # the other's sweeps; every step still uploads its whole field and reads its plaquette.
         fields = [lt.GaugeField(ext, a.prec) for _ in range(2)]
+        # warm-up: two uploads per handle (a handle streamed into sets up its pinned packing
+        # buffer at its second upload), a round and a plaquette
         for F in fields:
-            F.upload(host)
+            for _ in range(2):
+                F.upload(host)
             sweep_round(F)
             lt.PlaquetteSum(F)
         n_e2e = max(3, min(a.steps, 10))
