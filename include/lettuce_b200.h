@@ -378,6 +378,7 @@ int lt_parity_update(lt_lattice* h);
 #define LT_EXP_CLOSED       1  /* the closed form of ExpConstants (FP64 scalar chain)            */
 #define LT_EXP_SERIES_SHORT 2  /* Cayley-Hamilton series, short term count (valid for c1 <= 1/32) */
 #define LT_EXP_SERIES_LONG  3  /* Cayley-Hamilton series, long term count (valid for c1 <= 1/2)  */
+#define LT_EXP_SERIES_TINY  4  /* Cayley-Hamilton series, tiny term count (valid for c1 <= 1/512) */
 /* SU3::exp (math/su3_exp.hpp:419-432) on the device: out[k] = exp(i Q_k) for n traceless
  * Hermitian 3x3 matrices q_in[k] (18 doubles each, row-major, re/im interleaved; host
  * memory), computed in the arithmetic of storage format prec by the branch `path`

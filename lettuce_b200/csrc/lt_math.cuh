@@ -678,9 +678,15 @@ template <typename T> LT_D M3<T> exp_ah(const M3<T>& X, T c)
         T c0 = retr_mul(Q, Q2) * (T)(1.0 / 3.0);
         cx<T> g0, g1, g2;
         // the truncation error after N terms is below r^(N+1)/(N+1)! e^r for spectral radius
-        // r <= sqrt(2 c1): at r <= 1/4 (flow and HMC steps) 13 terms leave 3e-18 in FP64 and 7
-        // terms 1.6e-8 in FP32
-        if (c1 <= (T)(1.0 / 32.0))
+        // r <= sqrt(2 c1): at r <= 1/16 (the flow's steps of eps = 0.01) 10 terms leave 3e-19 in
+        // FP64 and 5 terms 9e-9 in FP32; at r <= 1/4 (HMC steps) 13 terms leave 3e-18 in FP64
+        // and 7 terms 1.6e-8 in FP32
+        if (c1 <= (T)(1.0 / 512.0))
+        {
+            if (sizeof(T) == 8) exp_series<9>(c0, c1, g0, g1, g2);
+            else exp_series<4>(c0, c1, g0, g1, g2);
+        }
+        else if (c1 <= (T)(1.0 / 32.0))
         {
             if (sizeof(T) == 8) exp_series<12>(c0, c1, g0, g1, g2);
             else exp_series<6>(c0, c1, g0, g1, g2);

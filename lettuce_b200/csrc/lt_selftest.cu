@@ -16,8 +16,8 @@ namespace {
 //   LT_EXP_DISPATCH  exp_ah as the flow, stout and HMC kernels call it (series below the
 //                    spectral bound, closed form above it)
 //   LT_EXP_CLOSED    the closed form (FP64 scalar chain, matrices in T)
-//   LT_EXP_SERIES_SHORT / _LONG  the Cayley-Hamilton series with the short (c1 <= 1/32) or
-//                    long (c1 <= 1/2) term count of exp_ah
+//   LT_EXP_SERIES_TINY / _SHORT / _LONG  the Cayley-Hamilton series with the tiny
+//                    (c1 <= 1/512), short (c1 <= 1/32) or long (c1 <= 1/2) term count of exp_ah
 template <typename T>
 __global__ void k_exp_test(const double* __restrict__ in, double* __restrict__ out, int n, int path)
 {
@@ -53,7 +53,12 @@ __global__ void k_exp_test(const double* __restrict__ in, double* __restrict__ o
             const T c1 = (T)0.5 * (Q2.e[0][0].r + Q2.e[1][1].r + Q2.e[2][2].r);
             const T c0 = lt::retr_mul(Q, Q2) * (T)(1.0 / 3.0);
             lt::cx<T> g0, g1, g2;
-            if (path == LT_EXP_SERIES_SHORT)
+            if (path == LT_EXP_SERIES_TINY)
+            {
+                if (sizeof(T) == 8) lt::exp_series<9>(c0, c1, g0, g1, g2);
+                else lt::exp_series<4>(c0, c1, g0, g1, g2);
+            }
+            else if (path == LT_EXP_SERIES_SHORT)
             {
                 if (sizeof(T) == 8) lt::exp_series<12>(c0, c1, g0, g1, g2);
                 else lt::exp_series<6>(c0, c1, g0, g1, g2);
@@ -96,7 +101,7 @@ extern "C" int lt_su3_exp_test(const double* q_in, double* out, int n, int prec,
     if (!q_in || !out || n < 0) return lt::set_error(LT_ERR_ARG, "lt_su3_exp_test: null pointer or negative count");
     if (prec != LT_PREC_FP64 && prec != LT_PREC_FP32 && prec != LT_PREC_FP32_12)
         return lt::set_error(LT_ERR_ARG, "lt_su3_exp_test: unknown precision");
-    if (path < LT_EXP_DISPATCH || path > LT_EXP_SERIES_LONG) return lt::set_error(LT_ERR_ARG, "lt_su3_exp_test: unknown path");
+    if (path < LT_EXP_DISPATCH || path > LT_EXP_SERIES_TINY) return lt::set_error(LT_ERR_ARG, "lt_su3_exp_test: unknown path");
     if (n == 0) return LT_OK;
     if ((long long)n * 18 > (1LL << 28)) return lt::set_error(LT_ERR_ARG, "lt_su3_exp_test: too many matrices");
     const size_t bytes = sizeof(double) * 18 * (size_t)n;

@@ -9,7 +9,7 @@ run on the same inputs by the reference harness.
 
 Each branch runs through the test entry point lt_su3_exp_test:
   * FP64: the dispatch the flow, stout and HMC kernels use, the closed form on every input,
-    and each series on the inputs inside its range -- 1e-12 absolute (entries are O(1));
+    and each series (tiny, short, long term counts) on the inputs inside its range -- 1e-12 absolute (entries are O(1));
   * FP32 (the arithmetic of both FP32 storages): the same branches, within 4e-6 max(1, c1)
     (the input is rounded to FP32 and Q^2 carries c1-sized entries).
 The outputs must also be unitary with unit determinant to the arithmetic's precision.
@@ -26,7 +26,7 @@ from lettuce_b200 import _lib
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-DISPATCH, CLOSED, SHORT, LONG = 0, 1, 2, 3
+DISPATCH, CLOSED, SHORT, LONG, TINY = 0, 1, 2, 3, 4
 
 
 @pytest.fixture(scope="module")
@@ -55,7 +55,8 @@ def test_inputs_cover_every_branch(cases):
     _, _, c1 = cases
     assert np.sum(c1 > 0.5) >= 16
     assert np.sum((c1 > 1 / 32) & (c1 <= 0.5)) >= 16
-    assert np.sum((c1 > 0) & (c1 <= 1 / 32)) >= 16
+    assert np.sum((c1 > 1 / 512) & (c1 <= 1 / 32)) >= 16
+    assert np.sum((c1 > 0) & (c1 <= 1 / 512)) >= 16
     assert np.sum(c1 == 0) >= 1
 
 
@@ -68,7 +69,7 @@ def test_fp64_against_reference(cases, path):
     assert u < 1e-13 and d < 1e-13
 
 
-@pytest.mark.parametrize("path,limit", [(SHORT, 1 / 32), (LONG, 0.5)])
+@pytest.mark.parametrize("path,limit", [(TINY, 1 / 512), (SHORT, 1 / 32), (LONG, 0.5)])
 def test_fp64_series_in_range(cases, path, limit):
     q, ref, c1 = cases
     m = c1 <= limit
@@ -87,7 +88,7 @@ def test_fp32_against_reference(cases, prec, path):
     assert u < 2e-6 * max(1.0, c1.max()) and d < 2e-6 * max(1.0, c1.max())
 
 
-@pytest.mark.parametrize("path,limit", [(SHORT, 1 / 32), (LONG, 0.5)])
+@pytest.mark.parametrize("path,limit", [(TINY, 1 / 512), (SHORT, 1 / 32), (LONG, 0.5)])
 def test_fp32_series_in_range(cases, path, limit):
     q, ref, c1 = cases
     m = c1 <= limit
