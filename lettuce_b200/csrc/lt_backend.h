@@ -38,6 +38,8 @@ public:
     virtual size_t clov_bytes(const Geom& g) const = 0;      // six anti-Hermitian planes per site
 
     virtual void from_aos(const Ctx& c, void* U, const double* aos) const = 0;
+    // sites [i0, i1) only (reference site order; aos is the whole field's base)
+    virtual void from_aos_sites(const Ctx& c, void* U, const double* aos, long long i0, long long i1) const = 0;
     virtual void to_aos(const Ctx& c, const void* U, double* aos) const = 0;
     virtual void alg_from_aos(const Ctx& c, void* P, const double* aos) const = 0;
     virtual void alg_to_aos(const Ctx& c, const void* P, double* aos) const = 0;

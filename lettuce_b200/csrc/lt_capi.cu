@@ -2,6 +2,8 @@
 // of kernels for sweeps, flow, stout smearing, HMC and the metadynamics force.
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <cmath>
 #include <mutex>
 #include <cstdio>
@@ -491,24 +493,59 @@ double accept_uniform(uint64_t seed, uint64_t counter)
 } // namespace
 
 // Two-row FP32 storage: the reference-layout FP64 links are rounded and packed into the device
-// layout on the host, by all host threads, chunk by chunk into a pinned staging buffer, and
-// each chunk is copied to the device while the threads pack the next: the PCIe link then
-// carries the stored 48 bytes per link instead of the 144 of the FP64 input, and the packing
-// overlaps the copies (32^4: 8.8 to 9.4 ms against 11.2 ms for the FP64 copy at 55 GB/s).  A
-// handle's first upload takes the device conversion: the pinned staging buffer (its
+// layout on the host, by a pool of host threads, chunk by chunk into a pinned staging buffer,
+// and each chunk is copied to the device while the threads pack the next: the PCIe link then
+// carries the stored 48 bytes per link instead of the 144 of the FP64 input.  From pinned
+// input a share of the sites goes over PCIe as FP64 at the same time and is converted on the
+// device, so that the copy engine and the host's memory bandwidth are both used (one 32^4
+// upload: 6.4 to 6.8 ms, against 8.0 ms packed whole and 11.2 ms for the FP64 copy at 55 GB/s).
+// A handle's first upload takes the device conversion: the pinned staging buffer (its
 // allocation costs more than one upload) is set up for handles that are uploaded again.  The
 // 18-real FP32 storage keeps the device conversion: its host packing (72 bytes per link) was
 // slower than the FP64 copy.  The rounding (IEEE round to nearest, double to float) and the
 // layout are those of the device conversion k_from_aos.
 namespace {
 
-constexpr int kUploadChunks = 8;
+#ifndef LT_UPLOAD_CHUNKS
+#define LT_UPLOAD_CHUNKS 8
+#endif
+constexpr int kUploadChunks = LT_UPLOAD_CHUNKS;
 
 // Packs the sites [i0, i1) (reference site order; i0 and i1 even) of the FP64 links into dst
 // in the device layout of the storage (nr = 2: three float4 chunks per link; nr = 3: nine
 // complex planes).  Sites 2s and 2s + 1 share the checkerboard index s and have opposite
 // parities (the z extent is even), so the loop walks site pairs and steps the coordinates
 // with carries instead of dividing.
+//
+// Two-row storage goes block by block: kPackBlock site pairs' input records (74 KB, held in
+// the core's L2) are located first, then each of the 24 (direction, parity, chunk) planes
+// receives one contiguous run of kPackBlock float4 by streaming stores, so the pinned staging
+// buffer is written in whole cache lines without being read first.  Site by site, every site
+// would touch 12 planes and the plain stores would read each destination line before writing
+// it (packing a 32^4 field on 8 cores: 25.3 ms site by site, 16.2 ms blocked with plain stores,
+// 12.2 ms blocked with streaming stores).
+// Share of the checkerboard indices packed on the host when the input is pinned (the rest is
+// copied as FP64 and converted on the device).  Host packing alone is bound by the host's
+// memory bandwidth, the FP64 copy by PCIe; one 32^4 upload from pinned memory takes 8.0 ms
+// packed whole, 6.6 to 6.8 ms with 0.65 to 0.75 packed, 8.0 ms with 0.85
+#ifndef LT_PACK_SHARE
+#define LT_PACK_SHARE 0.7
+#endif
+constexpr double kPackShare = LT_PACK_SHARE;
+
+#ifndef LT_PACK_RESERVE
+#define LT_PACK_RESERVE 2
+#endif
+// host threads left to the callers: the uploading thread, which hands the chunks to the copy
+// engine, and a second handle's thread waiting on its kernels (32^4 streamed through two
+// handles: 3.34e9 link updates/s end to end with 2 left, 3.14e9 with 1, 3.05e9 with none)
+constexpr unsigned kPackReserve = LT_PACK_RESERVE;
+
+#ifndef LT_PACK_BLOCK
+#define LT_PACK_BLOCK 64
+#endif
+constexpr int kPackBlock = LT_PACK_BLOCK;
+
 void pack_sites(const lt::Geom& g, int nr, const double* aos, float* dst, long long i0, long long i1)
 {
     const size_t vh = (size_t)g.vh;
@@ -520,43 +557,7 @@ void pack_sites(const lt::Geom& g, int nr, const double* aos, float* dst, long l
     r /= g.n[2];
     int x = (int)(r % g.n[1]);
     int t = (int)(r / g.n[1]);
-    for (long long i = i0; i < i1; i += 2)
-    {
-        const int p0 = (t + x + y + z) & 1;   // parity of site i; site i + 1 has the other
-        const size_t s = (size_t)(i >> 1);
-        for (int h = 0; h < 2; ++h)
-        {
-            const int par = p0 ^ h;
-            const double* site = aos + (size_t)72 * (size_t)(i + h);
-            for (int mu = 0; mu < 4; ++mu)
-            {
-                const double* a = site + 18 * mu;
-                if (nr == 2)
-                {
-                    // chunk c of plane (mu, par) holds floats 4c .. 4c + 3 of rows 0-1
-                    float* q = dst + 4 * ((size_t)(mu * 2 + par) * 3 * vh + s);
-                    for (int c = 0; c < 3; ++c)
-                    {
-#if defined(__SSE2__)
-                        const __m128 lo = _mm_cvtpd_ps(_mm_loadu_pd(a + 4 * c));
-                        const __m128 hi = _mm_cvtpd_ps(_mm_loadu_pd(a + 4 * c + 2));
-                        _mm_store_ps(q + 4 * c * vh, _mm_movelh_ps(lo, hi));
-#else
-                        for (int k = 0; k < 4; ++k) q[4 * c * vh + k] = (float)a[4 * c + k];
-#endif
-                    }
-                }
-                else
-                {
-                    for (int e = 0; e < 9; ++e)
-                    {
-                        float* q = dst + 2 * (((size_t)(mu * 2 + par) * 9 + e) * vh + s);
-                        q[0] = (float)a[2 * e];
-                        q[1] = (float)a[2 * e + 1];
-                    }
-                }
-            }
-        }
+    auto next_pair = [&] {
         z += 2;
         if (z == g.n[3])
         {
@@ -571,14 +572,137 @@ void pack_sites(const lt::Geom& g, int nr, const double* aos, float* dst, long l
                 }
             }
         }
+    };
+    if (nr == 2)
+    {
+        const double* src[2][kPackBlock];   // input record of checkerboard index sa + k, by parity
+        for (long long i = i0; i < i1;)
+        {
+            const size_t sa = (size_t)(i >> 1);
+            int n = 0;
+            for (; n < kPackBlock && i < i1; ++n, i += 2)
+            {
+                const int p0 = (t + x + y + z) & 1;   // parity of site i; site i + 1 has the other
+                src[p0][n] = aos + (size_t)72 * (size_t)i;
+                src[p0 ^ 1][n] = aos + (size_t)72 * (size_t)(i + 1);
+                next_pair();
+            }
+            for (int par = 0; par < 2; ++par)
+                for (int mu = 0; mu < 4; ++mu)
+                    for (int c = 0; c < 3; ++c)
+                    {
+                        // chunk c of plane (mu, par) holds floats 4c .. 4c + 3 of rows 0-1
+                        float* q = dst + 4 * (((size_t)(mu * 2 + par) * 3 + c) * vh + sa);
+                        const int off = 18 * mu + 4 * c;
+                        for (int k = 0; k < n; ++k)
+                        {
+                            const double* a = src[par][k] + off;
+#if defined(__SSE2__)
+                            const __m128 lo = _mm_cvtpd_ps(_mm_loadu_pd(a));
+                            const __m128 hi = _mm_cvtpd_ps(_mm_loadu_pd(a + 2));
+                            _mm_stream_ps(q + 4 * k, _mm_movelh_ps(lo, hi));
+#else
+                            for (int e = 0; e < 4; ++e) q[4 * k + e] = (float)a[e];
+#endif
+                        }
+                    }
+        }
+#if defined(__SSE2__)
+        _mm_sfence();   // the streamed chunks are visible before the caller reports them packed
+#endif
+        return;
+    }
+    for (long long i = i0; i < i1; i += 2)
+    {
+        const int p0 = (t + x + y + z) & 1;
+        const size_t s = (size_t)(i >> 1);
+        for (int h = 0; h < 2; ++h)
+        {
+            const int par = p0 ^ h;
+            const double* site = aos + (size_t)72 * (size_t)(i + h);
+            for (int mu = 0; mu < 4; ++mu)
+            {
+                const double* a = site + 18 * mu;
+                for (int e = 0; e < 9; ++e)
+                {
+                    float* q = dst + 2 * (((size_t)(mu * 2 + par) * 9 + e) * vh + s);
+                    q[0] = (float)a[2 * e];
+                    q[1] = (float)a[2 * e + 1];
+                }
+            }
+        }
+        next_pair();
     }
 }
 
 // One packing upload at a time per process: the packing is bound by host memory bandwidth and
-// uses every core, so handles packing at once only contend; serialised, one handle packs while
-// the other's copy and kernels run (two handles streamed from two host threads at 32^4:
-// 2.10e9 link updates/s end to end, against 1.98e9 to 2.05e9 with the cores shared).
+// uses the cores, so handles packing at once only contend; serialised, one handle packs while
+// the other's copy and kernels run (two handles streamed from two host threads at 32^4,
+// measured before the split uploads: 2.10e9 link updates/s end to end, against 1.98e9 to
+// 2.05e9 with the cores shared).
 std::mutex g_pack_mutex;
+
+// The packing threads: started by the first packing upload and kept for the life of the
+// process (starting and joining 16 threads cost about 0.4 ms of an 8 ms upload).  They are
+// detached and the pool is never freed, so nothing waits for them at exit; each waits on a
+// condition variable between jobs.  Jobs run one at a time (under g_pack_mutex).
+class PackPool
+{
+public:
+    static PackPool& get()
+    {
+        static PackPool* pool = new PackPool();
+        return *pool;
+    }
+    unsigned size() const { return n_; }
+
+    // runs job(t) on workers t = 0 .. size() - 1 and returns without waiting
+    void start(const std::function<void(unsigned)>& job)
+    {
+        std::lock_guard<std::mutex> lk(m_);
+        job_ = job;
+        finished_ = 0;
+        ++gen_;
+        cv_.notify_all();
+    }
+    // waits until every worker has returned from the current job
+    void wait()
+    {
+        std::unique_lock<std::mutex> lk(m_);
+        idle_.wait(lk, [this] { return finished_ == n_; });
+    }
+
+private:
+    PackPool()
+    {
+        const unsigned hc = std::thread::hardware_concurrency();
+        n_ = hc > kPackReserve ? hc - kPackReserve : 1;
+        for (unsigned t = 0; t < n_; ++t) std::thread([this, t] { loop(t); }).detach();
+    }
+    void loop(unsigned t)
+    {
+        unsigned long long seen = 0;
+        for (;;)
+        {
+            std::function<void(unsigned)> job;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+                job = job_;
+            }
+            job(t);
+            std::lock_guard<std::mutex> lk(m_);
+            if (++finished_ == n_) idle_.notify_all();
+        }
+    }
+    std::mutex m_;
+    std::condition_variable cv_, idle_;
+    std::function<void(unsigned)> job_;
+    unsigned long long gen_ = 0;
+    unsigned finished_ = 0;
+    unsigned n_ = 1;
+};
 
 int upload_packed_fp32(lt_lattice* h, const double* links)
 {
@@ -588,35 +712,52 @@ int upload_packed_fp32(lt_lattice* h, const double* links)
     const int planes = nr == 2 ? 24 : 72;           // (mu, par) x chunks or elements
     const size_t bytes = h->be->gauge_bytes(h->g);
     if (!h->h_stage) LT_CK(cudaMallocHost(&h->h_stage, bytes));
-    // the staging buffer may still feed a copy of an earlier call on this stream
+    // the staging buffers may still feed a copy of an earlier call on this stream
     LT_CK(cudaStreamSynchronize(h->stream));
     const long long vh = h->g.vh;
+    // From pinned input, the sites of the checkerboard indices [s_split, vh) cross PCIe as
+    // FP64 straight from the caller's buffer and are converted on the device, while the host
+    // threads pack the rest: the copy engine and the host cores then share the field
+    long long s_split = vh;
+    cudaPointerAttributes attr;
+    if (h->g.V >= 65536 && cudaPointerGetAttributes(&attr, links) == cudaSuccess && attr.type == cudaMemoryTypeHost)
+        s_split = (long long)(vh * kPackShare);
+    (void)cudaGetLastError();   // an unregistered pointer may leave an error behind on old drivers
+    if (s_split < vh)
+    {
+        LT_TRY(ensure_aos(h));
+        const size_t first = (size_t)72 * (size_t)(2 * s_split);   // doubles before the first raw site
+        LT_CK(cudaMemcpyAsync(h->d_aos + first, links + first, (size_t)72 * (size_t)(h->g.V - 2 * s_split) * sizeof(double),
+                              cudaMemcpyHostToDevice, h->stream));
+        h->be->from_aos_sites(h->ctx(), h->U, h->d_aos, 2 * s_split, h->g.V);
+        LT_TRY(launched("lt_upload_links"));
+    }
     long long bound[kUploadChunks + 1];
-    for (int k = 0; k <= kUploadChunks; ++k) bound[k] = vh * k / kUploadChunks;   // checkerboard indices
-    unsigned nt = std::thread::hardware_concurrency();
-    if (nt == 0) nt = 1;
-    if (h->g.V < 65536) nt = 1;
+    for (int k = 0; k <= kUploadChunks; ++k) bound[k] = s_split * k / kUploadChunks;   // checkerboard indices
+    // small lattices pack on the calling thread, chunk by chunk
+    PackPool* pool = h->g.V < 65536 ? nullptr : &PackPool::get();
+    const unsigned nt = pool ? pool->size() : 1;
     std::atomic<int> done[kUploadChunks];
     for (auto& d : done) d.store(0);
     float* dst = static_cast<float*>(h->h_stage);
-    std::vector<std::thread> pool;
     const lt::Geom g = h->g;
     // sites 2s and 2s + 1 share checkerboard index s (the z extent is even), so chunk k of
     // checkerboard indices is the contiguous site range [2 bound[k], 2 bound[k+1])
-    for (unsigned t = 0; t < nt; ++t)
-        pool.emplace_back([&, t] {
-            for (int k = 0; k < kUploadChunks; ++k)
-            {
-                // whole site pairs per thread: pair range [bound[k], bound[k+1]) split evenly
-                const long long n = bound[k + 1] - bound[k];
-                const long long a = bound[k] + n * t / nt, b = bound[k] + n * (t + 1) / nt;
-                pack_sites(g, nr, links, dst, 2 * a, 2 * b);
-                done[k].fetch_add(1, std::memory_order_release);
-            }
+    auto pack_chunk = [&](unsigned t, int k) {
+        // whole site pairs per thread: pair range [bound[k], bound[k+1]) split evenly
+        const long long n = bound[k + 1] - bound[k];
+        const long long a = bound[k] + n * t / nt, b = bound[k] + n * (t + 1) / nt;
+        pack_sites(g, nr, links, dst, 2 * a, 2 * b);
+        done[k].fetch_add(1, std::memory_order_release);
+    };
+    if (pool)
+        pool->start([&](unsigned t) {
+            for (int k = 0; k < kUploadChunks; ++k) pack_chunk(t, k);
         });
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < kUploadChunks; ++k)
     {
+        if (!pool) pack_chunk(0, k);
         while (done[k].load(std::memory_order_acquire) < (int)nt) std::this_thread::yield();
         const size_t off = (size_t)bound[k] * elem, width = (size_t)(bound[k + 1] - bound[k]) * elem;
         if (e == cudaSuccess && width)
@@ -624,7 +765,7 @@ int upload_packed_fp32(lt_lattice* h, const double* links)
                                   reinterpret_cast<const char*>(dst) + off, (size_t)vh * elem, width, planes,
                                   cudaMemcpyHostToDevice, h->stream);
     }
-    for (auto& th : pool) th.join();
+    if (pool) pool->wait();
     if (e != cudaSuccess) return lt::cuda_error(e, "lt_upload_links: copy");
     LT_CK(cudaStreamSynchronize(h->stream));
     return LT_OK;

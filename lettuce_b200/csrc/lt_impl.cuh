@@ -86,9 +86,12 @@ public:
     size_t full_bytes(const Geom& g) const override { return (size_t)4 * g.V * 9 * sizeof(cx<T>); }
     size_t clov_bytes(const Geom& g) const override { return (size_t)6 * g.V * 9 * sizeof(T); }
 
-    void from_aos(const Ctx& c, void* U, const double* aos) const override
+    void from_aos(const Ctx& c, void* U, const double* aos) const override { from_aos_sites(c, U, aos, 0, c.g.V); }
+    void from_aos_sites(const Ctx& c, void* U, const double* aos, long long i0, long long i1) const override
     {
-        k_from_aos<T, NR><<<nblocks(4LL * c.g.V, 256), 256, 0, c.stream>>>(gauge(U, c.g), c.g, aos);
+        if (i1 <= i0) return;
+        k_from_aos<T, NR><<<nblocks(4LL * (i1 - i0), 256), 256, 0, c.stream>>>(gauge(U, c.g), c.g, aos, (int)(4 * i0),
+                                                                              (int)(4 * i1));
     }
     void to_aos(const Ctx& c, const void* U, double* aos) const override
     {

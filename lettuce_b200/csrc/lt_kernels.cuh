@@ -334,11 +334,12 @@ template <typename T, int NR> LT_D M3<T> exp_update(const M3<T>& X, T c, const M
 }
 
 // ---------------------------------------------------------------- layout conversion
+// reference links [l0, l1) (link index site*4+mu) of the AoS field at aos into U
 template <typename T, int NR>
-__global__ void k_from_aos(Gauge<T, NR> U, Geom g, const double* __restrict__ aos)
+__global__ void k_from_aos(Gauge<T, NR> U, Geom g, const double* __restrict__ aos, int l0, int l1)
 {
-    int l = blockIdx.x * blockDim.x + threadIdx.x;   // reference link index site*4+mu
-    if (l >= 4 * g.V) return;
+    int l = l0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= l1) return;
     int i = l >> 2, mu = l & 3;
     int c[4];
     int r = i;

@@ -65,6 +65,27 @@ class TestContainer:
             G.upload(U)            # packed on the host
             assert np.array_equal(G.download(), fresh[k % 2]), k
 
+    @pytest.mark.parametrize("ext", [(16, 16, 16, 16), (16, 8, 18, 32)])
+    def test_repeated_upload_from_pinned_memory_splits_identically(self, ext):
+        """From pinned host memory the repeated upload sends the last quarter of the sites as
+        FP64 over PCIe (converted on the device) while the host threads pack the rest; the
+        stored field is again bit for bit the device conversion's."""
+        import torch
+        U1, U2 = lt.haar_links(ext, 73), lt.haar_links(ext, 74)
+        pinned = torch.empty(U1.size, dtype=torch.float64, pin_memory=True)
+        host = pinned.numpy().reshape(U1.shape)
+        fresh = []
+        for U in (U1, U2):
+            F = lt.GaugeField(ext, "fp32_12")
+            F.upload(U)
+            fresh.append(F.download())
+        G = lt.GaugeField(ext, "fp32_12")
+        G.upload(U1)
+        for k, U in enumerate((U1, U2, U1)):
+            host[...] = U
+            G.upload(host)
+            assert np.array_equal(G.download(), fresh[k % 2]), k
+
     def test_identity_and_copy_swap(self, golden4):
         ext = golden4["ext"]
         A, B = gpu(ext, golden4["U"]), lt.GaugeField(ext)
