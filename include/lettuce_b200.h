@@ -61,6 +61,10 @@ int lt_get_extents(const lt_lattice* h, int ext[4], int* prec);
  * lattice.hpp:113-136). */
 int lt_upload_links(lt_lattice* h, const double* links);
 int lt_download_links(lt_lattice* h, double* links);
+/* The bytes the next lt_upload_links(h, links) copies host to device (no counterpart in the
+ * reference): the FP64 field, or for a two-row FP32 handle uploaded before the packed field,
+ * with a share of the sites as FP64 when links is pinned host memory. */
+int lt_upload_bytes(const lt_lattice* h, const double* links, uint64_t* h2d_bytes);
 /* One link: GaugeField4D::operator()(link_coord) (lattice.hpp:113-136); site index as in
  * the reference layout, m = 18 doubles (row-major 3x3, re/im interleaved). */
 int lt_set_link(lt_lattice* h, int64_t site, int mu, const double* m);

@@ -33,6 +33,7 @@ SIGNATURES = {
     "lt_get_extents": (_i, [_vp, _ip, _pi]),
     "lt_upload_links": (_i, [_vp, _dp]),
     "lt_download_links": (_i, [_vp, _dp]),
+    "lt_upload_bytes": (_i, [_vp, _dp, _pu64]),
     "lt_set_link": (_i, [_vp, C.c_int64, _i, _dp]),
     "lt_get_link": (_i, [_vp, C.c_int64, _i, _dp]),
     "lt_copy": (_i, [_vp, _vp]),

@@ -70,6 +70,13 @@ class GaugeField:
             raise ValueError("link array has the wrong size")
         check(lib().lt_upload_links(self._h, a.reshape(-1)))
 
+    def upload_bytes(self, links: np.ndarray) -> int:
+        """Bytes the next upload(links) copies host to device (lt_upload_bytes)."""
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        n = C.c_uint64()
+        check(lib().lt_upload_bytes(self._h, a.reshape(-1), C.byref(n)))
+        return int(n.value)
+
     def download(self) -> np.ndarray:
         out = np.empty((self.Volume(), 4, 3, 3, 2))
         check(lib().lt_download_links(self._h, out.reshape(-1)))

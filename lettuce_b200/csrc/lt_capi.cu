@@ -704,6 +704,17 @@ private:
     unsigned n_ = 1;
 };
 
+// From pinned input, the sites of the checkerboard indices [pack_split, vh) cross PCIe as FP64
+// straight from the caller's buffer and are converted on the device, while the host threads
+// pack the rest: the copy engine and the host cores then share the field
+long long pack_split(const lt_lattice* h, const double* links)
+{
+    cudaPointerAttributes attr;
+    const bool pinned = cudaPointerGetAttributes(&attr, links) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+    (void)cudaGetLastError();   // an unregistered pointer may leave an error behind on old drivers
+    return pinned && h->g.V >= 65536 ? (long long)(h->g.vh * kPackShare) : h->g.vh;
+}
+
 int upload_packed_fp32(lt_lattice* h, const double* links)
 {
     std::lock_guard<std::mutex> pack_lock(g_pack_mutex);
@@ -715,14 +726,7 @@ int upload_packed_fp32(lt_lattice* h, const double* links)
     // the staging buffers may still feed a copy of an earlier call on this stream
     LT_CK(cudaStreamSynchronize(h->stream));
     const long long vh = h->g.vh;
-    // From pinned input, the sites of the checkerboard indices [s_split, vh) cross PCIe as
-    // FP64 straight from the caller's buffer and are converted on the device, while the host
-    // threads pack the rest: the copy engine and the host cores then share the field
-    long long s_split = vh;
-    cudaPointerAttributes attr;
-    if (h->g.V >= 65536 && cudaPointerGetAttributes(&attr, links) == cudaSuccess && attr.type == cudaMemoryTypeHost)
-        s_split = (long long)(vh * kPackShare);
-    (void)cudaGetLastError();   // an unregistered pointer may leave an error behind on old drivers
+    const long long s_split = pack_split(h, links);
     if (s_split < vh)
     {
         LT_TRY(ensure_aos(h));
@@ -870,6 +874,22 @@ int lt_upload_links(lt_lattice* h, const double* links)
     h->be->from_aos(h->ctx(), h->U, h->d_aos);
     LT_TRY(launched("lt_upload_links"));
     LT_CK(cudaStreamSynchronize(h->stream));
+    return LT_OK;
+}
+
+int lt_upload_bytes(const lt_lattice* h, const double* links, uint64_t* h2d_bytes)
+{
+    LT_TRY(check_h(h, "lt_upload_bytes"));
+    if (!links || !h2d_bytes) return lt::set_error(LT_ERR_ARG, "lt_upload_bytes: null pointer");
+    const lt::DeviceScope device_scope(h->device);
+    const uint64_t V = (uint64_t)h->g.V;
+    if (h->prec == LT_PREC_FP32_12 && h->uploads > 0)
+    {
+        const uint64_t s_split = (uint64_t)pack_split(h, links);
+        *h2d_bytes = s_split * 24 * 16 + (V - 2 * s_split) * 72 * sizeof(double);
+    }
+    else
+        *h2d_bytes = V * 72 * sizeof(double);
     return LT_OK;
 }
 

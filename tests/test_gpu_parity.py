@@ -67,7 +67,7 @@ class TestContainer:
 
     @pytest.mark.parametrize("ext", [(16, 16, 16, 16), (16, 8, 18, 32)])
     def test_repeated_upload_from_pinned_memory_splits_identically(self, ext):
-        """From pinned host memory the repeated upload sends the last quarter of the sites as
+        """From pinned host memory the repeated upload sends a share of the sites (the last) as
         FP64 over PCIe (converted on the device) while the host threads pack the rest; the
         stored field is again bit for bit the device conversion's."""
         import torch
@@ -80,7 +80,12 @@ class TestContainer:
             F.upload(U)
             fresh.append(F.download())
         G = lt.GaugeField(ext, "fp32_12")
+        V = int(np.prod(ext))
+        assert G.upload_bytes(host) == V * 576            # first upload: the FP64 field
         G.upload(U1)
+        assert G.upload_bytes(U1) == V * 4 * 48           # pageable: packed whole
+        split = G.upload_bytes(host)
+        assert V * 4 * 48 < split < V * 576               # pinned: partly FP64
         for k, U in enumerate((U1, U2, U1)):
             host[...] = U
             G.upload(host)
