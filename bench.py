@@ -215,6 +215,17 @@ class CpuReference:
     def threads(self) -> int:
         return int(self.lib.ref_threads())
 
+    def metad_force_rate(self, links, n: int) -> float:
+        """Force evaluations/s of the reference's HMCMetaDKernel::CalculateTopologicalForce
+        (4 stout levels of rho = 0.12, a linear bias) over n timed calls after one untimed."""
+        import ctypes as C
+        import numpy as np
+        f = self.lib.ref_metad_force_seconds
+        f.restype = C.c_double
+        f.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        return n / f(a.ctypes.data, 0.12, 1.0, n)
+
 
 def cpu_reference_sample(size: int, links, n_round: int, n_flow: int):
     """A bounded sample of the reference CPU path: n_round steps (1 HB + 4 OR sweeps) and
@@ -620,7 +631,9 @@ def main():
         therm = G.download()
         res = {}
         n_flow = 10
-        for prec in (a.prec, "fp64"):
+        # the bulk storage, the 18-real FP32 storage beside two-row links, and plain FP64
+        precs = [a.prec] + (["fp32"] if a.prec == "fp32_12" else []) + ["fp64"]
+        for prec in precs:
             A, B = lt.GaugeField(ext, prec), lt.GaugeField(ext, prec)
             A.upload(therm)
             flow = lt.GradientFlowKernel(A, B, lt.RK3, None, FLOW_EPS)
@@ -660,6 +673,15 @@ def main():
                                 "start": f"{N_THERM} further rounds after the timed steps"}
         line["dP_flow_max"] = max(dP)
         line["dQ_flow_max"] = max(dQ)
+        if "fp32" in res and a.prec != "fp32":
+            r18 = res["fp32"]
+            line["fp32_18"] = {
+                "link_updates_per_s": r18["link_updates_per_s"], "flow_steps_per_s": r18["flow_steps_per_s"],
+                "sweep_roofline": r18["sweep_roofline"],
+                "over_fp64": {"link_updates": r18["link_updates_per_s"] / res["fp64"]["link_updates_per_s"],
+                              "flow_steps": r18["flow_steps_per_s"] / res["fp64"]["flow_steps_per_s"]},
+                "dP_vs_fp64": max(abs(x - y) for x, y in zip(r18["plaq"], res["fp64"]["plaq"])),
+                "dQ_vs_fp64": max(abs(x - y) for x, y in zip(r18["Q"], res["fp64"]["Q"]))}
         # the error against the FP64 oracle: the FP64 GPU flow is pinned to the reference's own
         # FP64 flow within 1e-10 in Q and 1e-12 in P over 400 steps at 32^4
         # (tests/test_gpu_large.py::TestFlowToFour::test_fp64), so the FP32-vs-FP64 differences
@@ -739,6 +761,19 @@ def main():
                     "fp64_link_updates": line["fp64"]["link_updates_per_s"] / cb["value"],
                     "bulk_flow_steps": line["flow_steps_per_s"] / cb["flow_steps_per_s"],
                     "fp64_flow_steps": line["fp64"]["flow_steps_per_s"] / cb["flow_steps_per_s"]}
+            # the MetaD force at 16^4 on the reference's code (3 evaluations, about 3 s on 16 cores)
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            from ltref import haar_links_numpy as _haar
+            try:
+                ref16 = CpuReference(16)
+            except (FileNotFoundError, OSError):
+                ref16 = None
+            if ref16 is not None and hasattr(ref16.lib, "ref_metad_force_seconds"):
+                cpu_force = ref16.metad_force_rate(_haar((16,) * 4, SEED), 3)
+                line["cpu_baseline"]["metad_force_evals_per_s_16^4"] = cpu_force
+                gpu_force = line.get("secondary", {}).get("metad_force_evals_per_s_16^4")
+                if gpu_force and "gpu_over_cpu" in line:
+                    line["gpu_over_cpu"]["metad_force"] = gpu_force / cpu_force
 
     if rank == 0:
         print(json.dumps(line, default=_jsonable))

@@ -446,6 +446,29 @@ double ref_metad_force(const double* links, double rho, double slope, double* ou
     return TopChargeClover(data->Clover);
 }
 
+// Wall-clock seconds of n calls of HMCMetaDKernel::CalculateTopologicalForce (the reference's
+// MetaD force, hmc_metadynamics.hpp:374-436) on the given links, after one untimed call; the
+// kernel, its fields and the bias are set up once outside the timed region.  For the CPU
+// baseline of the force evaluations/s.
+double ref_metad_force_seconds(const double* links, double rho, double slope, int n)
+{
+    auto U  = std::make_unique<GaugeField>();
+    auto Uc = std::make_unique<GaugeField>();
+    auto P  = std::make_unique<GaugeField>();
+    load(*U, links);
+    auto bias = linear_bias(slope);
+    auto data = std::make_unique<GaugeUpdates::HMCMetaDData>(n_smear_meta);
+    Integrators::HMC::OMF_2 omf2;
+    RunStatistics stats;
+    std::string log_path {"/dev/null"};
+    GaugeUpdates::HMCMetaDKernel kern(*U, *Uc, *P, *bias, *data, omf2, GaugeAction::WilsonAction, prng(), stats,
+                                      std::cout, log_path, 1.0, rho);
+    kern.CalculateTopologicalForce(false);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int k = 0; k < n; ++k) kern.CalculateTopologicalForce(false);
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 int ref_n_smear_meta()
 {
     return n_smear_meta;
