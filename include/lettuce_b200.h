@@ -391,6 +391,12 @@ int lt_su3_exp_test(const double* q_in, double* out, int n, int prec, int path);
 /* binaryVersion and ptxVersion (cudaFuncGetAttributes) of the library's kernels on the
  * current device: 100 for code built for sm_100a. */
 int lt_device_arch(int* binary_version, int* ptx_version);
+/* The host packing of lt_upload_links for two-row FP32 storage, on the calling thread and
+ * without a device: links (reference layout, V = ext[0] ext[1] ext[2] ext[3] sites) rounded to
+ * FP32 and written to out (48 V floats, 16-byte aligned) in the device layout of the two-row
+ * storage: chunk c (0..2) of plane (mu, parity) at ((mu * 2 + parity) * 3 + c) * V/2 float4s,
+ * checkerboard index s = site / 2, floats 4c .. 4c + 3 of the link's rows 0-1. */
+int lt_pack_links_test(const int ext[4], const double* links, float* out);
 
 /* ---- bias potential: MetaBiasPotential (actions/bias_potential/metadynamics.hpp:29-507) -- */
 /* Constructor (:60-91); fails with LT_ERR_ARG where the reference throws (:70-77). */

@@ -59,6 +59,7 @@ SIGNATURES = {
     "lt_plaquette_sum_noalloc": (_i, [_vp, _ip, _vp, _vp]),
     "lt_su3_exp_test": (_i, [_dp, _dp, _i, _i, _i]),
     "lt_device_arch": (_i, [_pi, _pi]),
+    "lt_pack_links_test": (_i, [_ip, _dp, C.POINTER(C.c_float)]),
     "lt_overrelax_sweeps": (_i, [_vp, _i]),
     "lt_heatbath_sweeps": (_i, [_vp, _d, _i, _u64, _pu64]),
     "lt_update_sweeps": (_i, [_vp, _d, _i, _i, _i, _u64, _pu64]),

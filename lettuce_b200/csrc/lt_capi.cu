@@ -927,6 +927,22 @@ int lt_upload_bytes(const lt_lattice* h, const double* links, uint64_t* h2d_byte
     return LT_OK;
 }
 
+int lt_pack_links_test(const int ext[4], const double* links, float* out)
+{
+    if (!ext || !links || !out) return lt::set_error(LT_ERR_ARG, "lt_pack_links_test: null pointer");
+    if (reinterpret_cast<uintptr_t>(out) % 16) return lt::set_error(LT_ERR_ARG, "lt_pack_links_test: out not 16-byte aligned");
+    long long V = 1;
+    for (int d = 0; d < 4; ++d)
+    {
+        if (ext[d] < 2 || ext[d] % 2) return lt::set_error(LT_ERR_ARG, "lt_pack_links_test: extents must be even and >= 2");
+        V *= ext[d];
+        if (V * 4 * 9 >= (1LL << 31)) return lt::set_error(LT_ERR_ARG, "lt_pack_links_test: lattice too large");
+    }
+    const lt::Geom g = lt::make_geom(ext);
+    pack_sites(g, 2, links, out, 0, g.V);
+    return LT_OK;
+}
+
 int lt_download_links(lt_lattice* h, double* links)
 {
     LT_TRY(check_h(h, "lt_download_links"));
