@@ -132,11 +132,6 @@ public:
                               void* Tloc, double rho, const void* st_in) const = 0;
     virtual void stout_recursion(const Ctx& c, const void* U, const void* Lam, const void* Tloc, void* Sigma,
                                  double rho) const = 0;
-    // the fused seams of the force chain (k_clover_deriv_lambda, k_stout_recursion_lambda)
-    virtual void clover_deriv_lambda(const Ctx& c, const void* Utop, const void* R, double scale, const void* U,
-                                     void* LamOut, void* Tloc, const void* St, double rho) const = 0;
-    virtual void stout_recursion_lambda(const Ctx& c, const void* U, const void* LamIn, void* Tloc, double rho,
-                                        const void* Uprev, void* LamOut, const void* St) const = 0;
 };
 
 const Backend* backend_fp64();

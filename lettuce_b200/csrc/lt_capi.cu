@@ -207,13 +207,6 @@ int charge_from_R(lt_lattice* h, double* q)
     return LT_OK;
 }
 
-// 0: every kernel of the chain separate; 1: the clover derivative fused with the top Lambda;
-// 2: also every recursion fused with the next Lambda
-#ifndef LT_FUSE_FORCE_CHAIN
-#define LT_FUSE_FORCE_CHAIN 2
-#endif
-constexpr int kFuseForceChain = LT_FUSE_FORCE_CHAIN;
-
 int metad_backward(lt_lattice* h, double rho, int n_stout, double dvdq, bool have_R = false)
 {
     LT_TRY(ensure(h, &h->F, h->be->alg_bytes(h->g)));
@@ -222,39 +215,12 @@ int metad_backward(lt_lattice* h, double rho, int n_stout, double dvdq, bool hav
     if (!have_R) LT_TRY(metad_clover(h, n_stout));
     const lt::Ctx c = h->ctx();
     const void* top = level(h, n_stout);
-    if (n_stout == 0 || kFuseForceChain == 0)
+    h->be->clover_deriv(c, top, h->R, h->F, dvdq);
+    for (int k = n_stout; k > 0; --k)
     {
-        h->be->clover_deriv(c, top, h->R, h->F, dvdq);
-        for (int k = n_stout; k > 0; --k)
-        {
-            h->be->stout_lambda(c, level(h, k - 1), level(h, k), h->F, h->Lam, h->Tloc, rho, h->staples[k - 1]);
-            h->be->stout_recursion(c, level(h, k - 1), h->Lam, h->Tloc, h->F, rho);
-        }
-        return launched("metad_backward");
+        h->be->stout_lambda(c, level(h, k - 1), level(h, k), h->F, h->Lam, h->Tloc, rho, h->staples[k - 1]);
+        h->be->stout_recursion(c, level(h, k - 1), h->Lam, h->Tloc, h->F, rho);
     }
-    // the same chain with each Lambda computed by the kernel that produces its Sigma: n + 1
-    // launches instead of 2n + 1; Lambda alternates between two buffers, since a recursion
-    // reads the Lambda of the step above at neighbouring links while writing its own
-    LT_TRY(ensure(h, &h->Lam2, h->be->alg_bytes(h->g)));
-    void* lam_in = h->Lam;
-    void* lam_out = h->Lam2;
-    h->be->clover_deriv_lambda(c, top, h->R, dvdq, level(h, n_stout - 1), lam_in, h->Tloc, h->staples[n_stout - 1],
-                               rho);
-    for (int k = n_stout; k > 1; --k)
-    {
-        if (kFuseForceChain == 2)
-        {
-            h->be->stout_recursion_lambda(c, level(h, k - 1), lam_in, h->Tloc, rho, level(h, k - 2), lam_out,
-                                          h->staples[k - 2]);
-            std::swap(lam_in, lam_out);
-        }
-        else
-        {
-            h->be->stout_recursion(c, level(h, k - 1), lam_in, h->Tloc, h->F, rho);
-            h->be->stout_lambda(c, level(h, k - 2), level(h, k - 1), h->F, lam_in, h->Tloc, rho, h->staples[k - 2]);
-        }
-    }
-    h->be->stout_recursion(c, level(h, 0), lam_in, h->Tloc, h->F, rho);
     return launched("metad_backward");
 }
 
@@ -872,7 +838,7 @@ int lt_destroy(lt_lattice* h)
     const lt::DeviceScope device_scope(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = { h->U,   h->U2,   h->Z,        h->P,       h->F,     h->Ubak,   h->R,      h->chainA,
-                     h->Lam, h->Lam2, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB, h->Xz,
+                     h->Lam, h->Tloc, h->partials, h->results, h->d_aos, h->status, h->chainB, h->Xz,
                      h->tensor };
     for (void* p : bufs)
         if (p) cudaFree(p);

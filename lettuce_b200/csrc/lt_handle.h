@@ -57,7 +57,6 @@ struct lt_lattice
     void* Ubak = nullptr;    // HMC backup of the links
     void* R = nullptr;       // clover planes
     void* Lam = nullptr;     // Lambda (algebra)
-    void* Lam2 = nullptr;    // Lambda of the next stout step down in the fused force chain
     void* Tloc = nullptr;    // link-local recursion term (full matrix)
     std::vector<void*> levels;   // smeared levels 1..n of the MetaD chain
     std::vector<void*> staples;  // the staples of levels 0..n-1 (full 3x3 per link), for the adjoint

@@ -430,20 +430,6 @@ public:
         launch_chained(k_stout_recursion<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
                        gauge(U, c.g), alg(Lam, c.g), full(Tloc, c.g), alg(Sigma, c.g), c.g, (T)rho);
     }
-    void clover_deriv_lambda(const Ctx& c, const void* Utop, const void* R, double scale, const void* U, void* LamOut,
-                             void* Tloc, const void* St, double rho) const override
-    {
-        launch_chained(k_clover_deriv_lambda<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
-                       gauge(Utop, c.g), clov(R, c.g), c.g, (T)scale, gauge(U, c.g), alg(LamOut, c.g),
-                       full(Tloc, c.g), full(St, c.g), (T)rho);
-    }
-    void stout_recursion_lambda(const Ctx& c, const void* U, const void* LamIn, void* Tloc, double rho,
-                                const void* Uprev, void* LamOut, const void* St) const override
-    {
-        launch_chained(k_stout_recursion_lambda<T, NR>, nblocks(c.g.V, kSitesPerBlock), 4 * kSitesPerBlock, c.stream,
-                       gauge(U, c.g), alg(LamIn, c.g), full(Tloc, c.g), c.g, (T)rho, gauge(Uprev, c.g),
-                       alg(LamOut, c.g), full(St, c.g));
-    }
 };
 
 } // namespace lt

@@ -2224,11 +2224,16 @@ template <typename T> struct CloverDerivMinBlocks
 {
     static constexpr int value = sizeof(T) == 4 ? 3 : 1;
 };
-// Sigma of the link (mu, x) (checkerboard index s of parity par, site i, coordinates c)
 template <typename T, int NR>
-LT_D A8<T> clover_deriv_link(const Gauge<T, NR>& U, const Clov<T>& R, const Geom& g, int mu, int par, int s, int i,
-                             const int c[4], T scale)
+__global__ void __launch_bounds__(kThreads, CloverDerivMinBlocks<T>::value) k_clover_deriv(Gauge<T, NR> U, Clov<T> R, Alg<T> out, Geom g, T scale)
 {
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
     // the three epsilon-tensor terms of direction mu: nu = the k-th other direction, (rho,
     // sigma) the remaining two in ascending order, sign = parity of (mu, nu, rho, sigma)
     const int o0 = mu == 0 ? 1 : 0, o1 = mu <= 1 ? 2 : 1, o2 = mu <= 2 ? 3 : 2;
@@ -2246,20 +2251,7 @@ LT_D A8<T> clover_deriv_link(const Gauge<T, NR>& U, const Clov<T>& R, const Geom
     const T pref = (T)(-2.0 / (512.0 * kPi * kPi)) * scale;
 #pragma unroll
     for (int k = 0; k < 8; ++k) a.a[k] *= pref;
-    return a;
-}
-
-template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, CloverDerivMinBlocks<T>::value) k_clover_deriv(Gauge<T, NR> U, Clov<T> R, Alg<T> out, Geom g, T scale)
-{
-    pdl_release();
-    pdl_wait();
-    int mu, x;
-    if (!link_of_thread(g, mu, x)) return;
-    const int par = x >= g.vh, s = x - par * g.vh;
-    int c[4];
-    const int i = site_coords(g, par, s, c);
-    out.st(mu, par, s, clover_deriv_link(U, R, g, mu, par, s, i, c, scale));
+    out.st(mu, par, s, a);
 }
 
 // First half of StoutForceRecursion (smearing/stout_smearing.hpp:152-175) with CalculateLambda
@@ -2281,10 +2273,10 @@ template <typename T> struct LambdaMinBlocks
 // First half of StoutForceRecursion for the link (mu, x) given its level-(k-1) link u and
 // staple st: Lambda (written) and the link-local term Tloc (written)
 template <typename T, int NR>
-LT_D void stout_lambda_core(const Gauge<T, NR>& Up, const A8<T>& sigma, const Alg<T>& Lam, const Full<T>& Tloc,
+LT_D void stout_lambda_core(const Gauge<T, NR>& Up, const Alg<T>& Sigma, const Alg<T>& Lam, const Full<T>& Tloc,
                             T rho, int mu, int par, int s, const M3<T>& u, const M3<T>& st)
 {
-    M3<T> sp = mul_dn(Up.ld(mu, par, s), unpack_ah(sigma));
+    M3<T> sp = mul_dn(Up.ld(mu, par, s), unpack_ah(Sigma.ld(mu, par, s)));
     // Q = -i rho C with C = Algebra(st U^dag), packed as a Hermitian matrix (real diagonal):
     // for C = unpack_ah(c), Q = unpack_h(rho (c0, c1, c3, -c2, c5, -c4, c7, -c6))
     const A8<T> c8 = algebra8(mul_nd(st, u));
@@ -2370,7 +2362,7 @@ __global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_l
     int par = x >= g.vh, s = x - par * g.vh;
     int c[4];
     int i = site_coords(g, par, s, c);
-    stout_lambda_core(Up, Sigma.ld(mu, par, s), Lam, Tloc, rho, mu, par, s, U.ld(mu, par, s), staple(U, g, par, i, c, mu));
+    stout_lambda_core(Up, Sigma, Lam, Tloc, rho, mu, par, s, U.ld(mu, par, s), staple(U, g, par, i, c, mu));
 }
 
 // k_stout_lambda with the staple stored by the forward stout step of the level (St)
@@ -2383,7 +2375,7 @@ __global__ void __launch_bounds__(kThreads, LambdaMinBlocks<T>::value) k_stout_l
     int mu, x;
     if (!link_of_thread(g, mu, x)) return;
     const int par = x >= g.vh, s = x - par * g.vh;
-    stout_lambda_core(Up, Sigma.ld(mu, par, s), Lam, Tloc, rho, mu, par, s, U.ld(mu, par, s), St.ld(mu, par, s));
+    stout_lambda_core(Up, Sigma, Lam, Tloc, rho, mu, par, s, U.ld(mu, par, s), St.ld(mu, par, s));
 }
 
 // k_stout_lambda on two-row FP32 storage with the staged staple
@@ -2402,15 +2394,22 @@ __global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_LAMBDA_F32)
     const int i = site_coords(g, par, s, c);
     M3<float> u;
     const M3<float> st = staple_staged<true>(ring, U, g, par, i, s, c, mu, u);
-    stout_lambda_core(Up, Sigma.ld(mu, par, s), Lam, Tloc, rho, mu, par, s, u, st);
+    stout_lambda_core(Up, Sigma, Lam, Tloc, rho, mu, par, s, u, st);
 }
 
 // Second half of StoutForceRecursion (smearing/stout_smearing.hpp:177-230):
 // Sigma_{k-1} = Algebra(U (Tloc - i rho sum_{nu != mu} [six-term neighbour sum of U and Lambda]))
 template <typename T, int NR>
-LT_D A8<T> stout_recursion_link(const Gauge<T, NR>& U, const Alg<T>& Lam, const Full<T>& Tloc, const Geom& g, T rho,
-                                int mu, int par, int s, int i, const int c[4])
+__global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Alg<T> Lam, Full<T> Tloc, Alg<T> Sigma,
+                                                              Geom g, T rho)
 {
+    pdl_release();
+    pdl_wait();
+    int mu, x;
+    if (!link_of_thread(g, mu, x)) return;
+    int par = x >= g.vh, s = x - par * g.vh;
+    int c[4];
+    int i = site_coords(g, par, s, c);
     const int op = par ^ 1;
     const int dmu = step_up_rt(g, mu, c);
     const int imu = i + dmu;
@@ -2440,71 +2439,7 @@ LT_D A8<T> stout_recursion_link(const Gauge<T, NR>& U, const Alg<T>& Lam, const 
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b) loc.e[a][b] = loc.e[a][b] - rho * timesi(fs.e[a][b]);
-    return algebra8(mul(U.ld(mu, par, s), loc));
-}
-
-template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads) k_stout_recursion(Gauge<T, NR> U, Alg<T> Lam, Full<T> Tloc, Alg<T> Sigma,
-                                                              Geom g, T rho)
-{
-    pdl_release();
-    pdl_wait();
-    int mu, x;
-    if (!link_of_thread(g, mu, x)) return;
-    const int par = x >= g.vh, s = x - par * g.vh;
-    int c[4];
-    const int i = site_coords(g, par, s, c);
-    Sigma.st(mu, par, s, stout_recursion_link(U, Lam, Tloc, g, rho, mu, par, s, i, c));
-}
-
-// The force chain fused at its link-local seams: Lambda and Tloc of a stout step need Sigma of
-// their own link only, so the kernel that produces that Sigma (the clover derivative of the
-// most smeared level, or the force recursion of the step above) goes straight on to them for
-// the same link, Sigma staying in registers.  Lambda of the step is written to LamOut (the
-// recursion still reads the step above's Lambda at neighbouring links from LamIn); Tloc is read
-// and then overwritten by the same thread.
-#ifndef LT_MINB_FUSED_F32
-#define LT_MINB_FUSED_F32 3
-#endif
-template <typename T> struct FusedMinBlocks
-{
-    static constexpr int value = sizeof(T) == 4 ? LT_MINB_FUSED_F32 : 1;
-};
-
-// k_clover_deriv of level n (Utop) and k_stout_lambda_st of stout step n (U = level n-1, its
-// staple St)
-template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, FusedMinBlocks<T>::value)
-    k_clover_deriv_lambda(Gauge<T, NR> Utop, Clov<T> R, Geom g, T scale, Gauge<T, NR> U, Alg<T> LamOut,
-                          Full<T> Tloc, Full<T> St, T rho)
-{
-    pdl_release();
-    pdl_wait();
-    int mu, x;
-    if (!link_of_thread(g, mu, x)) return;
-    const int par = x >= g.vh, s = x - par * g.vh;
-    int c[4];
-    const int i = site_coords(g, par, s, c);
-    const A8<T> sigma = clover_deriv_link(Utop, R, g, mu, par, s, i, c, scale);
-    stout_lambda_core(Utop, sigma, LamOut, Tloc, rho, mu, par, s, U.ld(mu, par, s), St.ld(mu, par, s));
-}
-
-// k_stout_recursion of stout step k (U = level k-1) and k_stout_lambda_st of step k-1
-// (Uprev = level k-2, its staple St)
-template <typename T, int NR>
-__global__ void __launch_bounds__(kThreads, FusedMinBlocks<T>::value)
-    k_stout_recursion_lambda(Gauge<T, NR> U, Alg<T> LamIn, Full<T> Tloc, Geom g, T rho, Gauge<T, NR> Uprev,
-                             Alg<T> LamOut, Full<T> St)
-{
-    pdl_release();
-    pdl_wait();
-    int mu, x;
-    if (!link_of_thread(g, mu, x)) return;
-    const int par = x >= g.vh, s = x - par * g.vh;
-    int c[4];
-    const int i = site_coords(g, par, s, c);
-    const A8<T> sigma = stout_recursion_link(U, LamIn, Tloc, g, rho, mu, par, s, i, c);
-    stout_lambda_core(U, sigma, LamOut, Tloc, rho, mu, par, s, Uprev.ld(mu, par, s), St.ld(mu, par, s));
+    Sigma.st(mu, par, s, algebra8(mul(U.ld(mu, par, s), loc)));
 }
 
 } // namespace lt
