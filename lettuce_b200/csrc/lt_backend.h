@@ -108,7 +108,7 @@ public:
     // lattices described by the device array desc (LatDesc[n_lat]); sel picks 64/128/256
     // threads per block and n_blocks is the batch's block count for that size.
     virtual void batch_sweep(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int sel, int op, int mu,
-                             int par, const uint64_t* counter, int max_iter) const = 0;
+                             int par, const uint64_t* counter, int max_iter, int flip) const = 0;
 
     // FullTensor4D of CalculateClover<1, 1> in the reference layout (FP64, device memory,
     // zeroed by the caller); Q sum of a tensor into results[slot] (unnormalised)

@@ -106,15 +106,24 @@ int join_out(lt_ensemble* e)
 // the reference's (mu, parity) order (iterators/iterators.hpp:65-87); reverse = the whole
 // sequence backwards (with the single-sub-sweep updates being reversible, the even mixture
 // of a round and its reverse is a reversible Markov step).
+#ifndef LT_BATCH_FLIP
+#define LT_BATCH_FLIP 1
+#endif
+constexpr bool kBatchFlip = LT_BATCH_FLIP;
+
 void enqueue_round(lt_ensemble* e, cudaStream_t s, int n_hb, int n_or, int reverse, int sel_hb, int sel_or,
                    const uint64_t* counter)
 {
     const int n = (int)e->lats.size();
+    // consecutive launches take the work units in ascending and descending order in turn
+    int launch = 0;
+    auto flip = [&] { return kBatchFlip ? (launch++ & 1) : 0; };
     auto hb_sweep = [&](bool rev) {
         for (int q = 0; q < 8; ++q)
         {
             const int idx = rev ? 7 - q : q;
-            e->be->batch_sweep(s, e->d_desc, n, e->n_blocks[sel_hb], sel_hb, 0, idx >> 1, idx & 1, counter, 10);
+            e->be->batch_sweep(s, e->d_desc, n, e->n_blocks[sel_hb], sel_hb, 0, idx >> 1, idx & 1, counter, 10,
+                               flip());
         }
         lt::k_counter_add<<<1, 32, 0, s>>>(const_cast<uint64_t*>(counter), 1);
     };
@@ -122,7 +131,8 @@ void enqueue_round(lt_ensemble* e, cudaStream_t s, int n_hb, int n_or, int rever
         for (int q = 0; q < 8; ++q)
         {
             const int idx = rev ? 7 - q : q;
-            e->be->batch_sweep(s, e->d_desc, n, e->n_blocks[sel_or], sel_or, 1, idx >> 1, idx & 1, counter, 10);
+            e->be->batch_sweep(s, e->d_desc, n, e->n_blocks[sel_or], sel_or, 1, idx >> 1, idx & 1, counter, 10,
+                               flip());
         }
     };
     if (!reverse)
@@ -338,11 +348,11 @@ int lt_ensemble_autotune(lt_ensemble* e, int* threads_hb, int* threads_or)
         {
             // one untimed sub-sweep, then 8 timed ones
             e->be->batch_sweep(e->stream, e->d_desc, (int)e->lats.size(), e->n_blocks[sel], sel, op, 0, 0,
-                               d_scratch_counter, 10);
+                               d_scratch_counter, 10, 0);
             cudaEventRecord(t0, e->stream);
             for (int q = 0; q < 8; ++q)
                 e->be->batch_sweep(e->stream, e->d_desc, (int)e->lats.size(), e->n_blocks[sel], sel, op, q >> 1,
-                                   q & 1, d_scratch_counter, 10);
+                                   q & 1, d_scratch_counter, 10, q & 1);
             cudaEventRecord(t1, e->stream);
             cudaError_t ce = cudaEventSynchronize(t1);
             if (ce != cudaSuccess)

@@ -329,27 +329,29 @@ public:
 
     template <int SEL>
     static void batch_launch(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int op, int mu, int par,
-                             const uint64_t* counter, int max_iter)
+                             const uint64_t* counter, int max_iter, int flip)
     {
         const LatDesc* d = static_cast<const LatDesc*>(desc);
         if (op == 0)
         {
             if constexpr (kStaged && kBatchBlocks[SEL] <= 128) prefer_shared<k_batch_sweep<T, NR, SEL, 0>>();
-            k_batch_sweep<T, NR, SEL, 0><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter);
+            k_batch_sweep<T, NR, SEL, 0><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter,
+                                                                                 flip);
         }
         else
         {
             if constexpr (kStaged && kBatchBlocks[SEL] <= 128) prefer_shared<k_batch_sweep<T, NR, SEL, 1>>();
-            k_batch_sweep<T, NR, SEL, 1><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter);
+            k_batch_sweep<T, NR, SEL, 1><<<n_blocks, kBatchBlocks[SEL], 0, s>>>(d, n_lat, mu, par, counter, max_iter,
+                                                                                 flip);
         }
     }
 
     void batch_sweep(cudaStream_t s, const void* desc, int n_lat, int n_blocks, int sel, int op, int mu, int par,
-                     const uint64_t* counter, int max_iter) const override
+                     const uint64_t* counter, int max_iter, int flip) const override
     {
-        if (sel == 0) batch_launch<0>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
-        else if (sel == 1) batch_launch<1>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
-        else batch_launch<2>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter);
+        if (sel == 0) batch_launch<0>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter, flip);
+        else if (sel == 1) batch_launch<1>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter, flip);
+        else batch_launch<2>(s, desc, n_lat, n_blocks, op, mu, par, counter, max_iter, flip);
     }
 
     cudaError_t batch_round(cudaStream_t s, const void* desc, int n_lat, int n_units, int blocks_per_sm, int n_hb,

@@ -1197,12 +1197,15 @@ template <typename T, int NR, int BLOCK> struct BatchMinBlocks
 template <typename T, int NR, int SEL, int OP>   // OP: 0 heatbath, 1 overrelaxation
 __global__ void __launch_bounds__(kBatchBlocks[SEL], (BatchMinBlocks<T, NR, kBatchBlocks[SEL]>::value))
     k_batch_sweep(const LatDesc* __restrict__ d, int n, int mu, int par, const uint64_t* __restrict__ counter,
-                  int max_iter)
+                  int max_iter, int flip)
 {
     constexpr int BLOCK = kBatchBlocks[SEL];
-    const int k = find_lattice<SEL>(d, n, blockIdx.x);
+    // flip: the work units in descending order, so that a launch starts on the lattices the
+    // previous one (ascending) ended on, which are still in L2
+    const int b = flip ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+    const int k = find_lattice<SEL>(d, n, b);
     const Geom g = d[k].g;
-    const int s = (blockIdx.x - d[k].blk_begin[SEL]) * BLOCK + threadIdx.x;
+    const int s = (b - d[k].blk_begin[SEL]) * BLOCK + threadIdx.x;
     if (s >= g.vh) return;
     Gauge<T, NR> U;
     U.p = (cx<T>*)d[k].U;
