@@ -306,10 +306,10 @@ public:
         if (op == 0)
             launch_chained(c.rect ? k_heatbath4<T, NR, true> : k_heatbath4<T, NR, false>, nb, kThreads, c.stream,
                            gauge(U, c.g), c.g, mu, sub, (T)prefactor, counter, (uint32_t)seed, (uint32_t)(seed >> 32),
-                           max_iter, c.status, (T)c.cp, (T)c.cr);
+                           max_iter, c.status, (T)c.cp, (T)c.cr, next_order(c));
         else
             launch_chained(c.rect ? k_overrelax4<T, NR, true> : k_overrelax4<T, NR, false>, nb, kThreads, c.stream,
-                           gauge(U, c.g), c.g, mu, sub, (T)c.cp, (T)c.cr);
+                           gauge(U, c.g), c.g, mu, sub, (T)c.cp, (T)c.cr, next_order(c));
     }
     void alg_axpby(const Ctx& c, void* P, const void* F, double a, double b) const override
     {

@@ -897,12 +897,13 @@ __global__ void __launch_bounds__(kStagedThreads, LT_MINB_STAGED) k_overrelax_st
 
 // One (mu, sublattice) sub-sweep of Iterator::Checkerboard4 with the handle's action
 template <typename T, int NR, bool RECT>
-__global__ void __launch_bounds__(kThreads, (RECT ? RectMinBlocks<T, NR>::value : Cb4MinBlocks<T, NR>::value)) k_overrelax4(Gauge<T, NR> U, Geom g, int mu, int sub, T cp, T cr)
+__global__ void __launch_bounds__(kThreads, (RECT ? RectMinBlocks<T, NR>::value : Cb4MinBlocks<T, NR>::value)) k_overrelax4(Gauge<T, NR> U, Geom g, int mu, int sub, T cp, T cr, int rev)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_release();
     pdl_wait();
     if (k >= (g.V >> 2)) return;
+    if (rev) k = (g.V >> 2) - 1 - k;   // descending on alternate launches, as half_site_of_thread
     int c[4];
     const int i = cb4_site(g, mu, sub, k, c);
     const int par = (c[0] + c[1] + c[2] + c[3]) & 1, s = i >> 1;
@@ -1107,12 +1108,13 @@ __global__ void __launch_bounds__(kStagedThreads, LT_MINB_STAGED) k_heatbath_sta
 template <typename T, int NR, bool RECT>
 __global__ void __launch_bounds__(kThreads, (RECT ? RectMinBlocks<T, NR>::value : Cb4MinBlocks<T, NR>::value)) k_heatbath4(Gauge<T, NR> U, Geom g, int mu, int sub, T prefactor,
                                                         uint64_t counter, uint32_t k0, uint32_t k1, int max_iter,
-                                                        unsigned* status, T cp, T cr)
+                                                        unsigned* status, T cp, T cr, int rev)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_release();
     pdl_wait();
     if (k >= (g.V >> 2)) return;
+    if (rev) k = (g.V >> 2) - 1 - k;
     int c[4];
     const int i = cb4_site(g, mu, sub, k, c);
     const int par = (c[0] + c[1] + c[2] + c[3]) & 1;
