@@ -1455,8 +1455,19 @@ __global__ void __launch_bounds__(4 * kSitesPerBlock, LT_MINB_FLOW_STAGED)
 // integrated with the stages of the flow integrators exactly as the plain force.
 // Pass 1 of a stage: X for every link.
 // (Also the first half of the split FP64 flow stage, below, with the handle's action.)
+// The rectangle force pass (the Zeuthen flow's Luescher-Weisz force) on two-row FP32 links:
+// 6 blocks of 128 per SM (80 registers; the spills, 412 bytes, stay in L1) for 14.8 Zeuthen
+// RK3 steps/s at 48^4, against 14.6 at 5 blocks, 14.2 at 4 (128 registers) and 12.5 uncapped
+// (149 registers, 3 blocks)
+#ifndef LT_MINB_FLOW_FORCE_RECT_F32C
+#define LT_MINB_FLOW_FORCE_RECT_F32C 6
+#endif
+template <typename T, int NR, bool RECT> struct FlowForceMinBlocks
+{
+    static constexpr int value = (sizeof(T) == 4 && NR == 2 && RECT) ? LT_MINB_FLOW_FORCE_RECT_F32C : 1;
+};
 template <typename T, int NR, bool RECT>
-__global__ void __launch_bounds__(kThreads) k_flow_force(Gauge<T, NR> U, Alg<T> X, Geom g, T cp, T cr, int rev)
+__global__ void __launch_bounds__(kThreads, (FlowForceMinBlocks<T, NR, RECT>::value)) k_flow_force(Gauge<T, NR> U, Alg<T> X, Geom g, T cp, T cr, int rev)
 {
     pdl_release();
     pdl_wait();
